@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Benchmark of the Grains3D DEM time step on B200 (pacific_b200).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
+                    [--workload polydisperse_200k|settling_1k|adjoint_4k] [--impl reference]
+
+One bench step = one chunk of `--chunk` DEM time steps (default 100) of the
+workload, replayed from CUDA graphs on resident device state.  L2 is flushed
+(a 256 MiB write) between timed chunks.  `value` is particle-steps/s of the
+whole job (all ranks); `e2e` is the same metric through the C ABI with host
+buffers: upload of the state, the chunk, download of the state.
+
+With --gpus N (launched by torchrun) every rank runs an independent replica
+(the single system is not partitioned across GPUs): weak scaling.
+`--impl reference` times the reference's CPU implementation of the step
+(oracle/_ref when it was built from the reference sources, otherwise the
+oracle restatement) on the host cores, rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+# algorithmic HBM bytes per particle and force evaluation of the forces kernel:
+# own state in (position+radius 32, v, w, mass/crust 16, id/material 8, upload index 4),
+# force + torque + coordination + memory count out, owned memory entries read + written
+FORCES_BYTES = {"mixed": (32 + 12 + 12 + 16 + 8 + 4 + 12 + 12 + 4 + 8, 40.0),
+                "fp64": (32 + 24 + 24 + 16 + 8 + 4 + 24 + 24 + 4 + 8, 76.0)}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--chunk", type=int, default=100)
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--workload", default="polydisperse_200k")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-steps", type=int, default=30)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def scenario(name):
+    from pacific_b200 import scenarios as S
+    return {"polydisperse_200k": S.polydisperse_200k, "settling_1k": S.settling_1k,
+            "adjoint_4k": S.adjoint_4k}[name]()
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return d["hbm_gbs"], "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel, workload, precision):
+    """dram bytes per launch of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "%s_%s_%s.md" % (kernel, workload, precision))
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while running."""
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.stop = threading.Event()
+        self.t = threading.Thread(target=self.run, daemon=True)
+
+    def run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 2 + k and "Active" in r[2 + k]
+                          and "Not" not in r[2 + k]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def cpu_baseline(sc, steps, lib_path=None):
+    """Times the CPU implementation of the step on a bounded window of the
+    same workload: `steps` DEM steps from the initial state, one core."""
+    from pacific_b200.abi import FP64, GrainsLib, Simulation
+    from pacific_b200 import scenarios as S
+    ref = os.path.join(ROOT, "oracle", "_ref", "libgrains_ref.so")
+    if lib_path is None:
+        if os.path.exists(ref):
+            lib_path, prefix, kind = ref, "grains_ref_", "reference"
+        else:
+            lib_path = os.path.join(ROOT, "oracle", "_build", "libgrains_oracle.so")
+            if not os.path.exists(lib_path):
+                subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-s"], check=True)
+            prefix, kind = "grains_oracle_", "port"
+    lib = GrainsLib(lib_path, prefix)
+    sim = Simulation(lib, FP64, max_particles=sc.n, n_systems=len(sc.domains))
+    S.apply(sim, sc)
+    sim.initialize_leapfrog(0.0, sc.dt)
+    t0 = time.perf_counter()
+    sim.step(steps, 0.0, sc.dt)
+    el = time.perf_counter() - t0
+    return {"value": sc.n * steps / el, "unit": "particle-steps/s", "cores": 1, "kind": kind,
+            "sample": "%s, %d DEM steps from the initial state after the leapfrog start, serial" % (sc.name, steps)}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    sc = scenario(args.workload)
+    per = []
+    for _ in range(args.warmup):
+        pass
+    steps = max(1, args.cpu_steps // max(1, args.steps))
+    for _ in range(args.steps):
+        b = cpu_baseline(sc, steps)
+        per.append(b["value"])
+    v = float(np.median(per))
+    line = {"metric": "particle-steps/s", "value": v, "unit": "particle-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
+            "dtype": "f64", "data": "synthetic", "scaling": "weak",
+            "config": {"workload": sc.name, "particles": sc.n, "dem_steps_per_step": steps},
+            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": 1, "kind": b["kind"],
+                             "sample": b["sample"]},
+            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "vs_baseline": None}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    import pacific_b200
+    from pacific_b200 import scenarios as S
+    from pacific_b200.abi import FP64, MIXED, Simulation
+
+    lib = pacific_b200.load_library()
+    prec = MIXED if args.precision == "mixed" else FP64
+    sc = scenario(args.workload)
+    sim = Simulation(lib, prec, max_particles=sc.n, n_systems=len(sc.domains), device=local)
+    S.apply(sim, sc)
+    sim.initialize_leapfrog(0.0, sc.dt)
+    stream = torch.cuda.ExternalStream(sim.stream_handle(), device=local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:%d" % local)
+
+    t = 0.0
+    for _ in range(args.warmup):
+        t = sim.step(args.chunk, t, sc.dt)
+    sim.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(k & 0xFF)          # L2 flush between timed chunks (untimed)
+                ev[k][0].record(stream)
+            t = sim.step(args.chunk, t, sc.dt)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        sim.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda:%d" % local, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    st = sim.stats()
+    total_particles = sc.n * world
+    value = total_particles * args.chunk * args.steps / (ms / 1e3)
+
+    # dominant kernel: per-kernel CUDA-event timing of uncaptured steps
+    n_prof = 20
+    t, prof = sim.profile_kernels(n_prof, t, sc.dt)
+    fk_ms, fk_n = prof["forces"]
+    sim.reset_stats()
+    sim.compute_forces(t, sc.dt)
+    st3 = sim.stats()
+    z = (2.0 * st3["n_contacts"] + st3["n_obstacle_contacts"]) / sc.n
+    base, per_contact = FORCES_BYTES[args.precision]
+    alg_bytes = sc.n * (base + per_contact * z / 2.0)
+    achieved = alg_bytes / (fk_ms / fk_n / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = profiled_traffic("forces", sc.name, args.precision)
+
+    # end to end through the C ABI with host buffers: state up, one chunk, state down
+    host = sim.download()
+    e2e_times = []
+    h2d = d2h = 0
+    for k in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.update(host)
+        t = sim.step(args.chunk, t, sc.dt)
+        host = sim.download()
+        el = time.perf_counter() - t0
+        h2d = sum(host[kk].nbytes for kk in ["position", "quaternion", "velocity", "omega"])
+        d2h = sum(v.nbytes for v in host.values())
+        if k > 0:
+            e2e_times.append(el)
+    e2e_s = float(np.median(e2e_times))
+    e2e_value = total_particles * args.chunk / e2e_s
+
+    line = {"metric": "particle-steps/s", "value": v, "unit": "particle-steps/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
+            "dtype": "f64", "data": "synthetic", "scaling": "weak",
+            "config": {"workload": sc.name, "particles": sc.n, "dem_steps_per_step": steps},
+            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": 1, "kind": b["kind"],
+                             "sample": b["sample"]},
+            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "vs_baseline": None}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    import pacific_b200
+    from pacific_b200 import scenarios as S
+    from pacific_b200.abi import FP64, MIXED, Simulation
+
+    lib = pacific_b200.load_library()
+    prec = MIXED if args.precision == "mixed" else FP64
+    sc = scenario(args.workload)
+    sim = Simulation(lib, prec, max_particles=sc.n, n_systems=len(sc.domains), device=local)
+    S.apply(sim, sc)
+    sim.initialize_leapfrog(0.0, sc.dt)
+    stream = torch.cuda.ExternalStream(sim.stream_handle(), device=local)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:%d" % local)
+
+    t = 0.0
+    for _ in range(args.warmup):
+        t = sim.step(args.chunk, t, sc.dt)
+    sim.synchronize()
+
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.fill_(k & 0xFF)          # L2 flush between timed chunks (untimed)
+                ev[k][0].record(stream)
+            t = sim.step(args.chunk, t, sc.dt)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        sim.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda:%d" % local, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    st = sim.stats()
+    total_particles = sc.n * world
+    value = total_particles * args.chunk * args.steps / (ms / 1e3)
+
+    # dominant kernel: per-kernel CUDA-event timing of uncaptured steps
+    t, prof = sim.profile_kernels(20, t, sc.dt)
+    fk_ms, fk_n = prof["forces"]
+    st2 = sim.stats()
+    z = 2.0 * (st2["n_contacts"]) / max(1, st2["n_steps_done"] and sc.n) / max(1, (st2["n_steps_done"] or 1))
+    sim.reset_stats()
+    sim.compute_forces(t, sc.dt)
+    st3 = sim.stats()
+    z = (2.0 * st3["n_contacts"] + st3["n_obstacle_contacts"]) / sc.n
+    base, per_contact = FORCES_BYTES[args.precision]
+    alg_bytes = sc.n * (base + per_contact * z / 2.0)
+    achieved = alg_bytes / (fk_ms / fk_n / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    traffic = profiled_traffic("forces", sc.name, args.precision)
+
+    # end to end through the C ABI with host buffers
+    host = sim.download()
+    up = dict(sc.particles)
+    for k in ["position", "quaternion", "velocity", "omega"]:
+        up[k] = host[k]
+    up["basis"] = None
+    ids = [0]
+    e2e_times = []
+    h2d = sum(np.asarray(up[k]).nbytes for k in ["id", "shape", "material", "radius", "crust", "mass", "inertia",
+                                                 "position", "quaternion", "velocity", "omega"])
+    d2h = 0
+    for k in range(args.e2e_steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p = dict(up)
+        p["shape"] = np.zeros(sc.n, np.int32) + ids[0]
+        sim.upload(p)
+        sim.initialize_leapfrog(t, sc.dt)
+        t = sim.step(args.chunk, t, sc.dt)
+        out = sim.download()
+        el = time.perf_counter() - t0
+        d2h = sum(v.nbytes for v in out.values())
+        for kk in ["position", "quaternion", "velocity", "omega"]:
+            up[kk] = out[kk]
+        if k > 0:
+            e2e_times.append(el)
+    e2e_s = float(np.median(e2e_times))
+    e2e_value = total_particles * args.chunk / e2e_s
+
+    line = {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64" if args.precision == "mixed" else "f64",
+        "data": "synthetic",
+        "config": {"workload": sc.name, "particles_per_gpu": sc.n, "precision": args.precision,
+                   "dem_steps_per_step": args.chunk, "dt": sc.dt, "parallelism": "replicas" if world > 1 else "1gpu",
+                   "l2": "flushed (256 MiB write) between timed steps"},
+        "gpu_launches": int(sim.launches_per_step() * args.chunk * args.steps),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "kernel": "forces_kernel", "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": alg_bytes, "mean_coordination": z,
+                     "launch_ms": fk_ms / fk_n},
+        "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "kernels_ms_per_dem_step": {k: v[0] / n_prof for k, v in prof.items()},
+        "status": st["status"],
+    }
+    line["clocks"] = clk.summary()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(scenario(args.workload), args.cpu_steps)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,266 @@
+/*
+ * grains_gpu.h -- C ABI of the B200 implementation of the Grains3D DEM time
+ * step (LinkedCell broadphase, sphere / box / cylinder / polyhedron
+ * narrowphase, Hooke and HookeMemory contact laws, second-order leapfrog with
+ * quaternion rotation update).
+ *
+ * Conventions
+ *   - Every entry point returns an int status: 0 (GRAINS_GPU_OK) or a bit set
+ *     of GRAINS_GPU_* error codes.  The message of the last failure is returned
+ *     by grains_gpu_last_error().  The reference signals the same conditions
+ *     with C++ exceptions (ContactError, MotionError, SimulationError,
+ *     Grains/Base/include/Error.hh:19,75,129); the C++ adaptor in
+ *     grains_gpu.hpp rethrows them.
+ *   - Plain pointers and sizes only.  All arrays are HOST arrays unless a
+ *     function name ends in _device.  Vectors are packed xyz, quaternions
+ *     xyzw (vector part first, like Quaternion(x,y,z,w) in
+ *     Grains/Geometry/src/Quaternion.cpp:46), 3x3 matrices row major.
+ *   - One context per host thread; all work of a context is ordered on its
+ *     own CUDA stream.  There is no global mutable state.
+ *   - Particle arrays are indexed in upload order.  The device keeps the
+ *     particles sorted by cell internally; downloads return upload order.
+ */
+#ifndef GRAINS_GPU_H
+#define GRAINS_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status bits (reference: Error.hh exceptions + device conditions) --- */
+#define GRAINS_GPU_OK                 0
+#define GRAINS_GPU_CONTACT_ERROR      (1 << 0) /* ContactError: overlap >= crust sum, RigidBodyWithCrust.cpp:620-629 */
+#define GRAINS_GPU_MOTION_ERROR       (1 << 1) /* MotionError: |dx| > crust, Particle.cpp:447-457 */
+#define GRAINS_GPU_OUT_OF_GRID        (1 << 2) /* SimulationError: particle left the grid, LinkedCell.cpp:1525-1531 */
+#define GRAINS_GPU_PAIR_OVERFLOW      (1 << 3) /* a diagnostic pair buffer was too small */
+#define GRAINS_GPU_HISTORY_FULL       (1 << 4) /* more contacts than history slots for one particle */
+#define GRAINS_GPU_CUDA_ERROR         (1 << 5)
+#define GRAINS_GPU_TIMEOUT            (1 << 6) /* a bounded device wait gave up */
+#define GRAINS_GPU_INVALID_ARGUMENT   (1 << 7)
+#define GRAINS_GPU_NOT_READY          (1 << 8) /* call order violated (e.g. step before upload) */
+#define GRAINS_GPU_GJK_NOT_CONVERGED  (1 << 9) /* GJK hit its iteration cap (Convex.cpp:566) */
+#define GRAINS_GPU_CONTACT_HANDLED    (1 << 10) /* informational: a contact went through the crust x10 retry */
+
+/* ---- enumerations ------------------------------------------------------- */
+enum grains_gpu_precision {
+  GRAINS_GPU_FP64  = 0, /* everything in double */
+  GRAINS_GPU_MIXED = 1  /* positions, quaternions, bases and overlap distances in
+                           double; velocities, forces, contact law, history in float */
+};
+
+enum grains_gpu_shape_type {   /* Grains/Geometry/include/Convex.hh ConvexType */
+  GRAINS_GPU_SPHERE     = 0,   /* params: radius */
+  GRAINS_GPU_BOX        = 1,   /* params: LX, LY, LZ (full edge lengths) */
+  GRAINS_GPU_CYLINDER   = 2,   /* params: radius, height (axis = local Y) */
+  GRAINS_GPU_POLYHEDRON = 3    /* params: nv, nv*(x,y,z), nf, then per face:
+                                  k, k vertex indices (reference file format,
+                                  Grains/Geometry/src/Polyhedron.cpp:75-115) */
+};
+
+enum grains_gpu_contact_law {
+  GRAINS_GPU_HOOKE        = 0, /* params: kn, en, etat, muc, kr            (HookeContactForceModel.cpp:170-199) */
+  GRAINS_GPU_HOOKE_MEMORY = 1  /* params: kn, en, etat, muc, kt, mur, etarpf, epst
+                                                                     (HookeMemoryContactForceModel.cpp:11-29) */
+};
+
+/* ---- configuration ------------------------------------------------------ */
+typedef struct grains_gpu_config {
+  int32_t precision;          /* enum grains_gpu_precision */
+  int32_t device;             /* CUDA device ordinal */
+  int32_t n_systems;          /* independent systems in one context (>=1) */
+  int32_t history_capacity;   /* contact-memory slots per particle, 0 = 24 */
+  int64_t max_particles;      /* capacity summed over systems */
+  int32_t max_obstacles;      /* capacity summed over systems, 0 = 256 */
+  int32_t max_shapes;         /* shape-table capacity, 0 = 64 */
+  int32_t max_materials;      /* materials per system, 0 = 4 */
+  int32_t reserved[7];
+} grains_gpu_config;
+
+/* Domain of one system.  cell_size is the requested linked-cell edge
+ * (2 * CellSizeFactor * max circumscribed radius, Grains.cpp:1005-1022,
+ * 2522-2526); the grid is built like LinkedCell::set (LinkedCell.cpp:47-140):
+ * n_i = int((L_i + 1e-10) / cell_size), edge_i = L_i / n_i.  Periodicity is
+ * not supported (out of scope). */
+typedef struct grains_gpu_domain {
+  double origin[3];
+  double size[3];
+  double cell_size;
+  double gravity[3];
+} grains_gpu_domain;
+
+/* Obstacle of one system (a Grains SimpleObstacle).  Obstacles are rigid
+ * bodies of mass 1e20 (Component.cpp:16) that are moved by imposed kinematics
+ * only.  'moving' != 0 marks an obstacle with a constant imposed rotation
+ * about 'rotation_center' with angular velocity 'omega' and translation
+ * velocity 'velocity' (ObstacleImposedVelocity.cpp:195-208). */
+typedef struct grains_gpu_obstacle {
+  int32_t id;            /* component id (reference obstacles carry their own ids) */
+  int32_t shape;         /* shape id from grains_gpu_add_shape (a BOX for walls) */
+  int32_t material;
+  int32_t moving;
+  double  crust;
+  double  transform[12]; /* basis (row-major 3x3) then origin, Transform(double m[12]) layout */
+  double  velocity[3];
+  double  omega[3];
+  double  rotation_center[3];
+} grains_gpu_obstacle;
+
+/* Particle state, structure of arrays, n entries each.  Static fields are
+ * read by upload only; dynamic fields are read by upload and written by
+ * download.  'basis' may be NULL on upload (then basis = R(q)). */
+typedef struct grains_gpu_particles {
+  int64_t  n;
+  int32_t* id;           /* component id, unique within a system, >= 0 */
+  int32_t* system;       /* system index, may be NULL when n_systems == 1 */
+  int32_t* shape;        /* shape id */
+  int32_t* material;
+  double*  radius;       /* circumscribed radius (sphere: its radius) */
+  double*  crust;        /* crust thickness */
+  double*  mass;         /* density * volume, Particle.cpp:158 */
+  double*  inertia;      /* 3n: body-frame principal inertia (density scaled), Particle.cpp:159-163 */
+  double*  position;     /* 3n: transform origin */
+  double*  quaternion;   /* 4n: xyzw */
+  double*  basis;        /* 9n: row-major rotation part of the transform (may be NULL) */
+  double*  velocity;     /* 3n */
+  double*  omega;        /* 3n: world-frame angular velocity */
+  double*  force;        /* 3n: download only, current torsor force */
+  double*  torque;       /* 3n: download only, current torsor torque */
+  int32_t* coordination; /* download only, number of contacting components (Particle.cpp:1703-1707) */
+} grains_gpu_particles;
+
+/* Contact memory entries (HookeMemory), reference map
+ * Component::m_contactMap (Component.hh:507-513): entry held by component
+ * 'owner' about neighbour 'other' (ids; obstacle ids as given). */
+typedef struct grains_gpu_contact_memory {
+  int64_t  n;
+  int32_t* owner;
+  int32_t* other;
+  double*  kdelta;       /* 3n */
+  double*  prev_normal;  /* 3n */
+  double*  spring_torque;/* 3n */
+} grains_gpu_contact_memory;
+
+typedef struct grains_gpu_stats {
+  int64_t n_particles;
+  int64_t n_candidate_pairs;      /* particle-particle candidates of the last force evaluation */
+  int64_t n_obstacle_candidates;  /* particle-obstacle candidates after the InZone prefilter */
+  int64_t n_contacts;             /* particle-particle contacts */
+  int64_t n_obstacle_contacts;
+  int64_t n_gjk_calls;
+  int64_t n_gjk_iterations;
+  double  overlap_max;            /* AppCollision::addToContactsFeatures, AppCollision.cpp:160-187 */
+  double  overlap_sum;
+  int64_t n_steps_done;
+  int32_t status;                 /* accumulated status bits */
+  int32_t reserved;
+} grains_gpu_stats;
+
+typedef struct grains_gpu_ctx grains_gpu_ctx;
+
+/* ---- lifetime ----------------------------------------------------------- */
+/* replaces: Grains::Construction creating `new LinkedCell` (Grains.cpp:778-780) */
+int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out);
+int grains_gpu_destroy(grains_gpu_ctx* ctx);
+/* copies the message of the last failure (NUL terminated) */
+int grains_gpu_last_error(const grains_gpu_ctx* ctx, char* buf, size_t len);
+/* CUDA stream of the context, as a void* (cudaStream_t) */
+int grains_gpu_get_stream(const grains_gpu_ctx* ctx, void** stream);
+
+/* ---- set-up ------------------------------------------------------------- */
+/* replaces: LinkedCell::set (LinkedCell.cpp:47-140) and the gravity of
+ * GrainsExec::m_vgravity */
+int grains_gpu_set_domain(grains_gpu_ctx* ctx, int32_t system, const grains_gpu_domain* dom);
+/* replaces: ConvexBuilderFactory::create (Grains/Geometry/src/ConvexBuilderFactory.cpp) */
+int grains_gpu_add_shape(grains_gpu_ctx* ctx, int32_t type, const double* params,
+                         int32_t n_params, int32_t* shape_id);
+/* replaces: ContactBuilderFactory::define / defineParameters
+ * (ContactBuilderFactory.cpp:81-169); symmetric in (matA, matB) */
+int grains_gpu_set_contact_law(grains_gpu_ctx* ctx, int32_t system, int32_t mat_a,
+                               int32_t mat_b, int32_t law, const double* params,
+                               int32_t n_params);
+/* replaces: AppCollision::Link(Obstacle*) / LinkedCell::Link(Obstacle*)
+ * (LinkedCell.cpp:1371-1445) */
+int grains_gpu_set_obstacles(grains_gpu_ctx* ctx, int32_t system, int32_t n,
+                             const grains_gpu_obstacle* obstacles);
+/* replaces: LinkedCell::Link(Particle*) for all active particles
+ * (LinkedCell.cpp:1330-1365) + AllComponents state upload */
+int grains_gpu_upload_particles(grains_gpu_ctx* ctx, const grains_gpu_particles* p);
+int grains_gpu_download_particles(grains_gpu_ctx* ctx, grains_gpu_particles* p);
+/* Overwrites the kinematic state (position, quaternion, basis when given,
+ * velocity, omega) of the particles already uploaded, in upload order (p->n
+ * must equal the uploaded count; static fields are ignored).  Contact memory,
+ * forces and set-up tables are kept: this is the per-step host->device path
+ * of an adaptor whose host copy of the state stays authoritative, like
+ * AllComponents in the reference (AllComponents.cpp:151-233). */
+int grains_gpu_update_particles(grains_gpu_ctx* ctx, const grains_gpu_particles* p);
+int grains_gpu_upload_contact_memory(grains_gpu_ctx* ctx, const grains_gpu_contact_memory* m);
+/* n on input = capacity; on output = number of entries written (owner-side
+ * and mirrored entries both listed, like the reference's two maps) */
+int grains_gpu_download_contact_memory(grains_gpu_ctx* ctx, grains_gpu_contact_memory* m);
+/* obstacle poses after imposed motion: 12 doubles per obstacle of 'system' */
+int grains_gpu_download_obstacles(grains_gpu_ctx* ctx, int32_t system, int32_t n,
+                                  double* transforms);
+
+/* ---- the time step ------------------------------------------------------ */
+/* replaces: App::ComputeForces(time, dt, particles) of LinkedCell
+ * (App.hh:38-39, LinkedCell.cpp:1019-1103) together with the per-step resets
+ * of Grains::computeParticlesForceAndTorque (Grains.cpp:459-482) */
+int grains_gpu_compute_forces(grains_gpu_ctx* ctx, double time, double dt);
+/* replaces: AllComponents::Move (AllComponents.cpp:151-222) ->
+ * SecondOrderLeapFrog::Move (SecondOrderLeapFrog.cpp:44-69), obstacle motion */
+int grains_gpu_move(grains_gpu_ctx* ctx, double time, double dt_vel, double dt_disp);
+/* replaces: AppCollision::LinkUpdate (LinkedCell.cpp:1452-1547) */
+int grains_gpu_link_update(grains_gpu_ctx* ctx, double time, double dt);
+/* replaces: AllComponents::advanceParticlesVelocity ->
+ * SecondOrderLeapFrog::advanceVelocity (SecondOrderLeapFrog.cpp:74-95) */
+int grains_gpu_advance_velocity(grains_gpu_ctx* ctx, double time, double dt_vel);
+/* The leapfrog initialisation of Grains::do_before_time_stepping
+ * (Grains.cpp:169-174): one force evaluation, then kdelta and the rolling
+ * spring torque of every memory entry are zeroed. */
+int grains_gpu_initialize_leapfrog(grains_gpu_ctx* ctx, double time, double dt);
+/* n_steps kick-drift-kick steps of Grains::Simulation (Grains.cpp:344-364),
+ * replayed from a CUDA graph.  *time is advanced by n_steps*dt. */
+int grains_gpu_step(grains_gpu_ctx* ctx, int32_t n_steps, double* time, double dt);
+/* blocks until the stream is idle; returns accumulated device status bits */
+int grains_gpu_synchronize(grains_gpu_ctx* ctx);
+
+/* ---- diagnostics -------------------------------------------------------- */
+/* Candidate pairs of the current cell assignment (LinkedCell::ComputeForces
+ * enumeration as a set): pairs[2k], pairs[2k+1] = ids with pairs[2k] <
+ * pairs[2k+1], sorted.  Obstacle candidates follow with the obstacle id in
+ * the second slot when include_obstacles != 0.  *n = pairs found (may exceed
+ * cap, then GRAINS_GPU_PAIR_OVERFLOW). */
+int grains_gpu_get_candidate_pairs(grains_gpu_ctx* ctx, int32_t system, int32_t include_obstacles,
+                                   int64_t cap, int32_t* pairs, int64_t* n);
+/* Contact pairs (overlap distance < 0) of the last force evaluation, same layout. */
+int grains_gpu_get_contact_pairs(grains_gpu_ctx* ctx, int32_t system, int64_t cap,
+                                 int32_t* pairs, int64_t* n);
+int grains_gpu_get_stats(grains_gpu_ctx* ctx, grains_gpu_stats* st);
+/* Reset the accumulated status bits and statistics. */
+int grains_gpu_reset_stats(grains_gpu_ctx* ctx);
+
+/* ---- timing helpers for benchmarks ---------------------------------------- */
+/* Times each kernel of n_steps uncaptured steps with CUDA events on the
+ * context stream.  names: '\n'-separated kernel names (cap bytes); ms[k]:
+ * total milliseconds of kernel k; launches[k]: its launch count. */
+int grains_gpu_profile_kernels(grains_gpu_ctx* ctx, int32_t n_steps, double* time, double dt,
+                               char* names, size_t cap, double* ms, int64_t* launches,
+                               int32_t max_kernels, int32_t* n_kernels);
+/* Number of kernel launches one call of grains_gpu_step(n_steps) issues. */
+int grains_gpu_launches_per_step(grains_gpu_ctx* ctx, int64_t* launches);
+
+/* ---- shape helpers (reference geometry formulas, host only) -------------- */
+/* volume, circumscribed radius and body-frame principal inertia per unit
+ * density: Sphere.cpp:61-81,152-155; Box.cpp:181-210; Cylinder.cpp:61-85;
+ * Polyhedron.cpp:324-367. */
+int grains_gpu_shape_properties(int32_t type, const double* params, int32_t n_params,
+                                double* volume, double* circumscribed_radius,
+                                double inertia[3]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRAINS_GPU_H */

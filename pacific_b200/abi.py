@@ -1,0 +1,430 @@
+"""ctypes binding of the C ABI in include/grains_gpu.h.
+
+`GrainsLib` loads a shared library that exports the grains_gpu entry points
+(or the same set under another prefix) and `Simulation` wraps one context with
+numpy arrays.  Errors raise the Python counterparts of the reference's C++
+exceptions (Grains/Base/include/Error.hh): ContactError, MotionError,
+SimulationError.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+# ---- status bits (include/grains_gpu.h) ----------------------------------------
+OK = 0
+CONTACT_ERROR = 1 << 0
+MOTION_ERROR = 1 << 1
+OUT_OF_GRID = 1 << 2
+PAIR_OVERFLOW = 1 << 3
+HISTORY_FULL = 1 << 4
+CUDA_ERROR = 1 << 5
+TIMEOUT = 1 << 6
+INVALID_ARGUMENT = 1 << 7
+NOT_READY = 1 << 8
+GJK_NOT_CONVERGED = 1 << 9
+CONTACT_HANDLED = 1 << 10
+
+FP64 = 0
+MIXED = 1
+
+SPHERE, BOX, CYLINDER, POLYHEDRON = 0, 1, 2, 3
+HOOKE, HOOKE_MEMORY = 0, 1
+
+
+class GrainsError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__("status 0x%x: %s" % (code, message))
+        self.code = code
+
+
+class ContactError(GrainsError):
+    """Overlap reached the crust sum (RigidBodyWithCrust.cpp:620-629)."""
+
+
+class MotionError(GrainsError):
+    """Displacement over one step larger than the crust (Particle.cpp:447-457)."""
+
+
+class SimulationError(GrainsError):
+    """A particle left the linked-cell grid (LinkedCell.cpp:1525-1531)."""
+
+
+def error_for(code, message):
+    if code & CONTACT_ERROR:
+        return ContactError(code, message)
+    if code & MOTION_ERROR:
+        return MotionError(code, message)
+    if code & OUT_OF_GRID:
+        return SimulationError(code, message)
+    return GrainsError(code, message)
+
+
+# ---- structures --------------------------------------------------------------
+class Config(C.Structure):
+    _fields_ = [("precision", C.c_int32), ("device", C.c_int32), ("n_systems", C.c_int32),
+                ("history_capacity", C.c_int32), ("max_particles", C.c_int64), ("max_obstacles", C.c_int32),
+                ("max_shapes", C.c_int32), ("max_materials", C.c_int32), ("reserved", C.c_int32 * 7)]
+
+
+class Domain(C.Structure):
+    _fields_ = [("origin", C.c_double * 3), ("size", C.c_double * 3), ("cell_size", C.c_double),
+                ("gravity", C.c_double * 3)]
+
+
+class Obstacle(C.Structure):
+    _fields_ = [("id", C.c_int32), ("shape", C.c_int32), ("material", C.c_int32), ("moving", C.c_int32),
+                ("crust", C.c_double), ("transform", C.c_double * 12), ("velocity", C.c_double * 3),
+                ("omega", C.c_double * 3), ("rotation_center", C.c_double * 3)]
+
+
+_P_I32 = C.POINTER(C.c_int32)
+_P_F64 = C.POINTER(C.c_double)
+
+
+class Particles(C.Structure):
+    _fields_ = [("n", C.c_int64), ("id", _P_I32), ("system", _P_I32), ("shape", _P_I32), ("material", _P_I32),
+                ("radius", _P_F64), ("crust", _P_F64), ("mass", _P_F64), ("inertia", _P_F64),
+                ("position", _P_F64), ("quaternion", _P_F64), ("basis", _P_F64), ("velocity", _P_F64),
+                ("omega", _P_F64), ("force", _P_F64), ("torque", _P_F64), ("coordination", _P_I32)]
+
+
+class ContactMemory(C.Structure):
+    _fields_ = [("n", C.c_int64), ("owner", _P_I32), ("other", _P_I32), ("kdelta", _P_F64),
+                ("prev_normal", _P_F64), ("spring_torque", _P_F64)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("n_particles", C.c_int64), ("n_candidate_pairs", C.c_int64),
+                ("n_obstacle_candidates", C.c_int64), ("n_contacts", C.c_int64),
+                ("n_obstacle_contacts", C.c_int64), ("n_gjk_calls", C.c_int64), ("n_gjk_iterations", C.c_int64),
+                ("overlap_max", C.c_double), ("overlap_sum", C.c_double), ("n_steps_done", C.c_int64),
+                ("status", C.c_int32), ("reserved", C.c_int32)]
+
+
+_VP = C.c_void_p
+_SIGS = {
+    "create": [C.POINTER(Config), C.POINTER(_VP)],
+    "destroy": [_VP],
+    "last_error": [_VP, C.c_char_p, C.c_size_t],
+    "set_domain": [_VP, C.c_int32, C.POINTER(Domain)],
+    "add_shape": [_VP, C.c_int32, _P_F64, C.c_int32, _P_I32],
+    "set_contact_law": [_VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P_F64, C.c_int32],
+    "set_obstacles": [_VP, C.c_int32, C.c_int32, C.POINTER(Obstacle)],
+    "upload_particles": [_VP, C.POINTER(Particles)],
+    "download_particles": [_VP, C.POINTER(Particles)],
+    "update_particles": [_VP, C.POINTER(Particles)],
+    "upload_contact_memory": [_VP, C.POINTER(ContactMemory)],
+    "download_contact_memory": [_VP, C.POINTER(ContactMemory)],
+    "download_obstacles": [_VP, C.c_int32, C.c_int32, _P_F64],
+    "compute_forces": [_VP, C.c_double, C.c_double],
+    "move": [_VP, C.c_double, C.c_double, C.c_double],
+    "link_update": [_VP, C.c_double, C.c_double],
+    "advance_velocity": [_VP, C.c_double, C.c_double],
+    "initialize_leapfrog": [_VP, C.c_double, C.c_double],
+    "step": [_VP, C.c_int32, _P_F64, C.c_double],
+    "get_candidate_pairs": [_VP, C.c_int32, C.c_int32, C.c_int64, _P_I32, C.POINTER(C.c_int64)],
+    "get_contact_pairs": [_VP, C.c_int32, C.c_int64, _P_I32, C.POINTER(C.c_int64)],
+    "get_stats": [_VP, C.POINTER(Stats)],
+    "reset_stats": [_VP],
+}
+_GPU_ONLY = {
+    "get_stream": [_VP, C.POINTER(_VP)],
+    "synchronize": [_VP],
+    "launches_per_step": [_VP, C.POINTER(C.c_int64)],
+    "profile_kernels": [_VP, C.c_int32, _P_F64, C.c_double, C.c_char_p, C.c_size_t, _P_F64,
+                        C.POINTER(C.c_int64), C.c_int32, _P_I32],
+    "shape_properties": [C.c_int32, _P_F64, C.c_int32, _P_F64, _P_F64, _P_F64],
+}
+
+
+class GrainsLib:
+    """A loaded implementation of the grains_gpu C ABI (entry points `prefix + name`)."""
+
+    def __init__(self, path, prefix="grains_gpu_"):
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.path = path
+        self.prefix = prefix
+        self.dll = C.CDLL(path)
+        self.fn = {}
+        for name, args in list(_SIGS.items()) + list(_GPU_ONLY.items()):
+            sym = prefix + name
+            if not hasattr(self.dll, sym):
+                if name in _GPU_ONLY:
+                    continue
+                raise AttributeError("%s does not export %s" % (path, sym))
+            f = getattr(self.dll, sym)
+            f.argtypes = args
+            f.restype = C.c_int
+            self.fn[name] = f
+        if "set_gjk_tolerance" not in self.fn and hasattr(self.dll, prefix + "set_gjk_tolerance"):
+            f = getattr(self.dll, prefix + "set_gjk_tolerance")
+            f.argtypes = [_VP, C.c_double]
+            f.restype = C.c_int
+            self.fn["set_gjk_tolerance"] = f
+
+    def shape_properties(self, shape_type, params):
+        p = np.ascontiguousarray(params, dtype=np.float64)
+        vol, circ = C.c_double(), C.c_double()
+        inertia = (C.c_double * 3)()
+        rc = self.fn["shape_properties"](shape_type, p.ctypes.data_as(_P_F64), len(p), C.byref(vol),
+                                         C.byref(circ), inertia)
+        if rc:
+            raise GrainsError(rc, "shape_properties failed")
+        return vol.value, circ.value, np.array(inertia[:])
+
+
+def _ptr(a, ctype):
+    return None if a is None else a.ctypes.data_as(C.POINTER(ctype))
+
+
+def f64(a, n=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a if n is None else a.reshape(-1)
+
+
+def i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Simulation:
+    """One context of the DEM step (a drop-in for the LinkedCell App + integrator)."""
+
+    def __init__(self, lib, precision=MIXED, max_particles=1024, n_systems=1, history_capacity=0, device=0,
+                 max_materials=4, max_obstacles=0):
+        self.lib = lib
+        cfg = Config()
+        cfg.precision = precision
+        cfg.device = device
+        cfg.n_systems = n_systems
+        cfg.history_capacity = history_capacity
+        cfg.max_particles = max_particles
+        cfg.max_obstacles = max_obstacles
+        cfg.max_materials = max_materials
+        self.ctx = _VP()
+        rc = lib.fn["create"](C.byref(cfg), C.byref(self.ctx))
+        if rc:
+            msg = self.last_error() if self.ctx else "create failed"
+            if self.ctx:
+                lib.fn["destroy"](self.ctx)
+                self.ctx = _VP()
+            raise error_for(rc, msg)
+        self.n = 0
+        self.n_systems = n_systems
+        self._keep = []
+
+    def close(self):
+        if self.ctx:
+            self.lib.fn["destroy"](self.ctx)
+            self.ctx = _VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def last_error(self):
+        buf = C.create_string_buffer(4096)
+        self.lib.fn["last_error"](self.ctx, buf, 4096)
+        return buf.value.decode(errors="replace")
+
+    def _check(self, rc):
+        if rc:
+            raise error_for(rc, self.last_error())
+
+    # ---- set-up ----
+    def set_domain(self, system, origin, size, cell_size, gravity=(0.0, 0.0, -9.81)):
+        d = Domain()
+        d.origin[:] = list(origin)
+        d.size[:] = list(size)
+        d.cell_size = cell_size
+        d.gravity[:] = list(gravity)
+        self._check(self.lib.fn["set_domain"](self.ctx, system, C.byref(d)))
+
+    def add_shape(self, shape_type, params):
+        p = f64(params)
+        sid = C.c_int32()
+        self._check(self.lib.fn["add_shape"](self.ctx, shape_type, _ptr(p, C.c_double), len(p), C.byref(sid)))
+        return sid.value
+
+    def set_contact_law(self, system, mat_a, mat_b, law, params):
+        p = f64(params)
+        self._check(self.lib.fn["set_contact_law"](self.ctx, system, mat_a, mat_b, law, _ptr(p, C.c_double), len(p)))
+
+    def set_obstacles(self, system, obstacles):
+        arr = (Obstacle * max(1, len(obstacles)))()
+        for k, o in enumerate(obstacles):
+            ob = arr[k]
+            ob.id = o["id"]
+            ob.shape = o["shape"]
+            ob.material = o.get("material", 0)
+            ob.moving = int(o.get("moving", 0))
+            ob.crust = o["crust"]
+            ob.transform[:] = [float(x) for x in o["transform"]]
+            ob.velocity[:] = list(o.get("velocity", (0.0, 0.0, 0.0)))
+            ob.omega[:] = list(o.get("omega", (0.0, 0.0, 0.0)))
+            ob.rotation_center[:] = list(o.get("rotation_center", (0.0, 0.0, 0.0)))
+        self._check(self.lib.fn["set_obstacles"](self.ctx, system, len(obstacles), arr))
+
+    # ---- state ----
+    def upload(self, p):
+        n = len(p["id"])
+        arrs = {
+            "id": i32(p["id"]),
+            "system": i32(p["system"]) if p.get("system") is not None else None,
+            "shape": i32(p["shape"]),
+            "material": i32(p["material"]),
+            "radius": f64(p["radius"]),
+            "crust": f64(p["crust"]),
+            "mass": f64(p["mass"]),
+            "inertia": f64(p["inertia"]),
+            "position": f64(p["position"]),
+            "quaternion": f64(p["quaternion"]),
+            "basis": f64(p["basis"]) if p.get("basis") is not None else None,
+            "velocity": f64(p["velocity"]),
+            "omega": f64(p["omega"]),
+        }
+        s = Particles()
+        s.n = n
+        for k, a in arrs.items():
+            setattr(s, k, _ptr(a, C.c_int32 if a is not None and a.dtype == np.int32 else C.c_double))
+        self._keep = list(arrs.values())
+        self._check(self.lib.fn["upload_particles"](self.ctx, C.byref(s)))
+        self.n = n
+
+    def update(self, p):
+        """Overwrites position, quaternion, (basis), velocity and omega of the
+        uploaded particles (upload order) keeping contact memory and forces."""
+        arrs = {k: f64(p[k]) for k in ["position", "quaternion", "velocity", "omega"]}
+        arrs["basis"] = f64(p["basis"]) if p.get("basis") is not None else None
+        s = Particles()
+        s.n = self.n
+        for k, a in arrs.items():
+            setattr(s, k, _ptr(a, C.c_double))
+        self._keep_update = list(arrs.values())
+        self._check(self.lib.fn["update_particles"](self.ctx, C.byref(s)))
+
+    def download(self):
+        n = self.n
+        out = {
+            "id": np.zeros(n, np.int32),
+            "position": np.zeros((n, 3)),
+            "quaternion": np.zeros((n, 4)),
+            "basis": np.zeros((n, 9)),
+            "velocity": np.zeros((n, 3)),
+            "omega": np.zeros((n, 3)),
+            "force": np.zeros((n, 3)),
+            "torque": np.zeros((n, 3)),
+            "coordination": np.zeros(n, np.int32),
+        }
+        s = Particles()
+        s.n = n
+        for k, a in out.items():
+            setattr(s, k, _ptr(a, C.c_int32 if a.dtype == np.int32 else C.c_double))
+        self._check(self.lib.fn["download_particles"](self.ctx, C.byref(s)))
+        return out
+
+    def upload_contact_memory(self, mem):
+        n = len(mem["owner"])
+        owner, other = i32(mem["owner"]), i32(mem["other"])
+        kd, pn, sp = f64(mem["kdelta"]), f64(mem["prev_normal"]), f64(mem["spring_torque"])
+        m = ContactMemory()
+        m.n = n
+        m.owner, m.other = _ptr(owner, C.c_int32), _ptr(other, C.c_int32)
+        m.kdelta, m.prev_normal, m.spring_torque = _ptr(kd, C.c_double), _ptr(pn, C.c_double), _ptr(sp, C.c_double)
+        self._check(self.lib.fn["upload_contact_memory"](self.ctx, C.byref(m)))
+
+    def contact_memory(self, cap=None):
+        cap = cap or max(64, 32 * self.n)
+        owner, other = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
+        kd, pn, sp = np.zeros((cap, 3)), np.zeros((cap, 3)), np.zeros((cap, 3))
+        m = ContactMemory()
+        m.n = cap
+        m.owner, m.other = _ptr(owner, C.c_int32), _ptr(other, C.c_int32)
+        m.kdelta, m.prev_normal, m.spring_torque = _ptr(kd, C.c_double), _ptr(pn, C.c_double), _ptr(sp, C.c_double)
+        self._check(self.lib.fn["download_contact_memory"](self.ctx, C.byref(m)))
+        k = m.n
+        return {"owner": owner[:k], "other": other[:k], "kdelta": kd[:k], "prev_normal": pn[:k],
+                "spring_torque": sp[:k]}
+
+    # ---- the step ----
+    def compute_forces(self, time, dt):
+        self._check(self.lib.fn["compute_forces"](self.ctx, time, dt))
+
+    def move(self, time, dt_vel, dt_disp):
+        self._check(self.lib.fn["move"](self.ctx, time, dt_vel, dt_disp))
+
+    def link_update(self, time=0.0, dt=0.0):
+        self._check(self.lib.fn["link_update"](self.ctx, time, dt))
+
+    def advance_velocity(self, time, dt_vel):
+        self._check(self.lib.fn["advance_velocity"](self.ctx, time, dt_vel))
+
+    def initialize_leapfrog(self, time, dt):
+        self._check(self.lib.fn["initialize_leapfrog"](self.ctx, time, dt))
+
+    def step(self, n_steps, time, dt):
+        t = C.c_double(time)
+        self._check(self.lib.fn["step"](self.ctx, n_steps, C.byref(t), dt))
+        return t.value
+
+    def synchronize(self):
+        if "synchronize" in self.lib.fn:
+            self._check(self.lib.fn["synchronize"](self.ctx))
+
+    # ---- diagnostics ----
+    def candidate_pairs(self, system=0, include_obstacles=False, cap=None):
+        cap = cap or max(1024, 40 * self.n)
+        buf = np.zeros(2 * cap, np.int32)
+        n = C.c_int64()
+        self._check(self.lib.fn["get_candidate_pairs"](self.ctx, system, int(include_obstacles), cap,
+                                                       _ptr(buf, C.c_int32), C.byref(n)))
+        return buf[: 2 * n.value].reshape(-1, 2)
+
+    def contact_pairs(self, system=0, cap=None):
+        cap = cap or max(1024, 16 * self.n)
+        buf = np.zeros(2 * cap, np.int32)
+        n = C.c_int64()
+        self._check(self.lib.fn["get_contact_pairs"](self.ctx, system, cap, _ptr(buf, C.c_int32), C.byref(n)))
+        return buf[: 2 * n.value].reshape(-1, 2)
+
+    def stats(self):
+        st = Stats()
+        self._check(self.lib.fn["get_stats"](self.ctx, C.byref(st)))
+        return {f: getattr(st, f) for f, _ in Stats._fields_ if f != "reserved"}
+
+    def reset_stats(self):
+        self._check(self.lib.fn["reset_stats"](self.ctx))
+
+    def set_gjk_tolerance(self, tol):
+        self._check(self.lib.fn["set_gjk_tolerance"](self.ctx, tol))
+
+    # ---- benchmark helpers (CUDA implementation only) ----
+    def stream_handle(self):
+        h = _VP()
+        self._check(self.lib.fn["get_stream"](self.ctx, C.byref(h)))
+        return h.value
+
+    def launches_per_step(self):
+        n = C.c_int64()
+        self._check(self.lib.fn["launches_per_step"](self.ctx, C.byref(n)))
+        return n.value
+
+    def profile_kernels(self, n_steps, time, dt, max_kernels=8):
+        t = C.c_double(time)
+        names = C.create_string_buffer(1024)
+        ms = (C.c_double * max_kernels)()
+        launches = (C.c_int64 * max_kernels)()
+        nk = C.c_int32()
+        self._check(self.lib.fn["profile_kernels"](self.ctx, n_steps, C.byref(t), dt, names, 1024, ms, launches,
+                                                   max_kernels, C.byref(nk)))
+        keys = names.value.decode().split("\n")
+        return t.value, {keys[i]: (ms[i], launches[i]) for i in range(nk.value)}

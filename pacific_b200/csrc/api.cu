@@ -1,0 +1,1452 @@
+// api.cu -- the C ABI of include/grains_gpu.h: context, device memory, set-up
+// tables (shapes, domains, contact laws, obstacles, obstacle-cell links) and
+// the orchestration of the DEM step kernels, with the fused step loop
+// replayed from CUDA graphs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/grains_gpu.h"
+#include "device_state.h"
+#include "gjk.cuh"
+#include "sphere_contact.cuh"
+
+using namespace gg;
+
+namespace {
+
+struct ShapeHost {
+  int type = 0;
+  std::vector<double> params;
+  std::vector<double> verts;
+  std::vector<std::vector<int>> faces;
+  double volume = 0, circ = 0;
+  double inertia[3] = {0, 0, 0};
+  double lext[3] = {0, 0, 0};
+  D3 ext{0, 0, 0};
+  double radius = 0, half_height = 0;
+};
+
+struct LawHost {
+  int type = -1;
+  double p[10] = {0};  // kn, en, etat, muc, kt, mur, etarpf, epst, kr
+  double beta = 0;
+};
+
+struct SysHost {
+  bool has_domain = false;
+  grains_gpu_domain dom{};
+  int nbi = 1, nbj = 1, nbk = 1;
+  double ex = 0, ey = 0, ez = 0;
+  std::map<std::pair<int, int>, LawHost> laws;
+  std::vector<grains_gpu_obstacle> obs;
+};
+
+template <typename T>
+T* dalloc(size_t n, std::vector<void*>& pool) {
+  void* p = nullptr;
+  if (n == 0) n = 1;
+  if (cudaMalloc(&p, n * sizeof(T)) != cudaSuccess) return nullptr;
+  pool.push_back(p);
+  return static_cast<T*>(p);
+}
+
+}  // namespace
+
+struct grains_gpu_ctx {
+  grains_gpu_config cfg{};
+  int precision = GRAINS_GPU_MIXED;
+  int hist_cap = 24;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  std::vector<ShapeHost> shapes;
+  std::vector<SysHost> sys;
+  // device memory
+  std::vector<void*> pool;        // capacity-sized buffers (allocated at create)
+  std::vector<void*> table_pool;  // tables rebuilt at upload
+  size_t rsize = 4;               // sizeof(R)
+  int64_t cap = 0;
+  int64_t n = 0;
+  int n_cells = 0;
+  bool uploaded = false;
+  bool tables_dirty = true;
+  double* stage = nullptr;        // host-ordered staging of the kinematic state (13 doubles / particle)
+  double* stage_basis = nullptr;  // 9 doubles / particle
+  bool sorted = false;      // cur arrays are in cell order for the current positions
+  bool keys_valid = false;  // key/rank hold the cells of the current positions
+  bool pending_kick2 = false;
+  double pending_dt = 0;
+  bool has_basis = false;
+  StepArgs<float> af{};
+  StepArgs<double> ad{};
+  // raw buffer pointers (two copies of particle arrays)
+  struct Bufs {
+    double4 *xr, *q;
+    double* basis;
+    void *v, *w, *wbf, *F, *T, *inertia;
+    double4* md;
+    int4* meta;
+    int* orig;
+  } buf[2]{};
+  int cur = 0;  // which copy is current
+  void* hist[2] = {nullptr, nullptr};
+  int* hist_n[2] = {nullptr, nullptr};
+  int hcur = 0;  // hist[hcur] = latest memory (prev for the next force evaluation)
+  int* coord = nullptr;
+  unsigned *key = nullptr, *rank = nullptr;
+  int* perm = nullptr;
+  int *cell_count = nullptr, *cell_start = nullptr, *block_sums = nullptr;
+  StatsDev* stats = nullptr;
+  int* pairs = nullptr;
+  int pairs_cap = 0;
+  unsigned long long* pairs_n = nullptr;
+  // tables
+  SysDev* d_sys = nullptr;
+  ShapeDev* d_shapes = nullptr;
+  double* d_verts = nullptr;
+  ObstacleDev* d_obs = nullptr;
+  int *d_cell_obs_start = nullptr, *d_cell_obs_idx = nullptr, *d_moving = nullptr;
+  void* d_laws = nullptr;
+  std::vector<SysDev> h_sys;
+  std::vector<ObstacleDev> h_obs;
+  // graphs of two fused steps, by the starting (cur, hcur) buffer selection
+  cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
+  double graph_dt[4] = {0, 0, 0, 0};
+  int64_t steps_done = 0;
+  double gjk_tol = kEpsilon;
+};
+
+namespace {
+
+int fail(grains_gpu_ctx* c, int code, const std::string& m) {
+  c->err = m;
+  return code;
+}
+int cuda_fail(grains_gpu_ctx* c, cudaError_t e, const char* where) {
+  c->err = std::string(where) + ": " + cudaGetErrorString(e);
+  return GRAINS_GPU_CUDA_ERROR;
+}
+#define CK(call)                                                 \
+  do {                                                           \
+    cudaError_t e_ = (call);                                     \
+    if (e_ != cudaSuccess) return cuda_fail(c, e_, #call);       \
+  } while (0)
+
+// ---- shapes ------------------------------------------------------------------
+// Tetrahedron (0, a, b, c) volume and second moments (F. Tonon, "Explicit exact
+// formulas for the 3-D tetrahedron inertia tensor in terms of its vertex
+// coordinates", J. Math. Stat. 1(1), 2004), as used for polyhedra by
+// GrainsExec::computeVolumeInertiaContrib (Base/src/GrainsExec.cpp:748-800).
+void tetra_contrib(D3 a, D3 b, D3 cc, double& vol, double I[3]) {
+  double x[4] = {0, a.x, b.x, cc.x}, y[4] = {0, a.y, b.y, cc.y}, z[4] = {0, a.z, b.z, cc.z};
+  double det = std::fabs((x[1] - x[0]) * (y[2] - y[0]) * (z[3] - z[0]) + (y[1] - y[0]) * (z[2] - z[0]) * (x[3] - x[0]) +
+                         (z[1] - z[0]) * (x[2] - x[0]) * (y[3] - y[0]) - (z[1] - z[0]) * (y[2] - y[0]) * (x[3] - x[0]) -
+                         (x[1] - x[0]) * (z[2] - z[0]) * (y[3] - y[0]) - (y[1] - y[0]) * (x[2] - x[0]) * (z[3] - z[0]));
+  vol += det / 6.;
+  auto sq = [](const double* u) {
+    return u[0] * u[0] + u[0] * u[1] + u[1] * u[1] + u[0] * u[2] + u[1] * u[2] + u[2] * u[2] + u[0] * u[3] +
+           u[1] * u[3] + u[2] * u[3] + u[3] * u[3];
+  };
+  I[0] += det * (sq(y) + sq(z)) / 60.;
+  I[1] += det * (sq(x) + sq(z)) / 60.;
+  I[2] += det * (sq(x) + sq(y)) / 60.;
+}
+
+// support of a shape in its local frame (for the local bounding box)
+D3 shape_support(const ShapeHost& s, D3 v) {
+  LocalBody<double> B{};
+  B.type = s.type;
+  B.nverts = (int)s.verts.size() / 3;
+  B.verts = s.verts.data();
+  B.radius = s.radius;
+  B.cyl_r = s.radius;
+  B.cyl_hh = s.half_height;
+  B.ext = v3<double>(s.ext.x, s.ext.y, s.ext.z);
+  V3<double> r = support_local(B, v3<double>(v.x, v.y, v.z));
+  return d3(r.x, r.y, r.z);
+}
+
+int build_shape(int type, const double* p, int np, ShapeHost& s, std::string& err) {
+  s.type = type;
+  s.params.assign(p, p + np);
+  if (type == GRAINS_GPU_SPHERE) {
+    if (np < 1 || !(p[0] > 0)) return err = "sphere needs a positive radius", GRAINS_GPU_INVALID_ARGUMENT;
+    s.radius = p[0];
+    s.volume = 4.0 * kPi * std::pow(s.radius, 3.) / 3.0;                           // Sphere.cpp:152-155
+    s.circ = s.radius;                                                              // Sphere.cpp:78-81
+    double I = 8.0 * kPi * std::pow(s.radius, 5.) / 15.0;                           // Sphere.cpp:61-70
+    s.inertia[0] = s.inertia[1] = s.inertia[2] = I;
+  } else if (type == GRAINS_GPU_BOX) {
+    if (np < 3) return err = "box needs LX, LY, LZ", GRAINS_GPU_INVALID_ARGUMENT;
+    s.ext = d3(std::fabs(p[0]) / 2., std::fabs(p[1]) / 2., std::fabs(p[2]) / 2.);    // Box.cpp:27-33
+    s.volume = 8.0 * s.ext.x * s.ext.y * s.ext.z;                                    // Box.cpp:286-292
+    s.circ = xnorm(s.ext);                                                          // Box.cpp:230-233
+    double e8 = 8.0 * s.ext.x * s.ext.y * s.ext.z;                                  // Box.cpp:181-210
+    s.inertia[0] = e8 * (s.ext.y * s.ext.y + s.ext.z * s.ext.z) / 3.0;
+    s.inertia[1] = e8 * (s.ext.x * s.ext.x + s.ext.z * s.ext.z) / 3.0;
+    s.inertia[2] = e8 * (s.ext.y * s.ext.y + s.ext.x * s.ext.x) / 3.0;
+  } else if (type == GRAINS_GPU_CYLINDER) {
+    if (np < 2) return err = "cylinder needs radius and height", GRAINS_GPU_INVALID_ARGUMENT;
+    s.radius = p[0];
+    s.half_height = p[1] / 2.;
+    s.volume = 2 * s.half_height * kPi * s.radius * s.radius;                       // Cylinder.cpp:97-100
+    s.circ = std::sqrt(s.radius * s.radius + s.half_height * s.half_height);        // Cylinder.cpp:82-85
+    double cst = 0.5 * s.half_height * s.radius * s.radius * kPi;                   // Cylinder.cpp:61-75
+    s.inertia[0] = s.inertia[2] = cst * (4.0 * s.half_height * s.half_height / 3.0 + s.radius * s.radius);
+    s.inertia[1] = 2.0 * cst * s.radius * s.radius;
+  } else if (type == GRAINS_GPU_POLYHEDRON) {
+    if (np < 1) return err = "polyhedron needs vertices", GRAINS_GPU_INVALID_ARGUMENT;
+    int nv = (int)p[0], k = 1;
+    if (nv < 4 || np < 1 + 3 * nv + 1) return err = "bad polyhedron description", GRAINS_GPU_INVALID_ARGUMENT;
+    for (int i = 0; i < 3 * nv; ++i) s.verts.push_back(p[k++]);
+    int nf = (int)p[k++];
+    double I[3] = {0, 0, 0}, vol = 0;
+    for (int f = 0; f < nf; ++f) {
+      if (k >= np) return err = "truncated polyhedron faces", GRAINS_GPU_INVALID_ARGUMENT;
+      int m = (int)p[k++];
+      std::vector<int> face;
+      for (int j = 0; j < m; ++j) {
+        int vi = (int)p[k++];
+        if (vi < 0 || vi >= nv) return err = "polyhedron face index out of range", GRAINS_GPU_INVALID_ARGUMENT;
+        face.push_back(vi);
+      }
+      s.faces.push_back(face);
+      auto V = [&](int i) { return d3(s.verts[3 * i], s.verts[3 * i + 1], s.verts[3 * i + 2]); };
+      if (m == 3) {
+        tetra_contrib(V(face[0]), V(face[1]), V(face[2]), vol, I);
+      } else {  // fan around the face centroid (Polyhedron.cpp:341-356)
+        D3 g = d3(0, 0, 0);
+        for (int j = 0; j < m; ++j) g = d3(g.x + V(face[j]).x, g.y + V(face[j]).y, g.z + V(face[j]).z);
+        g = d3(g.x / m, g.y / m, g.z / m);
+        for (int j = 0, kk = m - 1; j < m; kk = j++) tetra_contrib(g, V(face[kk]), V(face[j]), vol, I);
+      }
+    }
+    s.volume = vol;
+    for (int i = 0; i < 3; ++i) s.inertia[i] = I[i];
+    double r2 = 0;  // Polyhedron::computeCircumscribedRadius, Polyhedron.cpp:201-210
+    for (int i = 0; i < nv; ++i) {
+      double d = s.verts[3 * i] * s.verts[3 * i] + s.verts[3 * i + 1] * s.verts[3 * i + 1] +
+                 s.verts[3 * i + 2] * s.verts[3 * i + 2];
+      if (i == 0 || d > r2) r2 = d;
+    }
+    s.circ = std::sqrt(r2);
+  } else {
+    return err = "unknown shape type", GRAINS_GPU_INVALID_ARGUMENT;
+  }
+  // local bounding box half extents, Convex::bbox with the identity (Convex.cpp:29-41)
+  for (int i = 0; i < 3; ++i) {
+    D3 e = d3(i == 0, i == 1, i == 2);
+    D3 ne = d3(-e.x, -e.y, -e.z);
+    double mn = xdot(e, shape_support(s, ne)), mx = xdot(e, shape_support(s, e));
+    s.lext[i] = (mx - mn) / 2.;
+  }
+  return 0;
+}
+
+ShapeDev shape_dev(const ShapeHost& s, int vert_offset) {
+  ShapeDev d{};
+  d.type = s.type;
+  d.nverts = (int)s.verts.size() / 3;
+  d.vert_offset = vert_offset;
+  d.radius = s.radius;
+  d.half_height = s.half_height;
+  d.ext[0] = s.ext.x;
+  d.ext[1] = s.ext.y;
+  d.ext[2] = s.ext.z;
+  d.circ = s.circ;
+  for (int i = 0; i < 3; ++i) d.scaling_ext[i] = s.lext[i];
+  d.volume = s.volume;
+  return d;
+}
+
+// ---- obstacles ----------------------------------------------------------------
+ObstacleDev obstacle_dev(const grains_gpu_obstacle& o, const ShapeHost& sh) {
+  ObstacleDev d{};
+  for (int i = 0; i < 9; ++i) d.b[i] = o.transform[i];
+  for (int i = 0; i < 3; ++i) d.o[i] = o.transform[9 + i];
+  for (int i = 0; i < 3; ++i) {
+    d.vel[i] = o.velocity[i];
+    d.omega[i] = o.omega[i];
+    d.rot_center[i] = o.rotation_center[i];
+  }
+  d.crust = o.crust;
+  d.circ = sh.circ;
+  for (int i = 0; i < 3; ++i) d.scaling[i] = sh.lext[i] < kEpsilon ? 1. : (sh.lext[i] - o.crust) / sh.lext[i];
+  d.id = o.id;
+  d.material = o.material;
+  d.shape = o.shape;
+  d.moving = o.moving;
+  // world AABB: Convex::bbox (Convex.cpp:29-41) -> BBox centre / extent (BBox.cpp:235-239)
+  M3 b;
+  for (int i = 0; i < 9; ++i) b.m[i] = d.b[i];
+  double mn[3], mx[3];
+  for (int i = 0; i < 3; ++i) {
+    D3 r = mrow(b, i);
+    D3 nr = d3(-r.x, -r.y, -r.z);
+    mn[i] = xadd(d.o[i], xdot(r, shape_support(sh, nr)));
+    mx[i] = xadd(d.o[i], xdot(r, shape_support(sh, r)));
+  }
+  for (int i = 0; i < 3; ++i) {
+    d.bbe[i] = xdiv(xsub(mx[i], mn[i]), 2.);
+    d.bbc[i] = xadd(mn[i], d.bbe[i]);
+  }
+  return d;
+}
+
+BodyRef obstacle_body(const ObstacleDev& o, const ShapeHost& sh) {
+  BodyRef b{};
+  b.type = sh.type;
+  b.nverts = (int)sh.verts.size() / 3;
+  b.verts = sh.verts.data();
+  b.radius = sh.circ;
+  b.cyl_r = sh.radius;
+  b.cyl_hh = sh.half_height;
+  b.ext = sh.ext;
+  b.crust = o.crust;
+  for (int i = 0; i < 9; ++i) b.basis.m[i] = o.b[i];
+  b.origin = d3(o.o[0], o.o[1], o.o[2]);
+  for (int i = 0; i < 3; ++i) {
+    b.scaling[i] = o.scaling[i];
+    b.lext[i] = sh.lext[i];
+  }
+  return b;
+}
+
+// LinkedCell::Link(Obstacle*) (Base/src/LinkedCell.cpp:1371-1445): a cell is
+// linked to a static obstacle when the obstacle's AABB is within one cell edge
+// of the cell centre and a crust GJK test between the twice-expanded cell box
+// and the obstacle says contact (RigidBodyWithCrust::isContact,
+// RigidBodyWithCrust.cpp:842-956: distance < crust_cell + crust_obs - EPSILON).
+void link_static_obstacles(const SysHost& s, const std::vector<ShapeHost>& shapes,
+                           const std::vector<ObstacleDev>& obs, int first_obs,
+                           std::vector<std::vector<int>>& cell_lists) {
+  const double hx = 0.5 * 2. * s.ex, hy = 0.5 * 2. * s.ey, hz = 0.5 * 2. * s.ez;
+  ShapeHost cellbox;
+  std::string unused;
+  const double cell_edges[3] = {2. * hx, 2. * hy, 2. * hz};
+  build_shape(GRAINS_GPU_BOX, cell_edges, 3, cellbox, unused);
+  const int nb = s.nbi * s.nbj * s.nbk;
+  for (size_t oi = 0; oi < s.obs.size(); ++oi) {
+    const ObstacleDev& O = obs[first_obs + oi];
+    if (O.moving) continue;
+    const ShapeHost& sh = shapes[O.shape];
+    BodyRef B = obstacle_body(O, sh);
+    for (int c = 0; c < nb; ++c) {
+      int i = c % s.nbi, k = (c / s.nbi) % s.nbk, j = c / (s.nbi * s.nbk);
+      D3 cg = d3(s.dom.origin[0] + i * s.ex + s.ex / 2., s.dom.origin[1] + j * s.ey + s.ey / 2.,
+                 s.dom.origin[2] + k * s.ez + s.ez / 2.);  // Cell::setCentre, Cell.cpp:74-82
+      if (!in_zone(d3(O.bbc[0], O.bbc[1], O.bbc[2]), d3(O.bbe[0], O.bbe[1], O.bbe[2]), cg, hx, hy, hz)) continue;
+      bool add;
+      if (sh.type == GRAINS_GPU_SPHERE) {
+        add = true;
+      } else {
+        BodyRef A{};
+        A.type = GRAINS_GPU_BOX;
+        A.verts = nullptr;
+        A.radius = cellbox.circ;
+        A.ext = cellbox.ext;
+        A.crust = O.crust;
+        for (int t = 0; t < 9; ++t) A.basis.m[t] = (t % 4 == 0) ? 1. : 0.;
+        A.origin = cg;
+        for (int t = 0; t < 3; ++t) {
+          A.lext[t] = cellbox.lext[t];
+          A.scaling[t] = cellbox.lext[t] < kEpsilon ? 1. : (cellbox.lext[t] - A.crust) / cellbox.lext[t];
+        }
+        add = false;
+        D3 g = xsub3(A.origin, B.origin);
+        if (xnorm(g) < A.radius + B.radius) {
+          LocalBody<double> la = local_body<double>(A, d3(0, 0, 0), A.scaling);
+          LocalBody<double> lb = local_body<double>(B, d3(0, 0, 0), B.scaling);
+          GjkResult<double> r = gjk_distance(la, lb, kEpsilon);
+          add = r.dist < A.crust + B.crust - kEpsilon;
+        }
+      }
+      if (add) cell_lists[c].push_back(first_obs + (int)oi);
+    }
+  }
+}
+
+template <typename R>
+void fill_arrays(grains_gpu_ctx* c, ParticleArrays<R>& P, int which) {
+  auto& b = c->buf[which];
+  P.xr = b.xr;
+  P.q = b.q;
+  P.basis = b.basis;
+  P.v = (typename Vec4<R>::type*)b.v;
+  P.w = (typename Vec4<R>::type*)b.w;
+  P.wbf = (typename Vec4<R>::type*)b.wbf;
+  P.F = (typename Vec4<R>::type*)b.F;
+  P.T = (typename Vec4<R>::type*)b.T;
+  P.inertia = (typename Vec4<R>::type*)b.inertia;
+  P.md = b.md;
+  P.meta = b.meta;
+  P.orig = b.orig;
+}
+
+template <typename R>
+StepArgs<R> make_args(grains_gpu_ctx* c) {
+  StepArgs<R> a{};
+  a.n = (int)c->n;
+  a.n_cells = c->n_cells;
+  a.n_sys = (int)c->sys.size();
+  a.hist_cap = c->hist_cap;
+  a.has_basis = c->has_basis ? 1 : 0;
+  a.sys = c->d_sys;
+  a.shapes = c->d_shapes;
+  a.verts = c->d_verts;
+  a.obs = c->d_obs;
+  a.cell_obs_start = c->d_cell_obs_start;
+  a.cell_obs_idx = c->d_cell_obs_idx;
+  a.moving_idx = c->d_moving;
+  a.laws = (const LawParams<R>*)c->d_laws;
+  fill_arrays<R>(c, a.cur, c->cur);
+  fill_arrays<R>(c, a.alt, 1 - c->cur);
+  a.coord = c->coord;
+  a.key = c->key;
+  a.rank = c->rank;
+  a.cell_count = c->cell_count;
+  a.cell_start = c->cell_start;
+  a.block_sums = c->block_sums;
+  a.perm = c->perm;
+  a.hist_prev = (HistEntry<R>*)c->hist[c->hcur];
+  a.hist_n_prev = c->hist_n[c->hcur];
+  a.hist_next = (HistEntry<R>*)c->hist[1 - c->hcur];
+  a.hist_n_next = c->hist_n[1 - c->hcur];
+  a.stats = c->stats;
+  a.pairs = c->pairs;
+  a.pairs_cap = c->pairs_cap;
+  a.pairs_n = c->pairs_n;
+  a.gjk_tol = c->gjk_tol;
+  return a;
+}
+
+// Runs f(args) with the StepArgs of the context's precision
+template <typename F>
+int with_args(grains_gpu_ctx* c, F f) {
+  if (c->precision == GRAINS_GPU_FP64) {
+    StepArgs<double> a = make_args<double>(c);
+    return f(a);
+  }
+  StepArgs<float> a = make_args<float>(c);
+  return f(a);
+}
+
+int sort_now(grains_gpu_ctx* c, int gather_forces) {
+  int rc = 0;
+  if (!c->keys_valid) {
+    rc = with_args(c, [&](auto& a) { return launch_bin(a, c->stream); });
+    if (rc) return fail(c, rc, "bin kernel launch failed");
+  }
+  rc = with_args(c, [&](auto& a) { return launch_sort_and_gather(a, c->stream, gather_forces); });
+  if (rc) return fail(c, rc, "sort kernels launch failed");
+  c->cur = 1 - c->cur;
+  c->sorted = true;
+  c->keys_valid = false;
+  return 0;
+}
+
+int read_status(grains_gpu_ctx* c) {
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, &c->stats->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return st;
+}
+
+std::string status_message(int st) {
+  std::string m;
+  if (st & GRAINS_GPU_CONTACT_ERROR) m += "ContactError (overlap exceeded the crust sum); ";
+  if (st & GRAINS_GPU_MOTION_ERROR) m += "MotionError (displacement larger than the crust); ";
+  if (st & GRAINS_GPU_OUT_OF_GRID) m += "SimulationError (particle outside the linked-cell grid); ";
+  if (st & GRAINS_GPU_HISTORY_FULL) m += "contact-memory row full; ";
+  if (st & GRAINS_GPU_GJK_NOT_CONVERGED) m += "GJK iteration cap reached; ";
+  return m;
+}
+
+// errors that end a run (informational bits excluded)
+int fatal_bits(int st) { return st & ~(GRAINS_GPU_CONTACT_HANDLED | GRAINS_GPU_GJK_NOT_CONVERGED); }
+
+int finish_call(grains_gpu_ctx* c) {
+  int st = read_status(c);
+  if (st < 0) return GRAINS_GPU_CUDA_ERROR;
+  int f = fatal_bits(st);
+  if (f) c->err = status_message(st);
+  return f;
+}
+
+int flush_kick(grains_gpu_ctx* c) {
+  if (!c->pending_kick2) return 0;
+  int rc = with_args(c, [&](auto& a) { return launch_kick_move(a, c->stream, 1, c->pending_dt, 0, 0., 0.); });
+  c->pending_kick2 = false;
+  return rc ? fail(c, rc, "advance-velocity launch failed") : 0;
+}
+
+int forces_now(grains_gpu_ctx* c, double dt, int diag) {
+  if (!c->sorted) {
+    if (int rc = sort_now(c, 1)) return rc;
+  }
+  int rc = with_args(c, [&](auto& a) { return launch_forces(a, c->stream, dt, diag); });
+  if (rc) return fail(c, rc, "force kernel launch failed");
+  c->hcur = 1 - c->hcur;
+  return 0;
+}
+
+// One fused DEM step (pending kick2 + move, sort, gather, forces)
+int fused_step(grains_gpu_ctx* c, double dt) {
+  int rc = with_args(c, [&](auto& a) {
+    return launch_kick_move(a, c->stream, c->pending_kick2 ? 1 : 0, 0.5 * dt, 1, 0.5 * dt, dt);
+  });
+  if (rc) return fail(c, rc, "kick/move launch failed");
+  c->keys_valid = true;
+  c->sorted = false;
+  if ((rc = sort_now(c, 0))) return rc;
+  if ((rc = forces_now(c, dt, 0))) return rc;
+  c->pending_kick2 = true;
+  c->pending_dt = 0.5 * dt;
+  return 0;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
+  if (!cfg || !out) return GRAINS_GPU_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (cfg->n_systems < 1 || cfg->max_particles < 1 || cfg->max_particles > (int64_t)1 << 30)
+    return GRAINS_GPU_INVALID_ARGUMENT;
+  if (cfg->precision != GRAINS_GPU_FP64 && cfg->precision != GRAINS_GPU_MIXED) return GRAINS_GPU_INVALID_ARGUMENT;
+  grains_gpu_ctx* c = new grains_gpu_ctx();
+  c->cfg = *cfg;
+  c->precision = cfg->precision;
+  c->hist_cap = cfg->history_capacity > 0 ? cfg->history_capacity : 24;
+  c->rsize = cfg->precision == GRAINS_GPU_FP64 ? 8 : 4;
+  c->cap = cfg->max_particles;
+  c->sys.resize(cfg->n_systems);
+  cudaError_t e = cudaSetDevice(cfg->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    int rc = cuda_fail(c, e, "cudaSetDevice/cudaStreamCreate");
+    *out = c;  // keep the message readable
+    return rc;
+  }
+  const size_t N = (size_t)c->cap;
+  const size_t r4 = 4 * c->rsize;
+  bool ok = true;
+  for (int k = 0; k < 2 && ok; ++k) {
+    auto& b = c->buf[k];
+    b.xr = dalloc<double4>(N, c->pool);
+    b.q = dalloc<double4>(N, c->pool);
+    b.basis = nullptr;
+    b.v = dalloc<char>(N * r4, c->pool);
+    b.w = dalloc<char>(N * r4, c->pool);
+    b.wbf = dalloc<char>(N * r4, c->pool);
+    b.F = dalloc<char>(N * r4, c->pool);
+    b.T = dalloc<char>(N * r4, c->pool);
+    b.inertia = dalloc<char>(N * r4, c->pool);
+    b.md = dalloc<double4>(N, c->pool);
+    b.meta = dalloc<int4>(N, c->pool);
+    b.orig = dalloc<int>(N, c->pool);
+    ok = b.xr && b.q && b.v && b.w && b.wbf && b.F && b.T && b.inertia && b.md && b.meta && b.orig;
+  }
+  const size_t hsz = c->precision == GRAINS_GPU_FP64 ? sizeof(HistEntry<double>) : sizeof(HistEntry<float>);
+  for (int k = 0; k < 2 && ok; ++k) {
+    c->hist[k] = dalloc<char>(N * c->hist_cap * hsz, c->pool);
+    c->hist_n[k] = dalloc<int>(N, c->pool);
+    ok = c->hist[k] && c->hist_n[k];
+  }
+  if (ok) {
+    c->coord = dalloc<int>(N, c->pool);
+    c->key = dalloc<unsigned>(N, c->pool);
+    c->rank = dalloc<unsigned>(N, c->pool);
+    c->perm = dalloc<int>(N, c->pool);
+    c->stats = dalloc<StatsDev>(1, c->pool);
+    c->pairs_cap = (int)std::min<size_t>(16 * N + 1024, (size_t)1 << 30);
+    c->pairs = dalloc<int>(2 * (size_t)c->pairs_cap, c->pool);
+    c->pairs_n = dalloc<unsigned long long>(1, c->pool);
+    ok = c->coord && c->key && c->rank && c->perm && c->stats && c->pairs && c->pairs_n;
+  }
+  if (!ok) {
+    c->err = "cudaMalloc failed for the requested capacity";
+    *out = c;
+    return GRAINS_GPU_CUDA_ERROR;
+  }
+  for (int k = 0; k < 2; ++k) cudaMemsetAsync(c->hist_n[k], 0, N * sizeof(int), c->stream);
+  cudaMemsetAsync(c->stats, 0, sizeof(StatsDev), c->stream);
+  cudaStreamSynchronize(c->stream);
+  *out = c;
+  return 0;
+}
+
+int grains_gpu_destroy(grains_gpu_ctx* c) {
+  if (!c) return 0;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int k = 0; k < 4; ++k)
+    if (c->graph[k]) cudaGraphExecDestroy(c->graph[k]);
+  for (void* p : c->pool) cudaFree(p);
+  for (void* p : c->table_pool) cudaFree(p);
+  for (int k = 0; k < 2; ++k)
+    if (c->buf[k].basis) cudaFree(c->buf[k].basis);
+  if (c->stage) cudaFree(c->stage);
+  if (c->stage_basis) cudaFree(c->stage_basis);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return 0;
+}
+
+int grains_gpu_last_error(const grains_gpu_ctx* c, char* buf, size_t len) {
+  if (!c || !buf || !len) return GRAINS_GPU_INVALID_ARGUMENT;
+  std::snprintf(buf, len, "%s", c->err.c_str());
+  return 0;
+}
+
+int grains_gpu_get_stream(const grains_gpu_ctx* c, void** stream) {
+  if (!c || !stream) return GRAINS_GPU_INVALID_ARGUMENT;
+  *stream = (void*)c->stream;
+  return 0;
+}
+
+int grains_gpu_set_domain(grains_gpu_ctx* c, int32_t system, const grains_gpu_domain* d) {
+  if (!c || !d) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (system < 0 || system >= (int)c->sys.size()) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "bad system index");
+  for (int i = 0; i < 3; ++i)
+    if (!(d->size[i] > 0)) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "domain size must be positive");
+  SysHost& s = c->sys[system];
+  s.dom = *d;
+  const double cs = d->cell_size;
+  // LinkedCell::set (LinkedCell.cpp:69-98)
+  if (cs > kEpsilon) {
+    s.nbi = (int)((d->size[0] + kEpsilon) / cs);
+    if (!s.nbi) s.nbi = 1;
+    s.ex = d->size[0] / s.nbi;
+    s.nbj = (int)((d->size[1] + kEpsilon) / cs);
+    if (!s.nbj) s.nbj = 1;
+    s.ey = d->size[1] / s.nbj;
+    s.nbk = (int)((d->size[2] + kEpsilon) / cs);
+    if (!s.nbk) s.nbk = 1;
+    s.ez = d->size[2] / s.nbk;
+  } else {
+    s.nbi = s.nbj = s.nbk = 1;
+    s.ex = d->size[0];
+    s.ey = d->size[1];
+    s.ez = d->size[2];
+  }
+  if ((double)s.nbi * s.nbj * s.nbk > 2.0e9) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "too many cells");
+  s.has_domain = true;
+  c->uploaded = false;
+  c->tables_dirty = true;
+  return 0;
+}
+
+int grains_gpu_add_shape(grains_gpu_ctx* c, int32_t type, const double* params, int32_t n, int32_t* id) {
+  if (!c || !params || !id) return GRAINS_GPU_INVALID_ARGUMENT;
+  ShapeHost s;
+  std::string err;
+  if (int rc = build_shape(type, params, n, s, err)) return fail(c, rc, err);
+  c->shapes.push_back(s);
+  *id = (int32_t)c->shapes.size() - 1;
+  c->tables_dirty = true;
+  return 0;
+}
+
+int grains_gpu_set_contact_law(grains_gpu_ctx* c, int32_t system, int32_t a, int32_t b, int32_t law,
+                               const double* p, int32_t n) {
+  if (!c || !p) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (system < 0 || system >= (int)c->sys.size() || a < 0 || b < 0)
+    return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "bad system or material index");
+  int maxmat = c->cfg.max_materials > 0 ? c->cfg.max_materials : 4;
+  if (a >= maxmat || b >= maxmat) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "material index >= max_materials");
+  LawHost L;
+  L.type = law;
+  if (law == GRAINS_GPU_HOOKE_MEMORY) {
+    if (n < 8) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "HookeMemory needs kn, en, etat, muc, kt, mur, etarpf, epst");
+    for (int i = 0; i < 8; ++i) L.p[i] = p[i];
+  } else if (law == GRAINS_GPU_HOOKE) {
+    if (n < 5) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "Hooke needs kn, en, etat, muc, kr");
+    L.p[0] = p[0];
+    L.p[1] = p[1];
+    L.p[2] = p[2];
+    L.p[3] = p[3];
+    L.p[8] = p[4];
+  } else {
+    return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "unknown contact law");
+  }
+  if (!(L.p[1] > 0 && L.p[1] <= 1)) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "restitution must be in (0, 1]");
+  // m_beta, HookeMemoryContactForceModel.cpp:28 / HookeContactForceModel.cpp:17
+  L.beta = std::log(L.p[1]) / std::sqrt(kPi * kPi + std::log(L.p[1]) * std::log(L.p[1]));
+  c->sys[system].laws[std::make_pair(std::min(a, b), std::max(a, b))] = L;
+  c->uploaded = false;
+  c->tables_dirty = true;
+  return 0;
+}
+
+int grains_gpu_set_obstacles(grains_gpu_ctx* c, int32_t system, int32_t n, const grains_gpu_obstacle* o) {
+  if (!c || (n > 0 && !o)) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (system < 0 || system >= (int)c->sys.size()) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "bad system index");
+  for (int i = 0; i < n; ++i)
+    if (o[i].shape < 0 || o[i].shape >= (int)c->shapes.size())
+      return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "obstacle shape id out of range");
+  c->sys[system].obs.assign(o, o + n);
+  c->uploaded = false;
+  c->tables_dirty = true;
+  return 0;
+}
+
+namespace {
+// Builds the device tables and the per-cell obstacle links (set-up time)
+int build_tables(grains_gpu_ctx* c) {
+  for (void* p : c->table_pool) cudaFree(p);
+  c->table_pool.clear();
+  const int maxmat = c->cfg.max_materials > 0 ? c->cfg.max_materials : 4;
+  std::vector<SysDev> hs;
+  std::vector<ObstacleDev> ho;
+  std::vector<int> moving;
+  std::vector<int> cstart;
+  std::vector<int> cidx;
+  int cells = 0;
+  for (size_t si = 0; si < c->sys.size(); ++si) {
+    SysHost& s = c->sys[si];
+    if (!s.has_domain) return fail(c, GRAINS_GPU_NOT_READY, "a system has no domain");
+    SysDev d{};
+    d.ox = s.dom.origin[0];
+    d.oy = s.dom.origin[1];
+    d.oz = s.dom.origin[2];
+    d.ex = s.ex;
+    d.ey = s.ey;
+    d.ez = s.ez;
+    d.gx = s.dom.gravity[0];
+    d.gy = s.dom.gravity[1];
+    d.gz = s.dom.gravity[2];
+    d.nbi = s.nbi;
+    d.nbj = s.nbj;
+    d.nbk = s.nbk;
+    d.cell_offset = cells;
+    d.law_offset = (int)si * maxmat * maxmat;
+    d.n_mat = maxmat;
+    d.obs_offset = (int)ho.size();
+    d.n_obs = (int)s.obs.size();
+    d.moving_offset = (int)moving.size();
+    for (size_t k = 0; k < s.obs.size(); ++k) {
+      ho.push_back(obstacle_dev(s.obs[k], c->shapes[s.obs[k].shape]));
+      if (s.obs[k].moving) moving.push_back(d.obs_offset + (int)k);
+    }
+    d.n_moving = (int)moving.size() - d.moving_offset;
+    const int nb = s.nbi * s.nbj * s.nbk;
+    std::vector<std::vector<int>> lists(nb);
+    link_static_obstacles(s, c->shapes, ho, d.obs_offset, lists);
+    for (int k = 0; k < nb; ++k) {
+      cstart.push_back((int)cidx.size());
+      cidx.insert(cidx.end(), lists[k].begin(), lists[k].end());
+    }
+    if ((long long)cells + nb > 2000000000LL) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "too many cells");
+    cells += nb;
+    hs.push_back(d);
+  }
+  cstart.push_back((int)cidx.size());
+  c->n_cells = cells;
+  c->h_sys = hs;
+  c->h_obs = ho;
+  // laws
+  std::vector<LawParams<double>> ld(c->sys.size() * maxmat * maxmat);
+  std::vector<LawParams<float>> lf(ld.size());
+  for (auto& x : ld) x.type = -1;
+  for (auto& x : lf) x.type = -1;
+  for (size_t si = 0; si < c->sys.size(); ++si)
+    for (auto& kv : c->sys[si].laws)
+      for (int flip = 0; flip < 2; ++flip) {
+        int a = flip ? kv.first.second : kv.first.first, b = flip ? kv.first.first : kv.first.second;
+        size_t k = si * maxmat * maxmat + a * maxmat + b;
+        const LawHost& L = kv.second;
+        LawParams<double> P{};
+        P.type = L.type;
+        P.kn = L.p[0];
+        P.en = L.p[1];
+        P.etat = L.p[2];
+        P.muc = L.p[3];
+        P.kt = L.p[4];
+        P.mur = L.p[5];
+        P.etarpf = L.p[6];
+        P.epst = L.p[7];
+        P.kr = L.p[8];
+        P.beta = L.beta;
+        P.rolling = (L.type == GRAINS_GPU_HOOKE_MEMORY && P.mur != 0.) ? 1 : 0;
+        ld[k] = P;
+        LawParams<float> Q{};
+        Q.type = P.type;
+        Q.rolling = P.rolling;
+        Q.kn = (float)P.kn; Q.en = (float)P.en; Q.etat = (float)P.etat; Q.muc = (float)P.muc;
+        Q.kt = (float)P.kt; Q.mur = (float)P.mur; Q.etarpf = (float)P.etarpf; Q.epst = (float)P.epst;
+        Q.kr = (float)P.kr; Q.beta = (float)P.beta;
+        lf[k] = Q;
+      }
+  // shapes
+  std::vector<ShapeDev> sd;
+  std::vector<double> verts;
+  for (auto& s : c->shapes) {
+    sd.push_back(shape_dev(s, (int)verts.size() / 3));
+    verts.insert(verts.end(), s.verts.begin(), s.verts.end());
+  }
+  auto up = [&](const void* src, size_t bytes, void** dst) -> int {
+    void* p = nullptr;
+    CK(cudaMalloc(&p, bytes ? bytes : 16));
+    c->table_pool.push_back(p);
+    if (bytes) CK(cudaMemcpyAsync(p, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    *dst = p;
+    return 0;
+  };
+  int rc = 0;
+  rc |= up(hs.data(), hs.size() * sizeof(SysDev), (void**)&c->d_sys);
+  rc |= up(sd.data(), sd.size() * sizeof(ShapeDev), (void**)&c->d_shapes);
+  rc |= up(verts.data(), verts.size() * sizeof(double), (void**)&c->d_verts);
+  rc |= up(ho.data(), ho.size() * sizeof(ObstacleDev), (void**)&c->d_obs);
+  rc |= up(cstart.data(), cstart.size() * sizeof(int), (void**)&c->d_cell_obs_start);
+  rc |= up(cidx.data(), cidx.size() * sizeof(int), (void**)&c->d_cell_obs_idx);
+  rc |= up(moving.data(), moving.size() * sizeof(int), (void**)&c->d_moving);
+  if (c->precision == GRAINS_GPU_FP64)
+    rc |= up(ld.data(), ld.size() * sizeof(LawParams<double>), &c->d_laws);
+  else
+    rc |= up(lf.data(), lf.size() * sizeof(LawParams<float>), &c->d_laws);
+  if (rc) return rc;
+  // cell arrays
+  void* p = nullptr;
+  CK(cudaMalloc(&p, (size_t)cells * sizeof(int)));
+  c->table_pool.push_back(p);
+  c->cell_count = (int*)p;
+  CK(cudaMalloc(&p, ((size_t)cells + 1) * sizeof(int)));
+  c->table_pool.push_back(p);
+  c->cell_start = (int*)p;
+  CK(cudaMalloc(&p, ((size_t)cells / 4096 + 2) * sizeof(int)));
+  c->table_pool.push_back(p);
+  c->block_sums = (int*)p;
+  CK(cudaMemsetAsync(c->cell_count, 0, (size_t)cells * sizeof(int), c->stream));
+  if (((size_t)cells / 4096 + 1) > 4096) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "too many cells for the scan");
+  for (int k = 0; k < 4; ++k)
+    if (c->graph[k]) {
+      cudaGraphExecDestroy(c->graph[k]);
+      c->graph[k] = nullptr;
+    }
+  return 0;
+}
+}  // namespace
+
+int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p) {
+  if (!c || !p) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (p->n < 0 || p->n > c->cap) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "particle count exceeds capacity");
+  if (!p->id || !p->shape || !p->material || !p->radius || !p->crust || !p->mass || !p->inertia || !p->position ||
+      !p->quaternion || !p->velocity || !p->omega)
+    return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "missing particle array");
+  const int64_t n = p->n;
+  const int maxmat = c->cfg.max_materials > 0 ? c->cfg.max_materials : 4;
+  bool basis_needed = false;
+  for (int64_t i = 0; i < n; ++i) {
+    if (p->shape[i] < 0 || p->shape[i] >= (int)c->shapes.size())
+      return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "particle shape id out of range");
+    if (p->material[i] < 0 || p->material[i] >= maxmat)
+      return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "particle material out of range");
+    int si = p->system ? p->system[i] : 0;
+    if (si < 0 || si >= (int)c->sys.size()) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "particle system out of range");
+    if (c->shapes[p->shape[i]].type != GRAINS_GPU_SPHERE) basis_needed = true;
+  }
+  if (c->tables_dirty) {
+    if (int rc = build_tables(c)) return rc;
+    c->tables_dirty = false;
+  }
+  c->has_basis = basis_needed;
+  if (basis_needed) {
+    for (int k = 0; k < 2; ++k)
+      if (!c->buf[k].basis) {
+        void* q = nullptr;
+        CK(cudaMalloc(&q, (size_t)c->cap * 9 * sizeof(double)));
+        c->buf[k].basis = (double*)q;
+      }
+  }
+  c->n = n;
+  c->cur = 0;
+  auto& b = c->buf[0];
+  std::vector<double4> xr(n), q(n), md(n);
+  std::vector<int4> meta(n);
+  std::vector<int> orig(n);
+  std::vector<double> basis(basis_needed ? 9 * n : 0);
+  std::vector<double> vd, wd, wbfd, Id, zd;
+  std::vector<float> vf, wf, wbff, If, zf;
+  const bool dbl = c->precision == GRAINS_GPU_FP64;
+  auto put = [&](std::vector<double>& D, std::vector<float>& Fv, int64_t i, double x, double y, double z) {
+    if (dbl) {
+      D[4 * i] = x; D[4 * i + 1] = y; D[4 * i + 2] = z; D[4 * i + 3] = 0;
+    } else {
+      Fv[4 * i] = (float)x; Fv[4 * i + 1] = (float)y; Fv[4 * i + 2] = (float)z; Fv[4 * i + 3] = 0;
+    }
+  };
+  if (dbl) { vd.resize(4 * n); wd.resize(4 * n); wbfd.resize(4 * n); Id.resize(4 * n); zd.assign(4 * n, 0.); }
+  else { vf.resize(4 * n); wf.resize(4 * n); wbff.resize(4 * n); If.resize(4 * n); zf.assign(4 * n, 0.f); }
+  for (int64_t i = 0; i < n; ++i) {
+    const ShapeHost& sh = c->shapes[p->shape[i]];
+    xr[i] = make_double4(p->position[3 * i], p->position[3 * i + 1], p->position[3 * i + 2], p->radius[i]);
+    Qt<double> qq{v3<double>(p->quaternion[4 * i], p->quaternion[4 * i + 1], p->quaternion[4 * i + 2]),
+                  p->quaternion[4 * i + 3]};
+    q[i] = make_double4(qq.v.x, qq.v.y, qq.v.z, qq.w);
+    double vol = sh.type == GRAINS_GPU_SPHERE ? 4.0 * kPi * std::pow(p->radius[i], 3.) / 3.0 : sh.volume;
+    double req = std::pow((0.75 / kPi) * vol, 1. / 3.);  // Component::getEquivalentSphereRadius
+    md[i] = make_double4(p->mass[i], p->crust[i], req, 0.);
+    meta[i] = make_int4(p->id[i], p->material[i], p->shape[i], p->system ? p->system[i] : 0);
+    orig[i] = (int)i;
+    put(vd, vf, i, p->velocity[3 * i], p->velocity[3 * i + 1], p->velocity[3 * i + 2]);
+    V3<double> w = v3<double>(p->omega[3 * i], p->omega[3 * i + 1], p->omega[3 * i + 2]);
+    put(wd, wf, i, w.x, w.y, w.z);
+    V3<double> wbf = q_to_body(qq, w);  // ParticleKinematics::setAngularVelocity, ParticleKinematics.cpp:197-203
+    put(wbfd, wbff, i, wbf.x, wbf.y, wbf.z);
+    put(Id, If, i, p->inertia[3 * i], p->inertia[3 * i + 1], p->inertia[3 * i + 2]);
+    if (basis_needed) {
+      if (p->basis) {
+        for (int k = 0; k < 9; ++k) basis[9 * i + k] = p->basis[9 * i + k];
+      } else {  // rotation matrix of the quaternion
+        double x = qq.v.x, y = qq.v.y, z = qq.v.z, w0 = qq.w;
+        double m[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - w0 * z), 2 * (x * z + w0 * y),
+                       2 * (x * y + w0 * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w0 * x),
+                       2 * (x * z - w0 * y), 2 * (y * z + w0 * x), 1 - 2 * (x * x + y * y)};
+        for (int k = 0; k < 9; ++k) basis[9 * i + k] = m[k];
+      }
+    }
+  }
+  const size_t r4 = 4 * c->rsize;
+  auto cp = [&](void* dst, const void* src, size_t bytes) -> int {
+    if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c->stream));
+    return 0;
+  };
+  int rc = 0;
+  rc |= cp(b.xr, xr.data(), n * sizeof(double4));
+  rc |= cp(b.q, q.data(), n * sizeof(double4));
+  rc |= cp(b.md, md.data(), n * sizeof(double4));
+  rc |= cp(b.meta, meta.data(), n * sizeof(int4));
+  rc |= cp(b.orig, orig.data(), n * sizeof(int));
+  if (basis_needed) rc |= cp(b.basis, basis.data(), 9 * n * sizeof(double));
+  const void* srcs[6];
+  if (dbl) {
+    srcs[0] = vd.data(); srcs[1] = wd.data(); srcs[2] = wbfd.data(); srcs[3] = zd.data(); srcs[4] = zd.data();
+    srcs[5] = Id.data();
+  } else {
+    srcs[0] = vf.data(); srcs[1] = wf.data(); srcs[2] = wbff.data(); srcs[3] = zf.data(); srcs[4] = zf.data();
+    srcs[5] = If.data();
+  }
+  void* dsts[6] = {b.v, b.w, b.wbf, b.F, b.T, b.inertia};
+  for (int k = 0; k < 6; ++k) rc |= cp(dsts[k], srcs[k], n * r4);
+  if (rc) return rc;
+  for (int k = 0; k < 2; ++k) CK(cudaMemsetAsync(c->hist_n[k], 0, (size_t)c->cap * sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->stats, 0, sizeof(StatsDev), c->stream));
+  c->keys_valid = false;
+  c->sorted = false;
+  c->pending_kick2 = false;
+  c->uploaded = true;
+  if (int e = sort_now(c, 1)) return e;
+  return finish_call(c);
+}
+
+int grains_gpu_download_particles(grains_gpu_ctx* c, grains_gpu_particles* p) {
+  if (!c || !p) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  if (int rc = flush_kick(c)) return rc;
+  const int64_t n = c->n;
+  auto& b = c->buf[c->cur];
+  std::vector<double4> xr(n), q(n);
+  std::vector<int4> meta(n);
+  std::vector<int> orig(n), coord(n);
+  std::vector<double> basis(c->has_basis ? 9 * n : 0);
+  const size_t r4 = 4 * c->rsize;
+  std::vector<char> v(n * r4), w(n * r4), F(n * r4), T(n * r4);
+  CK(cudaMemcpyAsync(xr.data(), b.xr, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(q.data(), b.q, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(meta.data(), b.meta, n * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(orig.data(), b.orig, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(coord.data(), c->coord, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  if (c->has_basis) CK(cudaMemcpyAsync(basis.data(), b.basis, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(v.data(), b.v, n * r4, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(w.data(), b.w, n * r4, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(F.data(), b.F, n * r4, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(T.data(), b.T, n * r4, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const bool dbl = c->precision == GRAINS_GPU_FP64;
+  auto get = [&](const std::vector<char>& src, int64_t s, int k) -> double {
+    return dbl ? ((const double*)src.data())[4 * s + k] : (double)((const float*)src.data())[4 * s + k];
+  };
+  const int64_t m = std::min<int64_t>(p->n, n);
+  for (int64_t s = 0; s < n; ++s) {
+    int64_t i = orig[s];
+    if (i >= m) continue;
+    if (p->id) p->id[i] = meta[s].x;
+    if (p->position) { p->position[3 * i] = xr[s].x; p->position[3 * i + 1] = xr[s].y; p->position[3 * i + 2] = xr[s].z; }
+    if (p->quaternion) {
+      p->quaternion[4 * i] = q[s].x; p->quaternion[4 * i + 1] = q[s].y;
+      p->quaternion[4 * i + 2] = q[s].z; p->quaternion[4 * i + 3] = q[s].w;
+    }
+    if (p->basis) {
+      if (c->has_basis) {
+        for (int k = 0; k < 9; ++k) p->basis[9 * i + k] = basis[9 * s + k];
+      } else {  // spheres: the rotation matrix of the quaternion
+        double x = q[s].x, y = q[s].y, z = q[s].z, w0 = q[s].w;
+        double mm[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - w0 * z), 2 * (x * z + w0 * y),
+                        2 * (x * y + w0 * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w0 * x),
+                        2 * (x * z - w0 * y), 2 * (y * z + w0 * x), 1 - 2 * (x * x + y * y)};
+        for (int k = 0; k < 9; ++k) p->basis[9 * i + k] = mm[k];
+      }
+    }
+    for (int k = 0; k < 3; ++k) {
+      if (p->velocity) p->velocity[3 * i + k] = get(v, s, k);
+      if (p->omega) p->omega[3 * i + k] = get(w, s, k);
+      if (p->force) p->force[3 * i + k] = get(F, s, k);
+      if (p->torque) p->torque[3 * i + k] = get(T, s, k);
+    }
+    if (p->coordination) p->coordination[i] = coord[s];
+  }
+  p->n = m;
+  return 0;
+}
+
+int grains_gpu_update_particles(grains_gpu_ctx* c, const grains_gpu_particles* p) {
+  if (!c || !p) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "upload particles first");
+  if (p->n != c->n) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "update must cover every uploaded particle");
+  if (!p->position || !p->quaternion || !p->velocity || !p->omega)
+    return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "missing kinematic array");
+  const int64_t n = c->n;
+  if (!c->stage) {
+    void* q = nullptr;
+    CK(cudaMalloc(&q, (size_t)c->cap * 13 * sizeof(double)));
+    c->stage = (double*)q;
+  }
+  if (c->has_basis && p->basis && !c->stage_basis) {
+    void* q = nullptr;
+    CK(cudaMalloc(&q, (size_t)c->cap * 9 * sizeof(double)));
+    c->stage_basis = (double*)q;
+  }
+  std::vector<double> h((size_t)n * 13);
+  for (int64_t i = 0; i < n; ++i) {
+    double* e = &h[13 * i];
+    for (int k = 0; k < 3; ++k) e[k] = p->position[3 * i + k];
+    for (int k = 0; k < 4; ++k) e[3 + k] = p->quaternion[4 * i + k];
+    for (int k = 0; k < 3; ++k) e[7 + k] = p->velocity[3 * i + k];
+    for (int k = 0; k < 3; ++k) e[10 + k] = p->omega[3 * i + k];
+  }
+  if (int rc = flush_kick(c)) return rc;
+  CK(cudaMemcpyAsync(c->stage, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  const bool with_basis = c->has_basis && p->basis;
+  if (with_basis)
+    CK(cudaMemcpyAsync(c->stage_basis, p->basis, (size_t)n * 9 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int rc = with_args(c, [&](auto& a) {
+    return launch_update_dynamic(a, c->stream, c->stage, with_basis ? c->stage_basis : nullptr);
+  });
+  if (rc) return fail(c, rc, "update launch failed");
+  c->keys_valid = false;
+  c->sorted = false;
+  if ((rc = sort_now(c, 1))) return rc;
+  return finish_call(c);
+}
+
+int grains_gpu_upload_contact_memory(grains_gpu_ctx* c, const grains_gpu_contact_memory* m) {
+  if (!c || !m) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "upload particles first");
+  const int64_t n = c->n;
+  std::vector<int4> meta(n);
+  std::vector<int> orig(n);
+  auto& b = c->buf[c->cur];
+  CK(cudaMemcpyAsync(meta.data(), b.meta, n * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(orig.data(), b.orig, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::map<std::pair<int, int>, int> row_of;  // (system, id) -> row (upload index)
+  for (int64_t s = 0; s < n; ++s) row_of[std::make_pair(meta[s].w, meta[s].x)] = orig[s];
+  std::vector<int> sys_of_row(n);
+  for (int64_t s = 0; s < n; ++s) sys_of_row[orig[s]] = meta[s].w;
+  const int H = c->hist_cap;
+  std::vector<int> cnt(n, 0);
+  const bool dbl = c->precision == GRAINS_GPU_FP64;
+  std::vector<HistEntry<double>> hd(dbl ? n * H : 0);
+  std::vector<HistEntry<float>> hf(dbl ? 0 : n * H);
+  for (int64_t k = 0; k < m->n; ++k) {
+    // find the owner row in any system holding that id (ids are unique per system;
+    // the owner's system decides)
+    int owner = m->owner[k], other = m->other[k];
+    for (size_t si = 0; si < c->sys.size(); ++si) {
+      auto it = row_of.find(std::make_pair((int)si, owner));
+      if (it == row_of.end()) continue;
+      int row = it->second;
+      int flags = 0, key = other;
+      auto jt = row_of.find(std::make_pair((int)si, other));
+      if (jt == row_of.end()) {  // an obstacle of the system
+        const SysHost& s = c->sys[si];
+        int found = -1;
+        for (size_t oi = 0; oi < s.obs.size(); ++oi)
+          if (s.obs[oi].id == other) found = (int)oi;
+        if (found < 0) break;
+        flags = 1;
+        key = found;
+      } else if (!(owner < other)) {
+        break;  // the lower id holds the pair's memory
+      }
+      if (cnt[row] >= H) return fail(c, GRAINS_GPU_HISTORY_FULL, "contact memory row full at upload");
+      size_t e = (size_t)row * H + cnt[row]++;
+      if (dbl) {
+        HistEntry<double>& x = hd[e];
+        x.other = key; x.flags = flags;
+        for (int t = 0; t < 3; ++t) {
+          x.kd[t] = m->kdelta[3 * k + t]; x.n[t] = m->prev_normal[3 * k + t]; x.sp[t] = m->spring_torque[3 * k + t];
+        }
+      } else {
+        HistEntry<float>& x = hf[e];
+        x.other = key; x.flags = flags;
+        for (int t = 0; t < 3; ++t) {
+          x.kd[t] = (float)m->kdelta[3 * k + t]; x.n[t] = (float)m->prev_normal[3 * k + t];
+          x.sp[t] = (float)m->spring_torque[3 * k + t];
+        }
+      }
+      break;
+    }
+  }
+  const size_t esz = dbl ? sizeof(HistEntry<double>) : sizeof(HistEntry<float>);
+  CK(cudaMemcpyAsync(c->hist[c->hcur], dbl ? (void*)hd.data() : (void*)hf.data(), (size_t)n * H * esz,
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->hist_n[c->hcur], cnt.data(), n * sizeof(int), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int grains_gpu_download_contact_memory(grains_gpu_ctx* c, grains_gpu_contact_memory* m) {
+  if (!c || !m) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "upload particles first");
+  const int64_t n = c->n;
+  const int H = c->hist_cap;
+  const bool dbl = c->precision == GRAINS_GPU_FP64;
+  const size_t esz = dbl ? sizeof(HistEntry<double>) : sizeof(HistEntry<float>);
+  std::vector<char> h((size_t)n * H * esz);
+  std::vector<int> cnt(n);
+  std::vector<int4> meta(n);
+  std::vector<int> orig(n);
+  auto& b = c->buf[c->cur];
+  CK(cudaMemcpyAsync(h.data(), c->hist[c->hcur], h.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(cnt.data(), c->hist_n[c->hcur], n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(meta.data(), b.meta, n * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(orig.data(), b.orig, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::vector<int> id_of_row(n), sys_of_row(n);
+  for (int64_t s = 0; s < n; ++s) {
+    id_of_row[orig[s]] = meta[s].x;
+    sys_of_row[orig[s]] = meta[s].w;
+  }
+  int64_t k = 0, cap = m->n;
+  auto emit = [&](int owner, int other, const double* kd, const double* nn, const double* sp, double sign) {
+    if (k < cap) {
+      m->owner[k] = owner;
+      m->other[k] = other;
+      for (int t = 0; t < 3; ++t) {
+        m->kdelta[3 * k + t] = sign * kd[t];
+        m->prev_normal[3 * k + t] = sign * nn[t];
+        m->spring_torque[3 * k + t] = sign * sp[t];
+      }
+    }
+    ++k;
+  };
+  for (int64_t row = 0; row < n; ++row) {
+    for (int e = 0; e < cnt[row]; ++e) {
+      double kd[3], nn[3], sp[3];
+      int other, flags;
+      if (dbl) {
+        const HistEntry<double>& x = ((const HistEntry<double>*)h.data())[(size_t)row * H + e];
+        other = x.other; flags = x.flags;
+        for (int t = 0; t < 3; ++t) { kd[t] = x.kd[t]; nn[t] = x.n[t]; sp[t] = x.sp[t]; }
+      } else {
+        const HistEntry<float>& x = ((const HistEntry<float>*)h.data())[(size_t)row * H + e];
+        other = x.other; flags = x.flags;
+        for (int t = 0; t < 3; ++t) { kd[t] = x.kd[t]; nn[t] = x.n[t]; sp[t] = x.sp[t]; }
+      }
+      int owner = id_of_row[row];
+      if (flags & 1) {
+        const SysHost& s = c->sys[sys_of_row[row]];
+        int oid = (other >= 0 && other < (int)s.obs.size()) ? s.obs[other].id : other;
+        emit(owner, oid, kd, nn, sp, 1.);
+        emit(oid, owner, kd, nn, sp, -1.);
+      } else {
+        emit(owner, other, kd, nn, sp, 1.);
+        emit(other, owner, kd, nn, sp, -1.);  // mirrored entry (HookeMemoryContactForceModel.cpp:191-192)
+      }
+    }
+  }
+  m->n = k;
+  return k > cap ? fail(c, GRAINS_GPU_PAIR_OVERFLOW, "contact memory buffer too small") : 0;
+}
+
+int grains_gpu_download_obstacles(grains_gpu_ctx* c, int32_t system, int32_t n, double* t) {
+  if (!c || !t) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (system < 0 || system >= (int)c->sys.size()) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "bad system");
+  const SysHost& s = c->sys[system];
+  for (int i = 0; i < n && i < (int)s.obs.size(); ++i)
+    for (int k = 0; k < 12; ++k) t[12 * i + k] = s.obs[i].transform[k];
+  return 0;
+}
+
+int grains_gpu_compute_forces(grains_gpu_ctx* c, double time, double dt) {
+  (void)time;
+  if (!c) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  if (int rc = flush_kick(c)) return rc;
+  CK(cudaMemsetAsync(c->pairs_n, 0, sizeof(unsigned long long), c->stream));
+  if (int rc = forces_now(c, dt, 1)) return rc;
+  return finish_call(c);
+}
+
+int grains_gpu_move(grains_gpu_ctx* c, double time, double dt_v, double dt_x) {
+  (void)time;
+  if (!c) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  if (int rc = flush_kick(c)) return rc;
+  if (!c->sorted) {
+    if (int rc = sort_now(c, 1)) return rc;
+  }
+  int rc = with_args(c, [&](auto& a) { return launch_kick_move(a, c->stream, 0, 0., 1, dt_v, dt_x); });
+  if (rc) return fail(c, rc, "move launch failed");
+  c->keys_valid = true;
+  c->sorted = false;
+  return finish_call(c);
+}
+
+int grains_gpu_link_update(grains_gpu_ctx* c, double time, double dt) {
+  (void)time;
+  (void)dt;
+  if (!c) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  if (!c->sorted)
+    if (int rc = sort_now(c, 1)) return rc;
+  return finish_call(c);
+}
+
+int grains_gpu_advance_velocity(grains_gpu_ctx* c, double time, double dt_v) {
+  (void)time;
+  if (!c) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  if (int rc = flush_kick(c)) return rc;
+  int rc = with_args(c, [&](auto& a) { return launch_kick_move(a, c->stream, 1, dt_v, 0, 0., 0.); });
+  if (rc) return fail(c, rc, "advance-velocity launch failed");
+  return finish_call(c);
+}
+
+int grains_gpu_initialize_leapfrog(grains_gpu_ctx* c, double time, double dt) {
+  if (int rc = grains_gpu_compute_forces(c, time, dt)) return rc;
+  int rc = with_args(c, [&](auto& a) { return launch_zero_kdelta(a, c->stream); });
+  if (rc) return fail(c, rc, "zero-kdelta launch failed");
+  return finish_call(c);
+}
+
+int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt) {
+  if (!c || !time || n_steps < 0 || !(dt > 0)) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  if (!c->sorted)
+    if (int rc = sort_now(c, 1)) return rc;
+  int left = n_steps;
+  // the first step of a run has no pending half kick; run it outside the graph
+  while (left > 0 && !c->pending_kick2) {
+    if (int rc = fused_step(c, dt)) return rc;
+    --left;
+    *time += dt;
+  }
+  while (left >= 2) {
+    const int slot = 2 * c->cur + c->hcur;  // graph keyed by the starting buffer selection
+    if (!c->graph[slot] || c->graph_dt[slot] != dt) {
+      if (c->graph[slot]) {
+        cudaGraphExecDestroy(c->graph[slot]);
+        c->graph[slot] = nullptr;
+      }
+      const int cur0 = c->cur, h0 = c->hcur;
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = fused_step(c, dt);
+      if (!rc) rc = fused_step(c, dt);
+      cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+      c->cur = cur0;  // capture does not execute: restore the buffer parity
+      c->hcur = h0;
+      if (rc) return rc;
+      if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
+      e = cudaGraphInstantiate(&c->graph[slot], g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return cuda_fail(c, e, "cudaGraphInstantiate");
+      c->graph_dt[slot] = dt;
+    }
+    CK(cudaGraphLaunch(c->graph[slot], c->stream));
+    // two steps flip cur twice and hcur twice: parity unchanged
+    left -= 2;
+    *time += 2 * dt;
+  }
+  while (left > 0) {
+    if (int rc = fused_step(c, dt)) return rc;
+    --left;
+    *time += dt;
+  }
+  c->steps_done += n_steps;
+  return 0;
+}
+
+int grains_gpu_synchronize(grains_gpu_ctx* c) {
+  if (!c) return GRAINS_GPU_INVALID_ARGUMENT;
+  return finish_call(c);
+}
+
+int grains_gpu_get_candidate_pairs(grains_gpu_ctx* c, int32_t system, int32_t include_obstacles, int64_t cap,
+                                   int32_t* pairs, int64_t* n) {
+  if (!c || !n || (cap > 0 && !pairs)) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  if (!c->sorted)
+    if (int rc = sort_now(c, 1)) return rc;
+  CK(cudaMemsetAsync(c->pairs_n, 0, sizeof(unsigned long long), c->stream));
+  int rc = with_args(c, [&](auto& a) {
+    return launch_candidate_pairs(a, c->stream, system, include_obstacles, c->pairs, c->pairs_cap, c->pairs_n);
+  });
+  if (rc) return fail(c, rc, "candidate pair launch failed");
+  unsigned long long cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, c->pairs_n, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (cnt > (unsigned long long)c->pairs_cap) return fail(c, GRAINS_GPU_PAIR_OVERFLOW, "device pair buffer too small");
+  std::vector<int> h(2 * cnt);
+  if (cnt) CK(cudaMemcpy(h.data(), c->pairs, 2 * cnt * sizeof(int), cudaMemcpyDeviceToHost));
+  std::vector<std::pair<int, int>> pp, po;
+  for (size_t k = 0; k < cnt; ++k) {
+    // particle pairs were emitted as (lower, higher); obstacle pairs as (particle, obstacle id)
+    bool is_obs = false;
+    const SysHost& s = c->sys[system];
+    for (auto& o : s.obs)
+      if (o.id == h[2 * k + 1]) is_obs = true;
+    (is_obs ? po : pp).push_back(std::make_pair(h[2 * k], h[2 * k + 1]));
+  }
+  std::sort(pp.begin(), pp.end());
+  std::sort(po.begin(), po.end());
+  pp.insert(pp.end(), po.begin(), po.end());
+  *n = (int64_t)pp.size();
+  for (int64_t k = 0; k < (int64_t)pp.size() && k < cap; ++k) {
+    pairs[2 * k] = pp[k].first;
+    pairs[2 * k + 1] = pp[k].second;
+  }
+  return (int64_t)pp.size() > cap ? fail(c, GRAINS_GPU_PAIR_OVERFLOW, "pair buffer too small") : 0;
+}
+
+int grains_gpu_get_contact_pairs(grains_gpu_ctx* c, int32_t system, int64_t cap, int32_t* pairs, int64_t* n) {
+  if (!c || !n || (cap > 0 && !pairs)) return GRAINS_GPU_INVALID_ARGUMENT;
+  (void)system;
+  unsigned long long cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, c->pairs_n, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (cnt > (unsigned long long)c->pairs_cap) return fail(c, GRAINS_GPU_PAIR_OVERFLOW, "device pair buffer too small");
+  std::vector<int> h(2 * cnt);
+  if (cnt) CK(cudaMemcpy(h.data(), c->pairs, 2 * cnt * sizeof(int), cudaMemcpyDeviceToHost));
+  std::vector<std::pair<int, int>> pp;
+  for (size_t k = 0; k < cnt; ++k) pp.push_back(std::make_pair(h[2 * k], h[2 * k + 1]));
+  std::sort(pp.begin(), pp.end());
+  *n = (int64_t)pp.size();
+  for (int64_t k = 0; k < (int64_t)pp.size() && k < cap; ++k) {
+    pairs[2 * k] = pp[k].first;
+    pairs[2 * k + 1] = pp[k].second;
+  }
+  return (int64_t)pp.size() > cap ? fail(c, GRAINS_GPU_PAIR_OVERFLOW, "pair buffer too small") : 0;
+}
+
+int grains_gpu_get_stats(grains_gpu_ctx* c, grains_gpu_stats* st) {
+  if (!c || !st) return GRAINS_GPU_INVALID_ARGUMENT;
+  StatsDev d{};
+  CK(cudaMemcpyAsync(&d, c->stats, sizeof(d), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::memset(st, 0, sizeof(*st));
+  st->n_particles = c->n;
+  st->n_candidate_pairs = (int64_t)d.n_cand;
+  st->n_obstacle_candidates = (int64_t)d.n_obs_cand;
+  st->n_contacts = (int64_t)d.n_contacts;
+  st->n_obstacle_contacts = (int64_t)d.n_obs_contacts;
+  st->n_gjk_calls = (int64_t)d.n_gjk_calls;
+  st->n_gjk_iterations = (int64_t)d.n_gjk_iters;
+  double omax;
+  std::memcpy(&omax, &d.overlap_max_bits, sizeof(double));
+  st->overlap_max = omax;
+  st->overlap_sum = d.overlap_sum;
+  st->n_steps_done = c->steps_done;
+  st->status = d.status;
+  return 0;
+}
+
+int grains_gpu_reset_stats(grains_gpu_ctx* c) {
+  if (!c) return GRAINS_GPU_INVALID_ARGUMENT;
+  CK(cudaMemsetAsync(c->stats, 0, sizeof(StatsDev), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int grains_gpu_launches_per_step(grains_gpu_ctx* c, int64_t* launches) {
+  if (!c || !launches) return GRAINS_GPU_INVALID_ARGUMENT;
+  // kick_move, scan (3), scatter, cell_sort, gather, forces
+  *launches = 8;
+  return 0;
+}
+
+int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt, char* names,
+                               size_t cap, double* ms, int64_t* launches, int32_t max_kernels, int32_t* n_kernels) {
+  if (!c || !time || !names || !ms || !launches || !n_kernels || max_kernels < 3)
+    return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  if (!c->sorted)
+    if (int rc = sort_now(c, 1)) return rc;
+  cudaEvent_t ev[4];
+  for (auto& e : ev) CK(cudaEventCreate(&e));
+  double t_move = 0, t_sort = 0, t_force = 0;
+  for (int k = 0; k < n_steps; ++k) {
+    CK(cudaEventRecord(ev[0], c->stream));
+    int rc = with_args(c, [&](auto& a) {
+      return launch_kick_move(a, c->stream, c->pending_kick2 ? 1 : 0, 0.5 * dt, 1, 0.5 * dt, dt);
+    });
+    if (rc) return fail(c, rc, "kick/move launch failed");
+    c->keys_valid = true;
+    c->sorted = false;
+    CK(cudaEventRecord(ev[1], c->stream));
+    if ((rc = sort_now(c, 0))) return rc;
+    CK(cudaEventRecord(ev[2], c->stream));
+    if ((rc = forces_now(c, dt, 0))) return rc;
+    CK(cudaEventRecord(ev[3], c->stream));
+    c->pending_kick2 = true;
+    c->pending_dt = 0.5 * dt;
+    CK(cudaEventSynchronize(ev[3]));
+    float a = 0, b = 0, d = 0;
+    cudaEventElapsedTime(&a, ev[0], ev[1]);
+    cudaEventElapsedTime(&b, ev[1], ev[2]);
+    cudaEventElapsedTime(&d, ev[2], ev[3]);
+    t_move += a;
+    t_sort += b;
+    t_force += d;
+    *time += dt;
+  }
+  for (auto& e : ev) cudaEventDestroy(e);
+  c->steps_done += n_steps;
+  std::snprintf(names, cap, "kick_move\nsort_gather\nforces");
+  ms[0] = t_move;
+  ms[1] = t_sort;
+  ms[2] = t_force;
+  launches[0] = n_steps;
+  launches[1] = 6LL * n_steps;
+  launches[2] = n_steps;
+  *n_kernels = 3;
+  return finish_call(c);
+}
+
+int grains_gpu_shape_properties(int32_t type, const double* params, int32_t n, double* volume, double* circ,
+                                double inertia[3]) {
+  if (!params || !volume || !circ || !inertia) return GRAINS_GPU_INVALID_ARGUMENT;
+  ShapeHost s;
+  std::string err;
+  if (int rc = build_shape(type, params, n, s, err)) return rc;
+  *volume = s.volume;
+  *circ = s.circ;
+  for (int i = 0; i < 3; ++i) inertia[i] = s.inertia[i];
+  return 0;
+}
+
+}  // extern "C"
+
+namespace gg {
+int launches_per_fused_step() { return 8; }
+}  // namespace gg

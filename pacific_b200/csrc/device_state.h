@@ -1,0 +1,179 @@
+// device_state.h -- layout of the device-resident state of a context and the
+// launch interface between the C ABI (api.cu) and the per-precision kernel
+// translation units (kernels_fp64.cu, kernels_mixed.cu).
+//
+// HBM layout (N = particles of all systems, C = cells of all systems):
+//   particles are kept sorted by (global cell, id) and re-sorted after every
+//   move; two copies of every per-particle array alternate (cur / alt).
+//     xr     double4  (x, y, z, circumscribed radius)       32 B
+//     q      double4  quaternion (x, y, z, w)                32 B
+//     basis  double[9] rotation part of the transform       72 B (non-spheres only)
+//     v, w, wbf, F, T  R4 (R = float or double)            16/32 B each
+//     inertia R4 (Ixx, Iyy, Izz, 0)
+//     md     double4 (mass, crust, equivalent radius, 0)
+//     meta   int4    (id, material, shape, system)
+//     orig   int     upload index (history row, download order)
+//   cells: count[C], start[C+1] (exclusive scan), perm[N]
+//   contact memory: rows of H entries per particle, indexed by upload
+//     index, double buffered (prev -> next each force evaluation).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/grains_gpu.h"
+#include "common.cuh"
+#include "contact_law.cuh"
+
+namespace gg {
+
+template <typename R>
+struct Vec4;
+template <>
+struct Vec4<float> {
+  using type = float4;
+};
+template <>
+struct Vec4<double> {
+  using type = double4;
+};
+
+struct ShapeDev {
+  int type;
+  int nverts;
+  int vert_offset;  // into the vertex table
+  int pad;
+  double radius;       // sphere / cylinder radius
+  double half_height;  // cylinder
+  double ext[3];       // box half edges
+  double circ;         // circumscribed radius
+  double scaling_ext[3];  // local bounding-box half extents (RigidBodyWithCrust scaling)
+  double volume;
+};
+
+struct SysDev {
+  double ox, oy, oz;  // grid origin
+  double ex, ey, ez;  // cell edges
+  double gx, gy, gz;  // gravity
+  int nbi, nbj, nbk;
+  int cell_offset;
+  int law_offset;
+  int n_mat;
+  int obs_offset;  // first obstacle of the system in the obstacle table
+  int n_obs;
+  int moving_offset;  // first entry of the system in the moving-obstacle list
+  int n_moving;
+  int pad[2];
+};
+
+struct ObstacleDev {
+  double b[9];   // basis
+  double o[3];   // origin
+  double bbc[3], bbe[3];  // world AABB centre / half extent
+  double vel[3], omega[3];  // velocity of the obstacle centre, angular velocity
+  double rot_center[3];
+  double crust;
+  double circ;
+  double scaling[3];
+  int id;
+  int material;
+  int shape;
+  int moving;
+};
+
+template <typename R>
+struct HistEntry {
+  int other;  // neighbour id (particle) or obstacle table index (flags & 1)
+  int flags;
+  R kd[3];
+  R n[3];
+  R sp[3];
+};
+
+struct StatsDev {
+  unsigned long long n_cand;
+  unsigned long long n_obs_cand;
+  unsigned long long n_contacts;
+  unsigned long long n_obs_contacts;
+  unsigned long long n_gjk_calls;
+  unsigned long long n_gjk_iters;
+  unsigned long long overlap_max_bits;
+  double overlap_sum;
+  int status;
+  int pad;
+};
+
+template <typename R>
+struct ParticleArrays {
+  double4* xr;
+  double4* q;
+  double* basis;
+  typename Vec4<R>::type* v;
+  typename Vec4<R>::type* w;
+  typename Vec4<R>::type* wbf;
+  typename Vec4<R>::type* F;
+  typename Vec4<R>::type* T;
+  typename Vec4<R>::type* inertia;
+  double4* md;
+  int4* meta;
+  int* orig;
+};
+
+template <typename R>
+struct StepArgs {
+  int n;                 // particles
+  int n_cells;           // total cells
+  int n_sys;
+  int hist_cap;          // H
+  int has_basis;         // non-spherical particles present
+  const SysDev* sys;
+  const ShapeDev* shapes;
+  const double* verts;   // polyhedron vertices (xyz)
+  const ObstacleDev* obs;
+  const int* cell_obs_start;  // static obstacle CSR per cell (C+1)
+  const int* cell_obs_idx;
+  const int* moving_idx;
+  const LawParams<R>* laws;
+  ParticleArrays<R> cur;
+  ParticleArrays<R> alt;
+  int* coord;            // coordination number (sorted order)
+  unsigned* key;
+  unsigned* rank;
+  int* cell_count;
+  int* cell_start;
+  int* block_sums;
+  int* perm;
+  HistEntry<R>* hist_prev;
+  int* hist_n_prev;
+  HistEntry<R>* hist_next;
+  int* hist_n_next;
+  StatsDev* stats;
+  int* pairs;            // diagnostic contact pair output (2 ints per pair) or null
+  int pairs_cap;
+  unsigned long long* pairs_n;
+  double gjk_tol;
+};
+
+// kernel launchers, instantiated for float and double
+template <typename R>
+int launch_kick_move(const StepArgs<R>& a, cudaStream_t s, int do_kick2, double dt_kick2, int do_move,
+                     double dt_v, double dt_x);
+template <typename R>
+int launch_bin(const StepArgs<R>& a, cudaStream_t s);
+template <typename R>
+int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forces);
+template <typename R>
+int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag);
+template <typename R>
+int launch_zero_kdelta(const StepArgs<R>& a, cudaStream_t s);
+// stage: 13 doubles per particle in upload order (position 3, quaternion 4,
+// velocity 3, omega 3) and optionally 9 basis doubles per particle
+template <typename R>
+int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const double* stage, const double* stage_basis);
+template <typename R>
+int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int include_obstacles, int* out,
+                           int cap, unsigned long long* count);
+// number of kernel launches issued by one fused step
+int launches_per_fused_step();
+
+}  // namespace gg

@@ -1,0 +1,362 @@
+// gjk.cuh -- closest points of two convex bodies with crust by the Johnson
+// GJK distance algorithm (van den Bergen, "A fast and robust GJK
+// implementation for collision detection of convex objects", J. Graphics
+// Tools 4(2), 1999: Johnson's sub-algorithm with cached sub-determinants and
+// the backup procedure).  Behaviour follows the reference's closest_points
+// (Geometry/src/Convex.cpp:536-627): same start point, same termination tests
+// (relative / absolute optimality gap, degenerate support point, full simplex,
+// distance <= EPSILON2, 1000 iterations) so that iteration counts and witness
+// points match.
+//
+// Support functions: Sphere.cpp:99-109, Box.cpp:307-316, Cylinder.cpp:112-133
+// (axis = local Y), Polyhedron.cpp:265-293.  The polyhedron support here is a
+// stateless arg-max over the vertices (first maximum wins); the reference's
+// warm-started hill climb returns the same vertex except on exact ties.
+//
+// Precision: the iteration runs in T.  With T = float the two bodies are
+// expressed relative to body A's origin (the translation difference is formed
+// in double) so that FP32 keeps the body-size scale; contact decisions near
+// the crust threshold are re-checked by a double run (guard band).
+#pragma once
+
+#include "common.cuh"
+#include "device_state.h"
+#include "sphere_contact.cuh"
+
+namespace gg {
+
+struct BodyRef {
+  int type;
+  int nverts;
+  const double* verts;
+  double radius;       // sphere radius / circumscribed radius
+  double cyl_r, cyl_hh;
+  D3 ext;              // box half edges
+  double crust;
+  M3 basis;            // rotation part
+  D3 origin;
+  double scaling[3];   // crust shrink factors (RigidBodyWithCrust.cpp:60-72)
+  double lext[3];      // local bounding-box half extents (Convex::bbox with identity)
+};
+
+template <typename T>
+struct LocalBody {
+  int type;
+  int nverts;
+  const double* verts;
+  T radius, cyl_r, cyl_hh;
+  V3<T> ext;
+  T b[9];   // shrunk basis
+  V3<T> o;  // origin in the working frame
+};
+
+template <typename T>
+GG_HD V3<T> support_local(const LocalBody<T>& B, V3<T> v) {
+  switch (B.type) {
+    case 0: {  // sphere
+      T s = norm(v);
+      if (s > T(kEpsilon)) {
+        T r = B.radius / s;
+        return v3<T>(v.x * r, v.y * r, v.z * r);
+      }
+      return v3<T>(T(0), T(0), T(0));
+    }
+    case 1: {  // box
+      T n = norm(v);
+      if (n < T(kEpsilon)) return v3<T>(T(0), T(0), T(0));
+      return v3<T>(v.x < T(0) ? -B.ext.x : B.ext.x, v.y < T(0) ? -B.ext.y : B.ext.y,
+                   v.z < T(0) ? -B.ext.z : B.ext.z);
+    }
+    case 2: {  // cylinder, axis local Y
+      T n = norm(v);
+      if (n > T(kEpsilon)) {
+        T s = std::sqrt(v.x * v.x + v.z * v.z);
+        if (s > T(kEpsilon)) {
+          T d = B.cyl_r / s;
+          if (std::fabs(v.y) < T(kEpsilon)) return v3<T>(v.x * d, T(0), v.z * d);
+          return v3<T>(v.x * d, v.y < T(0) ? -B.cyl_hh : B.cyl_hh, v.z * d);
+        }
+        return v3<T>(T(0), v.y < T(0) ? -B.cyl_hh : B.cyl_hh, T(0));
+      }
+      return v3<T>(T(0), T(0), T(0));
+    }
+    default: {  // polyhedron
+      T n = norm(v);
+      if (!(n > T(kEpsilon))) return v3<T>(T(0), T(0), T(0));
+      int best = 0;
+      V3<T> p0 = v3<T>(T(B.verts[0]), T(B.verts[1]), T(B.verts[2]));
+      T h = dot(p0, v);
+      for (int i = 1; i < B.nverts; ++i) {
+        V3<T> p = v3<T>(T(B.verts[3 * i]), T(B.verts[3 * i + 1]), T(B.verts[3 * i + 2]));
+        T d = dot(p, v);
+        if (d > h) {
+          h = d;
+          best = i;
+        }
+      }
+      return v3<T>(T(B.verts[3 * best]), T(B.verts[3 * best + 1]), T(B.verts[3 * best + 2]));
+    }
+  }
+}
+
+template <typename T>
+GG_HD V3<T> lb_apply(const LocalBody<T>& B, V3<T> p) {
+  return v3<T>(B.b[0] * p.x + B.b[1] * p.y + B.b[2] * p.z + B.o.x,
+               B.b[3] * p.x + B.b[4] * p.y + B.b[5] * p.z + B.o.y,
+               B.b[6] * p.x + B.b[7] * p.y + B.b[8] * p.z + B.o.z);
+}
+template <typename T>
+GG_HD V3<T> lb_vecmat(V3<T> v, const LocalBody<T>& B) {  // v * basis
+  return v3<T>(B.b[0] * v.x + B.b[3] * v.y + B.b[6] * v.z, B.b[1] * v.x + B.b[4] * v.y + B.b[7] * v.z,
+               B.b[2] * v.x + B.b[5] * v.y + B.b[8] * v.z);
+}
+
+// Builds the working-frame body (crust-shrunk basis, origin relative to 'shift')
+template <typename T>
+GG_HD LocalBody<T> local_body(const BodyRef& r, D3 shift, const double scale[3]) {
+  LocalBody<T> B;
+  B.type = r.type;
+  B.nverts = r.nverts;
+  B.verts = r.verts;
+  B.radius = T(r.radius);
+  B.cyl_r = T(r.cyl_r);
+  B.cyl_hh = T(r.cyl_hh);
+  B.ext = v3<T>(T(r.ext.x), T(r.ext.y), T(r.ext.z));
+  M3 s = mscale_cols(r.basis, scale[0], scale[1], scale[2]);
+  for (int i = 0; i < 9; ++i) B.b[i] = T(s.m[i]);
+  D3 o = xsub3(r.origin, shift);
+  B.o = v3<T>(T(o.x), T(o.y), T(o.z));
+  return B;
+}
+
+template <typename T>
+struct GjkState {
+  T det[16][4];
+  T dp[4][4];
+};
+
+template <typename T>
+GG_HD void gjk_det(unsigned bits, unsigned last, unsigned last_bit, unsigned all_bits, const V3<T> y[4],
+                   GjkState<T>& g) {
+  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+    if (bits & bit) g.dp[i][last] = g.dp[last][i] = dot(y[i], y[last]);
+  g.dp[last][last] = dot(y[last], y[last]);
+  g.det[last_bit][last] = T(1);
+  for (unsigned j = 0, sj = 1; j < 4; ++j, sj <<= 1) {
+    if (!(bits & sj)) continue;
+    unsigned s2 = sj | last_bit;
+    g.det[s2][j] = g.dp[last][last] - g.dp[last][j];
+    g.det[s2][last] = g.dp[j][j] - g.dp[j][last];
+    for (unsigned k = 0, sk = 1; k < j; ++k, sk <<= 1) {
+      if (!(bits & sk)) continue;
+      unsigned s3 = sk | s2;
+      g.det[s3][k] = g.det[s2][j] * (g.dp[j][j] - g.dp[j][k]) + g.det[s2][last] * (g.dp[last][j] - g.dp[last][k]);
+      g.det[s3][j] = g.det[sk | last_bit][k] * (g.dp[k][k] - g.dp[k][j]) +
+                     g.det[sk | last_bit][last] * (g.dp[last][k] - g.dp[last][j]);
+      g.det[s3][last] = g.det[sk | sj][k] * (g.dp[k][k] - g.dp[k][last]) +
+                        g.det[sk | sj][j] * (g.dp[j][k] - g.dp[j][last]);
+    }
+  }
+  if (all_bits == 15) {
+    g.det[15][0] = g.det[14][1] * (g.dp[1][1] - g.dp[1][0]) + g.det[14][2] * (g.dp[2][1] - g.dp[2][0]) +
+                   g.det[14][3] * (g.dp[3][1] - g.dp[3][0]);
+    g.det[15][1] = g.det[13][0] * (g.dp[0][0] - g.dp[0][1]) + g.det[13][2] * (g.dp[2][0] - g.dp[2][1]) +
+                   g.det[13][3] * (g.dp[3][0] - g.dp[3][1]);
+    g.det[15][2] = g.det[11][0] * (g.dp[0][0] - g.dp[0][2]) + g.det[11][1] * (g.dp[1][0] - g.dp[1][2]) +
+                   g.det[11][3] * (g.dp[3][0] - g.dp[3][2]);
+    g.det[15][3] = g.det[7][0] * (g.dp[0][0] - g.dp[0][3]) + g.det[7][1] * (g.dp[1][0] - g.dp[1][3]) +
+                   g.det[7][2] * (g.dp[2][0] - g.dp[2][3]);
+  }
+}
+
+template <typename T>
+GG_HD bool gjk_valid(unsigned s, unsigned all_bits, const GjkState<T>& g) {
+  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1) {
+    if (!(all_bits & bit)) continue;
+    if (s & bit) {
+      if (g.det[s][i] <= T(kEpsilon3)) return false;
+    } else if (g.det[s | bit][i] > T(0)) {
+      return false;
+    }
+  }
+  return true;
+}
+
+template <typename T>
+GG_HD V3<T> gjk_vector(unsigned bits, const V3<T> y[4], const GjkState<T>& g) {
+  T sum = T(0);
+  V3<T> v = v3<T>(T(0), T(0), T(0));
+  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+    if (bits & bit) {
+      sum += g.det[bits][i];
+      v = v + sc(y[i], g.det[bits][i]);
+    }
+  return sc(v, T(1) / sum);
+}
+
+template <typename T>
+GG_HD bool gjk_proper(unsigned s, const GjkState<T>& g) {
+  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+    if ((s & bit) && g.det[s][i] <= T(kEpsilon3)) return false;
+  return true;
+}
+
+template <typename T>
+GG_HD bool gjk_closest(unsigned& bits, unsigned last, unsigned last_bit, unsigned all_bits, const V3<T> y[4],
+                       GjkState<T>& g, V3<T>& v) {
+  gjk_det(bits, last, last_bit, all_bits, y, g);
+  for (unsigned s = bits; s; --s) {
+    if ((s & bits) == s && gjk_valid(s | last_bit, all_bits, g)) {
+      bits = s | last_bit;
+      v = gjk_vector(bits, y, g);
+      return true;
+    }
+  }
+  if (gjk_valid(last_bit, all_bits, g)) {
+    bits = last_bit;
+    v = y[last];
+    return true;
+  }
+  T best = T(INFINITY);
+  for (unsigned s = all_bits; s; --s) {  // backup procedure
+    if ((s & all_bits) == s && gjk_proper(s, g)) {
+      V3<T> u = gjk_vector(s, y, g);
+      T d2 = norm2(u);
+      if (d2 < best) {
+        best = d2;
+        bits = s;
+        v = u;
+      }
+    }
+  }
+  return false;
+}
+
+template <typename T>
+struct GjkResult {
+  T dist;
+  V3<T> pa, pb;  // witness points in the working frame
+  int iters;
+};
+
+template <typename T>
+GG_HD GjkResult<T> gjk_distance(const LocalBody<T>& A, const LocalBody<T>& B, T rel_error) {
+  unsigned bits = 0, last = 0, last_bit = 0, all_bits = 0;
+  V3<T> p[4], q[4], y[4];
+  GjkState<T> g;
+  for (int i = 0; i < 4; ++i) {
+    p[i] = q[i] = y[i] = v3<T>(T(0), T(0), T(0));
+    for (int j = 0; j < 4; ++j) g.dp[i][j] = T(0);
+  }
+  for (int i = 0; i < 16; ++i)
+    for (int j = 0; j < 4; ++j) g.det[i][j] = T(0);
+  const T abs_error = T(1.e-4) * rel_error;
+  const V3<T> zero = v3<T>(T(0), T(0), T(0));
+  V3<T> v = lb_apply(A, support_local(A, zero)) - lb_apply(B, support_local(B, zero));
+  V3<T> w = v;
+  T dist = norm(v);
+  int num = 0;
+  while (bits < 15 && dist > T(kEpsilon2) && num < 1000) {
+    ++num;
+    last = 0;
+    last_bit = 1;
+    while (bits & last_bit) {
+      ++last;
+      last_bit <<= 1;
+    }
+    p[last] = support_local(A, lb_vecmat(-v, A));
+    q[last] = support_local(B, lb_vecmat(v, B));
+    w = lb_apply(A, p[last]) - lb_apply(B, q[last]);
+    T mu = dist - dot(v, w) / dist;
+    if (mu < dist * rel_error || mu < abs_error) break;
+    bool degen = false;
+    for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+      if ((all_bits & bit) && y[i].x == w.x && y[i].y == w.y && y[i].z == w.z) degen = true;
+    if (degen) break;
+    y[last] = w;
+    all_bits = bits | last_bit;
+    if (!gjk_closest(bits, last, last_bit, all_bits, y, g, v)) break;
+    dist = norm(v);
+  }
+  GjkResult<T> r;
+  T sum = T(0);
+  V3<T> pa = zero, pb = zero;
+  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+    if (bits & bit) {
+      sum += g.det[bits][i];
+      pa = pa + sc(p[i], g.det[bits][i]);
+      pb = pb + sc(q[i], g.det[bits][i]);
+    }
+  T s = T(1) / sum;
+  r.pa = lb_apply(A, sc(pa, s));
+  r.pb = lb_apply(B, sc(pb, s));
+  r.dist = dist;
+  r.iters = num;
+  return r;
+}
+
+// RigidBodyWithCrust::ClosestPoint general case (RigidBodyWithCrust.cpp:278-348).
+// status: 0 = features valid, 1 = ContactError, 2 = bounding spheres apart.
+template <typename T>
+GG_HD ContactGeom convex_closest_point_t(const BodyRef& A, const BodyRef& B, double tol, int* iters) {
+  ContactGeom c = no_contact();
+  D3 g = xsub3(A.origin, B.origin);
+  if (!(xnorm(g) < xadd(A.radius, B.radius))) {
+    c.status = 2;
+    return c;
+  }
+  const D3 shift = sizeof(T) == 4 ? A.origin : d3(0., 0., 0.);
+  LocalBody<T> la = local_body<T>(A, shift, A.scaling);
+  LocalBody<T> lb = local_body<T>(B, shift, B.scaling);
+  GjkResult<T> r = gjk_distance(la, lb, T(tol));
+  *iters = r.iters;
+  double distance = double(r.dist);
+  if (distance < kEpsilon) {
+    c.status = 1;
+    return c;
+  }
+  V3<T> ba = r.pa - r.pb;
+  V3<T> pc = dv(r.pa, T(2)) + dv(r.pb, T(2));
+  double crust_sum = xadd(A.crust, B.crust);
+  V3<T> ov = round3(dv(ba, r.dist));
+  ov = sc(ov, T(crust_sum) - r.dist);
+  c.point = xadd3(d3(double(pc.x), double(pc.y), double(pc.z)), shift);
+  c.overlap_vector = d3(double(ov.x), double(ov.y), double(ov.z));
+  c.overlap = distance - crust_sum;
+  c.status = 0;
+  return c;
+}
+
+// RigidBodyWithCrust::ClosestPoint_ErreurHandling (RigidBodyWithCrust.cpp:532-588):
+// bodies shrunk by 'factor' crusts (scaling capped below at 0.5); the contact
+// is imposed with overlap = -(crust sum) along the witness direction B->A.
+// status 1 when even the shrunk bodies touch (fatal ContactError).
+GG_HD ContactGeom convex_error_handling(const BodyRef& A, const BodyRef& B, const double ext_a[3],
+                                        const double ext_b[3], double factor, double tol) {
+  double sa[3], sb[3];
+  for (int i = 0; i < 3; ++i) {
+    sa[i] = ext_a[i] < kEpsilon ? 1. : xdiv(xsub(ext_a[i], xmul(factor, A.crust)), ext_a[i]);
+    sb[i] = ext_b[i] < kEpsilon ? 1. : xdiv(xsub(ext_b[i], xmul(factor, B.crust)), ext_b[i]);
+    sa[i] = fmax(sa[i], 0.5);
+    sb[i] = fmax(sb[i], 0.5);
+  }
+  LocalBody<double> la = local_body<double>(A, d3(0., 0., 0.), sa);
+  LocalBody<double> lb = local_body<double>(B, d3(0., 0., 0.), sb);
+  GjkResult<double> r = gjk_distance(la, lb, tol);
+  ContactGeom c = no_contact();
+  if (r.dist < kEpsilon) {
+    c.status = 1;
+    return c;
+  }
+  V3<double> ba = r.pa - r.pb;
+  ba = dv(ba, norm(ba));
+  V3<double> pc = dv(r.pa, 2.0) + dv(r.pb, 2.0);
+  double imp = 1. * xadd(A.crust, B.crust);
+  c.point = d3(pc.x, pc.y, pc.z);
+  c.overlap_vector = d3(ba.x * imp, ba.y * imp, ba.z * imp);
+  c.overlap = -imp;
+  c.status = 0;
+  return c;
+}
+
+}  // namespace gg

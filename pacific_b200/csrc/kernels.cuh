@@ -1,0 +1,861 @@
+// kernels.cuh -- sm_100a kernels of the Grains3D DEM time step, templated on
+// the arithmetic type R of velocities, forces, the contact law and the
+// contact memory (float: mixed precision, double: plain FP64).  Positions,
+// quaternions, bases and every contact decision are double in both.
+//
+// One DEM step (KDK leapfrog, Grains.cpp:344-364) is:
+//   kick_move      second half kick of the previous step (when pending),
+//                  first half kick + drift + rotation (SecondOrderLeapFrog),
+//                  new cell key and in-cell arrival rank (atomic)
+//   scan x3        exclusive scan of the per-cell counts -> cell ranges
+//   scatter        slot = start[cell] + rank
+//   cell_sort      each cell's particles ordered by id (deterministic order)
+//   gather         every per-particle array permuted into the new order
+//   forces         broadphase over the 27 surrounding cells, sphere/box
+//                  narrowphase, contact law + memory, per-particle sums,
+//                  static and moving obstacles
+// The second half kick of the last step is flushed by kick_move with
+// do_move = 0.
+#pragma once
+
+#include "common.cuh"
+#include "contact_law.cuh"
+#include "device_state.h"
+#include "sphere_contact.cuh"
+#include "gjk.cuh"
+
+namespace gg {
+
+template <typename R>
+using R4 = typename Vec4<R>::type;
+
+template <typename R>
+__device__ __forceinline__ V3<R> ld3(const R4<R>& a) {
+  return v3<R>(a.x, a.y, a.z);
+}
+template <typename R>
+__device__ __forceinline__ R4<R> st3(V3<R> a, R wv = R(0)) {
+  R4<R> r;
+  r.x = a.x;
+  r.y = a.y;
+  r.z = a.z;
+  r.w = wv;
+  return r;
+}
+
+__device__ __forceinline__ void set_status(StatsDev* st, int bits) { atomicOr(&st->status, bits); }
+
+// Cell::GetCell (Base/src/Cell.cpp:172-184) + LinkedCell::getCell validity
+__device__ __forceinline__ bool cell_of(const SysDev& S, double x, double y, double z, int& i, int& j, int& k) {
+  i = int(floor(xdiv(xsub(x, S.ox), S.ex)));
+  j = int(floor(xdiv(xsub(y, S.oy), S.ey)));
+  k = int(floor(xdiv(xsub(z, S.oz), S.ez)));
+  bool ok = -1 < i && i < S.nbi && -1 < j && j < S.nbj && -1 < k && k < S.nbk;
+  if (!ok) {
+    i = min(max(i, 0), S.nbi - 1);
+    j = min(max(j, 0), S.nbj - 1);
+    k = min(max(k, 0), S.nbk - 1);
+  }
+  return ok;
+}
+// LinkedCell::getCellNumber (LinkedCell.cpp:1165-1168) + system offset
+__device__ __forceinline__ int cell_index(const SysDev& S, int i, int j, int k) {
+  return S.cell_offset + j * S.nbk * S.nbi + k * S.nbi + i;
+}
+
+// ---------------------------------------------------------------------------
+// Angular acceleration in the body frame (ParticleKinematicsSphere.cpp:47-54,
+// ParticleKinematics3D.cpp:56-75 with predictor mode on, Grains.cpp:18)
+template <typename R>
+__device__ __forceinline__ V3<R> dwdt(bool sphere, V3<R> I, V3<R> Tbf, V3<R> om) {
+  if (sphere) return v3<R>(Tbf.x / (R(1) * I.x), Tbf.y / (R(1) * I.y), Tbf.z / (R(1) * I.z));
+  return v3<R>(Tbf.x / (R(1) * I.x) + om.y * om.z * (I.y - I.z) / I.x,
+               Tbf.y / (R(1) * I.y) + om.z * om.x * (I.z - I.x) / I.y,
+               Tbf.z / (R(1) * I.z) + om.x * om.y * (I.x - I.y) / I.z);
+}
+// SSP-RK3 of SecondOrderLeapFrog::Move / advanceVelocity (SecondOrderLeapFrog.cpp:55-68)
+template <typename R>
+__device__ __forceinline__ V3<R> rk3(bool sphere, V3<R> I, V3<R> Tbf, V3<R> wbf, R dt) {
+  V3<R> K1 = sc(dwdt(sphere, I, Tbf, wbf), dt);
+  V3<R> K2 = sc(dwdt(sphere, I, Tbf, wbf + K1), dt);
+  V3<R> K3 = sc(dwdt(sphere, I, Tbf, wbf + sc(K1 + K2, R(0.25))), dt);
+  return wbf + dv((K1 + K2) + sc(K3, R(4)), R(6));
+}
+
+// ---------------------------------------------------------------------------
+// kick_move: optional pending second half kick, then ParticleKinematics::Move
+// (ParticleKinematics.cpp:62-105) and the cell key of the new position.
+template <typename R>
+__global__ void __launch_bounds__(256) kick_move_kernel(StepArgs<R> a, int do_kick2, R dt_kick2, int do_move,
+                                                        R dt_v, double dt_x) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const ParticleArrays<R>& P = a.cur;
+  double4 xr = P.xr[s];
+  double4 qd = P.q[s];
+  int4 meta = P.meta[s];
+  double4 md = P.md[s];
+  V3<R> F = ld3<R>(P.F[s]), T = ld3<R>(P.T[s]);
+  V3<R> v = ld3<R>(P.v[s]), w = ld3<R>(P.w[s]), wbf = ld3<R>(P.wbf[s]);
+  V3<R> I = ld3<R>(P.inertia[s]);
+  const bool sphere = a.shapes[meta.z].type == 0;
+  const R mass = R(md.x);
+  Qt<double> q{v3<double>(qd.x, qd.y, qd.z), qd.w};
+  Qt<R> qr{v3<R>(R(qd.x), R(qd.y), R(qd.z)), R(qd.w)};
+  if (do_kick2) {  // SecondOrderLeapFrog::advanceVelocity (SecondOrderLeapFrog.cpp:74-95)
+    V3<R> Tbf = q_to_body(qr, T);
+    v = v + sc(dv(F, mass * R(1)), dt_kick2);
+    wbf = rk3(sphere, I, Tbf, wbf, dt_kick2);
+    w = q_to_world(qr, wbf);
+  }
+  if (do_move) {
+    V3<R> Tbf = q_to_body(qr, T);
+    v = v + sc(dv(F, mass * R(1)), dt_v);
+    V3<double> tm = sc(v3<double>(double(v.x), double(v.y), double(v.z)), dt_x);
+    wbf = rk3(sphere, I, Tbf, wbf, dt_v);
+    w = q_to_world(qr, wbf);
+    V3<R> meanw = w;
+    xr.x = xr.x + tm.x;
+    xr.y = xr.y + tm.y;
+    xr.z = xr.z + tm.z;
+    V3<double> mw = v3<double>(double(meanw.x), double(meanw.y), double(meanw.z));
+    double nom = norm(mw);
+    Qt<double> dq{v3<double>(0., 0., 0.), 1.};
+    if (nom > kEpsilon) {
+      double c = cos(nom * dt_x / 2.), sn = sin(nom * dt_x / 2.);
+      dq = Qt<double>{sc(mw, sn * 1. / nom), c};
+    }
+    q = qmul(dq, q);
+    if (a.has_basis && !sphere) {
+      M3 b;
+      for (int t = 0; t < 9; ++t) b.m[t] = P.basis[9 * (size_t)s + t];
+      mrotate_left(b, dq);
+      for (int t = 0; t < 9; ++t) P.basis[9 * (size_t)s + t] = b.m[t];
+    }
+    if (norm(tm) > md.y) set_status(a.stats, GRAINS_GPU_MOTION_ERROR);
+    P.xr[s] = xr;
+    P.q[s] = make_double4(q.v.x, q.v.y, q.v.z, q.w);
+    // new cell key and arrival rank
+    const SysDev& S = a.sys[meta.w];
+    int ci, cj, ck;
+    if (!cell_of(S, xr.x, xr.y, xr.z, ci, cj, ck)) set_status(a.stats, GRAINS_GPU_OUT_OF_GRID);
+    unsigned key = (unsigned)cell_index(S, ci, cj, ck);
+    a.key[s] = key;
+    a.rank[s] = (unsigned)atomicAdd(&a.cell_count[key], 1);
+  }
+  P.v[s] = st3<R>(v);
+  P.w[s] = st3<R>(w);
+  P.wbf[s] = st3<R>(wbf);
+}
+
+// bin: cell keys of the current positions (after an upload)
+template <typename R>
+__global__ void bin_kernel(StepArgs<R> a) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  double4 xr = a.cur.xr[s];
+  int4 meta = a.cur.meta[s];
+  const SysDev& S = a.sys[meta.w];
+  int ci, cj, ck;
+  if (!cell_of(S, xr.x, xr.y, xr.z, ci, cj, ck)) set_status(a.stats, GRAINS_GPU_OUT_OF_GRID);
+  unsigned key = (unsigned)cell_index(S, ci, cj, ck);
+  a.key[s] = key;
+  a.rank[s] = (unsigned)atomicAdd(&a.cell_count[key], 1);
+}
+
+// ---------------------------------------------------------------------------
+// exclusive scan of cell counts: 1024 threads x 4 items per block
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
+  __shared__ int warp_sums[32];
+  int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[wid] = x;
+  __syncthreads();
+  if (wid == 0) {
+    int nw = blockDim.x >> 5;
+    int ws = lane < nw ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, ws, o);
+      if (lane >= o) ws += y;
+    }
+    if (lane < nw) warp_sums[lane] = ws;
+  }
+  __syncthreads();
+  int base = wid > 0 ? warp_sums[wid - 1] : 0;
+  *total = warp_sums[(blockDim.x >> 5) - 1];
+  __syncthreads();
+  return base + x - v;
+}
+
+static __global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(const int* in, int* out, int* block_sums, int n) {
+  int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+  int vals[kScanItems];
+  int sum = 0;
+#pragma unroll
+  for (int t = 0; t < kScanItems; ++t) {
+    vals[t] = (base + t < n) ? in[base + t] : 0;
+    sum += vals[t];
+  }
+  int total;
+  int pre = block_exclusive_scan(sum, &total);
+#pragma unroll
+  for (int t = 0; t < kScanItems; ++t) {
+    if (base + t < n) out[base + t] = pre;
+    pre += vals[t];
+  }
+  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+}
+
+static __global__ void __launch_bounds__(kScanThreads) scan_block_sums_kernel(int* block_sums, int nb, int* out, int n) {
+  // single block: exclusive scan of up to kScanTile block sums
+  int base = threadIdx.x * kScanItems;
+  int vals[kScanItems];
+  int sum = 0;
+#pragma unroll
+  for (int t = 0; t < kScanItems; ++t) {
+    vals[t] = (base + t < nb) ? block_sums[base + t] : 0;
+    sum += vals[t];
+  }
+  int total;
+  int pre = block_exclusive_scan(sum, &total);
+#pragma unroll
+  for (int t = 0; t < kScanItems; ++t) {
+    if (base + t < nb) block_sums[base + t] = pre;
+    pre += vals[t];
+  }
+  if (threadIdx.x == 0) out[n] = total;
+}
+
+static __global__ void scan_add_kernel(int* out, const int* block_sums, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] += block_sums[i / kScanTile];
+}
+
+template <typename R>
+__global__ void scatter_kernel(StepArgs<R> a) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  a.perm[a.cell_start[a.key[s]] + a.rank[s]] = s;
+}
+
+// order each cell's slots by particle id; resets the count for the next step
+template <typename R>
+__global__ void cell_sort_kernel(StepArgs<R> a) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= a.n_cells) return;
+  int b = a.cell_start[c], e = a.cell_start[c + 1];
+  a.cell_count[c] = 0;
+  for (int i = b + 1; i < e; ++i) {
+    int pi = a.perm[i];
+    int idi = a.cur.meta[pi].x;
+    int j = i - 1;
+    while (j >= b && a.cur.meta[a.perm[j]].x > idi) {
+      a.perm[j + 1] = a.perm[j];
+      --j;
+    }
+    a.perm[j + 1] = pi;
+  }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) gather_kernel(StepArgs<R> a, int gather_forces) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= a.n) return;
+  int s = a.perm[t];
+  const ParticleArrays<R>& C = a.cur;
+  const ParticleArrays<R>& D = a.alt;
+  D.xr[t] = C.xr[s];
+  D.q[t] = C.q[s];
+  D.v[t] = C.v[s];
+  D.w[t] = C.w[s];
+  D.wbf[t] = C.wbf[s];
+  D.inertia[t] = C.inertia[s];
+  D.md[t] = C.md[s];
+  D.meta[t] = C.meta[s];
+  D.orig[t] = C.orig[s];
+  if (gather_forces) {
+    D.F[t] = C.F[s];
+    D.T[t] = C.T[s];
+  }
+  if (a.has_basis) {
+    for (int k = 0; k < 9; ++k) D.basis[9 * (size_t)t + k] = C.basis[9 * (size_t)s + k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// contact memory lookup in the owner's row of the previous step
+template <typename R>
+__device__ __forceinline__ bool find_memory(const StepArgs<R>& a, int row, int other, int flags,
+                                            PairMemory<R>& m) {
+  const HistEntry<R>* h = a.hist_prev + (size_t)row * a.hist_cap;
+  int n = a.hist_n_prev[row];
+  for (int k = 0; k < n; ++k) {
+    HistEntry<R> e = h[k];
+    if (e.other == other && e.flags == flags) {
+      m.kdelta = v3<R>(e.kd[0], e.kd[1], e.kd[2]);
+      m.prev_normal = v3<R>(e.n[0], e.n[1], e.n[2]);
+      m.spring = v3<R>(e.sp[0], e.sp[1], e.sp[2]);
+      return true;
+    }
+  }
+  return false;
+}
+
+template <typename R>
+__device__ __forceinline__ void store_memory(const StepArgs<R>& a, int row, int& cnt, int other, int flags,
+                                             const PairMemory<R>& m) {
+  if (cnt >= a.hist_cap) {
+    set_status(a.stats, GRAINS_GPU_HISTORY_FULL);
+    return;
+  }
+  HistEntry<R> e;
+  e.other = other;
+  e.flags = flags;
+  e.kd[0] = m.kdelta.x; e.kd[1] = m.kdelta.y; e.kd[2] = m.kdelta.z;
+  e.n[0] = m.prev_normal.x; e.n[1] = m.prev_normal.y; e.n[2] = m.prev_normal.z;
+  e.sp[0] = m.spring.x; e.sp[1] = m.spring.y; e.sp[2] = m.spring.z;
+  a.hist_next[(size_t)row * a.hist_cap + cnt] = e;
+  ++cnt;
+}
+
+__device__ __forceinline__ void atomic_max_pos_double(unsigned long long* addr, double v) {
+  atomicMax(addr, (unsigned long long)__double_as_longlong(v));
+}
+
+// Applies the contact law for the pair (p0, p1) seen from p0 and returns the
+// force on p0 and the rolling torque on p0.
+template <typename R>
+__device__ __forceinline__ LawResult<R> pair_law(const StepArgs<R>& a, const LawParams<R>& L, R dt,
+                                                 const ContactGeom& g, const BodyAtContact<R>& b0,
+                                                 const BodyAtContact<R>& b1, bool existed, PairMemory<R>& mem) {
+  V3<R> pen = from_d3<R>(g.overlap_vector);
+  if (L.type == GRAINS_GPU_HOOKE_MEMORY) return hooke_memory(L, dt, pen, b0, b1, existed, mem);
+  return hooke(L, pen, b0, b1);
+}
+
+// Contact with a pair error: RigidBodyWithCrust::ClosestPoint_ErreurHandling
+// (RigidBodyWithCrust.cpp:532-588) for two spheres, whose crust-x10 shrunk
+// bodies are spheres of radius r * max((r - 10 crust) / r, 0.5): the contact
+// is imposed with an overlap equal to minus the crust sum along B->A.
+__device__ __forceinline__ ContactGeom sphere_sphere_error_handling(D3 A, double ra, double ca, D3 B, double rb,
+                                                                    double cb, bool& fatal) {
+  double sa = fmax(xdiv(xsub(ra, xmul(10., ca)), ra), 0.5);
+  double sb = fmax(xdiv(xsub(rb, xmul(10., cb)), rb), 0.5);
+  D3 ab = xsub3(B, A);
+  double nab = xnorm(ab);
+  double ras = xmul(ra, sa), rbs = xmul(rb, sb);
+  double dist = xsub(nab, xadd(ras, rbs));
+  ContactGeom g;
+  fatal = dist < kEpsilon;
+  D3 u = xdivs(ab, nab);
+  D3 pa = xadd3(A, xscale(u, ras));
+  D3 pb = xsub3(B, xscale(u, rbs));
+  g.point = xadd3(xdivs(pa, 2.0), xdivs(pb, 2.0));
+  double imp = xmul(1., xadd(ca, cb));
+  g.overlap_vector = xscale(d3(-u.x, -u.y, -u.z), imp);
+  g.overlap = -imp;
+  g.status = 0;
+  return g;
+}
+
+
+// ---------------------------------------------------------------------------
+// general convex narrowphase glue
+template <typename R>
+__device__ __forceinline__ void make_body_ref(const StepArgs<R>& a, int shape, int slot, double crust, BodyRef& b) {
+  const ShapeDev& sh = a.shapes[shape];
+  const double4 xr = a.cur.xr[slot];
+  b.type = sh.type;
+  b.nverts = sh.nverts;
+  b.verts = a.verts + 3 * sh.vert_offset;
+  b.radius = xr.w;
+  b.cyl_r = sh.radius;
+  b.cyl_hh = sh.half_height;
+  b.ext = d3(sh.ext[0], sh.ext[1], sh.ext[2]);
+  b.crust = crust;
+  if (a.has_basis) {
+    for (int t = 0; t < 9; ++t) b.basis.m[t] = a.cur.basis[9 * (size_t)slot + t];
+  } else {
+    for (int t = 0; t < 9; ++t) b.basis.m[t] = (t % 4 == 0) ? 1. : 0.;
+  }
+  b.origin = d3(xr.x, xr.y, xr.z);
+  for (int i = 0; i < 3; ++i) b.lext[i] = sh.type == GRAINS_GPU_SPHERE ? xr.w : sh.scaling_ext[i];
+  for (int i = 0; i < 3; ++i) b.scaling[i] = b.lext[i] < kEpsilon ? 1. : xdiv(xsub(b.lext[i], crust), b.lext[i]);
+}
+
+template <typename R>
+__device__ __forceinline__ void make_obstacle_ref(const StepArgs<R>& a, int oidx, BodyRef& b) {
+  const ObstacleDev& O = a.obs[oidx];
+  const ShapeDev& sh = a.shapes[O.shape];
+  b.type = sh.type;
+  b.nverts = sh.nverts;
+  b.verts = a.verts + 3 * sh.vert_offset;
+  b.radius = O.circ;
+  b.cyl_r = sh.radius;
+  b.cyl_hh = sh.half_height;
+  b.ext = d3(sh.ext[0], sh.ext[1], sh.ext[2]);
+  b.crust = O.crust;
+  for (int t = 0; t < 9; ++t) b.basis.m[t] = O.b[t];
+  b.origin = d3(O.o[0], O.o[1], O.o[2]);
+  for (int i = 0; i < 3; ++i) b.scaling[i] = O.scaling[i];
+  for (int i = 0; i < 3; ++i) b.lext[i] = sh.scaling_ext[i];
+}
+
+// Closest point of a general pair: FP32 GJK in the mixed path with a double
+// re-run when the FP32 overlap distance is inside a guard band around zero;
+// double GJK in the FP64 path.  Error handling (crust x10) on ContactError.
+template <typename R>
+__device__ ContactGeom convex_closest_point(const StepArgs<R>& a, const BodyRef& A, const BodyRef& B, int& iters,
+                                            int& handled) {
+  ContactGeom c;
+  handled = 0;
+  if (sizeof(R) == 4) {
+    c = convex_closest_point_t<float>(A, B, fmax(a.gjk_tol, 1.e-6), &iters);
+    if (c.status != 2) {
+      const double guard = 1.e-5 * (A.radius + B.radius);
+      if (c.status == 1 || fabs(c.overlap) < guard) c = convex_closest_point_t<double>(A, B, a.gjk_tol, &iters);
+    }
+  } else {
+    c = convex_closest_point_t<double>(A, B, a.gjk_tol, &iters);
+  }
+  if (c.status == 1) {
+    c = convex_error_handling(A, B, A.lext, B.lext, 10., a.gjk_tol);
+    handled = 1;
+  }
+  return c;
+}
+
+// ---------------------------------------------------------------------------
+// forces: one thread per particle (cell-sorted order).  Every pair is met by
+// both of its particles; both evaluate the same contact law with the lower id
+// as p0 (same inputs, same instructions -> bit-identical forces of opposite
+// sign), the lower id owns the pair's contact memory.
+template <typename R, bool DIAG>
+__global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const ParticleArrays<R>& P = a.cur;
+  const double4 xi = P.xr[s];
+  const int4 mi = P.meta[s];
+  const double4 mdi = P.md[s];
+  const V3<R> vi = ld3<R>(P.v[s]);
+  const V3<R> wi = ld3<R>(P.w[s]);
+  const int oi = P.orig[s];
+  const SysDev& S = a.sys[mi.w];
+  const D3 Xi = d3(xi.x, xi.y, xi.z);
+  const ShapeDev shi = a.shapes[mi.z];
+
+  // InitializeForces(withWeight): torsor = weight (Particle.cpp:1409-1416)
+  V3<R> F = v3<R>(R(S.gx * mdi.x), R(S.gy * mdi.x), R(S.gz * mdi.x));
+  V3<R> T = v3<R>(R(0), R(0), R(0));
+  int ncontact = 0, nnext = 0;
+  unsigned long long ncand = 0, nobs_cand = 0, ncont_own = 0, nobs_cont = 0, ngjk = 0, ngjk_it = 0;
+  double ov_max = 0., ov_sum = 0.;
+
+  int ci, cj, ck;
+  cell_of(S, xi.x, xi.y, xi.z, ci, cj, ck);
+  const int i0 = max(ci - 1, 0), i1 = min(ci + 1, S.nbi - 1);
+
+  for (int dj = -1; dj <= 1; ++dj) {
+    const int j = cj + dj;
+    if (j < 0 || j >= S.nbj) continue;
+    for (int dk = -1; dk <= 1; ++dk) {
+      const int k = ck + dk;
+      if (k < 0 || k >= S.nbk) continue;
+      const int t0 = a.cell_start[cell_index(S, i0, j, k)];
+      const int t1 = a.cell_start[cell_index(S, i1, j, k) + 1];
+      for (int t = t0; t < t1; ++t) {
+        if (t == s) continue;
+        const double4 xj = P.xr[t];
+        const int idj = P.meta[t].x;
+        const bool own = mi.x < idj;
+        if (own) ++ncand;
+        const D3 Xj = d3(xj.x, xj.y, xj.z);
+        const D3 A = own ? Xi : Xj, B = own ? Xj : Xi;
+        const double ra = own ? xi.w : xj.w, rb = own ? xj.w : xi.w;
+        const int4 mj = P.meta[t];
+        const ShapeDev shj = a.shapes[mj.z];
+        ContactGeom g;
+        if (shi.type == GRAINS_GPU_SPHERE && shj.type == GRAINS_GPU_SPHERE) {
+          D3 ab;
+          double nab;
+          const double dist = sphere_sphere_overlap(A, ra, B, rb, &ab, &nab);
+          if (!(dist < 0.)) continue;
+          const double4 mdj = P.md[t];
+          const double crust_sum = xadd(own ? mdi.y : mdj.y, own ? mdj.y : mdi.y);
+          g = sphere_sphere_features(A, ra, ab, nab, dist, crust_sum);
+          if (g.status) {
+            bool fatal;
+            g = sphere_sphere_error_handling(A, ra, own ? mdi.y : mdj.y, B, rb, own ? mdj.y : mdi.y, fatal);
+            set_status(a.stats, fatal ? GRAINS_GPU_CONTACT_ERROR : GRAINS_GPU_CONTACT_HANDLED);
+            if (fatal) continue;
+          }
+        } else {
+          // general convex pair: circumscribed-sphere test then GJK on crust-shrunk bodies
+          const double4 mdj = P.md[t];
+          BodyRef ba, bb;
+          const int sa = own ? s : t, sbx = own ? t : s;
+          make_body_ref(a, own ? mi.z : mj.z, sa, own ? mdi.y : mdj.y, ba);
+          make_body_ref(a, own ? mj.z : mi.z, sbx, own ? mdj.y : mdi.y, bb);
+          int it = 0, handled = 0;
+          g = convex_closest_point(a, ba, bb, it, handled);
+          if (own && g.status != 2) {
+            ++ngjk;
+            ngjk_it += it;
+          }
+          if (g.status == 2) continue;  // bounding spheres apart
+          if (handled) set_status(a.stats, g.status == 1 ? GRAINS_GPU_CONTACT_ERROR : GRAINS_GPU_CONTACT_HANDLED);
+          if (g.status == 1) continue;
+          if (!(g.overlap < 0.)) continue;
+          (void)mdj;
+        }
+        // contact: p0 = owner (lower id)
+        const double4 mdj = P.md[t];
+        const V3<R> vj = ld3<R>(P.v[t]), wj = ld3<R>(P.w[t]);
+        BodyAtContact<R> b0, b1;
+        const D3 lev0 = xsub3(g.point, A), lev1 = xsub3(g.point, B);
+        b0.v = own ? vi : vj;
+        b0.w = own ? wi : wj;
+        b0.lever = from_d3<R>(lev0);
+        b0.pos_minus_contact = from_d3<R>(xsub3(A, g.point));
+        b0.mass = R(own ? mdi.x : mdj.x);
+        b0.req = R(own ? mdi.z : mdj.z);
+        b1.v = own ? vj : vi;
+        b1.w = own ? wj : wi;
+        b1.lever = from_d3<R>(lev1);
+        b1.pos_minus_contact = from_d3<R>(xsub3(B, g.point));
+        b1.mass = R(own ? mdj.x : mdi.x);
+        b1.req = R(own ? mdj.z : mdi.z);
+        const int mat0 = own ? mi.y : mj.y, mat1 = own ? mj.y : mi.y;
+        const LawParams<R> L = a.laws[S.law_offset + mat0 * S.n_mat + mat1];
+        PairMemory<R> mem;
+        const int row0 = own ? oi : P.orig[t];
+        const int other = own ? idj : mi.x;
+        bool existed = false;
+        if (L.type == GRAINS_GPU_HOOKE_MEMORY) existed = find_memory(a, row0, other, 0, mem);
+        LawResult<R> res = pair_law(a, L, dt, g, b0, b1, existed, mem);
+        if (own && L.type == GRAINS_GPU_HOOKE_MEMORY) store_memory(a, oi, nnext, other, 0, mem);
+        // Torsor::addForce (Torsor.cpp:184-189); p1 gets -delFN - delFT
+        const V3<R> f = own ? res.force : -res.force;
+        F = F + f;
+        T = T + cross(own ? b0.lever : b1.lever, f);
+        if (L.rolling || L.kr != R(0)) T = T + (own ? res.torque : -res.torque);
+        ++ncontact;
+        if (own) {
+          ++ncont_own;
+          const double o = fabs(g.overlap);
+          ov_sum += o;
+          ov_max = fmax(ov_max, o);
+          if (DIAG && a.pairs) {
+            unsigned long long slot = atomicAdd(a.pairs_n, 1ull);
+            if (slot < (unsigned long long)a.pairs_cap) {
+              a.pairs[2 * slot] = mi.x;
+              a.pairs[2 * slot + 1] = idj;
+            }
+          }
+        }
+      }
+    }
+  }
+
+  // obstacles linked to the particle's cell (SimpleObstacle::InterAction, SimpleObstacle.cpp:222-270)
+  {
+    const int cell = cell_index(S, ci, cj, ck);
+    const int ob0 = a.cell_obs_start[cell], ob1 = a.cell_obs_start[cell + 1];
+    const int nstat = ob1 - ob0;
+    const int ntot = nstat + S.n_moving;
+    const D3 cg = d3(xadd(xadd(S.ox, xmul(double(ci), S.ex)), xdiv(S.ex, 2.)),
+                     xadd(xadd(S.oy, xmul(double(cj), S.ey)), xdiv(S.ey, 2.)),
+                     xadd(xadd(S.oz, xmul(double(ck), S.ez)), xdiv(S.ez, 2.)));
+    for (int u = 0; u < ntot; ++u) {
+      int oidx;
+      if (u < nstat) {
+        oidx = a.cell_obs_idx[ob0 + u];
+      } else {
+        oidx = a.moving_idx[S.moving_offset + (u - nstat)];
+        const ObstacleDev& O = a.obs[oidx];
+        // cell link of a moving obstacle: AABB vs twice-expanded cell (LinkedCell.cpp:1568-1585)
+        if (!in_zone(d3(O.bbc[0], O.bbc[1], O.bbc[2]), d3(O.bbe[0], O.bbe[1], O.bbe[2]), cg, S.ex, S.ey, S.ez))
+          continue;
+      }
+      const ObstacleDev& O = a.obs[oidx];
+      if (!in_zone(d3(O.bbc[0], O.bbc[1], O.bbc[2]), d3(O.bbe[0], O.bbe[1], O.bbe[2]), Xi, xi.w, xi.w, xi.w))
+        continue;
+      ++nobs_cand;
+      M3 ob;
+      for (int q = 0; q < 9; ++q) ob.m[q] = O.b[q];
+      const D3 oo = d3(O.o[0], O.o[1], O.o[2]);
+      const double crust_sum = xadd(mdi.y, O.crust);
+      ContactGeom g;
+      const ShapeDev& sho = a.shapes[O.shape];
+      if (shi.type == GRAINS_GPU_SPHERE && sho.type == GRAINS_GPU_BOX) {
+        g = sphere_box(Xi, xi.w, crust_sum, ob, oo, d3(sho.ext[0], sho.ext[1], sho.ext[2]));
+        if (g.status) {
+          set_status(a.stats, GRAINS_GPU_CONTACT_ERROR);
+          continue;
+        }
+      } else {
+        BodyRef ba, bb;
+        make_body_ref(a, mi.z, s, mdi.y, ba);
+        make_obstacle_ref(a, oidx, bb);
+        int it = 0, handled = 0;
+        g = convex_closest_point(a, ba, bb, it, handled);
+        if (g.status != 2) {
+          ++ngjk;
+          ngjk_it += it;
+        }
+        if (g.status == 2) continue;
+        if (handled) set_status(a.stats, g.status == 1 ? GRAINS_GPU_CONTACT_ERROR : GRAINS_GPU_CONTACT_HANDLED);
+        if (g.status == 1) continue;
+      }
+      if (!(g.overlap < 0.)) continue;
+      // contact: p0 = particle, p1 = obstacle (mass 1e20, velocity at point, Obstacle.cpp:128-133)
+      BodyAtContact<R> b0, b1;
+      b0.v = vi;
+      b0.w = wi;
+      b0.lever = from_d3<R>(xsub3(g.point, Xi));
+      b0.pos_minus_contact = from_d3<R>(xsub3(Xi, g.point));
+      b0.mass = R(mdi.x);
+      b0.req = R(mdi.z);
+      const D3 olev = xsub3(g.point, oo);
+      const V3<double> ow = v3<double>(O.omega[0], O.omega[1], O.omega[2]);
+      const V3<double> ovp = v3<double>(O.vel[0], O.vel[1], O.vel[2]) + cross(ow, v3<double>(olev.x, olev.y, olev.z));
+      b1.v = v3<R>(R(ovp.x), R(ovp.y), R(ovp.z));
+      b1.w = v3<R>(R(ow.x), R(ow.y), R(ow.z));
+      b1.lever = from_d3<R>(olev);
+      b1.pos_minus_contact = from_d3<R>(xsub3(oo, g.point));
+      b1.mass = R(kObstacleMass);
+      b1.req = R(pow((0.75 / kPi) * sho.volume, 1. / 3.));
+      const LawParams<R> L = a.laws[S.law_offset + mi.y * S.n_mat + O.material];
+      PairMemory<R> mem;
+      const int oloc = oidx - S.obs_offset;
+      bool existed = false;
+      if (L.type == GRAINS_GPU_HOOKE_MEMORY) existed = find_memory(a, oi, oloc, 1, mem);
+      LawResult<R> res = pair_law(a, L, dt, g, b0, b1, existed, mem);
+      if (L.type == GRAINS_GPU_HOOKE_MEMORY) store_memory(a, oi, nnext, oloc, 1, mem);
+      F = F + res.force;
+      T = T + cross(b0.lever, res.force);
+      if (L.rolling || L.kr != R(0)) T = T + res.torque;
+      ++ncontact;
+      ++nobs_cont;
+      const double o = fabs(g.overlap);
+      ov_sum += o;
+      ov_max = fmax(ov_max, o);
+    }
+  }
+
+  P.F[s] = st3<R>(F);
+  P.T[s] = st3<R>(T);
+  a.coord[s] = ncontact;
+  a.hist_n_next[oi] = nnext;
+
+  // statistics: warp reduction then one atomic per warp
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    ncand += __shfl_down_sync(full, ncand, o);
+    nobs_cand += __shfl_down_sync(full, nobs_cand, o);
+    ncont_own += __shfl_down_sync(full, ncont_own, o);
+    nobs_cont += __shfl_down_sync(full, nobs_cont, o);
+    ngjk += __shfl_down_sync(full, ngjk, o);
+    ngjk_it += __shfl_down_sync(full, ngjk_it, o);
+    ov_sum += __shfl_down_sync(full, ov_sum, o);
+    ov_max = fmax(ov_max, __shfl_down_sync(full, ov_max, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (ncand) atomicAdd(&a.stats->n_cand, ncand);
+    if (nobs_cand) atomicAdd(&a.stats->n_obs_cand, nobs_cand);
+    if (ncont_own) atomicAdd(&a.stats->n_contacts, ncont_own);
+    if (nobs_cont) atomicAdd(&a.stats->n_obs_contacts, nobs_cont);
+    if (ngjk) atomicAdd(&a.stats->n_gjk_calls, ngjk);
+    if (ngjk_it) atomicAdd(&a.stats->n_gjk_iters, ngjk_it);
+    if (ov_sum > 0.) atomicAdd(&a.stats->overlap_sum, ov_sum);
+    if (ov_max > 0.) atomic_max_pos_double(&a.stats->overlap_max_bits, ov_max);
+  }
+}
+
+template <typename R>
+__global__ void zero_kdelta_kernel(StepArgs<R> a) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  int row = a.cur.orig[s];
+  int n = a.hist_n_prev[row];
+  for (int k = 0; k < n; ++k) {
+    HistEntry<R>& e = a.hist_prev[(size_t)row * a.hist_cap + k];
+    e.kd[0] = e.kd[1] = e.kd[2] = R(0);
+    e.sp[0] = e.sp[1] = e.sp[2] = R(0);
+  }
+}
+
+// overwrite the kinematic state from a host-ordered staging area
+template <typename R>
+__global__ void update_dynamic_kernel(StepArgs<R> a, const double* st, const double* sb) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const ParticleArrays<R>& P = a.cur;
+  const size_t i = (size_t)P.orig[s];
+  const double* e = st + 13 * i;
+  double4 xr = P.xr[s];
+  xr.x = e[0];
+  xr.y = e[1];
+  xr.z = e[2];
+  P.xr[s] = xr;
+  P.q[s] = make_double4(e[3], e[4], e[5], e[6]);
+  P.v[s] = st3<R>(v3<R>(R(e[7]), R(e[8]), R(e[9])));
+  Qt<double> q{v3<double>(e[3], e[4], e[5]), e[6]};
+  V3<double> w = v3<double>(e[10], e[11], e[12]);
+  P.w[s] = st3<R>(v3<R>(R(w.x), R(w.y), R(w.z)));
+  V3<double> wbf = q_to_body(q, w);  // ParticleKinematics::setAngularVelocity
+  P.wbf[s] = st3<R>(v3<R>(R(wbf.x), R(wbf.y), R(wbf.z)));
+  if (a.has_basis && sb)
+    for (int k = 0; k < 9; ++k) P.basis[9 * (size_t)s + k] = sb[9 * i + k];
+}
+
+// candidate pairs (diagnostic): pairs with both cells equal or adjacent
+template <typename R>
+__global__ void candidate_pairs_kernel(StepArgs<R> a, int sys, int include_obstacles, int* out, int cap,
+                                       unsigned long long* count) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const ParticleArrays<R>& P = a.cur;
+  const int4 mi = P.meta[s];
+  if (mi.w != sys) return;
+  const double4 xi = P.xr[s];
+  const SysDev& S = a.sys[mi.w];
+  int ci, cj, ck;
+  cell_of(S, xi.x, xi.y, xi.z, ci, cj, ck);
+  const int i0 = max(ci - 1, 0), i1 = min(ci + 1, S.nbi - 1);
+  for (int dj = -1; dj <= 1; ++dj) {
+    const int j = cj + dj;
+    if (j < 0 || j >= S.nbj) continue;
+    for (int dk = -1; dk <= 1; ++dk) {
+      const int k = ck + dk;
+      if (k < 0 || k >= S.nbk) continue;
+      const int t0 = a.cell_start[cell_index(S, i0, j, k)];
+      const int t1 = a.cell_start[cell_index(S, i1, j, k) + 1];
+      for (int t = t0; t < t1; ++t) {
+        int idj = P.meta[t].x;
+        if (t == s || !(mi.x < idj)) continue;
+        unsigned long long slot = atomicAdd(count, 1ull);
+        if (slot < (unsigned long long)cap) {
+          out[2 * slot] = mi.x;
+          out[2 * slot + 1] = idj;
+        }
+      }
+    }
+  }
+  if (include_obstacles) {
+    const int cell = cell_index(S, ci, cj, ck);
+    const D3 cg = d3(xadd(xadd(S.ox, xmul(double(ci), S.ex)), xdiv(S.ex, 2.)),
+                     xadd(xadd(S.oy, xmul(double(cj), S.ey)), xdiv(S.ey, 2.)),
+                     xadd(xadd(S.oz, xmul(double(ck), S.ez)), xdiv(S.ez, 2.)));
+    for (int u = a.cell_obs_start[cell]; u < a.cell_obs_start[cell + 1]; ++u) {
+      unsigned long long slot = atomicAdd(count, 1ull);
+      if (slot < (unsigned long long)cap) {
+        out[2 * slot] = mi.x;
+        out[2 * slot + 1] = a.obs[a.cell_obs_idx[u]].id;
+      }
+    }
+    for (int u = 0; u < S.n_moving; ++u) {
+      const ObstacleDev& O = a.obs[a.moving_idx[S.moving_offset + u]];
+      if (!in_zone(d3(O.bbc[0], O.bbc[1], O.bbc[2]), d3(O.bbe[0], O.bbe[1], O.bbe[2]), cg, S.ex, S.ey, S.ez))
+        continue;
+      unsigned long long slot = atomicAdd(count, 1ull);
+      if (slot < (unsigned long long)cap) {
+        out[2 * slot] = mi.x;
+        out[2 * slot + 1] = O.id;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+inline int grid_for(long long n, int block) { return (int)((n + block - 1) / block); }
+
+inline int check_launch() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : GRAINS_GPU_CUDA_ERROR;
+}
+
+template <typename R>
+int launch_kick_move(const StepArgs<R>& a, cudaStream_t s, int do_kick2, double dt_kick2, int do_move, double dt_v,
+                     double dt_x) {
+  if (a.n == 0) return 0;
+  kick_move_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, do_kick2, R(dt_kick2), do_move, R(dt_v), dt_x);
+  return check_launch();
+}
+
+template <typename R>
+int launch_bin(const StepArgs<R>& a, cudaStream_t s) {
+  if (a.n == 0) return 0;
+  bin_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
+  return check_launch();
+}
+
+template <typename R>
+int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forces) {
+  const int C = a.n_cells;
+  const int nb = grid_for(C, kScanTile);
+  scan_tiles_kernel<<<nb, kScanThreads, 0, s>>>(a.cell_count, a.cell_start, a.block_sums, C);
+  scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(a.block_sums, nb, a.cell_start, C);
+  scan_add_kernel<<<grid_for(C, 256), 256, 0, s>>>(a.cell_start, a.block_sums, C);
+  if (a.n > 0) scatter_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
+  cell_sort_kernel<R><<<grid_for(C, 256), 256, 0, s>>>(a);
+  if (a.n > 0) gather_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, gather_forces);
+  return check_launch();
+}
+
+template <typename R>
+int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag) {
+  if (a.n == 0) return 0;
+  if (diag)
+    forces_kernel<R, true><<<grid_for(a.n, 128), 128, 0, s>>>(a, R(dt));
+  else
+    forces_kernel<R, false><<<grid_for(a.n, 128), 128, 0, s>>>(a, R(dt));
+  return check_launch();
+}
+
+template <typename R>
+int launch_zero_kdelta(const StepArgs<R>& a, cudaStream_t s) {
+  if (a.n == 0) return 0;
+  zero_kdelta_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
+  return check_launch();
+}
+
+template <typename R>
+int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const double* stage, const double* stage_basis) {
+  if (a.n == 0) return 0;
+  update_dynamic_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, stage, stage_basis);
+  return check_launch();
+}
+
+template <typename R>
+int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int include_obstacles, int* out, int cap,
+                           unsigned long long* count) {
+  if (a.n == 0) return 0;
+  candidate_pairs_kernel<R><<<grid_for(a.n, 128), 128, 0, s>>>(a, sys, include_obstacles, out, cap, count);
+  return check_launch();
+}
+
+#define GG_INSTANTIATE(R)                                                                                  \
+  template int launch_kick_move<R>(const StepArgs<R>&, cudaStream_t, int, double, int, double, double);    \
+  template int launch_bin<R>(const StepArgs<R>&, cudaStream_t);                                            \
+  template int launch_sort_and_gather<R>(const StepArgs<R>&, cudaStream_t, int);                           \
+  template int launch_forces<R>(const StepArgs<R>&, cudaStream_t, double, int);                            \
+  template int launch_zero_kdelta<R>(const StepArgs<R>&, cudaStream_t);                                    \
+  template int launch_update_dynamic<R>(const StepArgs<R>&, cudaStream_t, const double*, const double*);     \
+  template int launch_candidate_pairs<R>(const StepArgs<R>&, cudaStream_t, int, int, int*, int,           \
+                                         unsigned long long*);
+
+}  // namespace gg

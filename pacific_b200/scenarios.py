@@ -1,0 +1,236 @@
+"""Seeded synthetic inputs of the benchmark workloads (no public dataset exists
+for the Grains3D DEM step; these stand in for the reference's insertion).
+
+Every generator returns a `Scenario`: shapes, per-system domains, contact laws,
+wall obstacles and particle arrays, ready for `apply(sim, scenario)` on any
+implementation of the grains_gpu C ABI.  Masses and inertias follow the
+reference's formulas (Particle.cpp:158-163, Sphere.cpp:61-70,152-155,
+Box.cpp:181-210, Cylinder.cpp:61-100).  Walls are thin Box obstacles whose
+inner faces lie on the domain faces, like the reference's test layouts
+(Tests/data/spheres-settling-new-grains/Grains/Init/insert.xml).
+"""
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .abi import BOX, HOOKE_MEMORY, SPHERE
+
+MM = 1.0e-3
+PI = 3.14159265358979323846
+
+
+@dataclass
+class Scenario:
+    name: str
+    shapes: list                     # [(type, params)]
+    domains: list                    # per system: dict(origin, size, cell_size, gravity)
+    laws: list                       # per system: [(mat_a, mat_b, law, params)]
+    obstacles: list                  # per system: [dict(id, shape_index, material, crust, transform, ...)]
+    particles: dict                  # numpy arrays; 'shape' holds shape-list indices
+    dt: float
+    n_steps: int
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n(self):
+        return len(self.particles["id"])
+
+
+def sphere_mass_inertia(r, rho):
+    """mass = rho * 4 pi r^3 / 3 and principal inertia rho * 8 pi r^5 / 15."""
+    r = np.asarray(r, dtype=np.float64)
+    vol = np.array([4.0 * PI * math.pow(x, 3.0) / 3.0 for x in r.ravel()]).reshape(r.shape)
+    i0 = np.array([8.0 * PI * math.pow(x, 5.0) / 15.0 for x in r.ravel()]).reshape(r.shape)
+    return rho * vol, np.repeat((i0 * rho)[:, None], 3, axis=1)
+
+
+def hooke_memory_params(kn, en, muc, kt, etat=-1.0, mur=0.0, etarpf=0.0, epst=0.0):
+    """HookeMemory parameters in C ABI order.  epst = 0 is the effective value
+    when the XML omits it (the fallback writes key "eps" but the model reads
+    "epst", HookeMemoryContactForceModel.cpp:21, 300-306)."""
+    return [kn, en, etat, muc, kt, mur, etarpf, epst]
+
+
+def box_walls(lo, hi, faces, thickness, crust, shape_offset, id_start, material=1):
+    """Thin box walls on the chosen faces of the box [lo, hi].
+
+    faces: subset of 'xX yY zZ' letters (lower case = lower face).  Returns
+    (shapes, obstacles); obstacle 'shape' indexes into the returned shapes
+    list shifted by shape_offset.
+    """
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    size = hi - lo
+    t = thickness
+    shapes, obs = [], []
+    for k, f in enumerate(faces):
+        axis = "xyz".index(f.lower())
+        upper = f.isupper()
+        edges = size + 2 * t
+        edges[axis] = t
+        centre = (lo + hi) / 2.0
+        centre[axis] = (hi[axis] + t / 2.0) if upper else (lo[axis] - t / 2.0)
+        shapes.append((BOX, list(edges)))
+        obs.append(dict(id=id_start - k, shape=shape_offset + len(shapes) - 1, material=material, crust=crust,
+                        transform=[1, 0, 0, 0, 1, 0, 0, 0, 1, *centre]))
+    return shapes, obs
+
+
+def lattice(n, lo, hi, spacing, margin, jitter, rng):
+    """First n sites of a cubic lattice inside [lo, hi] (x fastest, then y, z),
+    with a uniform jitter in [-jitter, jitter] per coordinate."""
+    lo, hi = np.asarray(lo, float), np.asarray(hi, float)
+    counts = [int(math.floor((hi[a] - lo[a] - 2 * margin) / spacing + 1e-9)) + 1 for a in range(3)]
+    per_layer = counts[0] * counts[1]
+    if per_layer * counts[2] < n:
+        raise ValueError("lattice holds %d sites < %d" % (per_layer * counts[2], n))
+    k = np.arange(n)
+    ix, iy, iz = k % counts[0], (k // counts[0]) % counts[1], k // per_layer
+    pos = np.stack([lo[0] + margin + ix * spacing, lo[1] + margin + iy * spacing, lo[2] + margin + iz * spacing], 1)
+    return pos + rng.uniform(-jitter, jitter, size=(n, 3))
+
+
+def _spheres(n, radius, rho, pos, vel, crust, shape_index=0, material=0, system=None, id0=0):
+    mass, inertia = sphere_mass_inertia(radius, rho)
+    q = np.zeros((n, 4))
+    q[:, 3] = 1.0
+    return dict(id=np.arange(id0, id0 + n, dtype=np.int32), system=system,
+                shape=np.full(n, shape_index, np.int32), material=np.full(n, material, np.int32),
+                radius=np.asarray(radius, float), crust=np.full(n, crust), mass=mass, inertia=inertia,
+                position=pos, quaternion=q, basis=None, velocity=vel, omega=np.zeros((n, 3)))
+
+
+def settling_1k(n=1000, seed=0):
+    """1,000 monodisperse spheres (r = 1 mm, rho = 2500) in a closed 20x20x60 mm
+    box, jittered lattice (spacing 2.4 mm, +-0.1 mm), at rest, Hooke kn = 1e5,
+    en = 0.9, mu = 0.5, kt = 0.8 kn, dt = 1e-5 s, 10,000 steps."""
+    rng = np.random.default_rng(seed)
+    crust = 0.05 * MM
+    lo, hi = np.zeros(3), np.array([20.0, 20.0, 60.0]) * MM
+    pos = lattice(n, lo, hi, 2.4 * MM, 1.2 * MM, 0.1 * MM, rng)
+    r = np.full(n, 1.0 * MM)
+    shapes = [(SPHERE, [1.0 * MM])]
+    wshapes, obs = box_walls(lo, hi, "xXyYzZ", 0.5 * MM, crust, len(shapes), -1)
+    shapes += wshapes
+    kn = 1.0e5
+    laws = [[(0, 0, HOOKE_MEMORY, hooke_memory_params(kn, 0.9, 0.5, 0.8 * kn)),
+             (0, 1, HOOKE_MEMORY, hooke_memory_params(kn, 0.9, 0.5, 0.8 * kn))]]
+    dom = [dict(origin=lo, size=hi - lo, cell_size=2.0 * 1.0 * MM, gravity=(0.0, 0.0, -9.81))]
+    p = _spheres(n, r, 2500.0, pos, np.zeros((n, 3)), crust)
+    return Scenario("settling_1k", shapes, dom, laws, [obs], p, 1.0e-5, 10000)
+
+
+def polydisperse_200k(n=200_000, seed=1, vseed=2, height=370.0):
+    """200,000 spheres, r ~ U[0.8, 1.2] mm, rho = 2500, floor + 4 side walls of
+    a 100x100 mm box, lattice spacing 2.6 mm, velocities N(0, 0.05 m/s), same
+    law as settling_1k, dt = 5e-6 s.  200k spheres do not fit a jittered
+    cubic lattice in 100x100x200 mm, so the domain is 370 mm tall (the settled
+    bed, about 145 mm, stays inside 200 mm)."""
+    rng = np.random.default_rng(seed)
+    vrng = np.random.default_rng(vseed)
+    crust = 0.05 * MM
+    lo, hi = np.zeros(3), np.array([100.0, 100.0, height]) * MM
+    r = rng.uniform(0.8 * MM, 1.2 * MM, size=n)
+    pos = lattice(n, lo, hi, 2.6 * MM, 1.3 * MM, 0.1 * MM, rng)
+    vel = vrng.normal(0.0, 0.05, size=(n, 3))
+    shapes = [(SPHERE, [1.0 * MM])]
+    wshapes, obs = box_walls(lo, hi, "xXyYz", 0.5 * MM, crust, len(shapes), -1)
+    shapes += wshapes
+    kn = 1.0e5
+    laws = [[(0, 0, HOOKE_MEMORY, hooke_memory_params(kn, 0.9, 0.5, 0.8 * kn)),
+             (0, 1, HOOKE_MEMORY, hooke_memory_params(kn, 0.9, 0.5, 0.8 * kn))]]
+    dom = [dict(origin=lo, size=hi - lo, cell_size=2.0 * 1.2 * MM, gravity=(0.0, 0.0, -9.81))]
+    p = _spheres(n, r, 2500.0, pos, vel, crust)
+    return Scenario("polydisperse_200k", shapes, dom, laws, [obs], p, 5.0e-6, 20000)
+
+
+def ensemble_512(n_systems=512, seed=4, n_min=200, n_max=20000):
+    """512 independent settling boxes: N_s log-uniform in [200, 20000],
+    r ~ U[0.9, 1.1] mm, box w x w x 3w with w = 20 mm (N_s/1000)^(1/3), own
+    kn ~ logU[5e4, 5e5], en ~ U[0.5, 0.95], mu ~ U[0.1, 0.8], kt = 0.8 kn;
+    dt = 5e-6 s."""
+    rng = np.random.default_rng(seed)
+    crust = 0.05 * MM
+    ns = np.floor(np.exp(rng.uniform(math.log(n_min), math.log(n_max), size=n_systems))).astype(int)
+    shapes = [(SPHERE, [1.0 * MM])]
+    doms, laws, obstacles, parts = [], [], [], []
+    for s in range(n_systems):
+        n = int(ns[s])
+        w = 20.0 * MM * (n / 1000.0) ** (1.0 / 3.0)
+        lo, hi = np.zeros(3), np.array([w, w, 3 * w])
+        r = rng.uniform(0.9 * MM, 1.1 * MM, size=n)
+        pos = lattice(n, lo, hi, 2.4 * MM, 1.2 * MM, 0.1 * MM, rng)
+        wshapes, obs = box_walls(lo, hi, "xXyYzZ", 0.5 * MM, crust, len(shapes), -1)
+        shapes += wshapes
+        kn = math.exp(rng.uniform(math.log(5.0e4), math.log(5.0e5)))
+        en = rng.uniform(0.5, 0.95)
+        mu = rng.uniform(0.1, 0.8)
+        laws.append([(0, 0, HOOKE_MEMORY, hooke_memory_params(kn, en, mu, 0.8 * kn)),
+                     (0, 1, HOOKE_MEMORY, hooke_memory_params(kn, en, mu, 0.8 * kn))])
+        doms.append(dict(origin=lo, size=hi - lo, cell_size=2.0 * 1.1 * MM, gravity=(0.0, 0.0, -9.81)))
+        obstacles.append(obs)
+        parts.append(_spheres(n, r, 2500.0, pos, np.zeros((n, 3)), crust, system=np.full(n, s, np.int32)))
+    p = {k: (np.concatenate([q[k] for q in parts]) if parts[0][k] is not None else None) for k in parts[0]}
+    return Scenario("ensemble_512", shapes, doms, laws, obstacles, p, 5.0e-6, 5000, meta=dict(sizes=ns))
+
+
+def adjoint_4k(seed=5, vseed=6, kn=1.0e5, en=0.9, mu=0.5):
+    """4,096 spheres r = 1 mm on a 16^3 lattice (spacing 2.4 mm) in a
+    40x40x60 mm box with floor + 4 walls, velocities N(0, 0.2 m/s); kn = 1e5,
+    en = 0.9, mu = 0.5, kt = 0.8 kn, dt = 1e-5 s, 2,000 steps."""
+    rng = np.random.default_rng(seed)
+    vrng = np.random.default_rng(vseed)
+    n = 4096
+    crust = 0.05 * MM
+    lo, hi = np.zeros(3), np.array([40.0, 40.0, 60.0]) * MM
+    pos = lattice(n, lo, hi, 2.4 * MM, 1.2 * MM, 0.1 * MM, rng)
+    vel = vrng.normal(0.0, 0.2, size=(n, 3))
+    shapes = [(SPHERE, [1.0 * MM])]
+    wshapes, obs = box_walls(lo, hi, "xXyYz", 0.5 * MM, crust, len(shapes), -1)
+    shapes += wshapes
+    laws = [[(0, 0, HOOKE_MEMORY, hooke_memory_params(kn, en, mu, 0.8 * kn)),
+             (0, 1, HOOKE_MEMORY, hooke_memory_params(kn, en, mu, 0.8 * kn))]]
+    dom = [dict(origin=lo, size=hi - lo, cell_size=2.0 * 1.0 * MM, gravity=(0.0, 0.0, -9.81))]
+    p = _spheres(n, np.full(n, 1.0 * MM), 2500.0, pos, vel, crust)
+    return Scenario("adjoint_4k", shapes, dom, laws, [obs], p, 1.0e-5, 2000)
+
+
+def small_box(n=64, seed=0, velocity_sigma=0.05, spacing=2.04, jitter=0.02, radius_range=(1.0, 1.0)):
+    """A small dense cluster near the floor of a closed box (many contacts in
+    the first steps) for parity tests that the oracle finishes in seconds."""
+    rng = np.random.default_rng(seed)
+    crust = 0.05 * MM
+    side = max(8.0, math.ceil((n ** (1.0 / 3.0)) * spacing + 3.0))
+    lo, hi = np.zeros(3), np.array([side, side, side * 1.5]) * MM
+    r = rng.uniform(radius_range[0] * MM, radius_range[1] * MM, size=n)
+    pos = lattice(n, lo, hi, spacing * MM, (radius_range[1] + jitter + 0.01) * MM, jitter * MM, rng)
+    vel = rng.normal(0.0, velocity_sigma, size=(n, 3))
+    shapes = [(SPHERE, [1.0 * MM])]
+    wshapes, obs = box_walls(lo, hi, "xXyYzZ", 0.5 * MM, crust, len(shapes), -1)
+    shapes += wshapes
+    kn = 1.0e5
+    laws = [[(0, 0, HOOKE_MEMORY, hooke_memory_params(kn, 0.9, 0.5, 0.8 * kn)),
+             (0, 1, HOOKE_MEMORY, hooke_memory_params(kn, 0.9, 0.5, 0.8 * kn))]]
+    dom = [dict(origin=lo, size=hi - lo, cell_size=2.0 * radius_range[1] * MM, gravity=(0.0, 0.0, -9.81))]
+    p = _spheres(n, r, 2500.0, pos, vel, crust)
+    return Scenario("small_box", shapes, dom, laws, [obs], p, 1.0e-5, 100)
+
+
+def apply(sim, sc):
+    """Registers shapes, domains, laws and obstacles of `sc` on `sim` and
+    uploads the particles.  Returns the shape-id map."""
+    ids = [sim.add_shape(t, prm) for t, prm in sc.shapes]
+    for s, d in enumerate(sc.domains):
+        sim.set_domain(s, d["origin"], d["size"], d["cell_size"], d["gravity"])
+        for a, b, law, prm in sc.laws[s]:
+            sim.set_contact_law(s, a, b, law, prm)
+        obs = []
+        for o in sc.obstacles[s]:
+            o2 = dict(o)
+            o2["shape"] = ids[o["shape"]]
+            obs.append(o2)
+        sim.set_obstacles(s, obs)
+    p = dict(sc.particles)
+    p["shape"] = np.asarray(ids, np.int32)[np.asarray(p["shape"])]
+    sim.upload(p)
+    return ids

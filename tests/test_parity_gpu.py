@@ -1,0 +1,164 @@
+"""Parity of the CUDA path with the CPU oracle on identical states.
+
+* candidate pairs and contact pairs: bit-exact sets (both decide in double
+  with the reference's rounding);
+* one force evaluation: plain FP64 forces / torques within 1e-12 relative,
+  mixed precision within 1e-5 relative (force floor = the particle weight);
+* short trajectories: FP64 states within tight absolute bounds.
+"""
+import numpy as np
+import pytest
+
+from pacific_b200 import scenarios as S
+from pacific_b200.abi import FP64, MIXED
+
+from helpers import make, pair_set, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def evolved(oracle_lib, n=300, seed=1, steps=300, sigma=0.3):
+    """A dense cluster advanced by the oracle: returns the scenario whose
+    particle state (and contact memory) are the oracle's after `steps`."""
+    sc = S.small_box(n, seed=seed, velocity_sigma=sigma)
+    o = make(oracle_lib, sc)
+    o.initialize_leapfrog(0.0, sc.dt)
+    o.step(steps, 0.0, sc.dt)
+    st = o.download()
+    mem = o.contact_memory()
+    p = dict(sc.particles)
+    for k in ["position", "quaternion", "basis", "velocity", "omega"]:
+        p[k] = st[k]
+    sc.particles = p
+    return sc, mem
+
+
+def both(oracle_lib, gpu_lib, sc, mem=None, precision=FP64):
+    o = make(oracle_lib, sc)
+    g = make(gpu_lib, sc, precision)
+    if mem is not None:
+        o.upload_contact_memory(mem)
+        g.upload_contact_memory(mem)
+    return o, g
+
+
+@pytest.mark.parametrize("name", ["settling_1k", "small_box", "evolved"])
+def test_candidate_pairs_bit_exact(oracle_lib, gpu_lib, name):
+    if name == "settling_1k":
+        sc = S.settling_1k()
+    elif name == "small_box":
+        sc = S.small_box(125, seed=7)
+    else:
+        sc, _ = evolved(oracle_lib)
+    o, g = both(oracle_lib, gpu_lib, sc)
+    co = o.candidate_pairs(include_obstacles=True)
+    cg = g.candidate_pairs(include_obstacles=True)
+    assert len(co) == len(cg)
+    assert np.array_equal(co, cg)
+    assert len(pair_set(co)) == len(co)
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+def test_one_force_evaluation(oracle_lib, gpu_lib, precision):
+    sc, mem = evolved(oracle_lib)
+    o, g = both(oracle_lib, gpu_lib, sc, mem, precision)
+    o.reset_stats()
+    g.reset_stats()
+    o.compute_forces(0.0, sc.dt)
+    g.compute_forces(0.0, sc.dt)
+    po, pg = o.contact_pairs(), g.contact_pairs()
+    assert len(po) > 50, "the evolved state should have many contacts"
+    assert pair_set(po) == pair_set(pg)
+    so, sg = o.stats(), g.stats()
+    assert so["n_contacts"] == sg["n_contacts"]
+    assert so["n_obstacle_contacts"] == sg["n_obstacle_contacts"]
+    do, dg = o.download(), g.download()
+    assert np.array_equal(do["coordination"], dg["coordination"])
+    weight = sc.particles["mass"][0] * 9.81
+    tol = 1e-12 if precision == FP64 else 1e-5
+    assert rel_err(dg["force"], do["force"], weight) < tol
+    torque_scale = weight * 1e-3
+    assert rel_err(dg["torque"], do["torque"], torque_scale) < (1e-10 if precision == FP64 else 1e-5)
+    # contact memory after the evaluation
+    mo, mg = o.contact_memory(), g.contact_memory()
+    ko = {(a, b): i for i, (a, b) in enumerate(zip(mo["owner"], mo["other"]))}
+    kg = {(a, b): i for i, (a, b) in enumerate(zip(mg["owner"], mg["other"]))}
+    assert set(ko) == set(kg)
+    idx_o = np.array([ko[k] for k in sorted(ko)])
+    idx_g = np.array([kg[k] for k in sorted(ko)])
+    kscale = 1e-3 * weight
+    assert rel_err(mg["kdelta"][idx_g], mo["kdelta"][idx_o], kscale) < (1e-9 if precision == FP64 else 1e-4)
+    assert np.max(np.abs(mg["prev_normal"][idx_g] - mo["prev_normal"][idx_o])) < (1e-12 if precision == FP64 else 1e-6)
+
+
+def test_move_and_advance_velocity_fp64(oracle_lib, gpu_lib):
+    sc, mem = evolved(oracle_lib, steps=200)
+    sc.particles["omega"] = np.random.default_rng(3).normal(0, 50.0, size=(sc.n, 3))
+    o, g = both(oracle_lib, gpu_lib, sc, mem, FP64)
+    for s in (o, g):
+        s.compute_forces(0.0, sc.dt)
+        s.move(0.0, 0.5 * sc.dt, sc.dt)
+    do, dg = o.download(), g.download()
+    assert np.max(np.abs(dg["position"] - do["position"])) < 1e-15
+    assert np.max(np.abs(dg["velocity"] - do["velocity"])) < 1e-13
+    assert np.max(np.abs(dg["quaternion"] - do["quaternion"])) < 1e-14
+    assert np.max(np.abs(dg["omega"] - do["omega"])) < 1e-9
+    for s in (o, g):
+        s.link_update()
+        s.compute_forces(sc.dt, sc.dt)
+        s.advance_velocity(sc.dt, 0.5 * sc.dt)
+    do, dg = o.download(), g.download()
+    weight = sc.particles["mass"][0] * 9.81
+    assert rel_err(dg["force"], do["force"], weight) < 1e-11
+    assert np.max(np.abs(dg["velocity"] - do["velocity"])) < 1e-12
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+def test_trajectory_matches_oracle(oracle_lib, gpu_lib, precision):
+    sc, mem = evolved(oracle_lib, steps=150)
+    o, g = both(oracle_lib, gpu_lib, sc, mem, precision)
+    t = 0.0
+    for s in (o, g):
+        s.compute_forces(t, sc.dt)
+    steps = 40
+    to = o.step(steps, t, sc.dt)
+    tg = g.step(steps, t, sc.dt)
+    assert to == pytest.approx(tg)
+    do, dg = o.download(), g.download()
+    pos_tol = 1e-12 if precision == FP64 else 1e-8
+    assert np.max(np.abs(dg["position"] - do["position"])) < pos_tol
+    vel_tol = 1e-9 if precision == FP64 else 1e-4
+    assert np.max(np.abs(dg["velocity"] - do["velocity"])) < vel_tol
+
+
+def test_graph_steps_equal_single_steps(gpu_lib):
+    """The CUDA-graph replay of the fused step gives the same bits as stepping
+    one at a time through the per-phase entry points."""
+    sc = S.small_box(216, seed=11, velocity_sigma=0.3)
+    a = make(gpu_lib, sc, FP64)
+    b = make(gpu_lib, sc, FP64)
+    for s in (a, b):
+        s.initialize_leapfrog(0.0, sc.dt)
+    ta = a.step(20, 0.0, sc.dt)
+    tb = 0.0
+    for _ in range(20):
+        tb += sc.dt
+        b.move(tb, 0.5 * sc.dt, sc.dt)
+        b.link_update(tb, sc.dt)
+        b.compute_forces(tb, sc.dt)
+        b.advance_velocity(tb, 0.5 * sc.dt)
+    da, db = a.download(), b.download()
+    for k in ["position", "velocity", "omega", "quaternion", "force", "torque"]:
+        assert np.array_equal(da[k], db[k]), k
+
+
+def test_deterministic(gpu_lib):
+    sc = S.small_box(343, seed=5, velocity_sigma=0.3)
+    outs = []
+    for _ in range(2):
+        g = make(gpu_lib, sc, MIXED)
+        g.initialize_leapfrog(0.0, sc.dt)
+        g.step(60, 0.0, sc.dt)
+        outs.append(g.download())
+    for k in ["position", "velocity", "force"]:
+        assert np.array_equal(outs[0][k], outs[1][k]), k
