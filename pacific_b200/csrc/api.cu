@@ -83,6 +83,7 @@ struct grains_gpu_ctx {
   bool pending_kick2 = false;
   double pending_dt = 0;
   bool has_basis = false;
+  bool has_convex = false;
   StepArgs<float> af{};
   StepArgs<double> ad{};
   // raw buffer pointers (two copies of particle arrays)
@@ -397,6 +398,7 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   a.n_sys = (int)c->sys.size();
   a.hist_cap = c->hist_cap;
   a.has_basis = c->has_basis ? 1 : 0;
+  a.has_convex = c->has_convex ? 1 : 0;
   a.sys = c->d_sys;
   a.shapes = c->d_shapes;
   a.verts = c->d_verts;
@@ -440,6 +442,7 @@ int with_args(grains_gpu_ctx* c, F f) {
 int sort_now(grains_gpu_ctx* c, int gather_forces) {
   int rc = 0;
   if (!c->keys_valid) {
+    CK(cudaMemsetAsync(c->cell_count, 0, (size_t)c->n_cells * sizeof(int), c->stream));
     rc = with_args(c, [&](auto& a) { return launch_bin(a, c->stream); });
     if (rc) return fail(c, rc, "bin kernel launch failed");
   }
@@ -578,6 +581,7 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
     return GRAINS_GPU_CUDA_ERROR;
   }
   for (int k = 0; k < 2; ++k) cudaMemsetAsync(c->hist_n[k], 0, N * sizeof(int), c->stream);
+  cudaMemsetAsync(c->perm, 0, N * sizeof(int), c->stream);
   cudaMemsetAsync(c->stats, 0, sizeof(StatsDev), c->stream);
   cudaStreamSynchronize(c->stream);
   *out = c;
@@ -689,9 +693,13 @@ int grains_gpu_set_contact_law(grains_gpu_ctx* c, int32_t system, int32_t a, int
 int grains_gpu_set_obstacles(grains_gpu_ctx* c, int32_t system, int32_t n, const grains_gpu_obstacle* o) {
   if (!c || (n > 0 && !o)) return GRAINS_GPU_INVALID_ARGUMENT;
   if (system < 0 || system >= (int)c->sys.size()) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "bad system index");
-  for (int i = 0; i < n; ++i)
+  const int maxmat = c->cfg.max_materials > 0 ? c->cfg.max_materials : 4;
+  for (int i = 0; i < n; ++i) {
     if (o[i].shape < 0 || o[i].shape >= (int)c->shapes.size())
       return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "obstacle shape id out of range");
+    if (o[i].material < 0 || o[i].material >= maxmat)
+      return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "obstacle material out of range");
+  }
   c->sys[system].obs.assign(o, o + n);
   c->uploaded = false;
   c->tables_dirty = true;
@@ -858,6 +866,10 @@ int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
     c->tables_dirty = false;
   }
   c->has_basis = basis_needed;
+  c->has_convex = basis_needed;
+  for (auto& s : c->sys)
+    for (auto& o : s.obs)
+      if (c->shapes[o.shape].type != GRAINS_GPU_BOX) c->has_convex = true;
   if (basis_needed) {
     for (int k = 0; k < 2; ++k)
       if (!c->buf[k].basis) {

@@ -126,6 +126,7 @@ struct StepArgs {
   int n_sys;
   int hist_cap;          // H
   int has_basis;         // non-spherical particles present
+  int has_convex;        // a pair may need GJK (non-sphere particle or non-box obstacle)
   const SysDev* sys;
   const ShapeDev* shapes;
   const double* verts;   // polyhedron vertices (xyz)

@@ -245,7 +245,13 @@ template <typename R>
 __global__ void scatter_kernel(StepArgs<R> a) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
-  a.perm[a.cell_start[a.key[s]] + a.rank[s]] = s;
+  const unsigned key = a.key[s];
+  const long long slot = (key < (unsigned)a.n_cells) ? (long long)a.cell_start[key] + a.rank[s] : -1;
+  if (slot < 0 || slot >= a.n) {
+    set_status(a.stats, GRAINS_GPU_CUDA_ERROR);
+    return;
+  }
+  a.perm[slot] = s;
 }
 
 // order each cell's slots by particle id; resets the count for the next step
@@ -255,6 +261,7 @@ __global__ void cell_sort_kernel(StepArgs<R> a) {
   if (c >= a.n_cells) return;
   int b = a.cell_start[c], e = a.cell_start[c + 1];
   a.cell_count[c] = 0;
+  if (b < 0 || e > a.n || b > e) return;
   for (int i = b + 1; i < e; ++i) {
     int pi = a.perm[i];
     int idi = a.cur.meta[pi].x;
@@ -272,6 +279,10 @@ __global__ void __launch_bounds__(256) gather_kernel(StepArgs<R> a, int gather_f
   int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.n) return;
   int s = a.perm[t];
+  if (s < 0 || s >= a.n) {
+    set_status(a.stats, GRAINS_GPU_CUDA_ERROR);
+    return;
+  }
   const ParticleArrays<R>& C = a.cur;
   const ParticleArrays<R>& D = a.alt;
   D.xr[t] = C.xr[s];
@@ -440,7 +451,7 @@ __device__ ContactGeom convex_closest_point(const StepArgs<R>& a, const BodyRef&
 // both of its particles; both evaluate the same contact law with the lower id
 // as p0 (same inputs, same instructions -> bit-identical forces of opposite
 // sign), the lower id owns the pair's contact memory.
-template <typename R, bool DIAG>
+template <typename R, bool DIAG, bool CONVEX>
 __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
@@ -486,7 +497,7 @@ __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
         const int4 mj = P.meta[t];
         const ShapeDev shj = a.shapes[mj.z];
         ContactGeom g;
-        if (shi.type == GRAINS_GPU_SPHERE && shj.type == GRAINS_GPU_SPHERE) {
+        if (!CONVEX || (shi.type == GRAINS_GPU_SPHERE && shj.type == GRAINS_GPU_SPHERE)) {
           D3 ab;
           double nab;
           const double dist = sphere_sphere_overlap(A, ra, B, rb, &ab, &nab);
@@ -598,7 +609,7 @@ __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
       const double crust_sum = xadd(mdi.y, O.crust);
       ContactGeom g;
       const ShapeDev& sho = a.shapes[O.shape];
-      if (shi.type == GRAINS_GPU_SPHERE && sho.type == GRAINS_GPU_BOX) {
+      if (!CONVEX || (shi.type == GRAINS_GPU_SPHERE && sho.type == GRAINS_GPU_BOX)) {
         g = sphere_box(Xi, xi.w, crust_sum, ob, oo, d3(sho.ext[0], sho.ext[1], sho.ext[2]));
         if (g.status) {
           set_status(a.stats, GRAINS_GPU_CONTACT_ERROR);
@@ -819,10 +830,18 @@ int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forc
 template <typename R>
 int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag) {
   if (a.n == 0) return 0;
-  if (diag)
-    forces_kernel<R, true><<<grid_for(a.n, 128), 128, 0, s>>>(a, R(dt));
-  else
-    forces_kernel<R, false><<<grid_for(a.n, 128), 128, 0, s>>>(a, R(dt));
+  const int g = grid_for(a.n, 128);
+  if (a.has_convex) {
+    if (diag)
+      forces_kernel<R, true, true><<<g, 128, 0, s>>>(a, R(dt));
+    else
+      forces_kernel<R, false, true><<<g, 128, 0, s>>>(a, R(dt));
+  } else {
+    if (diag)
+      forces_kernel<R, true, false><<<g, 128, 0, s>>>(a, R(dt));
+    else
+      forces_kernel<R, false, false><<<g, 128, 0, s>>>(a, R(dt));
+  }
   return check_launch();
 }
 
