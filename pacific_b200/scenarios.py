@@ -216,6 +216,35 @@ def small_box(n=64, seed=0, velocity_sigma=0.05, spacing=2.04, jitter=0.02, radi
     return Scenario("small_box", shapes, dom, laws, [obs], p, 1.0e-5, 100)
 
 
+def dense_cluster(n=343, seed=0, overlap=0.5e-6, velocity_sigma=0.02, radius=1.0 * MM):
+    """Spheres on a cubic lattice whose spacing is 2r - overlap, so that every
+    lattice neighbour pair (and the outer layer with the walls) starts in
+    contact; small random velocities give tangential motion."""
+    rng = np.random.default_rng(seed)
+    crust = 0.05 * MM
+    spacing = 2 * radius - overlap
+    side_n = int(math.ceil(n ** (1.0 / 3.0)))
+    inner = (side_n - 1) * spacing + 2 * radius - overlap
+    lo = np.zeros(3)
+    hi = np.array([inner, inner, inner * 1.5])
+    k = np.arange(n)
+    ix, iy, iz = k % side_n, (k // side_n) % side_n, k // (side_n * side_n)
+    pos = np.stack([radius - overlap / 2 + ix * spacing, radius - overlap / 2 + iy * spacing,
+                    radius - overlap / 2 + iz * spacing], 1)
+    pos += rng.uniform(-0.2 * overlap, 0.2 * overlap, size=(n, 3))
+    vel = rng.normal(0.0, velocity_sigma, size=(n, 3))
+    r = np.full(n, radius)
+    shapes = [(SPHERE, [radius])]
+    wshapes, obs = box_walls(lo, hi, "xXyYzZ", 0.5 * MM, crust, len(shapes), -1)
+    shapes += wshapes
+    kn = 1.0e5
+    laws = [[(0, 0, HOOKE_MEMORY, hooke_memory_params(kn, 0.9, 0.5, 0.8 * kn)),
+             (0, 1, HOOKE_MEMORY, hooke_memory_params(kn, 0.9, 0.5, 0.8 * kn))]]
+    dom = [dict(origin=lo, size=hi - lo, cell_size=2.0 * radius, gravity=(0.0, 0.0, -9.81))]
+    p = _spheres(n, r, 2500.0, pos, vel, crust)
+    return Scenario("dense_cluster", shapes, dom, laws, [obs], p, 1.0e-5, 100)
+
+
 def apply(sim, sc):
     """Registers shapes, domains, laws and obstacles of `sc` on `sim` and
     uploads the particles.  Returns the shape-id map."""

@@ -17,10 +17,10 @@ from helpers import make, pair_set, rel_err
 pytestmark = pytest.mark.gpu
 
 
-def evolved(oracle_lib, n=300, seed=1, steps=300, sigma=0.3):
+def evolved(oracle_lib, n=343, seed=1, steps=20, sigma=0.05):
     """A dense cluster advanced by the oracle: returns the scenario whose
     particle state (and contact memory) are the oracle's after `steps`."""
-    sc = S.small_box(n, seed=seed, velocity_sigma=sigma)
+    sc = S.dense_cluster(n, seed=seed, velocity_sigma=sigma)
     o = make(oracle_lib, sc)
     o.initialize_leapfrog(0.0, sc.dt)
     o.step(steps, 0.0, sc.dt)
@@ -92,7 +92,7 @@ def test_one_force_evaluation(oracle_lib, gpu_lib, precision):
 
 
 def test_move_and_advance_velocity_fp64(oracle_lib, gpu_lib):
-    sc, mem = evolved(oracle_lib, steps=200)
+    sc, mem = evolved(oracle_lib, steps=10)
     sc.particles["omega"] = np.random.default_rng(3).normal(0, 50.0, size=(sc.n, 3))
     o, g = both(oracle_lib, gpu_lib, sc, mem, FP64)
     for s in (o, g):
@@ -115,7 +115,7 @@ def test_move_and_advance_velocity_fp64(oracle_lib, gpu_lib):
 
 @pytest.mark.parametrize("precision", [FP64, MIXED])
 def test_trajectory_matches_oracle(oracle_lib, gpu_lib, precision):
-    sc, mem = evolved(oracle_lib, steps=150)
+    sc, mem = evolved(oracle_lib, steps=15)
     o, g = both(oracle_lib, gpu_lib, sc, mem, precision)
     t = 0.0
     for s in (o, g):
@@ -134,7 +134,7 @@ def test_trajectory_matches_oracle(oracle_lib, gpu_lib, precision):
 def test_graph_steps_equal_single_steps(gpu_lib):
     """The CUDA-graph replay of the fused step gives the same bits as stepping
     one at a time through the per-phase entry points."""
-    sc = S.small_box(216, seed=11, velocity_sigma=0.3)
+    sc = S.dense_cluster(216, seed=11)
     a = make(gpu_lib, sc, FP64)
     b = make(gpu_lib, sc, FP64)
     for s in (a, b):
@@ -153,7 +153,7 @@ def test_graph_steps_equal_single_steps(gpu_lib):
 
 
 def test_deterministic(gpu_lib):
-    sc = S.small_box(343, seed=5, velocity_sigma=0.3)
+    sc = S.dense_cluster(343, seed=5)
     outs = []
     for _ in range(2):
         g = make(gpu_lib, sc, MIXED)
