@@ -181,7 +181,8 @@ def main():
     import torch
     import torch.distributed as dist
     if world > 1:
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+        import datetime
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(local)
     import pacific_b200
     from pacific_b200 import scenarios as S
@@ -256,115 +257,6 @@ def main():
     e2e_s = float(np.median(e2e_times))
     e2e_value = total_particles * args.chunk / e2e_s
 
-    line = {"metric": "particle-steps/s", "value": v, "unit": "particle-steps/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
-            "dtype": "f64", "data": "synthetic", "scaling": "weak",
-            "config": {"workload": sc.name, "particles": sc.n, "dem_steps_per_step": steps},
-            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": 1, "kind": b["kind"],
-                             "sample": b["sample"]},
-            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "vs_baseline": None}
-    print(json.dumps(line), flush=True)
-
-
-def main():
-    args = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        return run_reference(args, rank, world)
-
-    import torch
-    import torch.distributed as dist
-    if world > 1:
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
-    torch.cuda.set_device(local)
-    import pacific_b200
-    from pacific_b200 import scenarios as S
-    from pacific_b200.abi import FP64, MIXED, Simulation
-
-    lib = pacific_b200.load_library()
-    prec = MIXED if args.precision == "mixed" else FP64
-    sc = scenario(args.workload)
-    sim = Simulation(lib, prec, max_particles=sc.n, n_systems=len(sc.domains), device=local)
-    S.apply(sim, sc)
-    sim.initialize_leapfrog(0.0, sc.dt)
-    stream = torch.cuda.ExternalStream(sim.stream_handle(), device=local)
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:%d" % local)
-
-    t = 0.0
-    for _ in range(args.warmup):
-        t = sim.step(args.chunk, t, sc.dt)
-    sim.synchronize()
-
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
-        for k in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(k & 0xFF)          # L2 flush between timed chunks (untimed)
-                ev[k][0].record(stream)
-            t = sim.step(args.chunk, t, sc.dt)
-            ev[k][1].record(stream)
-        torch.cuda.synchronize()
-        sim.synchronize()
-    ms = sum(a.elapsed_time(b) for a, b in ev)
-    if world > 1:
-        tt = torch.tensor([ms], device="cuda:%d" % local, dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-        dist.barrier()
-    st = sim.stats()
-    total_particles = sc.n * world
-    value = total_particles * args.chunk * args.steps / (ms / 1e3)
-
-    # dominant kernel: per-kernel CUDA-event timing of uncaptured steps
-    t, prof = sim.profile_kernels(20, t, sc.dt)
-    fk_ms, fk_n = prof["forces"]
-    st2 = sim.stats()
-    z = 2.0 * (st2["n_contacts"]) / max(1, st2["n_steps_done"] and sc.n) / max(1, (st2["n_steps_done"] or 1))
-    sim.reset_stats()
-    sim.compute_forces(t, sc.dt)
-    st3 = sim.stats()
-    z = (2.0 * st3["n_contacts"] + st3["n_obstacle_contacts"]) / sc.n
-    base, per_contact = FORCES_BYTES[args.precision]
-    alg_bytes = sc.n * (base + per_contact * z / 2.0)
-    achieved = alg_bytes / (fk_ms / fk_n / 1e3) / 1e9
-    peak, peak_kind = measured_peaks()
-    traffic = profiled_traffic("forces", sc.name, args.precision)
-
-    # end to end through the C ABI with host buffers
-    host = sim.download()
-    up = dict(sc.particles)
-    for k in ["position", "quaternion", "velocity", "omega"]:
-        up[k] = host[k]
-    up["basis"] = None
-    ids = [0]
-    e2e_times = []
-    h2d = sum(np.asarray(up[k]).nbytes for k in ["id", "shape", "material", "radius", "crust", "mass", "inertia",
-                                                 "position", "quaternion", "velocity", "omega"])
-    d2h = 0
-    for k in range(args.e2e_steps + 1):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        p = dict(up)
-        p["shape"] = np.zeros(sc.n, np.int32) + ids[0]
-        sim.upload(p)
-        sim.initialize_leapfrog(t, sc.dt)
-        t = sim.step(args.chunk, t, sc.dt)
-        out = sim.download()
-        el = time.perf_counter() - t0
-        d2h = sum(v.nbytes for v in out.values())
-        for kk in ["position", "quaternion", "velocity", "omega"]:
-            up[kk] = out[kk]
-        if k > 0:
-            e2e_times.append(el)
-    e2e_s = float(np.median(e2e_times))
-    e2e_value = total_particles * args.chunk / e2e_s
-
     line = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -372,7 +264,8 @@ def main():
         "dtype": "f32+f64" if args.precision == "mixed" else "f64",
         "data": "synthetic",
         "config": {"workload": sc.name, "particles_per_gpu": sc.n, "precision": args.precision,
-                   "dem_steps_per_step": args.chunk, "dt": sc.dt, "parallelism": "replicas" if world > 1 else "1gpu",
+                   "dem_steps_per_step": args.chunk, "dt": sc.dt,
+                   "parallelism": "replicas" if world > 1 else "1gpu",
                    "l2": "flushed (256 MiB write) between timed steps"},
         "gpu_launches": int(sim.launches_per_step() * args.chunk * args.steps),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -383,8 +276,8 @@ def main():
                 "d2h_bytes_per_step": int(d2h)},
         "kernels_ms_per_dem_step": {k: v[0] / n_prof for k, v in prof.items()},
         "status": st["status"],
+        "clocks": clk.summary(),
     }
-    line["clocks"] = clk.summary()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scenario(args.workload), args.cpu_steps)
     if rank == 0:

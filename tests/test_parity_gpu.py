@@ -114,21 +114,36 @@ def test_move_and_advance_velocity_fp64(oracle_lib, gpu_lib):
 
 
 @pytest.mark.parametrize("precision", [FP64, MIXED])
-def test_trajectory_matches_oracle(oracle_lib, gpu_lib, precision):
+def test_short_trajectory_matches_oracle(oracle_lib, gpu_lib, precision):
+    """5 KDK steps of a dense cluster from identical states."""
     sc, mem = evolved(oracle_lib, steps=15)
     o, g = both(oracle_lib, gpu_lib, sc, mem, precision)
-    t = 0.0
     for s in (o, g):
-        s.compute_forces(t, sc.dt)
-    steps = 40
-    to = o.step(steps, t, sc.dt)
-    tg = g.step(steps, t, sc.dt)
-    assert to == pytest.approx(tg)
+        s.compute_forces(0.0, sc.dt)
+    o.step(5, 0.0, sc.dt)
+    g.step(5, 0.0, sc.dt)
     do, dg = o.download(), g.download()
-    pos_tol = 1e-12 if precision == FP64 else 1e-8
-    assert np.max(np.abs(dg["position"] - do["position"])) < pos_tol
-    vel_tol = 1e-9 if precision == FP64 else 1e-4
-    assert np.max(np.abs(dg["velocity"] - do["velocity"])) < vel_tol
+    assert np.max(np.abs(dg["position"] - do["position"])) < (1e-14 if precision == FP64 else 1e-11)
+    assert np.max(np.abs(dg["velocity"] - do["velocity"])) < (1e-10 if precision == FP64 else 1e-5)
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+def test_long_trajectory_statistics(oracle_lib, gpu_lib, precision):
+    """Dense granular dynamics is chaotic: rounding differences grow by orders
+    of magnitude per contact time.  After 300 steps individual trajectories
+    differ, while kinetic energy and coordination agree statistically."""
+    sc, mem = evolved(oracle_lib, steps=15)
+    o, g = both(oracle_lib, gpu_lib, sc, mem, precision)
+    for s in (o, g):
+        s.compute_forces(0.0, sc.dt)
+    o.step(300, 0.0, sc.dt)
+    g.step(300, 0.0, sc.dt)
+    do, dg = o.download(), g.download()
+    m = sc.particles["mass"]
+    ke = lambda d: 0.5 * float(np.sum(m * np.sum(d["velocity"] ** 2, axis=1)))
+    assert abs(ke(dg) - ke(do)) / ke(do) < 0.05
+    assert abs(dg["coordination"].mean() - do["coordination"].mean()) < 0.3
+    assert abs(dg["position"][:, 2].mean() - do["position"][:, 2].mean()) < 1e-5
 
 
 def test_graph_steps_equal_single_steps(gpu_lib):
