@@ -4,9 +4,11 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
                     [--workload polydisperse_200k|settling_1k|adjoint_4k] [--impl reference]
 
-One bench step = one chunk of `--chunk` DEM time steps (default 100) of the
-workload, replayed from CUDA graphs on resident device state.  L2 is flushed
-(a 256 MiB write) between timed chunks.  `value` is particle-steps/s of the
+One bench step = one chunk of `--chunk` DEM time steps (default 1000) of the
+workload, replayed from CUDA graphs on resident device state; the default
+--steps 20 therefore times the whole 20,000-step run from the initial state
+(after W warm-up chunks and a reset).  L2 is flushed (a 256 MiB write)
+between timed chunks.  `value` is particle-steps/s of the
 whole job (all ranks); `e2e` is the same metric through the C ABI with host
 buffers: upload of the state, the chunk, download of the state.
 
@@ -42,12 +44,13 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--chunk", type=int, default=100)
+    ap.add_argument("--chunk", type=int, default=1000)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--workload", default="polydisperse_200k")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--cpu-steps", type=int, default=30)
+    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--ref-dem-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -122,51 +125,83 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def cpu_baseline(sc, steps, lib_path=None):
-    """Times the CPU implementation of the step on a bounded window of the
-    same workload: `steps` DEM steps from the initial state, one core."""
+def quantize_radii(sc, n_classes=64):
+    """The reference builds one particle class per distinct sphere; radii are
+    rounded to n_classes values (spacing 6 um for U[0.8, 1.2] mm) so that its
+    set-up stays tractable at 200k particles."""
+    from pacific_b200 import scenarios as S
+    r = sc.particles["radius"]
+    lo, hi = float(r.min()), float(r.max())
+    if hi <= lo:
+        return sc
+    sc.meta["radius_classes"] = n_classes
+    q = lo + np.round((r - lo) / (hi - lo) * (n_classes - 1)) / (n_classes - 1) * (hi - lo)
+    sc.particles["radius"] = q
+    sc.particles["mass"], sc.particles["inertia"] = S.sphere_mass_inertia(q, 2500.0)
+    return sc
+
+
+def cpu_context(sc):
+    """A context of the CPU implementation: the reference built from its own
+    sources (oracle/_ref) when present, else the oracle restatement."""
     from pacific_b200.abi import FP64, GrainsLib, Simulation
     from pacific_b200 import scenarios as S
     ref = os.path.join(ROOT, "oracle", "_ref", "libgrains_ref.so")
-    if lib_path is None:
-        if os.path.exists(ref):
-            lib_path, prefix, kind = ref, "grains_ref_", "reference"
-        else:
-            lib_path = os.path.join(ROOT, "oracle", "_build", "libgrains_oracle.so")
-            if not os.path.exists(lib_path):
-                subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-s"], check=True)
-            prefix, kind = "grains_oracle_", "port"
-    lib = GrainsLib(lib_path, prefix)
+    if os.path.exists(ref):
+        lib, kind = GrainsLib(ref, "grains_ref_"), "reference"
+        sc = quantize_radii(sc)
+    else:
+        path = os.path.join(ROOT, "oracle", "_build", "libgrains_oracle.so")
+        if not os.path.exists(path):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-s"], check=True)
+        lib, kind = GrainsLib(path, "grains_oracle_"), "port"
     sim = Simulation(lib, FP64, max_particles=sc.n, n_systems=len(sc.domains))
     S.apply(sim, sc)
     sim.initialize_leapfrog(0.0, sc.dt)
+    return sim, kind, sc
+
+
+def cpu_baseline(sc, steps):
+    """Times `steps` DEM steps of the CPU implementation (serial, one core)
+    from the initial state of the same workload."""
+    sim, kind, sc = cpu_context(sc)
     t0 = time.perf_counter()
     sim.step(steps, 0.0, sc.dt)
     el = time.perf_counter() - t0
-    return {"value": sc.n * steps / el, "unit": "particle-steps/s", "cores": 1, "kind": kind,
-            "sample": "%s, %d DEM steps from the initial state after the leapfrog start, serial" % (sc.name, steps)}
+    sample = "%s, %d DEM steps after the leapfrog start, serial" % (sc.name, steps)
+    if "radius_classes" in sc.meta:
+        sample += ", sphere radii rounded to 64 classes (one reference particle class each)"
+    return {"value": sc.n * steps / el, "unit": "particle-steps/s", "cores": 1, "kind": kind, "sample": sample}
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the CPU implementation on the host cores, rank 0 only.
+    One bench step = `--ref-dem-steps` DEM steps of the workload."""
     if rank != 0:
         return
     sc = scenario(args.workload)
-    per = []
+    sim, kind, sc = cpu_context(sc)
+    t = 0.0
     for _ in range(args.warmup):
-        pass
-    steps = max(1, args.cpu_steps // max(1, args.steps))
+        t = sim.step(args.ref_dem_steps, t, sc.dt)
+    per = []
     for _ in range(args.steps):
-        b = cpu_baseline(sc, steps)
-        per.append(b["value"])
-    v = float(np.median(per))
-    line = {"metric": "particle-steps/s", "value": v, "unit": "particle-steps/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
-            "dtype": "f64", "data": "synthetic", "scaling": "weak",
-            "config": {"workload": sc.name, "particles": sc.n, "dem_steps_per_step": steps},
-            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": 1, "kind": b["kind"],
-                             "sample": b["sample"]},
-            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "vs_baseline": None}
+        t0 = time.perf_counter()
+        t = sim.step(args.ref_dem_steps, t, sc.dt)
+        per.append(time.perf_counter() - t0)
+    total = sum(per)
+    v = sc.n * args.ref_dem_steps * args.steps / total
+    sample = "%s, %d DEM steps per bench step from the initial state, serial" % (sc.name, args.ref_dem_steps)
+    if "radius_classes" in sc.meta:
+        sample += ", sphere radii rounded to 64 classes (one reference particle class each)"
+    line = {"metric": "particle-steps/s", "value": v, "unit": "particle-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "impl": "reference", "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "config": {"workload": sc.name, "particles": sc.n, "dem_steps_per_step": args.ref_dem_steps,
+                       "precision": "fp64"},
+            "cpu_baseline": {"value": v, "unit": "particle-steps/s", "cores": 1, "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -201,6 +236,12 @@ def main():
     for _ in range(args.warmup):
         t = sim.step(args.chunk, t, sc.dt)
     sim.synchronize()
+    # the timed run starts again from the initial state: K chunks of the
+    # workload's run (20 x 1000 = the whole 20,000-step run by default)
+    sim.update(sc.particles)
+    sim.reset_stats()
+    sim.initialize_leapfrog(0.0, sc.dt)
+    t = 0.0
 
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     if world > 1:

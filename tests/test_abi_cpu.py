@@ -28,9 +28,10 @@ def test_header_declares_entry_points():
         assert n in names
 
 
-def test_cuda_library_exports_every_declared_symbol(gpu_lib):
+def test_cuda_library_exports_every_declared_symbol():
     import ctypes
-    dll = ctypes.CDLL(gpu_lib.path)
+    import pacific_b200
+    dll = ctypes.CDLL(pacific_b200.LIB_PATH)
     for n in declared():
         assert hasattr(dll, "grains_gpu_" + n), n
 
@@ -44,7 +45,9 @@ def test_oracle_exports_the_same_contract(oracle_lib):
         assert hasattr(dll, "grains_oracle_" + n), n
 
 
-def test_shape_properties_match_reference_formulas(gpu_lib):
+def test_shape_properties_match_reference_formulas():
+    import pacific_b200
+    gpu_lib = pacific_b200.load_library()
     r = 1.0e-3
     vol, circ, inertia = gpu_lib.shape_properties(SPHERE, [r])
     assert vol == 4.0 * math.pi * math.pow(r, 3.0) / 3.0

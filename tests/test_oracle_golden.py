@@ -1,0 +1,62 @@
+"""Pins the CPU oracle to the reference: golden fixtures produced by the
+reference Grains3D built from its own sources (tests/golden/make_golden.py)
+are replayed through the oracle on identical states and memories.
+
+Bars: contact / candidate pair sets and coordination numbers identical;
+forces and torques within 1e-13 relative (floor: the particle weight);
+states after the KDK steps within 1e-14 m / 1e-10 m/s."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from helpers import make, pair_set, rel_err
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CASES = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
+
+
+def load(path):
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    import golden_io as G
+    z = np.load(path)
+    return G, z, G.scenario_from_npz(z)
+
+
+@pytest.mark.parametrize("path", CASES, ids=[os.path.basename(c)[:-4] for c in CASES])
+def test_oracle_matches_reference_fixture(oracle_lib, path):
+    G, z, sc = load(path)
+    sim = make(oracle_lib, sc)
+    sim.upload_contact_memory(G.memory_from(z, "mem_in_"))
+    t = float(z["time"])
+    sim.compute_forces(t, sc.dt)
+    d = sim.download()
+    weight = float(np.min(sc.particles["mass"])) * 9.81
+    assert np.array_equal(d["coordination"], z["coordination"])
+    assert np.array_equal(sim.candidate_pairs(), z["candidate_pairs"])
+    if bool(z["has_contact_pairs"]):
+        assert pair_set(sim.contact_pairs()) == pair_set(z["contact_pairs"])
+    assert rel_err(d["force"], z["force"], weight) < 1e-13
+    assert rel_err(d["torque"], z["torque"], weight * 1e-3) < 1e-12
+    mo = G.memory_from(z, "mem_out_")
+    m = sim.contact_memory()
+    assert set(zip(m["owner"].tolist(), m["other"].tolist())) == set(zip(mo["owner"].tolist(), mo["other"].tolist()))
+    steps = int(z["after_steps"])
+    sim.step(steps, t, sc.dt)
+    d = sim.download()
+    assert np.max(np.abs(d["position"] - z["after_position"])) < 1e-14
+    assert np.max(np.abs(d["velocity"] - z["after_velocity"])) < 1e-10
+    assert np.max(np.abs(d["quaternion"] - z["after_quaternion"])) < 1e-12
+    assert rel_err(d["force"], z["after_force"], weight) < 1e-9
+
+
+def test_fixtures_exercise_the_path():
+    """The fixture set covers particle-particle and wall contacts, memory,
+    rolling friction, the memory-less Hooke law and polydispersity."""
+    names = [os.path.basename(c)[:-4] for c in CASES]
+    for n in ["dense125", "dense216_rolling", "poly_box200", "hooke_dense125", "settling_1k"]:
+        assert n in names
+    z = np.load(os.path.join(HERE, "golden", "dense125.npz"))
+    assert len(z["contact_pairs"]) > 100 and len(z["mem_in_owner"]) > 100
