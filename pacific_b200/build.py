@@ -14,6 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libgrains_gpu.so")
+EXAMPLE = os.path.join(LIBDIR, "grains_host_example")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "nvcc")
 
@@ -59,6 +60,15 @@ def build(verbose=False, force=False):
         r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed: %s\n%s" % (" ".join(cmd), r.stdout))
+    # C++ caller of the adaptor in include/grains_gpu.hpp
+    src = os.path.join(CSRC, "host_example.cpp")
+    hpp = os.path.join(HERE, "..", "include", "grains_gpu.hpp")
+    if force or _newer(EXAMPLE, [src, hpp, LIB]):
+        cmd = ["g++", "-O2", "-std=c++17", src, "-o", EXAMPLE, "-L" + LIBDIR, "-lgrains_gpu",
+               "-Wl,-rpath,$ORIGIN"]
+        r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("example build failed: %s\n%s" % (" ".join(cmd), r.stdout))
     return LIB
 
 

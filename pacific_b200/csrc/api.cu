@@ -104,9 +104,16 @@ struct grains_gpu_ctx {
   int* perm = nullptr;
   int *cell_count = nullptr, *cell_start = nullptr, *block_sums = nullptr;
   StatsDev* stats = nullptr;
-  int* pairs = nullptr;
+  int* clist = nullptr;   // contact lists (scratch of the force evaluation)
+  int* ccount = nullptr;
+  int clist_cap = 0;
+  int64_t clist_alloc = 0;
+  int* pairs = nullptr;  // contact pairs of the last compute_forces (diagnostic)
   int pairs_cap = 0;
   unsigned long long* pairs_n = nullptr;
+  int* cand = nullptr;   // candidate pairs (diagnostic, separate from the contact pairs)
+  int cand_cap = 0;
+  unsigned long long* cand_n = nullptr;
   // tables
   SysDev* d_sys = nullptr;
   ShapeDev* d_shapes = nullptr;
@@ -421,6 +428,9 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   a.hist_next = (HistEntry<R>*)c->hist[1 - c->hcur];
   a.hist_n_next = c->hist_n[1 - c->hcur];
   a.stats = c->stats;
+  a.clist = c->clist;
+  a.ccount = c->ccount;
+  a.clist_cap = c->clist_cap;
   a.pairs = c->pairs;
   a.pairs_cap = c->pairs_cap;
   a.pairs_n = c->pairs_n;
@@ -598,6 +608,8 @@ int grains_gpu_destroy(grains_gpu_ctx* c) {
   for (int k = 0; k < 2; ++k)
     if (c->buf[k].basis) cudaFree(c->buf[k].basis);
   if (c->stage) cudaFree(c->stage);
+  if (c->clist) cudaFree(c->clist);
+  if (c->ccount) cudaFree(c->ccount);
   if (c->stage_basis) cudaFree(c->stage_basis);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -870,6 +882,23 @@ int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
   for (auto& s : c->sys)
     for (auto& o : s.obs)
       if (c->shapes[o.shape].type != GRAINS_GPU_BOX) c->has_convex = true;
+  {
+    // contact lists: 32 slots per particle for spheres, 64 when bounding
+    // spheres of other shapes are listed
+    const int cap_per = c->has_convex ? 64 : 32;
+    const int64_t need = (int64_t)c->cap * cap_per;
+    if (need > c->clist_alloc) {
+      if (c->clist) cudaFree(c->clist);
+      if (c->ccount) cudaFree(c->ccount);
+      void* q = nullptr;
+      CK(cudaMalloc(&q, (size_t)need * sizeof(int)));
+      c->clist = (int*)q;
+      CK(cudaMalloc(&q, (size_t)c->cap * sizeof(int)));
+      c->ccount = (int*)q;
+      c->clist_alloc = need;
+    }
+    c->clist_cap = cap_per;
+  }
   if (basis_needed) {
     for (int k = 0; k < 2; ++k)
       if (!c->buf[k].basis) {
@@ -1310,17 +1339,25 @@ int grains_gpu_get_candidate_pairs(grains_gpu_ctx* c, int32_t system, int32_t in
   if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
   if (!c->sorted)
     if (int rc = sort_now(c, 1)) return rc;
-  CK(cudaMemsetAsync(c->pairs_n, 0, sizeof(unsigned long long), c->stream));
+  if (!c->cand) {
+    void* q = nullptr;
+    c->cand_cap = (int)std::min<int64_t>(48 * c->cap + 4096, (int64_t)1 << 30);
+    CK(cudaMalloc(&q, 2 * (size_t)c->cand_cap * sizeof(int)));
+    c->cand = (int*)q;
+    CK(cudaMalloc(&q, sizeof(unsigned long long)));
+    c->cand_n = (unsigned long long*)q;
+  }
+  CK(cudaMemsetAsync(c->cand_n, 0, sizeof(unsigned long long), c->stream));
   int rc = with_args(c, [&](auto& a) {
-    return launch_candidate_pairs(a, c->stream, system, include_obstacles, c->pairs, c->pairs_cap, c->pairs_n);
+    return launch_candidate_pairs(a, c->stream, system, include_obstacles, c->cand, c->cand_cap, c->cand_n);
   });
   if (rc) return fail(c, rc, "candidate pair launch failed");
   unsigned long long cnt = 0;
-  CK(cudaMemcpyAsync(&cnt, c->pairs_n, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(&cnt, c->cand_n, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  if (cnt > (unsigned long long)c->pairs_cap) return fail(c, GRAINS_GPU_PAIR_OVERFLOW, "device pair buffer too small");
+  if (cnt > (unsigned long long)c->cand_cap) return fail(c, GRAINS_GPU_PAIR_OVERFLOW, "device pair buffer too small");
   std::vector<int> h(2 * cnt);
-  if (cnt) CK(cudaMemcpy(h.data(), c->pairs, 2 * cnt * sizeof(int), cudaMemcpyDeviceToHost));
+  if (cnt) CK(cudaMemcpy(h.data(), c->cand, 2 * cnt * sizeof(int), cudaMemcpyDeviceToHost));
   std::vector<std::pair<int, int>> pp, po;
   for (size_t k = 0; k < cnt; ++k) {
     // particle pairs were emitted as (lower, higher); obstacle pairs as (particle, obstacle id)
@@ -1392,8 +1429,8 @@ int grains_gpu_reset_stats(grains_gpu_ctx* c) {
 
 int grains_gpu_launches_per_step(grains_gpu_ctx* c, int64_t* launches) {
   if (!c || !launches) return GRAINS_GPU_INVALID_ARGUMENT;
-  // kick_move, scan (3), scatter, cell_sort, gather, forces
-  *launches = 8;
+  // kick_move, scan (3), scatter, cell_sort, gather, contacts, forces
+  *launches = 9;
   return 0;
 }
 
@@ -1440,7 +1477,7 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time,
   ms[2] = t_force;
   launches[0] = n_steps;
   launches[1] = 6LL * n_steps;
-  launches[2] = n_steps;
+  launches[2] = 2LL * n_steps;
   *n_kernels = 3;
   return finish_call(c);
 }
@@ -1460,5 +1497,5 @@ int grains_gpu_shape_properties(int32_t type, const double* params, int32_t n, d
 }  // extern "C"
 
 namespace gg {
-int launches_per_fused_step() { return 8; }
+int launches_per_fused_step() { return 9; }
 }  // namespace gg

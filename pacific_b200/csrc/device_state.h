@@ -149,6 +149,9 @@ struct StepArgs {
   HistEntry<R>* hist_next;
   int* hist_n_next;
   StatsDev* stats;
+  int* clist;            // per-particle contact lists (slots), clist_cap entries each
+  int* ccount;
+  int clist_cap;
   int* pairs;            // diagnostic contact pair output (2 ints per pair) or null
   int pairs_cap;
   unsigned long long* pairs_n;

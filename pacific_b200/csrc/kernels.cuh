@@ -447,10 +447,68 @@ __device__ ContactGeom convex_closest_point(const StepArgs<R>& a, const BodyRef&
 }
 
 // ---------------------------------------------------------------------------
-// forces: one thread per particle (cell-sorted order).  Every pair is met by
-// both of its particles; both evaluate the same contact law with the lower id
-// as p0 (same inputs, same instructions -> bit-identical forces of opposite
-// sign), the lower id owns the pair's contact memory.
+// contacts: the broadphase and the exact bounding-sphere test, one thread per
+// particle (cell-sorted order).  For every neighbour j != i of the 27
+// surrounding cells (LinkedCell::ComputeForces as a set, LinkedCell.cpp:
+// 1019-1103) it tests |x_j - x_i| - (r_i + r_j) < 0 in double with the
+// reference's rounding (for spheres this is the contact decision of
+// ClosestPointSPHERESPHERE, RigidBodyWithCrust.cpp:611-613; for other convex
+// bodies the circumscribed-sphere prefilter of ClosestPoint, :279-282) and
+// appends j's slot to the particle's contact list.  Few live registers: the
+// contact law runs in forces_kernel over the lists only.
+template <typename R>
+__global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const ParticleArrays<R>& P = a.cur;
+  const double4 xi = P.xr[s];
+  const SysDev& S = a.sys[P.meta[s].w];
+  const D3 Xi = d3(xi.x, xi.y, xi.z);
+  int ci, cj, ck;
+  cell_of(S, xi.x, xi.y, xi.z, ci, cj, ck);
+  const int i0 = max(ci - 1, 0), i1 = min(ci + 1, S.nbi - 1);
+  int* list = a.clist + (size_t)s * a.clist_cap;
+  int cnt = 0;
+  unsigned long long ncand = 0;
+  for (int dj = -1; dj <= 1; ++dj) {
+    const int j = cj + dj;
+    if (j < 0 || j >= S.nbj) continue;
+    for (int dk = -1; dk <= 1; ++dk) {
+      const int k = ck + dk;
+      if (k < 0 || k >= S.nbk) continue;
+      const int t0 = a.cell_start[cell_index(S, i0, j, k)];
+      const int t1 = a.cell_start[cell_index(S, i1, j, k) + 1];
+      ncand += (unsigned long long)(t1 - t0);
+      for (int t = t0; t < t1; ++t) {
+        const double4 xj = P.xr[t];
+        D3 ab;
+        double nab;
+        // |AB| and r_A + r_B are symmetric in IEEE arithmetic, so the test
+        // gives the same bits whichever body is A
+        const double dist = sphere_sphere_overlap(Xi, xi.w, d3(xj.x, xj.y, xj.z), xj.w, &ab, &nab);
+        if (dist < 0. && t != s) {
+          if (cnt < a.clist_cap) list[cnt] = t;
+          ++cnt;
+        }
+      }
+    }
+  }
+  if (cnt > a.clist_cap) {
+    set_status(a.stats, GRAINS_GPU_PAIR_OVERFLOW);
+    cnt = a.clist_cap;
+  }
+  a.ccount[s] = cnt;
+  ncand -= 1;  // the particle itself
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) ncand += __shfl_down_sync(0xffffffffu, ncand, o);
+  if ((threadIdx.x & 31) == 0 && ncand) atomicAdd(&a.stats->n_cand, ncand);
+}
+
+// ---------------------------------------------------------------------------
+// forces: one thread per particle over its contact list.  Every pair is met
+// by both of its particles; both evaluate the same contact law with the lower
+// id as p0 (same inputs, same instructions -> bit-identical forces of
+// opposite sign) and the lower id owns the pair's contact memory.
 template <typename R, bool DIAG, bool CONVEX>
 __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -470,27 +528,21 @@ __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
   V3<R> F = v3<R>(R(S.gx * mdi.x), R(S.gy * mdi.x), R(S.gz * mdi.x));
   V3<R> T = v3<R>(R(0), R(0), R(0));
   int ncontact = 0, nnext = 0;
-  unsigned long long ncand = 0, nobs_cand = 0, ncont_own = 0, nobs_cont = 0, ngjk = 0, ngjk_it = 0;
+  unsigned long long nobs_cand = 0, ncont_own = 0, nobs_cont = 0, ngjk = 0, ngjk_it = 0;
   double ov_max = 0., ov_sum = 0.;
 
   int ci, cj, ck;
   cell_of(S, xi.x, xi.y, xi.z, ci, cj, ck);
-  const int i0 = max(ci - 1, 0), i1 = min(ci + 1, S.nbi - 1);
 
-  for (int dj = -1; dj <= 1; ++dj) {
-    const int j = cj + dj;
-    if (j < 0 || j >= S.nbj) continue;
-    for (int dk = -1; dk <= 1; ++dk) {
-      const int k = ck + dk;
-      if (k < 0 || k >= S.nbk) continue;
-      const int t0 = a.cell_start[cell_index(S, i0, j, k)];
-      const int t1 = a.cell_start[cell_index(S, i1, j, k) + 1];
-      for (int t = t0; t < t1; ++t) {
-        if (t == s) continue;
+  {
+    const int nlist = a.ccount[s];
+    const int* list = a.clist + (size_t)s * a.clist_cap;
+    for (int q = 0; q < nlist; ++q) {
+      {
+        const int t = list[q];
         const double4 xj = P.xr[t];
         const int idj = P.meta[t].x;
         const bool own = mi.x < idj;
-        if (own) ++ncand;
         const D3 Xj = d3(xj.x, xj.y, xj.z);
         const D3 A = own ? Xi : Xj, B = own ? Xj : Xi;
         const double ra = own ? xi.w : xj.w, rb = own ? xj.w : xi.w;
@@ -674,7 +726,6 @@ __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
   const unsigned full = 0xffffffffu;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
-    ncand += __shfl_down_sync(full, ncand, o);
     nobs_cand += __shfl_down_sync(full, nobs_cand, o);
     ncont_own += __shfl_down_sync(full, ncont_own, o);
     nobs_cont += __shfl_down_sync(full, nobs_cont, o);
@@ -684,7 +735,6 @@ __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
     ov_max = fmax(ov_max, __shfl_down_sync(full, ov_max, o));
   }
   if ((threadIdx.x & 31) == 0) {
-    if (ncand) atomicAdd(&a.stats->n_cand, ncand);
     if (nobs_cand) atomicAdd(&a.stats->n_obs_cand, nobs_cand);
     if (ncont_own) atomicAdd(&a.stats->n_contacts, ncont_own);
     if (nobs_cont) atomicAdd(&a.stats->n_obs_contacts, nobs_cont);
@@ -830,6 +880,7 @@ int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forc
 template <typename R>
 int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag) {
   if (a.n == 0) return 0;
+  contacts_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
   const int g = grid_for(a.n, 128);
   if (a.has_convex) {
     if (diag)
