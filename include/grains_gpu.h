@@ -252,6 +252,37 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* ctx, int32_t n_steps, double* tim
 /* Number of kernel launches one call of grains_gpu_step(n_steps) issues. */
 int grains_gpu_launches_per_step(grains_gpu_ctx* ctx, int64_t* launches);
 
+/* ---- allocation-free contact detection ------------------------------------- */
+/* No counterpart in the reference: an allocation-free variant of the contact
+ * detection of grains_gpu_compute_forces for callers that cannot call
+ * cudaMalloc (code inside a stream capture that must not allocate, real-time
+ * loops that cannot afford cudaMalloc's implicit synchronisation, hosts that
+ * own all device memory through their own pool).  It bins n spheres into the
+ * linked-cell grid of (origin, size, cell_size) (LinkedCell::set rules), sorts
+ * them by cell and writes every pair of input indices (i < j) whose overlap
+ * distance |x_j - x_i| - (r_i + r_j) is negative, decided in double precision
+ * exactly like the context-based path.
+ *   position (3n doubles), radius (n doubles): device arrays, current device
+ *   pairs: device, 2*cap int32; *n_pairs (device int64) = pairs found (may
+ *     exceed cap: only cap are written); *status (device int32) = status bits
+ *     of this call (GRAINS_GPU_OUT_OF_GRID for a sphere outside the grid)
+ *   stream: cudaStream_t (NULL = legacy default stream); the call is
+ *     asynchronous on it.
+ * Limits: n <= 65,536 spheres and at most 262,144 cells; larger inputs return
+ * GRAINS_GPU_INVALID_ARGUMENT without launching anything.  The scratch (about
+ * 11.5 MB) is a file-scope device array present on every GPU that loads the
+ * library until the process exits; every call on a device shares it, so calls
+ * that overlap on the GPU (different streams, or several host threads) race
+ * and must be serialised by the caller.  The first call on a device looks up
+ * the array's device address (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  No cudaMalloc, cudaFree or allocating library
+ * routine is called.  Nothing has to start at zero: each call clears *n_pairs,
+ * *status and the part of the scratch it uses before it writes them. */
+int grains_gpu_sphere_contacts_noalloc(int32_t n, const double* position, const double* radius,
+                                       const double origin[3], const double size[3], double cell_size,
+                                       int32_t* pairs, int64_t cap, int64_t* n_pairs, int32_t* status,
+                                       void* stream);
+
 /* ---- shape helpers (reference geometry formulas, host only) -------------- */
 /* volume, circumscribed radius and body-frame principal inertia per unit
  * density: Sphere.cpp:61-81,152-155; Box.cpp:181-210; Cylinder.cpp:61-85;

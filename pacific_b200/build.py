@@ -22,6 +22,7 @@ UNITS = [
     ("kernels_fp64.cu", ["-fmad=false"]),
     ("kernels_mixed.cu", []),
     ("api.cu", []),
+    ("noalloc.cu", []),
 ]
 HEADERS = ["common.cuh", "sphere_contact.cuh", "contact_law.cuh", "gjk.cuh", "kernels.cuh", "device_state.h"]
 

@@ -13,7 +13,8 @@ from pacific_b200.abi import BOX, CYLINDER, POLYHEDRON, SPHERE
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "grains_gpu.h")
-GPU_ONLY = {"get_stream", "synchronize", "launches_per_step", "profile_kernels", "shape_properties"}
+GPU_ONLY = {"get_stream", "synchronize", "launches_per_step", "profile_kernels", "shape_properties",
+            "sphere_contacts_noalloc"}
 
 
 def declared():
