@@ -2,7 +2,7 @@
 """Benchmark of the Grains3D DEM time step on B200 (pacific_b200).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--precision mixed|fp64]
-                    [--workload polydisperse_200k|settling_1k|adjoint_4k] [--impl reference]
+                    [--workload polydisperse_200k|drum_100k|settling_1k|adjoint_4k] [--impl reference]
 
 One bench step = one chunk of `--chunk` DEM time steps (default 1000) of the
 workload, replayed from CUDA graphs on resident device state; the default
@@ -32,11 +32,25 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# algorithmic HBM bytes per particle and force evaluation of the forces kernel:
-# own state in (position+radius 32, v, w, mass/crust 16, id/material 8, upload index 4),
-# force + torque + coordination + memory count out, owned memory entries read + written
-FORCES_BYTES = {"mixed": (32 + 12 + 12 + 16 + 8 + 4 + 12 + 12 + 4 + 8, 40.0),
-                "fp64": (32 + 24 + 24 + 16 + 8 + 4 + 24 + 24 + 4 + 8, 76.0)}
+# Algorithmic HBM bytes per particle of the two force kernels of a middle step
+# (z = mean coordination number, contacts per particle incl. walls).
+#  contacts_kernel: own position+radius (32) and meta (16) in, the 9 cell-row
+#   ranges (72), list length (4) and z list entries (4 z) out; the neighbours'
+#   positions are re-read from L1/L2 and not counted.
+#  forces_kernel (fused with the move): own state in (xr 32, q 32, meta 16,
+#   md 32, v, w, wbf, inertia, upload index 4, list length 4, z list entries),
+#   the moved state out (xr, q, md 32 each, meta 16, index 4, v, w, wbf, F, T,
+#   inertia, cell key 4, rank 4, coordination 4, memory count 4), and the
+#   contact memory: z entries looked up + z/2 owned entries written.  Bodies
+#   that are not spheres also carry their rotation matrix (72 B in and out).
+def kernel_bytes(kernel, precision, z, basis=False):
+    r4 = 16 if precision == "mixed" else 32
+    entry = 44 if precision == "mixed" else 80
+    if kernel == "contacts":
+        return 32 + 16 + 72 + 4 + 4 * z
+    reads = 32 + 32 + 16 + 32 + 4 * r4 + 4 + 4 + 4 * z + z * entry
+    writes = 32 + 32 + 32 + 16 + 4 + 6 * r4 + 4 * 4 + (z / 2.0) * entry
+    return reads + writes + (144 if basis else 0)
 
 
 def parse():
@@ -58,7 +72,7 @@ def parse():
 def scenario(name):
     from pacific_b200 import scenarios as S
     return {"polydisperse_200k": S.polydisperse_200k, "settling_1k": S.settling_1k,
-            "adjoint_4k": S.adjoint_4k}[name]()
+            "adjoint_4k": S.adjoint_4k, "drum_100k": S.drum}[name]()
 
 
 def measured_peaks():
@@ -132,7 +146,7 @@ def quantize_radii(sc, n_classes=64):
     from pacific_b200 import scenarios as S
     r = sc.particles["radius"]
     lo, hi = float(r.min()), float(r.max())
-    if hi <= lo:
+    if hi <= lo or any(sc.shapes[k][0] != S.SPHERE for k in set(np.asarray(sc.particles["shape"]).tolist())):
         return sc
     sc.meta["radius_classes"] = n_classes
     q = lo + np.round((r - lo) / (hi - lo) * (n_classes - 1)) / (n_classes - 1) * (hi - lo)
@@ -266,19 +280,33 @@ def main():
     total_particles = sc.n * world
     value = total_particles * args.chunk * args.steps / (ms / 1e3)
 
-    # dominant kernel: per-kernel CUDA-event timing of uncaptured steps
-    n_prof = 20
-    t, prof = sim.profile_kernels(n_prof, t, sc.dt)
-    fk_ms, fk_n = prof["forces"]
-    sim.reset_stats()
-    sim.compute_forces(t, sc.dt)
-    st3 = sim.stats()
-    z = (2.0 * st3["n_contacts"] + st3["n_obstacle_contacts"]) / sc.n
-    base, per_contact = FORCES_BYTES[args.precision]
-    alg_bytes = sc.n * (base + per_contact * z / 2.0)
+    # kernel timing over the same run: from the initial state again, the whole
+    # window of K chunks uncaptured with CUDA events around each phase on the
+    # library's stream; the mean coordination is sampled once per chunk
+    sim.update(sc.particles)
+    sim.initialize_leapfrog(0.0, sc.dt)
+    tp = 0.0
+    prof_tot = {}
+    zs = []
+    for k in range(args.steps):
+        tp, prof = sim.profile_kernels(args.chunk, tp, sc.dt)
+        for name, (ms_k, n_k) in prof.items():
+            a0, b0 = prof_tot.get(name, (0.0, 0))
+            prof_tot[name] = (a0 + ms_k, b0 + n_k)
+        sim.reset_stats()
+        sim.compute_forces(tp, sc.dt)
+        st3 = sim.stats()
+        zs.append((2.0 * st3["n_contacts"] + st3["n_obstacle_contacts"]) / sc.n)
+    z = float(np.mean(zs))
+    dom = max(["contacts", "forces"], key=lambda k: prof_tot[k][0])
+    fk_ms, fk_n = prof_tot[dom]
+    basis = any(sc.shapes[k][0] != S.SPHERE for k in set(np.asarray(sc.particles["shape"]).tolist()))
+    alg_bytes = sc.n * kernel_bytes(dom, args.precision, z, basis)
     achieved = alg_bytes / (fk_ms / fk_n / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profiled_traffic("forces", sc.name, args.precision)
+    traffic = profiled_traffic(dom, sc.name, args.precision)
+    n_prof = args.chunk * args.steps
+    prof = prof_tot
 
     # end to end through the C ABI with host buffers: state up, one chunk, state down
     host = sim.download()
@@ -310,12 +338,13 @@ def main():
                    "l2": "flushed (256 MiB write) between timed steps"},
         "gpu_launches": int(sim.launches_per_step() * args.chunk * args.steps),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": "forces_kernel", "peak_source": peak_kind,
+                     "traffic": traffic, "kernel": dom + "_kernel", "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": alg_bytes, "mean_coordination": z,
                      "launch_ms": fk_ms / fk_n},
         "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
         "kernels_ms_per_dem_step": {k: v[0] / n_prof for k, v in prof.items()},
+        "kernel_timing": "uncaptured re-run of the timed window with CUDA events around each phase",
         "status": st["status"],
         "clocks": clk.summary(),
     }

@@ -93,9 +93,11 @@ typedef struct grains_gpu_domain {
 
 /* Obstacle of one system (a Grains SimpleObstacle).  Obstacles are rigid
  * bodies of mass 1e20 (Component.cpp:16) that are moved by imposed kinematics
- * only.  'moving' != 0 marks an obstacle with a constant imposed rotation
- * about 'rotation_center' with angular velocity 'omega' and translation
- * velocity 'velocity' (ObstacleImposedVelocity.cpp:195-208). */
+ * only.  'moving' != 0 marks an obstacle with imposed motion
+ * (ObstacleImposedVelocity.cpp:60-85, 195-208): a ConstantRotation about
+ * 'rotation_center' with angular velocity 'omega' when omega is not zero (its
+ * centre velocity becomes omega x (centre - rotation_center) at each move),
+ * otherwise a ConstantTranslation at 'velocity'. */
 typedef struct grains_gpu_obstacle {
   int32_t id;            /* component id (reference obstacles carry their own ids) */
   int32_t shape;         /* shape id from grains_gpu_add_shape (a BOX for walls) */
@@ -210,7 +212,10 @@ int grains_gpu_download_obstacles(grains_gpu_ctx* ctx, int32_t system, int32_t n
  * of Grains::computeParticlesForceAndTorque (Grains.cpp:459-482) */
 int grains_gpu_compute_forces(grains_gpu_ctx* ctx, double time, double dt);
 /* replaces: AllComponents::Move (AllComponents.cpp:151-222) ->
- * SecondOrderLeapFrog::Move (SecondOrderLeapFrog.cpp:44-69), obstacle motion */
+ * SecondOrderLeapFrog::Move (SecondOrderLeapFrog.cpp:44-69), obstacle motion.
+ * time = the clock after this step's increment (Grains::Simulation adds dt to
+ * m_time before the move); imposed obstacle motion acts over the interval
+ * time - (time - dt_disp), as in ObstacleImposedVelocity::isActif. */
 int grains_gpu_move(grains_gpu_ctx* ctx, double time, double dt_vel, double dt_disp);
 /* replaces: AppCollision::LinkUpdate (LinkedCell.cpp:1452-1547) */
 int grains_gpu_link_update(grains_gpu_ctx* ctx, double time, double dt);

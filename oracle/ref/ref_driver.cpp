@@ -40,6 +40,7 @@
 #include "LinkedCell.hh"
 #include "Obstacle.hh"
 #include "Particle.hh"
+#include "Polyhedron.hh"
 #include "Quaternion.hh"
 #include "ReaderXML.hh"
 #include "RigidBodyWithCrust.hh"
@@ -130,8 +131,41 @@ double density_for(double mass, double vol) {
   return rho;
 }
 
-void convex_xml(std::ostream& o, const ShapeSpec& s, double radius) {
+// polyhedron file of the reference's format (Polyhedron::create,
+// Geometry/src/Polyhedron.cpp:125-160, readFaces :374-408): dimension, vertex
+// count, one vertex per line, a blank line, face count, then one face per line
+// as its vertex indices only, without trailing blanks
+std::string polyhedron_file(const std::string& dir, int shape, const ShapeSpec& s) {
+  const std::string path = dir + "/poly" + std::to_string(shape) + ".txt";
+  std::ofstream f(path.c_str());
+  f.precision(17);
+  const int nv = (int)s.p[0];
+  f << "3\n" << nv << "\n";
+  for (int v = 0; v < nv; ++v) f << s.p[1 + 3 * v] << " " << s.p[2 + 3 * v] << " " << s.p[3 + 3 * v] << "\n";
+  size_t k = 1 + 3 * (size_t)nv;
+  const int nf = (int)s.p[k++];
+  f << "\n" << nf << "\n";
+  for (int q = 0; q < nf; ++q) {
+    const int m = (int)s.p[k++];
+    for (int j = 0; j < m; ++j) f << (j ? " " : "") << (int)s.p[k++];
+    f << "\n";
+  }
+  return path;
+}
+
+// the reference's own volume of a polyhedron file (Polyhedron::getVolume)
+double polyhedron_volume(const std::string& dir, const std::string& path) {
+  const std::string saved = GrainsExec::m_ReloadDirectory;
+  GrainsExec::m_ReloadDirectory = dir;
+  std::istringstream is(GrainsExec::extractFileName(path));
+  Polyhedron* P = Polyhedron::create(is);
+  GrainsExec::m_ReloadDirectory = saved;
+  return P->getVolume();
+}
+
+void convex_xml(std::ostream& o, const ShapeSpec& s, double radius, const std::string& poly_path = "") {
   if (s.type == GRAINS_GPU_SPHERE) o << "<Sphere Radius=\"" << num(radius) << "\"/>";
+  else if (s.type == GRAINS_GPU_POLYHEDRON) o << "<Polyhedron Name=\"" << poly_path << "\"/>";
   else if (s.type == GRAINS_GPU_BOX)
     o << "<Box LX=\"" << num(s.p[0]) << "\" LY=\"" << num(s.p[1]) << "\" LZ=\"" << num(s.p[2]) << "\"/>";
   else if (s.type == GRAINS_GPU_CYLINDER)
@@ -199,7 +233,6 @@ int grains_ref_set_domain(grains_gpu_ctx* c, int32_t system, const grains_gpu_do
 }
 
 int grains_ref_add_shape(grains_gpu_ctx* c, int32_t type, const double* p, int32_t n, int32_t* id) {
-  if (type == GRAINS_GPU_POLYHEDRON) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "polyhedra not wired in the driver");
   c->shapes.push_back(ShapeSpec{type, std::vector<double>(p, p + n)});
   *id = (int)c->shapes.size() - 1;
   return 0;
@@ -230,9 +263,17 @@ int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
   std::vector<Cls> classes;
   std::map<std::string, int> key_of;
   double rmax = 0;
+  std::map<int, std::string> poly_path;
+  std::map<int, double> poly_vol;
+  for (size_t k = 0; k < c->shapes.size(); ++k)
+    if (c->shapes[k].type == GRAINS_GPU_POLYHEDRON) {
+      poly_path[(int)k] = polyhedron_file(c->dir, (int)k, c->shapes[k]);
+      poly_vol[(int)k] = polyhedron_volume(c->dir, poly_path[(int)k]);
+    }
   for (int64_t i = 0; i < n; ++i) {
     const ShapeSpec& s = c->shapes[p->shape[i]];
     double vol = s.type == GRAINS_GPU_SPHERE ? sphere_volume(p->radius[i])
+                 : s.type == GRAINS_GPU_POLYHEDRON ? poly_vol[p->shape[i]]
                  : s.type == GRAINS_GPU_BOX ? s.p[0] * s.p[1] * s.p[2]
                                              : 2 * (s.p[1] / 2.) * kPI * s.p[0] * s.p[0];
     if (s.type == GRAINS_GPU_BOX) vol = 8.0 * (s.p[0] / 2.) * (s.p[1] / 2.) * (s.p[2] / 2.);
@@ -252,7 +293,17 @@ int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
   const grains_gpu_domain& d = c->dom;
   std::ostringstream x;
   x << "<Grains3D Type=\"Standard\">\n<Construction>\n";
-  x << "<LinkedCell MX=\"" << num(d.size[0]) << "\" MY=\"" << num(d.size[1]) << "\" MZ=\"" << num(d.size[2])
+  // the reference's domain is (origin, max corner) with size = max - origin
+  // (App::set_dimensions, Base/src/App.cpp:35-53): a max corner whose
+  // difference with the origin is exactly the requested size
+  double mxyz[3];
+  for (int a = 0; a < 3; ++a) {
+    double m = d.origin[a] + d.size[a];
+    for (int k = 0; k < 8 && m - d.origin[a] != d.size[a]; ++k)
+      m = std::nextafter(m, m - d.origin[a] < d.size[a] ? 1e300 : -1e300);
+    mxyz[a] = m;
+  }
+  x << "<LinkedCell MX=\"" << num(mxyz[0]) << "\" MY=\"" << num(mxyz[1]) << "\" MZ=\"" << num(mxyz[2])
     << "\" CellSizeFactor=\"" << num(d.cell_size / (2. * rmax)) << "\"/>\n";
   x << "<Origin OX=\"" << num(d.origin[0]) << "\" OY=\"" << num(d.origin[1]) << "\" OZ=\"" << num(d.origin[2])
     << "\"/>\n<Periodicity PX=\"0\" PY=\"0\" PZ=\"0\"/>\n";
@@ -277,7 +328,7 @@ int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
   for (auto& k : classes) {
     x << "<Particle Number=\"" << k.members.size() << "\" Density=\"" << num(k.rho) << "\"><Convex CrustThickness=\""
       << num(k.crust) << "\">\n";
-    convex_xml(x, c->shapes[k.shape], k.radius);
+    convex_xml(x, c->shapes[k.shape], k.radius, poly_path.count(k.shape) ? poly_path[k.shape] : "");
     x << "\n</Convex><AngularPosition Type=\"Identity\"></AngularPosition><Material>m" << k.material
       << "</Material></Particle>\n";
   }
@@ -288,8 +339,17 @@ int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
     x << "<Obstacle name=\"o" << k << "\" Type=\"Standard\"><Convex CrustThickness=\"" << num(o.crust) << "\">\n";
     convex_xml(x, s, 0.);
     x << "\n</Convex><Centre X=\"" << num(o.transform[9]) << "\" Y=\"" << num(o.transform[10]) << "\" Z=\""
-      << num(o.transform[11]) << "\"/><AngularPosition Type=\"Identity\"></AngularPosition><Material>m"
-      << o.material << "</Material></Obstacle>\n";
+      << num(o.transform[11]) << "\"/>";
+    bool identity = true;
+    for (int q = 0; q < 9; ++q) identity = identity && o.transform[q] == (q % 4 == 0 ? 1. : 0.);
+    if (identity) {
+      x << "<AngularPosition Type=\"Identity\"></AngularPosition>";
+    } else {  // row-major rotation matrix (Transform::load, Geometry/src/Transform.cpp:510-529)
+      x << "<AngularPosition Type=\"Matrix\">";
+      for (int q = 0; q < 9; ++q) x << (q ? " " : "") << num(o.transform[q]);
+      x << "</AngularPosition>";
+    }
+    x << "<Material>m" << o.material << "</Material></Obstacle>\n";
   }
   x << "</Obstacles>\n</Construction>\n<Forces><Gravity GX=\"" << num(d.gravity[0]) << "\" GY=\"" << num(d.gravity[1])
     << "\" GZ=\"" << num(d.gravity[2]) << "\"/></Forces>\n";
@@ -300,6 +360,29 @@ int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
        "<InitialAngularPosition Type=\"Fixed\"/><RandomGeneratorSeed Type=\"Default\"/><Frequency TryEvery=\"1\"/>"
        "<ForceInsertion Value=\"True\"/><ParticlePosition><File Name=\""
     << c->dir << "/positions.txt\"/></ParticlePosition></ParticleInsertion>\n";
+  // imposed obstacle motion (Grains::AdditionalFeatures, Base/src/Grains.cpp:1719-1745;
+  // ObstacleImposedVelocity.cpp:38-260): a constant rotation about the
+  // obstacle's rotation centre, or a constant translation
+  bool any_moving = false;
+  for (auto& o : c->obs) any_moving = any_moving || o.moving;
+  if (any_moving) {
+    x << "<ObstacleLoadings>\n";
+    for (size_t k = 0; k < c->obs.size(); ++k) {
+      const grains_gpu_obstacle& o = c->obs[k];
+      if (!o.moving) continue;
+      x << "<ObstacleLoading Type=\"Velocity\" ObstacleName=\"o" << k
+        << "\"><TimeInterval Start=\"0.\" End=\"1.e9\"/>";
+      if (o.omega[0] != 0. || o.omega[1] != 0. || o.omega[2] != 0.)
+        x << "<ConstantRotation><AngularVelocity WX=\"" << num(o.omega[0]) << "\" WY=\"" << num(o.omega[1])
+          << "\" WZ=\"" << num(o.omega[2]) << "\"/><RotationCenter CX=\"" << num(o.rotation_center[0]) << "\" CY=\""
+          << num(o.rotation_center[1]) << "\" CZ=\"" << num(o.rotation_center[2]) << "\"/></ConstantRotation>";
+      else
+        x << "<ConstantTranslation><TranslationalVelocity VX=\"" << num(o.velocity[0]) << "\" VY=\""
+          << num(o.velocity[1]) << "\" VZ=\"" << num(o.velocity[2]) << "\"/></ConstantTranslation>";
+      x << "</ObstacleLoading>\n";
+    }
+    x << "</ObstacleLoadings>\n";
+  }
   x << "</Simulation>\n</Grains3D>\n";
   {
     std::ofstream f((c->dir + "/input.xml").c_str());

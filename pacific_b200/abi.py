@@ -355,6 +355,13 @@ class Simulation:
         return {"owner": owner[:k], "other": other[:k], "kdelta": kd[:k], "prev_normal": pn[:k],
                 "spring_torque": sp[:k]}
 
+    def obstacles(self, system, n):
+        """Poses of the first n obstacles of `system` after their imposed
+        motion: (n, 12) = row-major rotation matrix, then the centre."""
+        out = np.zeros((n, 12))
+        self._check(self.lib.fn["download_obstacles"](self.ctx, system, n, _ptr(out, C.c_double)))
+        return out
+
     # ---- the step ----
     def compute_forces(self, time, dt):
         self._check(self.lib.fn["compute_forces"](self.ctx, time, dt))

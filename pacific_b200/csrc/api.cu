@@ -104,6 +104,7 @@ struct grains_gpu_ctx {
   int* perm = nullptr;
   int *cell_count = nullptr, *cell_start = nullptr, *block_sums = nullptr;
   StatsDev* stats = nullptr;
+  double* clock = nullptr;  // the reference's m_time, advanced by the obstacle moves
   int* clist = nullptr;   // contact lists (scratch of the force evaluation)
   int* ccount = nullptr;
   int clist_cap = 0;
@@ -123,6 +124,7 @@ struct grains_gpu_ctx {
   void* d_laws = nullptr;
   std::vector<SysDev> h_sys;
   std::vector<ObstacleDev> h_obs;
+  int n_moving = 0;  // moving obstacles over all systems
   // graphs of two fused steps, by the starting (cur, hcur) buffer selection
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   double graph_dt[4] = {0, 0, 0, 0};
@@ -279,8 +281,12 @@ ObstacleDev obstacle_dev(const grains_gpu_obstacle& o, const ShapeHost& sh) {
   for (int i = 0; i < 9; ++i) d.b[i] = o.transform[i];
   for (int i = 0; i < 3; ++i) d.o[i] = o.transform[9 + i];
   for (int i = 0; i < 3; ++i) {
-    d.vel[i] = o.velocity[i];
-    d.omega[i] = o.omega[i];
+    // velocities are zero until the first move (Grains.cpp:124 sets them at
+    // the start time, when an imposed motion starting then is not active yet)
+    d.vel[i] = 0.;
+    d.omega[i] = 0.;
+    d.ivel[i] = o.velocity[i];
+    d.iomega[i] = o.omega[i];
     d.rot_center[i] = o.rotation_center[i];
   }
   d.crust = o.crust;
@@ -499,26 +505,62 @@ int flush_kick(grains_gpu_ctx* c) {
   return rc ? fail(c, rc, "advance-velocity launch failed") : 0;
 }
 
-int forces_now(grains_gpu_ctx* c, double dt, int diag) {
+int forces_now(grains_gpu_ctx* c, double dt, int diag, int fused = 0, int phases = 3) {
   if (!c->sorted) {
     if (int rc = sort_now(c, 1)) return rc;
   }
-  int rc = with_args(c, [&](auto& a) { return launch_forces(a, c->stream, dt, diag); });
+  int rc = with_args(c, [&](auto& a) {
+    a.dt_disp = dt;
+    return launch_forces(a, c->stream, dt, diag, fused, phases);
+  });
   if (rc) return fail(c, rc, "force kernel launch failed");
-  c->hcur = 1 - c->hcur;
+  if (phases & 2) {
+    c->hcur = 1 - c->hcur;
+    if (fused) {  // the moved state is in the other buffer, keys computed
+      c->cur = 1 - c->cur;
+      c->keys_valid = true;
+      c->sorted = false;
+    }
+  }
   return 0;
 }
 
-// One fused DEM step (pending kick2 + move, sort, gather, forces)
-int fused_step(grains_gpu_ctx* c, double dt) {
+// moving obstacles follow the particles' drift (AllComponents::Move,
+// AllComponents.cpp:166-215)
+// from_host: 'time' is the clock after this step's increment, given by the
+// host (and stored in the device clock); otherwise the device clock advances
+// by dt, as Grains::Simulation advances m_time
+int move_obstacles(grains_gpu_ctx* c, double dt, int from_host = 0, double time = 0.) {
+  if (c->n_moving == 0) return 0;
+  int rc = launch_obstacle_move(c->d_obs, c->d_moving, c->n_moving, c->d_shapes, c->d_verts, dt, c->clock,
+                                time, from_host, c->stream);
+  return rc ? fail(c, rc, "obstacle move launch failed") : 0;
+}
+
+// First step of a run: move (finishing a pending second half kick), keys
+int first_move(grains_gpu_ctx* c, double dt, double time) {
   int rc = with_args(c, [&](auto& a) {
-    return launch_kick_move(a, c->stream, c->pending_kick2 ? 1 : 0, 0.5 * dt, 1, 0.5 * dt, dt);
+    return launch_kick_move(a, c->stream, c->pending_kick2 ? 1 : 0, c->pending_dt, 1, 0.5 * dt, dt);
   });
   if (rc) return fail(c, rc, "kick/move launch failed");
+  c->pending_kick2 = false;
   c->keys_valid = true;
   c->sorted = false;
-  if ((rc = sort_now(c, 0))) return rc;
-  if ((rc = forces_now(c, dt, 0))) return rc;
+  return move_obstacles(c, dt, 1, time + dt);
+}
+
+// A middle step: sort, contact lists, forces fused with the rest of the step
+// and the next step's first half kick and drift
+int fused_middle_step(grains_gpu_ctx* c, double dt) {
+  if (int rc = sort_now(c, 0)) return rc;
+  if (int rc = forces_now(c, dt, 0, 1)) return rc;
+  return move_obstacles(c, dt);
+}
+
+// The last step of a run: sort and forces; the second half kick stays pending
+int last_step(grains_gpu_ctx* c, double dt) {
+  if (int rc = sort_now(c, 0)) return rc;
+  if (int rc = forces_now(c, dt, 0, 0)) return rc;
   c->pending_kick2 = true;
   c->pending_dt = 0.5 * dt;
   return 0;
@@ -583,7 +625,8 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
     c->pairs_cap = (int)std::min<size_t>(16 * N + 1024, (size_t)1 << 30);
     c->pairs = dalloc<int>(2 * (size_t)c->pairs_cap, c->pool);
     c->pairs_n = dalloc<unsigned long long>(1, c->pool);
-    ok = c->coord && c->key && c->rank && c->perm && c->stats && c->pairs && c->pairs_n;
+    c->clock = dalloc<double>(1, c->pool);
+    ok = c->coord && c->key && c->rank && c->perm && c->stats && c->pairs && c->pairs_n && c->clock;
   }
   if (!ok) {
     c->err = "cudaMalloc failed for the requested capacity";
@@ -770,6 +813,7 @@ int build_tables(grains_gpu_ctx* c) {
   }
   cstart.push_back((int)cidx.size());
   c->n_cells = cells;
+  c->n_moving = (int)moving.size();
   c->h_sys = hs;
   c->h_obs = ho;
   // laws
@@ -1223,8 +1267,20 @@ int grains_gpu_download_obstacles(grains_gpu_ctx* c, int32_t system, int32_t n, 
   if (!c || !t) return GRAINS_GPU_INVALID_ARGUMENT;
   if (system < 0 || system >= (int)c->sys.size()) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "bad system");
   const SysHost& s = c->sys[system];
-  for (int i = 0; i < n && i < (int)s.obs.size(); ++i)
-    for (int k = 0; k < 12; ++k) t[12 * i + k] = s.obs[i].transform[k];
+  if (!c->uploaded || c->h_sys.empty()) {
+    for (int i = 0; i < n && i < (int)s.obs.size(); ++i)
+      for (int k = 0; k < 12; ++k) t[12 * i + k] = s.obs[i].transform[k];
+    return 0;
+  }
+  const int first = c->h_sys[system].obs_offset, cnt = c->h_sys[system].n_obs;
+  std::vector<ObstacleDev> h(cnt);
+  if (cnt) CK(cudaMemcpyAsync(h.data(), c->d_obs + first, cnt * sizeof(ObstacleDev), cudaMemcpyDeviceToHost,
+                              c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < n && i < cnt; ++i) {
+    for (int k = 0; k < 9; ++k) t[12 * i + k] = h[i].b[k];
+    for (int k = 0; k < 3; ++k) t[12 * i + 9 + k] = h[i].o[k];
+  }
   return 0;
 }
 
@@ -1239,7 +1295,6 @@ int grains_gpu_compute_forces(grains_gpu_ctx* c, double time, double dt) {
 }
 
 int grains_gpu_move(grains_gpu_ctx* c, double time, double dt_v, double dt_x) {
-  (void)time;
   if (!c) return GRAINS_GPU_INVALID_ARGUMENT;
   if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
   if (int rc = flush_kick(c)) return rc;
@@ -1250,6 +1305,7 @@ int grains_gpu_move(grains_gpu_ctx* c, double time, double dt_v, double dt_x) {
   if (rc) return fail(c, rc, "move launch failed");
   c->keys_valid = true;
   c->sorted = false;
+  if ((rc = move_obstacles(c, dt_x, 1, time))) return rc;
   return finish_call(c);
 }
 
@@ -1283,17 +1339,16 @@ int grains_gpu_initialize_leapfrog(grains_gpu_ctx* c, double time, double dt) {
 int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt) {
   if (!c || !time || n_steps < 0 || !(dt > 0)) return GRAINS_GPU_INVALID_ARGUMENT;
   if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  if (n_steps == 0) return 0;
   if (!c->sorted)
     if (int rc = sort_now(c, 1)) return rc;
-  int left = n_steps;
-  // the first step of a run has no pending half kick; run it outside the graph
-  while (left > 0 && !c->pending_kick2) {
-    if (int rc = fused_step(c, dt)) return rc;
-    --left;
-    *time += dt;
-  }
-  while (left >= 2) {
-    const int slot = 2 * c->cur + c->hcur;  // graph keyed by the starting buffer selection
+  // step 1 moves (finishing any pending half kick); steps 1..n-1 end with the
+  // fused force kernel, which already moves to the next step; step n ends
+  // with a plain force evaluation and leaves its second half kick pending
+  if (int rc = first_move(c, dt, *time)) return rc;
+  int middle = n_steps - 1;
+  while (middle >= 2) {
+    const int slot = 2 * c->cur + c->hcur;  // two middle steps restore (cur, hcur)
     if (!c->graph[slot] || c->graph_dt[slot] != dt) {
       if (c->graph[slot]) {
         cudaGraphExecDestroy(c->graph[slot]);
@@ -1302,11 +1357,13 @@ int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt)
       const int cur0 = c->cur, h0 = c->hcur;
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      int rc = fused_step(c, dt);
-      if (!rc) rc = fused_step(c, dt);
+      int rc = fused_middle_step(c, dt);
+      if (!rc) rc = fused_middle_step(c, dt);
       cudaError_t e = cudaStreamEndCapture(c->stream, &g);
-      c->cur = cur0;  // capture does not execute: restore the buffer parity
+      c->cur = cur0;  // capturing does not execute: restore the buffer selection
       c->hcur = h0;
+      c->keys_valid = true;
+      c->sorted = false;
       if (rc) return rc;
       if (e != cudaSuccess) return cuda_fail(c, e, "cudaStreamEndCapture");
       e = cudaGraphInstantiate(&c->graph[slot], g, 0);
@@ -1315,15 +1372,12 @@ int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt)
       c->graph_dt[slot] = dt;
     }
     CK(cudaGraphLaunch(c->graph[slot], c->stream));
-    // two steps flip cur twice and hcur twice: parity unchanged
-    left -= 2;
-    *time += 2 * dt;
+    middle -= 2;
   }
-  while (left > 0) {
-    if (int rc = fused_step(c, dt)) return rc;
-    --left;
-    *time += dt;
-  }
+  if (middle == 1)
+    if (int rc = fused_middle_step(c, dt)) return rc;
+  if (int rc = last_step(c, dt)) return rc;
+  for (int k = 0; k < n_steps; ++k) *time += dt;  // Grains::Simulation's clock
   c->steps_done += n_steps;
   return 0;
 }
@@ -1429,56 +1483,66 @@ int grains_gpu_reset_stats(grains_gpu_ctx* c) {
 
 int grains_gpu_launches_per_step(grains_gpu_ctx* c, int64_t* launches) {
   if (!c || !launches) return GRAINS_GPU_INVALID_ARGUMENT;
-  // kick_move, scan (3), scatter, cell_sort, gather, contacts, forces
-  *launches = 9;
+  // middle steps: scan (3), scatter, cell_sort, gather, contacts, forces (fused move)
+  *launches = 8;
   return 0;
 }
 
 int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt, char* names,
                                size_t cap, double* ms, int64_t* launches, int32_t max_kernels, int32_t* n_kernels) {
-  if (!c || !time || !names || !ms || !launches || !n_kernels || max_kernels < 3)
+  if (!c || !time || !names || !ms || !launches || !n_kernels || max_kernels < 4)
     return GRAINS_GPU_INVALID_ARGUMENT;
   if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  if (n_steps < 2) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "profile at least 2 steps");
   if (!c->sorted)
     if (int rc = sort_now(c, 1)) return rc;
-  cudaEvent_t ev[4];
+  // same schedule as grains_gpu_step, uncaptured, with events around each phase
+  cudaEvent_t ev[5];
   for (auto& e : ev) CK(cudaEventCreate(&e));
-  double t_move = 0, t_sort = 0, t_force = 0;
+  double acc[4] = {0, 0, 0, 0};  // first move, sort+gather, contact lists, contact law (+fused move)
+  int64_t cnt[4] = {0, 0, 0, 0};
+  CK(cudaEventRecord(ev[0], c->stream));
+  if (int rc = first_move(c, dt, *time)) return rc;
+  CK(cudaEventRecord(ev[1], c->stream));
+  CK(cudaEventSynchronize(ev[1]));
+  float m = 0;
+  cudaEventElapsedTime(&m, ev[0], ev[1]);
+  acc[0] += m;
+  cnt[0] += 1;
   for (int k = 0; k < n_steps; ++k) {
-    CK(cudaEventRecord(ev[0], c->stream));
-    int rc = with_args(c, [&](auto& a) {
-      return launch_kick_move(a, c->stream, c->pending_kick2 ? 1 : 0, 0.5 * dt, 1, 0.5 * dt, dt);
-    });
-    if (rc) return fail(c, rc, "kick/move launch failed");
-    c->keys_valid = true;
-    c->sorted = false;
+    const bool last = (k == n_steps - 1);
     CK(cudaEventRecord(ev[1], c->stream));
-    if ((rc = sort_now(c, 0))) return rc;
+    if (int rc = sort_now(c, 0)) return rc;
     CK(cudaEventRecord(ev[2], c->stream));
-    if ((rc = forces_now(c, dt, 0))) return rc;
+    if (int rc = forces_now(c, dt, 0, last ? 0 : 1, 1)) return rc;
     CK(cudaEventRecord(ev[3], c->stream));
-    c->pending_kick2 = true;
-    c->pending_dt = 0.5 * dt;
-    CK(cudaEventSynchronize(ev[3]));
+    if (int rc = forces_now(c, dt, 0, last ? 0 : 1, 2)) return rc;
+    if (!last)
+      if (int rc = move_obstacles(c, dt)) return rc;
+    CK(cudaEventRecord(ev[4], c->stream));
+    CK(cudaEventSynchronize(ev[4]));
     float a = 0, b = 0, d = 0;
-    cudaEventElapsedTime(&a, ev[0], ev[1]);
-    cudaEventElapsedTime(&b, ev[1], ev[2]);
-    cudaEventElapsedTime(&d, ev[2], ev[3]);
-    t_move += a;
-    t_sort += b;
-    t_force += d;
-    *time += dt;
+    cudaEventElapsedTime(&a, ev[1], ev[2]);
+    cudaEventElapsedTime(&b, ev[2], ev[3]);
+    cudaEventElapsedTime(&d, ev[3], ev[4]);
+    acc[1] += a;
+    acc[2] += b;
+    acc[3] += d;
+    cnt[1] += 6;
+    cnt[2] += 1;
+    cnt[3] += 1;
   }
+  c->pending_kick2 = true;
+  c->pending_dt = 0.5 * dt;
   for (auto& e : ev) cudaEventDestroy(e);
+  for (int k = 0; k < n_steps; ++k) *time += dt;
   c->steps_done += n_steps;
-  std::snprintf(names, cap, "kick_move\nsort_gather\nforces");
-  ms[0] = t_move;
-  ms[1] = t_sort;
-  ms[2] = t_force;
-  launches[0] = n_steps;
-  launches[1] = 6LL * n_steps;
-  launches[2] = 2LL * n_steps;
-  *n_kernels = 3;
+  std::snprintf(names, cap, "kick_move\nsort_gather\ncontacts\nforces");
+  for (int k = 0; k < 4; ++k) {
+    ms[k] = acc[k];
+    launches[k] = cnt[k];
+  }
+  *n_kernels = 4;
   return finish_call(c);
 }
 
@@ -1497,5 +1561,5 @@ int grains_gpu_shape_properties(int32_t type, const double* params, int32_t n, d
 }  // extern "C"
 
 namespace gg {
-int launches_per_fused_step() { return 9; }
+int launches_per_fused_step() { return 8; }
 }  // namespace gg

@@ -70,7 +70,8 @@ struct ObstacleDev {
   double b[9];   // basis
   double o[3];   // origin
   double bbc[3], bbe[3];  // world AABB centre / half extent
-  double vel[3], omega[3];  // velocity of the obstacle centre, angular velocity
+  double vel[3], omega[3];  // current velocity of the centre and angular velocity (zero until the first move)
+  double ivel[3], iomega[3];  // imposed motion: translation velocity, or angular velocity about rot_center
   double rot_center[3];
   double crust;
   double circ;
@@ -156,6 +157,7 @@ struct StepArgs {
   int pairs_cap;
   unsigned long long* pairs_n;
   double gjk_tol;
+  double dt_disp;        // drift time step of the fused force kernel
 };
 
 // kernel launchers, instantiated for float and double
@@ -166,8 +168,11 @@ template <typename R>
 int launch_bin(const StepArgs<R>& a, cudaStream_t s);
 template <typename R>
 int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forces);
+// fused != 0: forces + the rest of the step + the next step's first half kick
+// and drift, into the alternate buffer (then swap cur/alt)
+// phases: 1 = contact lists, 2 = contact law, 3 = both
 template <typename R>
-int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag);
+int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int fused, int phases = 3);
 template <typename R>
 int launch_zero_kdelta(const StepArgs<R>& a, cudaStream_t s);
 // stage: 13 doubles per particle in upload order (position 3, quaternion 4,
@@ -177,6 +182,10 @@ int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const double* st
 template <typename R>
 int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int include_obstacles, int* out,
                            int cap, unsigned long long* count);
+// moves every moving obstacle over dt (defined in kernels_mixed.cu)
+int launch_obstacle_move(ObstacleDev* obs, const int* moving_idx, int n_moving, const ShapeDev* shapes,
+                         const double* verts, double dt, double* clock, double host_time, int use_host_time,
+                         cudaStream_t s);
 // number of kernel launches issued by one fused step
 int launches_per_fused_step();
 

@@ -83,26 +83,26 @@ __device__ __forceinline__ V3<R> rk3(bool sphere, V3<R> I, V3<R> Tbf, V3<R> wbf,
 }
 
 // ---------------------------------------------------------------------------
-// kick_move: optional pending second half kick, then ParticleKinematics::Move
-// (ParticleKinematics.cpp:62-105) and the cell key of the new position.
+// integrate: optional pending second half kick (SecondOrderLeapFrog::
+// advanceVelocity, SecondOrderLeapFrog.cpp:74-95), then ParticleKinematics::
+// Move (ParticleKinematics.cpp:62-105) and the cell key of the new position.
+// Reads particle s of `src`, writes it to slot s of `dst` (dst == src: in
+// place).  F and T are the torsor of the last force evaluation.
 template <typename R>
-__global__ void __launch_bounds__(256) kick_move_kernel(StepArgs<R> a, int do_kick2, R dt_kick2, int do_move,
-                                                        R dt_v, double dt_x) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n) return;
-  const ParticleArrays<R>& P = a.cur;
-  double4 xr = P.xr[s];
-  double4 qd = P.q[s];
-  int4 meta = P.meta[s];
-  double4 md = P.md[s];
-  V3<R> F = ld3<R>(P.F[s]), T = ld3<R>(P.T[s]);
-  V3<R> v = ld3<R>(P.v[s]), w = ld3<R>(P.w[s]), wbf = ld3<R>(P.wbf[s]);
-  V3<R> I = ld3<R>(P.inertia[s]);
+__device__ __forceinline__ void integrate(const StepArgs<R>& a, const ParticleArrays<R>& src,
+                                          const ParticleArrays<R>& dst, int s, V3<R> F, V3<R> T, int do_kick2,
+                                          R dt_kick2, int do_move, R dt_v, double dt_x) {
+  double4 xr = src.xr[s];
+  const double4 qd = src.q[s];
+  const int4 meta = src.meta[s];
+  const double4 md = src.md[s];
+  V3<R> v = ld3<R>(src.v[s]), w = ld3<R>(src.w[s]), wbf = ld3<R>(src.wbf[s]);
+  const V3<R> I = ld3<R>(src.inertia[s]);
   const bool sphere = a.shapes[meta.z].type == 0;
   const R mass = R(md.x);
   Qt<double> q{v3<double>(qd.x, qd.y, qd.z), qd.w};
-  Qt<R> qr{v3<R>(R(qd.x), R(qd.y), R(qd.z)), R(qd.w)};
-  if (do_kick2) {  // SecondOrderLeapFrog::advanceVelocity (SecondOrderLeapFrog.cpp:74-95)
+  const Qt<R> qr{v3<R>(R(qd.x), R(qd.y), R(qd.z)), R(qd.w)};
+  if (do_kick2) {
     V3<R> Tbf = q_to_body(qr, T);
     v = v + sc(dv(F, mass * R(1)), dt_kick2);
     wbf = rk3(sphere, I, Tbf, wbf, dt_kick2);
@@ -128,13 +128,11 @@ __global__ void __launch_bounds__(256) kick_move_kernel(StepArgs<R> a, int do_ki
     q = qmul(dq, q);
     if (a.has_basis && !sphere) {
       M3 b;
-      for (int t = 0; t < 9; ++t) b.m[t] = P.basis[9 * (size_t)s + t];
+      for (int t = 0; t < 9; ++t) b.m[t] = src.basis[9 * (size_t)s + t];
       mrotate_left(b, dq);
-      for (int t = 0; t < 9; ++t) P.basis[9 * (size_t)s + t] = b.m[t];
+      for (int t = 0; t < 9; ++t) dst.basis[9 * (size_t)s + t] = b.m[t];
     }
     if (norm(tm) > md.y) set_status(a.stats, GRAINS_GPU_MOTION_ERROR);
-    P.xr[s] = xr;
-    P.q[s] = make_double4(q.v.x, q.v.y, q.v.z, q.w);
     // new cell key and arrival rank
     const SysDev& S = a.sys[meta.w];
     int ci, cj, ck;
@@ -142,10 +140,24 @@ __global__ void __launch_bounds__(256) kick_move_kernel(StepArgs<R> a, int do_ki
     unsigned key = (unsigned)cell_index(S, ci, cj, ck);
     a.key[s] = key;
     a.rank[s] = (unsigned)atomicAdd(&a.cell_count[key], 1);
+  } else if (a.has_basis && !sphere && dst.basis != src.basis) {
+    for (int t = 0; t < 9; ++t) dst.basis[9 * (size_t)s + t] = src.basis[9 * (size_t)s + t];
   }
-  P.v[s] = st3<R>(v);
-  P.w[s] = st3<R>(w);
-  P.wbf[s] = st3<R>(wbf);
+  dst.xr[s] = xr;
+  dst.q[s] = make_double4(q.v.x, q.v.y, q.v.z, q.w);
+  dst.v[s] = st3<R>(v);
+  dst.w[s] = st3<R>(w);
+  dst.wbf[s] = st3<R>(wbf);
+}
+
+// kick_move: integrate in place (the per-phase entry points and the first step
+// of a run)
+template <typename R>
+__global__ void __launch_bounds__(256) kick_move_kernel(StepArgs<R> a, int do_kick2, R dt_kick2, int do_move,
+                                                        R dt_v, double dt_x) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  integrate(a, a.cur, a.cur, s, ld3<R>(a.cur.F[s]), ld3<R>(a.cur.T[s]), do_kick2, dt_kick2, do_move, dt_v, dt_x);
 }
 
 // bin: cell keys of the current positions (after an upload)
@@ -481,6 +493,12 @@ __global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
       ncand += (unsigned long long)(t1 - t0);
       for (int t = t0; t < t1; ++t) {
         const double4 xj = P.xr[t];
+        // cheap rejection of far candidates: the squared distance against the
+        // squared radius sum with a 1e-12 relative margin (rounding of either
+        // side is below 1e-15 relative)
+        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+        const double rs = xi.w + xj.w;
+        if (dx * dx + dy * dy + dz * dz > rs * rs * (1. + 1.e-12)) continue;
         D3 ab;
         double nab;
         // |AB| and r_A + r_B are symmetric in IEEE arithmetic, so the test
@@ -509,7 +527,7 @@ __global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
 // by both of its particles; both evaluate the same contact law with the lower
 // id as p0 (same inputs, same instructions -> bit-identical forces of
 // opposite sign) and the lower id owns the pair's contact memory.
-template <typename R, bool DIAG, bool CONVEX>
+template <typename R, bool DIAG, bool CONVEX, bool FUSED>
 __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
@@ -721,6 +739,19 @@ __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
   P.T[s] = st3<R>(T);
   a.coord[s] = ncontact;
   a.hist_n_next[oi] = nnext;
+  if (FUSED) {
+    // the rest of this step (second half kick) and the next step's first half
+    // kick + drift, written to the other buffer in this slot: neighbours still
+    // read the unmoved state of `cur` in this kernel
+    const ParticleArrays<R>& D = a.alt;
+    integrate(a, P, D, s, F, T, 1, R(0.5) * dt, 1, R(0.5) * dt, a.dt_disp);
+    D.F[s] = st3<R>(F);
+    D.T[s] = st3<R>(T);
+    D.inertia[s] = P.inertia[s];
+    D.md[s] = mdi;
+    D.meta[s] = mi;
+    D.orig[s] = oi;
+  }
 
   // statistics: warp reduction then one atomic per warp
   const unsigned full = 0xffffffffu;
@@ -781,6 +812,86 @@ __global__ void update_dynamic_kernel(StepArgs<R> a, const double* st, const dou
   if (a.has_basis && sb)
     for (int k = 0; k < 9; ++k) P.basis[9 * (size_t)s + k] = sb[9 * i + k];
 }
+
+#ifdef GG_DEFINE_SHARED_KERNELS
+// moving obstacles: constant rotation about a centre over one step
+// (ObstacleImposedVelocity ConstantRotation, ObstacleImposedVelocity.cpp:
+// 332-370, 389-455; ObstacleKinematicsVelocity::ImposedMotion, :86-122;
+// SimpleObstacle::Move, SimpleObstacle.cpp:119-170), then the world AABB
+// (Convex::bbox, Convex.cpp:29-41 -> BBox::setValue, BBox.cpp:235-239).
+__device__ void obstacle_move_one(ObstacleDev& O, const ShapeDev* shapes, const double* verts, double sub) {
+  const V3<double> om = v3<double>(O.iomega[0], O.iomega[1], O.iomega[2]);
+  const V3<double> cg = v3<double>(O.o[0], O.o[1], O.o[2]);
+  M3 b;
+  for (int t = 0; t < 9; ++t) b.m[t] = O.b[t];
+  if (om.x == 0. && om.y == 0. && om.z == 0.) {
+    // ConstantTranslation: velocity x sub-interval, basis unchanged
+    for (int i = 0; i < 3; ++i) {
+      O.o[i] = xadd(O.o[i], xmul(O.ivel[i], sub));
+      O.vel[i] = O.ivel[i];
+      O.omega[i] = 0.;
+    }
+  } else {
+    const V3<double> c = v3<double>(O.rot_center[0], O.rot_center[1], O.rot_center[2]);
+    const V3<double> rota = sc(om, sub);
+    const double d = norm(rota);
+    Qt<double> q{v3<double>(0., 0., 0.), 1.};
+    if (d != 0.) q = Qt<double>{sc(rota, sin(d / 2.) / d), cos(d / 2.)};
+    const V3<double> rel = cg - c;
+    const V3<double> tr = q_rotate(q, rel) - rel;
+    const V3<double> vt = cross(om, cg - c);
+    const Qt<double> qdt = qmul(q, Qt<double>{v3<double>(0., 0., 0.), 1.});
+    O.o[0] = cg.x + tr.x;
+    O.o[1] = cg.y + tr.y;
+    O.o[2] = cg.z + tr.z;
+    mrotate_left(b, qdt);
+    for (int t = 0; t < 9; ++t) O.b[t] = b.m[t];
+    O.vel[0] = vt.x;
+    O.vel[1] = vt.y;
+    O.vel[2] = vt.z;
+    for (int i = 0; i < 3; ++i) O.omega[i] = O.iomega[i];
+  }
+  const ShapeDev& sh = shapes[O.shape];
+  LocalBody<double> L{};
+  L.type = sh.type;
+  L.nverts = sh.nverts;
+  L.verts = verts + 3 * sh.vert_offset;
+  L.radius = sh.radius;
+  L.cyl_r = sh.radius;
+  L.cyl_hh = sh.half_height;
+  L.ext = v3<double>(sh.ext[0], sh.ext[1], sh.ext[2]);
+  double mn[3], mx[3];
+  for (int i = 0; i < 3; ++i) {
+    const D3 r = mrow(b, i);
+    const V3<double> rv = v3<double>(r.x, r.y, r.z);
+    const V3<double> sp = support_local(L, rv), sn = support_local(L, -rv);
+    mn[i] = xadd(O.o[i], xdot(r, d3(sn.x, sn.y, sn.z)));
+    mx[i] = xadd(O.o[i], xdot(r, d3(sp.x, sp.y, sp.z)));
+  }
+  for (int i = 0; i < 3; ++i) {
+    O.bbe[i] = xdiv(xsub(mx[i], mn[i]), 2.);
+    O.bbc[i] = xadd(mn[i], O.bbe[i]);
+  }
+}
+
+
+// Imposed obstacle motion of one step (ObstacleKinematicsVelocity::ImposedMotion,
+// ObstacleKinematicsVelocity.cpp:86-122; ObstacleImposedVelocity.cpp:388-445).
+// The clock is the reference's m_time: T = clock + dt, and the motion acts over
+// the sub-interval T - (T - dt) (ObstacleImposedVelocity::isActif, :306-315).
+// With use_host_time the caller gives T directly.  One block: every thread
+// reads the clock before thread 0 advances it.
+__global__ void obstacle_move_kernel(ObstacleDev* obs, const int* moving_idx, int n_moving, const ShapeDev* shapes,
+                                     const double* verts, double dt, double* clock, double host_time,
+                                     int use_host_time) {
+  const double T = use_host_time ? host_time : xadd(*clock, dt);
+  const double sub = xsub(T, xsub(T, dt));
+  __syncthreads();
+  if (threadIdx.x == 0) *clock = T;
+  for (int u = threadIdx.x; u < n_moving; u += blockDim.x) obstacle_move_one(obs[moving_idx[u]], shapes, verts, sub);
+}
+
+#endif  // GG_DEFINE_SHARED_KERNELS
 
 // candidate pairs (diagnostic): pairs with both cells equal or adjacent
 template <typename R>
@@ -878,20 +989,25 @@ int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forc
 }
 
 template <typename R>
-int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag) {
+int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int fused, int phases) {
   if (a.n == 0) return 0;
-  contacts_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
+  if (phases & 1) contacts_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
+  if (!(phases & 2)) return check_launch();
   const int g = grid_for(a.n, 128);
   if (a.has_convex) {
     if (diag)
-      forces_kernel<R, true, true><<<g, 128, 0, s>>>(a, R(dt));
+      forces_kernel<R, true, true, false><<<g, 128, 0, s>>>(a, R(dt));
+    else if (fused)
+      forces_kernel<R, false, true, true><<<g, 128, 0, s>>>(a, R(dt));
     else
-      forces_kernel<R, false, true><<<g, 128, 0, s>>>(a, R(dt));
+      forces_kernel<R, false, true, false><<<g, 128, 0, s>>>(a, R(dt));
   } else {
     if (diag)
-      forces_kernel<R, true, false><<<g, 128, 0, s>>>(a, R(dt));
+      forces_kernel<R, true, false, false><<<g, 128, 0, s>>>(a, R(dt));
+    else if (fused)
+      forces_kernel<R, false, false, true><<<g, 128, 0, s>>>(a, R(dt));
     else
-      forces_kernel<R, false, false><<<g, 128, 0, s>>>(a, R(dt));
+      forces_kernel<R, false, false, false><<<g, 128, 0, s>>>(a, R(dt));
   }
   return check_launch();
 }
@@ -902,6 +1018,17 @@ int launch_zero_kdelta(const StepArgs<R>& a, cudaStream_t s) {
   zero_kdelta_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
   return check_launch();
 }
+
+#ifdef GG_DEFINE_SHARED_KERNELS
+int launch_obstacle_move(ObstacleDev* obs, const int* moving_idx, int n_moving, const ShapeDev* shapes,
+                         const double* verts, double dt, double* clock, double host_time, int use_host_time,
+                         cudaStream_t s) {
+  if (n_moving <= 0) return 0;
+  obstacle_move_kernel<<<1, 256, 0, s>>>(obs, moving_idx, n_moving, shapes, verts, dt, clock, host_time,
+                                         use_host_time);
+  return check_launch();
+}
+#endif
 
 template <typename R>
 int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const double* stage, const double* stage_basis) {
@@ -922,7 +1049,7 @@ int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int in
   template int launch_kick_move<R>(const StepArgs<R>&, cudaStream_t, int, double, int, double, double);    \
   template int launch_bin<R>(const StepArgs<R>&, cudaStream_t);                                            \
   template int launch_sort_and_gather<R>(const StepArgs<R>&, cudaStream_t, int);                           \
-  template int launch_forces<R>(const StepArgs<R>&, cudaStream_t, double, int);                            \
+  template int launch_forces<R>(const StepArgs<R>&, cudaStream_t, double, int, int, int);                  \
   template int launch_zero_kdelta<R>(const StepArgs<R>&, cudaStream_t);                                    \
   template int launch_update_dynamic<R>(const StepArgs<R>&, cudaStream_t, const double*, const double*);     \
   template int launch_candidate_pairs<R>(const StepArgs<R>&, cudaStream_t, int, int, int*, int,           \

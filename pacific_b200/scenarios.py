@@ -14,7 +14,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .abi import BOX, HOOKE_MEMORY, SPHERE
+from .abi import BOX, CYLINDER, HOOKE_MEMORY, POLYHEDRON, SPHERE
 
 MM = 1.0e-3
 PI = 3.14159265358979323846
@@ -243,6 +243,202 @@ def dense_cluster(n=343, seed=0, overlap=0.5e-6, velocity_sigma=0.02, radius=1.0
     dom = [dict(origin=lo, size=hi - lo, cell_size=2.0 * radius, gravity=(0.0, 0.0, -9.81))]
     p = _spheres(n, r, 2500.0, pos, vel, crust)
     return Scenario("dense_cluster", shapes, dom, laws, [obs], p, 1.0e-5, 100)
+
+
+def octahedron(a):
+    """Regular octahedron of circumradius a in the polyhedron parameter
+    layout: nv, vertices, nf, then (k, indices) per face, outward-oriented."""
+    v = [a, 0, 0, -a, 0, 0, 0, a, 0, 0, -a, 0, 0, 0, a, 0, 0, -a]
+    faces = [[0, 2, 4], [2, 1, 4], [1, 3, 4], [3, 0, 4], [2, 0, 5], [1, 2, 5], [3, 1, 5], [0, 3, 5]]
+    return [6] + v + [8] + sum([[3] + f for f in faces], [])
+
+
+def _tetra(a, b, c):
+    """Volume and principal second moments (x, y, z axes) of the tetrahedron
+    (0, a, b, c) (F. Tonon, J. Math. Stat. 1(1), 2004)."""
+    x = [0.0, a[0], b[0], c[0]]
+    y = [0.0, a[1], b[1], c[1]]
+    z = [0.0, a[2], b[2], c[2]]
+    det = abs(x[1] * y[2] * z[3] + y[1] * z[2] * x[3] + z[1] * x[2] * y[3]
+              - z[1] * y[2] * x[3] - x[1] * z[2] * y[3] - y[1] * x[2] * z[3])
+    def sq(u):
+        return (u[0] * u[0] + u[0] * u[1] + u[1] * u[1] + u[0] * u[2] + u[1] * u[2] + u[2] * u[2]
+                + u[0] * u[3] + u[1] * u[3] + u[2] * u[3] + u[3] * u[3])
+    return det / 6.0, np.array([det * (sq(y) + sq(z)) / 60.0, det * (sq(x) + sq(z)) / 60.0,
+                                det * (sq(x) + sq(y)) / 60.0])
+
+
+def shape_volume_inertia(shape_type, params):
+    """Volume and principal inertia per unit density of a shape, following the
+    reference's BuildInertia / getVolume formulas."""
+    if shape_type == SPHERE:
+        r = params[0]
+        return 4.0 * PI * math.pow(r, 3.0) / 3.0, np.full(3, 8.0 * PI * math.pow(r, 5.0) / 15.0)
+    if shape_type == BOX:
+        e = [abs(x) / 2.0 for x in params[:3]]
+        v = 8.0 * e[0] * e[1] * e[2]
+        return v, np.array([v * (e[1] ** 2 + e[2] ** 2) / 3.0, v * (e[0] ** 2 + e[2] ** 2) / 3.0,
+                            v * (e[1] ** 2 + e[0] ** 2) / 3.0])
+    if shape_type == CYLINDER:
+        r, hh = params[0], params[1] / 2.0
+        cst = 0.5 * hh * r * r * PI
+        i0 = cst * (4.0 * hh * hh / 3.0 + r * r)
+        return 2 * hh * PI * r * r, np.array([i0, 2.0 * cst * r * r, i0])
+    nv = int(params[0])
+    vert = np.array(params[1:1 + 3 * nv]).reshape(nv, 3)
+    k = 1 + 3 * nv
+    nf = int(params[k])
+    k += 1
+    vol, inertia = 0.0, np.zeros(3)
+    for _ in range(nf):
+        m = int(params[k])
+        f = [int(t) for t in params[k + 1:k + 1 + m]]
+        k += 1 + m
+        for j in range(1, m - 1):
+            dv, di = _tetra(vert[f[0]], vert[f[j]], vert[f[j + 1]])
+            vol += dv
+            inertia += di
+    return vol, inertia
+
+
+def circumscribed_radius(shape_type, params):
+    if shape_type == SPHERE:
+        return params[0]
+    if shape_type == BOX:
+        return math.sqrt(sum((abs(x) / 2.0) ** 2 for x in params[:3]))
+    if shape_type == CYLINDER:
+        return math.sqrt(params[0] ** 2 + (params[1] / 2.0) ** 2)
+    nv = int(params[0])
+    vert = np.array(params[1:1 + 3 * nv]).reshape(nv, 3)
+    return float(np.sqrt(np.max(np.sum(vert * vert, axis=1))))
+
+
+def random_quaternions(n, rng):
+    """Uniform random unit quaternions (K. Shoemake, "Uniform random
+    rotations", Graphics Gems III, 1992), xyzw."""
+    u1, u2, u3 = rng.random(n), rng.random(n), rng.random(n)
+    a, b = np.sqrt(1 - u1), np.sqrt(u1)
+    q = np.stack([a * np.sin(2 * PI * u2), a * np.cos(2 * PI * u2), b * np.sin(2 * PI * u3),
+                  b * np.cos(2 * PI * u3)], 1)
+    return q
+
+
+def quaternion_basis(q):
+    x, y, z, w = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    return np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y),
+                     2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                     2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)], 1)
+
+
+CONVEX_SHAPES = [(BOX, [2.0 * MM, 2.0 * MM, 2.0 * MM]), (CYLINDER, [1.0 * MM, 2.0 * MM]),
+                 (POLYHEDRON, octahedron(1.2 * MM))]
+CONVEX_FRACTIONS = [0.4, 0.3, 0.3]
+
+
+def _convex_particles(pos, rng, rho=2500.0, crust=0.05 * MM, fractions=CONVEX_FRACTIONS, shape_offset=0):
+    n = len(pos)
+    kinds = rng.choice(len(CONVEX_SHAPES), size=n, p=fractions)
+    q = random_quaternions(n, rng)
+    mass = np.zeros(n)
+    inertia = np.zeros((n, 3))
+    radius = np.zeros(n)
+    for k, (t, prm) in enumerate(CONVEX_SHAPES):
+        vol, inr = shape_volume_inertia(t, prm)
+        sel = kinds == k
+        mass[sel] = rho * vol
+        inertia[sel] = inr * rho
+        radius[sel] = circumscribed_radius(t, prm)
+    return dict(id=np.arange(n, dtype=np.int32), system=None, shape=(kinds + shape_offset).astype(np.int32),
+                material=np.zeros(n, np.int32), radius=radius, crust=np.full(n, crust), mass=mass,
+                inertia=inertia, position=pos, quaternion=q, basis=quaternion_basis(q),
+                velocity=np.zeros((n, 3)), omega=np.zeros((n, 3)))
+
+
+def convex_box(n=216, seed=0, spacing=3.6, jitter=0.05, velocity_sigma=0.2, kn=2.0e5, en=0.7, mu=0.4,
+               converge_time=None):
+    """Cubes, cylinders and octahedra (40/30/30 %) with random orientations on
+    a jittered lattice in a closed box: the static-wall counterpart of the
+    rotating-drum workload, for parity tests of the GJK narrowphase.  With
+    `converge_time` T every particle also moves towards the box centre at
+    (centre - x) / T, so the lattice collapses into a dense cluster after
+    about T."""
+    rng = np.random.default_rng(seed)
+    crust = 0.05 * MM
+    side_n = int(math.ceil(n ** (1.0 / 3.0)))
+    rmax = max(circumscribed_radius(t, p) for t, p in CONVEX_SHAPES)
+    lo = np.zeros(3)
+    side = (side_n - 1) * spacing * MM + 2 * (rmax * 1.0 + 0.3 * MM) + 0.0
+    hi = np.array([side, side, side * 1.2])
+    pos = lattice(n, lo, hi, spacing * MM, rmax + 0.2 * MM, jitter * MM, rng)
+    p = _convex_particles(pos, rng, crust=crust)
+    p["velocity"] = rng.normal(0.0, velocity_sigma, size=(n, 3))
+    if converge_time:
+        p["velocity"] += (0.5 * (lo + hi) - pos) / converge_time
+    p["omega"] = rng.normal(0.0, 50.0, size=(n, 3))
+    shapes = list(CONVEX_SHAPES)
+    wshapes, obs = box_walls(lo, hi, "xXyYzZ", 0.5 * MM, crust, len(shapes), -1)
+    shapes += wshapes
+    laws = [[(0, 0, HOOKE_MEMORY, hooke_memory_params(kn, en, mu, 0.8 * kn)),
+             (0, 1, HOOKE_MEMORY, hooke_memory_params(kn, en, mu, 0.8 * kn))]]
+    dom = [dict(origin=lo, size=hi - lo, cell_size=2.0 * rmax, gravity=(0.0, 0.0, -9.81))]
+    return Scenario("convex_box", shapes, dom, laws, [obs], p, 2.0e-6, 100)
+
+
+def drum(n=100_000, seed=3, radius=110.0 * MM, length=147.0 * MM, n_boxes=64, rpm=30.0, width=5.0 * MM,
+         spacing=3.7 * MM, initial_velocity=(0.0, 0.0, 0.0)):
+    """Cubes (edge 2 mm), cylinders (r 1 mm, h 2 mm) and regular octahedra
+    (circumradius 1.2 mm), 40/30/30 %, random orientations, in a drum whose
+    shell is n_boxes boxes on a circle (CylindricalShell with box elements,
+    CylindricalShell.cpp:12-100) closed by two end plates, rotating about its
+    axis (z) at `rpm`.  kn = 2e5, en = 0.7, mu = 0.4, kt = 0.8 kn,
+    dt = 2e-6 s.  100k such particles do not fit a 60 mm x 80 mm drum (the
+    particles alone are ~64 % of its volume), so the drum is 110 mm x 147 mm
+    (same L/R)."""
+    rng = np.random.default_rng(seed)
+    crust = 0.05 * MM
+    rmax = max(circumscribed_radius(t, p) for t, p in CONVEX_SHAPES)
+    # lattice sites inside the drum
+    m = int((2 * radius) / spacing) + 1
+    g = (np.arange(m) - (m - 1) / 2.0) * spacing
+    zs = np.arange(rmax + 0.5 * MM, length - rmax - 0.5 * MM, spacing)
+    X, Y, Z = np.meshgrid(g, g, zs, indexing="ij")
+    sites = np.stack([X.ravel(), Y.ravel(), Z.ravel()], 1)
+    sites = sites[np.hypot(sites[:, 0], sites[:, 1]) < radius - rmax - 0.5 * MM]
+    order = np.lexsort((sites[:, 0], sites[:, 2], sites[:, 1]))   # bottom (y) first
+    sites = sites[order]
+    if len(sites) < n:
+        raise ValueError("drum holds %d lattice sites < %d" % (len(sites), n))
+    pos = sites[:n] + rng.uniform(-0.1 * MM, 0.1 * MM, size=(n, 3))
+    p = _convex_particles(pos, rng, crust=crust)
+    p["velocity"] += np.asarray(initial_velocity, dtype=np.float64)
+    shapes = list(CONVEX_SHAPES)
+    omega = (0.0, 0.0, rpm * 2.0 * PI / 60.0)
+    centre = (0.0, 0.0, 0.5 * length)
+    delta = 2.0 * PI / n_boxes
+    ly = 2.0 * (radius + width) * (math.sin(delta) - (1.0 - math.cos(delta)) / math.tan(delta))
+    obs = []
+    shapes.append((BOX, [width, ly, length + 2 * width]))
+    shell = len(shapes) - 1
+    ext_r = radius + width / 2.0
+    for i in range(n_boxes):
+        ang = (0.5 + i) * delta
+        c, s_ = math.cos(ang), math.sin(ang)
+        obs.append(dict(id=-1 - i, shape=shell, material=1, crust=crust, moving=1,
+                        transform=[c, -s_, 0, s_, c, 0, 0, 0, 1, ext_r * c, ext_r * s_, 0.5 * length],
+                        omega=omega, rotation_center=centre))
+    shapes.append((BOX, [2 * (radius + width), 2 * (radius + width), width]))
+    cap = len(shapes) - 1
+    for k, zc in enumerate([-width / 2.0, length + width / 2.0]):
+        obs.append(dict(id=-1 - n_boxes - k, shape=cap, material=1, crust=crust, moving=1,
+                        transform=[1, 0, 0, 0, 1, 0, 0, 0, 1, 0.0, 0.0, zc], omega=omega,
+                        rotation_center=centre))
+    kn = 2.0e5
+    laws = [[(0, 0, HOOKE_MEMORY, hooke_memory_params(kn, 0.7, 0.4, 0.8 * kn)),
+             (0, 1, HOOKE_MEMORY, hooke_memory_params(kn, 0.7, 0.4, 0.8 * kn))]]
+    lo = np.array([-radius - 1.0 * MM, -radius - 1.0 * MM, 0.0])
+    dom = [dict(origin=lo, size=np.array([2 * radius + 2.0 * MM, 2 * radius + 2.0 * MM, length]),
+                cell_size=2.0 * rmax, gravity=(0.0, -9.81, 0.0))]
+    return Scenario("drum_100k", shapes, dom, laws, [obs], p, 2.0e-6, 10000)
 
 
 def apply(sim, sc):

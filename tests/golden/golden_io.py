@@ -19,6 +19,11 @@ def scenario_to_npz_dict(sc, prefix="in_"):
     out = {"spec": np.array(json.dumps(spec))}
     for k in STATIC_KEYS + STATE_KEYS:
         out[prefix + k] = np.asarray(sc.particles[k])
+    # the orientation matrix of non-spherical bodies: the reference composes it
+    # with each step's rotation, so after many steps it is not the matrix of the
+    # quaternion to the last bit
+    if sc.particles.get("basis") is not None:
+        out[prefix + "basis"] = np.asarray(sc.particles["basis"])
     return out
 
 
@@ -26,7 +31,7 @@ def scenario_from_npz(z, prefix="in_"):
     spec = json.loads(str(z["spec"]))
     p = {k: np.array(z[prefix + k]) for k in STATIC_KEYS + STATE_KEYS}
     p["system"] = None
-    p["basis"] = None
+    p["basis"] = np.array(z[prefix + "basis"]) if prefix + "basis" in z.files else None
     doms = [dict(origin=np.array(d["origin"]), size=np.array(d["size"]), cell_size=d["cell_size"],
                  gravity=tuple(d["gravity"])) for d in spec["domains"]]
     laws = [[(l[0], l[1], l[2], l[3]) for l in ls] for ls in spec["laws"]]

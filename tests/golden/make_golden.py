@@ -4,11 +4,12 @@ reference Grains3D itself (oracle/_ref/libgrains_ref.so, built from the
 reference sources by oracle/ref/Makefile) on seeded scenarios.
 
 Each case: the reference advances a scenario for `warm` steps (building up
-contact memory), its state and memory are recorded as the input, then one
-force evaluation (forces, torques, coordination, contact and candidate pairs,
-memory) and `steps` further KDK steps (positions, velocities, quaternions,
-angular velocities) are recorded as the expected output.  Every case runs in
-its own process because the reference keeps process-wide static state.
+contact memory) and its state and memory are recorded as the input.  A fresh
+reference context then replays that input: one force evaluation (forces,
+torques, coordination, contact and candidate pairs, memory) and `steps`
+further KDK steps (positions, velocities, quaternions, angular velocities) are
+recorded as the expected output.  Each of the two runs has its own process
+because the reference keeps process-wide static state.
 
     python tests/golden/make_golden.py            # all cases
 """
@@ -33,7 +34,17 @@ CASES = {
                     "radius_range=(0.8, 1.2))", 400, 40),
     "hooke_dense125": ("hooke(S.dense_cluster(125, seed=4, velocity_sigma=0.1))", 5, 20),
     "settling_1k": ("S.settling_1k()", 1000, 30),
+    "convex216": ("S.convex_box(216, seed=0, converge_time=0.004, velocity_sigma=0.05)", 900, 5),
+    "drum300": ("converge(S.drum(n=300, radius=25e-3, length=30e-3, n_boxes=32), (0.0, -25e-3, 15e-3), 0.006)",
+                1500, 3),
 }
+
+
+def converge(sc, target, T):
+    """Adds a velocity field that brings every particle to `target` in time T:
+    a dense cluster against the drum's rotating shell after about T."""
+    sc.particles["velocity"] = sc.particles["velocity"] + (np.asarray(target) - sc.particles["position"]) / T
+    return sc
 
 
 def rolling(sc):
@@ -53,7 +64,9 @@ def hooke(sc):
     return sc
 
 
-def run_case(name):
+def warm_case(name):
+    """First process: the reference advances the scenario `warm` steps; its
+    state and contact memory become the fixture's input."""
     from pacific_b200 import scenarios as S  # noqa: F401
     from pacific_b200.abi import FP64, GrainsLib, Simulation
     import golden_io as G
@@ -68,9 +81,34 @@ def run_case(name):
     mem = sim.contact_memory()
     for k in G.STATE_KEYS:
         sc.particles[k] = st[k]
+    if any(sc.shapes[k][0] != S.SPHERE for k in set(np.asarray(sc.particles["shape"]).tolist())):
+        sc.particles["basis"] = st["basis"]
     out = G.scenario_to_npz_dict(sc)
     out.update(G.memory_arrays(mem, "mem_in_"))
     out["time"] = np.array(t)
+    out["after_steps"] = np.array(steps)
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+
+
+def replay_case(name):
+    """Second process: a fresh reference context is given the recorded input,
+    exactly as the tests give it to the oracle and the CUDA path, and its
+    results become the fixture's expected output.  (A fresh context matters:
+    the reference's cell lists keep an order that depends on the history, so
+    the order of the force sums, and hence their last bits, differs between a
+    continuing run and a replay.)"""
+    from pacific_b200 import scenarios as S  # noqa: F401
+    from pacific_b200.abi import FP64, GrainsLib, Simulation
+    import golden_io as G
+    path = os.path.join(HERE, name + ".npz")
+    z = np.load(path)
+    out = {k: z[k] for k in z.files}
+    sc = G.scenario_from_npz(z)
+    lib = GrainsLib(REF_SO, "grains_ref_")
+    sim = Simulation(lib, FP64, max_particles=sc.n)
+    S.apply(sim, sc)
+    sim.upload_contact_memory(G.memory_from(z, "mem_in_"))
+    t = float(z["time"])
     sim.compute_forces(t, sc.dt)
     d = sim.download()
     out["force"] = d["force"]
@@ -82,22 +120,25 @@ def run_case(name):
     out["contact_pairs"] = sim.contact_pairs()
     out["candidate_pairs"] = sim.candidate_pairs()
     out.update(G.memory_arrays(sim.contact_memory(), "mem_out_"))
-    t2 = sim.step(steps, t, sc.dt)
+    steps = int(z["after_steps"])
+    sim.step(steps, t, sc.dt)
     d = sim.download()
     for k in G.STATE_KEYS + ["force", "torque"]:
         out["after_" + k] = d[k]
-    out["after_steps"] = np.array(steps)
+    if "in_basis" in out:
+        out["after_basis"] = d["basis"]
     out.update(G.memory_arrays(sim.contact_memory(), "mem_after_"))
-    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    np.savez_compressed(path, **out)
     print("%s: %d particles, %d contacts, %d candidates" % (name, sc.n, len(out["contact_pairs"]),
                                                            len(out["candidate_pairs"])))
 
 
 if __name__ == "__main__":
-    if len(sys.argv) > 2 and sys.argv[1] == "--case":
-        run_case(sys.argv[2])
+    if len(sys.argv) > 2 and sys.argv[1] in ("--warm", "--replay"):
+        (warm_case if sys.argv[1] == "--warm" else replay_case)(sys.argv[2])
         sys.exit(0)
     if not os.path.exists(REF_SO):
         sys.exit("build the reference first: make -C oracle/ref")
     for name in (sys.argv[1:] or CASES):
-        subprocess.run([sys.executable, __file__, "--case", name], check=True)
+        subprocess.run([sys.executable, __file__, "--warm", name], check=True)
+        subprocess.run([sys.executable, __file__, "--replay", name], check=True)

@@ -38,7 +38,10 @@ def test_gpu_matches_reference_fixture(gpu_lib, path, precision):
     tol = 1e-12 if precision == FP64 else 1e-5
     assert rel_err(d["force"], z["force"], weight) < tol
     assert rel_err(d["torque"], z["torque"], weight * 1e-3) < (1e-10 if precision == FP64 else 1e-5)
+    # 20-40 further steps: FP64 stays at rounding level; in mixed precision the
+    # FP32 rounding of forces is amplified by the chaotic dense-packing
+    # dynamics (observed up to 3e-8 m after 20 steps of a dense cluster)
     steps = int(z["after_steps"])
     sim.step(steps, t, sc.dt)
     d = sim.download()
-    assert np.max(np.abs(d["position"] - z["after_position"])) < (1e-13 if precision == FP64 else 1e-9)
+    assert np.max(np.abs(d["position"] - z["after_position"])) < (1e-13 if precision == FP64 else 2e-7)

@@ -4,8 +4,14 @@ are replayed through the oracle on identical states and memories.
 
 Bars: contact / candidate pair sets and coordination numbers identical;
 forces and torques within 1e-13 relative (floor: the particle weight);
-states after the KDK steps within 1e-14 m / 1e-10 m/s."""
+states after the KDK steps within 1e-14 m / 1e-10 m/s / 1e-11 in the
+quaternion components, forces then within 1e-8.  (Rolling resistance and the
+flat-face contacts of convex bodies amplify last-bit differences of the force
+sums over the steps: the reference's own continuing run and its replay of the
+same recorded state differ by 1.1e-12 in quaternions and 1.1e-9 in forces after
+the 20 steps of dense216_rolling.)"""
 import glob
+import json
 import os
 
 import numpy as np
@@ -48,15 +54,25 @@ def test_oracle_matches_reference_fixture(oracle_lib, path):
     d = sim.download()
     assert np.max(np.abs(d["position"] - z["after_position"])) < 1e-14
     assert np.max(np.abs(d["velocity"] - z["after_velocity"])) < 1e-10
-    assert np.max(np.abs(d["quaternion"] - z["after_quaternion"])) < 1e-12
-    assert rel_err(d["force"], z["after_force"], weight) < 1e-9
+    assert np.max(np.abs(d["quaternion"] - z["after_quaternion"])) < 1e-11
+    assert rel_err(d["force"], z["after_force"], weight) < 1e-8
 
 
 def test_fixtures_exercise_the_path():
     """The fixture set covers particle-particle and wall contacts, memory,
-    rolling friction, the memory-less Hooke law and polydispersity."""
+    rolling friction, the memory-less Hooke law, polydispersity, boxes,
+cylinders and polyhedra through the GJK narrowphase, and a rotating drum."""
     names = [os.path.basename(c)[:-4] for c in CASES]
-    for n in ["dense125", "dense216_rolling", "poly_box200", "hooke_dense125", "settling_1k"]:
+    for n in ["dense125", "dense216_rolling", "poly_box200", "hooke_dense125", "settling_1k", "convex216",
+              "drum300"]:
         assert n in names
     z = np.load(os.path.join(HERE, "golden", "dense125.npz"))
     assert len(z["contact_pairs"]) > 100 and len(z["mem_in_owner"]) > 100
+    z = np.load(os.path.join(HERE, "golden", "convex216.npz"))
+    shapes = {s[0] for s in json.loads(str(z["spec"]))["shapes"]}
+    assert {1, 2, 3} <= shapes and len(z["contact_pairs"]) > 40
+    # the drum: a rotating shell of boxes, with particle-obstacle contact memory
+    z = np.load(os.path.join(HERE, "golden", "drum300.npz"))
+    obstacles = json.loads(str(z["spec"]))["obstacles"][0]
+    assert sum(o["moving"] for o in obstacles) == len(obstacles) > 30
+    assert np.any(z["mem_in_owner"] < 0) or np.any(z["mem_in_other"] < 0)

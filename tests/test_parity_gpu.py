@@ -179,3 +179,88 @@ def test_deterministic(gpu_lib):
         outs.append(g.download())
     for k in ["position", "velocity", "force"]:
         assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+def small_drum(n=300, converge_time=0.006):
+    """The rotating drum at a test size: 300 cubes, cylinders and octahedra
+    converging onto the shell bottom of a 25 mm x 30 mm drum of 32 boxes."""
+    sc = S.drum(n=n, radius=25e-3, length=30e-3, n_boxes=32)
+    target = np.array([0.0, -25e-3, 15e-3])
+    sc.particles["velocity"] = sc.particles["velocity"] + (target - sc.particles["position"]) / converge_time
+    return sc
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED], ids=["fp64", "mixed"])
+def test_rotating_obstacles_follow_the_oracle(oracle_lib, gpu_lib, precision):
+    """Imposed rotation of the drum's 34 obstacles (ConstantRotation about the
+    drum axis) over 400 steps, through the graph-captured step: poses within
+    1e-15 m (device and host sin/cos may differ in the last bit)."""
+    sc = small_drum()
+    o, g = both(oracle_lib, gpu_lib, sc, precision=precision)
+    n_obs = len(sc.obstacles[0])
+    t = 0.0
+    for sim in (o, g):
+        sim.initialize_leapfrog(0.0, sc.dt)
+    for _ in range(4):
+        to = o.step(100, t, sc.dt)
+        t = g.step(100, t, sc.dt)
+        assert t == to
+        po, pg = o.obstacles(0, n_obs), g.obstacles(0, n_obs)
+        assert np.max(np.abs(po - pg)) < 1e-15
+    assert g.stats()["status"] == 0
+
+
+def test_translating_obstacle_one_step_fp64(oracle_lib, gpu_lib):
+    """A floor moving up (ConstantTranslation) under a dense cluster: forces
+    of the first evaluations (obstacle velocity zero before the first move,
+    then the imposed velocity) and the floor's position after 10 steps."""
+    sc = S.dense_cluster(125, seed=1, velocity_sigma=0.0)
+    floor = sc.obstacles[0][4]
+    floor["moving"] = 1
+    floor["velocity"] = [0.0, 0.0, 0.02]
+    o, g = both(oracle_lib, gpu_lib, sc)
+    weight = float(np.min(sc.particles["mass"])) * 9.81
+    for sim in (o, g):
+        sim.initialize_leapfrog(0.0, sc.dt)
+    assert rel_err(g.download()["force"], o.download()["force"], weight) < 1e-12
+    t = 0.0
+    for _ in range(10):
+        o.step(1, t, sc.dt)
+        t = g.step(1, t, sc.dt)
+        assert rel_err(g.download()["force"], o.download()["force"], weight) < 1e-9
+    po, pg = o.obstacles(0, 6), g.obstacles(0, 6)
+    assert np.max(np.abs(po - pg)) == 0.0
+    assert pg[4, 11] > sc.obstacles[0][4]["transform"][11]
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED], ids=["fp64", "mixed"])
+def test_drum_contacts_match_oracle(oracle_lib, gpu_lib, precision):
+    """The drum advanced by the oracle into a dense cluster against the shell,
+    then one evaluation on both: pair sets identical, FP64 forces within
+    1e-12, mixed within 1e-5 of the weight-floored force."""
+    sc = small_drum()
+    o = make(oracle_lib, sc)
+    o.initialize_leapfrog(0.0, sc.dt)
+    t = o.step(1500, 0.0, sc.dt)
+    st = o.download()
+    mem = o.contact_memory()
+    n_obs = len(sc.obstacles[0])
+    poses = o.obstacles(0, n_obs)
+    p = dict(sc.particles)
+    for k in ["position", "quaternion", "basis", "velocity", "omega"]:
+        p[k] = st[k]
+    sc.particles = p
+    obs = [dict(ob) for ob in sc.obstacles[0]]
+    for k, ob in enumerate(obs):
+        ob["transform"] = list(poses[k])
+        ob["rotation_center"] = list(ob["rotation_center"])
+    sc.obstacles = [obs]
+    o2, g = both(oracle_lib, gpu_lib, sc, mem, precision)
+    o2.compute_forces(t, sc.dt)
+    g.compute_forces(t, sc.dt)
+    do, dg = o2.download(), g.download()
+    assert pair_set(g.contact_pairs()) == pair_set(o2.contact_pairs())
+    assert len(o2.contact_pairs()) > 100
+    assert np.array_equal(dg["coordination"], do["coordination"])
+    weight = float(np.min(sc.particles["mass"])) * 9.81
+    assert rel_err(dg["force"], do["force"], weight) < (1e-12 if precision == FP64 else 1e-5)
