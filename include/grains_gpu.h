@@ -145,9 +145,11 @@ typedef struct grains_gpu_contact_memory {
   double*  spring_torque;/* 3n */
 } grains_gpu_contact_memory;
 
+/* Counters and overlap statistics accumulate over the force evaluations since
+ * the last grains_gpu_reset_stats (or the context's creation). */
 typedef struct grains_gpu_stats {
   int64_t n_particles;
-  int64_t n_candidate_pairs;      /* particle-particle candidates of the last force evaluation */
+  int64_t n_candidate_pairs;      /* particle-particle candidates (27-cell neighbourhoods) */
   int64_t n_obstacle_candidates;  /* particle-obstacle candidates after the InZone prefilter */
   int64_t n_contacts;             /* particle-particle contacts */
   int64_t n_obstacle_contacts;
@@ -243,6 +245,14 @@ int grains_gpu_get_candidate_pairs(grains_gpu_ctx* ctx, int32_t system, int32_t 
 /* Contact pairs (overlap distance < 0) of the last force evaluation, same layout. */
 int grains_gpu_get_contact_pairs(grains_gpu_ctx* ctx, int32_t system, int64_t cap,
                                  int32_t* pairs, int64_t* n);
+/* Contact pairs of the last force evaluation of grains_gpu_compute_forces
+ * with the contact force (delFN + delFT of the contact law) on the lower id of
+ * each: forces[3k..3k+2] for pairs[2k], pairs[2k+1], same order as
+ * grains_gpu_get_contact_pairs.  The reference applies the same force at the
+ * contact point through Component::addForce (Component.cpp:67-71) inside
+ * HookeMemoryContactForceModel::computeForces (:200-249); it keeps no list. */
+int grains_gpu_get_contact_forces(grains_gpu_ctx* ctx, int32_t system, int64_t cap, int32_t* pairs,
+                                  double* forces, int64_t* n);
 int grains_gpu_get_stats(grains_gpu_ctx* ctx, grains_gpu_stats* st);
 /* Reset the accumulated status bits and statistics. */
 int grains_gpu_reset_stats(grains_gpu_ctx* ctx);

@@ -125,6 +125,7 @@ _SIGS = {
     "step": [_VP, C.c_int32, _P_F64, C.c_double],
     "get_candidate_pairs": [_VP, C.c_int32, C.c_int32, C.c_int64, _P_I32, C.POINTER(C.c_int64)],
     "get_contact_pairs": [_VP, C.c_int32, C.c_int64, _P_I32, C.POINTER(C.c_int64)],
+    "get_contact_forces": [_VP, C.c_int32, C.c_int64, _P_I32, _P_F64, C.POINTER(C.c_int64)],
     "get_stats": [_VP, C.POINTER(Stats)],
     "reset_stats": [_VP],
 }
@@ -163,6 +164,11 @@ class GrainsLib:
             f.argtypes = [_VP, C.c_double]
             f.restype = C.c_int
             self.fn["set_gjk_tolerance"] = f
+        if hasattr(self.dll, prefix + "set_polyhedron_support"):  # oracle-only test switch
+            f = getattr(self.dll, prefix + "set_polyhedron_support")
+            f.argtypes = [_VP, C.c_int32]
+            f.restype = C.c_int
+            self.fn["set_polyhedron_support"] = f
 
     def shape_properties(self, shape_type, params):
         p = np.ascontiguousarray(params, dtype=np.float64)
@@ -403,6 +409,16 @@ class Simulation:
         self._check(self.lib.fn["get_contact_pairs"](self.ctx, system, cap, _ptr(buf, C.c_int32), C.byref(n)))
         return buf[: 2 * n.value].reshape(-1, 2)
 
+    def contact_forces(self, system=0, cap=None):
+        """(pairs (k, 2), force on the lower id (k, 3)) of the last compute_forces."""
+        cap = cap or max(1024, 16 * self.n)
+        buf = np.zeros(2 * cap, np.int32)
+        f = np.zeros(3 * cap, np.float64)
+        n = C.c_int64()
+        self._check(self.lib.fn["get_contact_forces"](self.ctx, system, cap, _ptr(buf, C.c_int32),
+                                                      _ptr(f, C.c_double), C.byref(n)))
+        return buf[: 2 * n.value].reshape(-1, 2), f[: 3 * n.value].reshape(-1, 3)
+
     def stats(self):
         st = Stats()
         self._check(self.lib.fn["get_stats"](self.ctx, C.byref(st)))
@@ -413,6 +429,12 @@ class Simulation:
 
     def set_gjk_tolerance(self, tol):
         self._check(self.lib.fn["set_gjk_tolerance"](self.ctx, tol))
+
+    def set_polyhedron_support(self, stateless):
+        """Oracle only: stateless=True makes the polyhedron support the
+        order-independent arg-max of the CUDA path instead of the reference's
+        warm-started hill climb."""
+        self._check(self.lib.fn["set_polyhedron_support"](self.ctx, 1 if stateless else 0))
 
     # ---- benchmark helpers (CUDA implementation only) ----
     def stream_handle(self):

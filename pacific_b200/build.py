@@ -2,9 +2,11 @@
 
     python -m pacific_b200.build          # -> pacific_b200/lib/libgrains_gpu.so
 
-The plain-FP64 kernels are compiled with -fmad=false so that every double
-expression rounds like the reference's x86-64 build; the mixed-precision
-kernels keep contraction on.
+Both kernel units are compiled with -fmad=false.  In the plain-FP64 kernels
+every double expression then rounds like the reference's x86-64 build.  The
+mixed-precision kernels run the same double narrowphase for every contact
+(GJK witness points on flat faces hinge on the last bit of near-equal support
+values), so they must round it the same way as the FP64 kernels.
 """
 import os
 import subprocess
@@ -20,7 +22,7 @@ NVCC = os.environ.get("NVCC", "nvcc")
 
 UNITS = [
     ("kernels_fp64.cu", ["-fmad=false"]),
-    ("kernels_mixed.cu", []),
+    ("kernels_mixed.cu", ["-fmad=false"]),
     ("api.cu", []),
     ("noalloc.cu", []),
 ]
@@ -40,6 +42,7 @@ def build(verbose=False, force=False):
     os.makedirs(objdir, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS]
     hdrs.append(os.path.join(HERE, "..", "include", "grains_gpu.h"))
+    hdrs.append(os.path.abspath(__file__))  # compiler flags live here
     objs = []
     procs = []
     for src, extra in UNITS:

@@ -112,6 +112,7 @@ struct grains_gpu_ctx {
   int* pairs = nullptr;  // contact pairs of the last compute_forces (diagnostic)
   int pairs_cap = 0;
   unsigned long long* pairs_n = nullptr;
+  double* pair_force = nullptr;  // force on the lower id of each diagnostic contact pair
   int* cand = nullptr;   // candidate pairs (diagnostic, separate from the contact pairs)
   int cand_cap = 0;
   unsigned long long* cand_n = nullptr;
@@ -440,6 +441,7 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   a.pairs = c->pairs;
   a.pairs_cap = c->pairs_cap;
   a.pairs_n = c->pairs_n;
+  a.pair_force = c->pair_force;
   a.gjk_tol = c->gjk_tol;
   return a;
 }
@@ -625,8 +627,9 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
     c->pairs_cap = (int)std::min<size_t>(16 * N + 1024, (size_t)1 << 30);
     c->pairs = dalloc<int>(2 * (size_t)c->pairs_cap, c->pool);
     c->pairs_n = dalloc<unsigned long long>(1, c->pool);
+    c->pair_force = dalloc<double>(3 * (size_t)c->pairs_cap, c->pool);
     c->clock = dalloc<double>(1, c->pool);
-    ok = c->coord && c->key && c->rank && c->perm && c->stats && c->pairs && c->pairs_n && c->clock;
+    ok = c->coord && c->key && c->rank && c->perm && c->stats && c->pairs && c->pairs_n && c->pair_force && c->clock;
   }
   if (!ok) {
     c->err = "cudaMalloc failed for the requested capacity";
@@ -1450,6 +1453,34 @@ int grains_gpu_get_contact_pairs(grains_gpu_ctx* c, int32_t system, int64_t cap,
     pairs[2 * k + 1] = pp[k].second;
   }
   return (int64_t)pp.size() > cap ? fail(c, GRAINS_GPU_PAIR_OVERFLOW, "pair buffer too small") : 0;
+}
+
+int grains_gpu_get_contact_forces(grains_gpu_ctx* c, int32_t system, int64_t cap, int32_t* pairs, double* forces,
+                                  int64_t* n) {
+  if (!c || !n || (cap > 0 && (!pairs || !forces))) return GRAINS_GPU_INVALID_ARGUMENT;
+  (void)system;
+  unsigned long long cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, c->pairs_n, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (cnt > (unsigned long long)c->pairs_cap) return fail(c, GRAINS_GPU_PAIR_OVERFLOW, "device pair buffer too small");
+  std::vector<int> h(2 * cnt);
+  std::vector<double> f(3 * cnt);
+  if (cnt) {
+    CK(cudaMemcpy(h.data(), c->pairs, 2 * cnt * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(f.data(), c->pair_force, 3 * cnt * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  std::vector<size_t> idx(cnt);
+  for (size_t k = 0; k < cnt; ++k) idx[k] = k;
+  std::sort(idx.begin(), idx.end(), [&](size_t x, size_t y) {
+    return std::make_pair(h[2 * x], h[2 * x + 1]) < std::make_pair(h[2 * y], h[2 * y + 1]);
+  });
+  *n = (int64_t)cnt;
+  for (int64_t k = 0; k < (int64_t)cnt && k < cap; ++k) {
+    pairs[2 * k] = h[2 * idx[k]];
+    pairs[2 * k + 1] = h[2 * idx[k] + 1];
+    for (int d = 0; d < 3; ++d) forces[3 * k + d] = f[3 * idx[k] + d];
+  }
+  return (int64_t)cnt > cap ? fail(c, GRAINS_GPU_PAIR_OVERFLOW, "pair buffer too small") : 0;
 }
 
 int grains_gpu_get_stats(grains_gpu_ctx* c, grains_gpu_stats* st) {

@@ -156,6 +156,7 @@ struct StepArgs {
   int* pairs;            // diagnostic contact pair output (2 ints per pair) or null
   int pairs_cap;
   unsigned long long* pairs_n;
+  double* pair_force;    // diagnostic: force on the lower id of each contact pair (3 doubles) or null
   double gjk_tol;
   double dt_disp;        // drift time step of the fused force kernel
 };

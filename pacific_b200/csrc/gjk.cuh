@@ -10,13 +10,17 @@
 //
 // Support functions: Sphere.cpp:99-109, Box.cpp:307-316, Cylinder.cpp:112-133
 // (axis = local Y), Polyhedron.cpp:265-293.  The polyhedron support here is a
-// stateless arg-max over the vertices (first maximum wins); the reference's
-// warm-started hill climb returns the same vertex except on exact ties.
+// stateless arg-max over the vertices (first maximum wins).  The reference
+// hill-climbs from a warm-start vertex kept per body between calls and moves
+// only for a gain above 1e-16, so the two differ when face vertices tie within
+// that margin (flat-face contacts): the distance is the same, the witness
+// points, hence the contact point, may not be.
 //
 // Precision: the iteration runs in T.  With T = float the two bodies are
 // expressed relative to body A's origin (the translation difference is formed
-// in double) so that FP32 keeps the body-size scale; contact decisions near
-// the crust threshold are re-checked by a double run (guard band).
+// in double) so that FP32 keeps the body-size scale.  The FP32 run only
+// certifies separation (GjkResult::lower); pairs it cannot rule out are run
+// again in double.
 #pragma once
 
 #include "common.cuh"
@@ -237,6 +241,9 @@ struct GjkResult {
   T dist;
   V3<T> pa, pb;  // witness points in the working frame
   int iters;
+  T lower;   // largest support-plane separation dot(v, w) / |v| met: a lower bound of the distance
+  int exit;  // 0 optimality gap, 1 degenerate support point, 2 Johnson/backup failed, 3 other (full simplex,
+             // distance <= EPSILON2, iteration cap)
 };
 
 template <typename T>
@@ -255,7 +262,8 @@ GG_HD GjkResult<T> gjk_distance(const LocalBody<T>& A, const LocalBody<T>& B, T 
   V3<T> v = lb_apply(A, support_local(A, zero)) - lb_apply(B, support_local(B, zero));
   V3<T> w = v;
   T dist = norm(v);
-  int num = 0;
+  int num = 0, exit_reason = 3;
+  T lower = -dist;
   while (bits < 15 && dist > T(kEpsilon2) && num < 1000) {
     ++num;
     last = 0;
@@ -267,15 +275,26 @@ GG_HD GjkResult<T> gjk_distance(const LocalBody<T>& A, const LocalBody<T>& B, T 
     p[last] = support_local(A, lb_vecmat(-v, A));
     q[last] = support_local(B, lb_vecmat(v, B));
     w = lb_apply(A, p[last]) - lb_apply(B, q[last]);
-    T mu = dist - dot(v, w) / dist;
-    if (mu < dist * rel_error || mu < abs_error) break;
+    const T sep = dot(v, w) / dist;
+    if (sep > lower) lower = sep;
+    T mu = dist - sep;
+    if (mu < dist * rel_error || mu < abs_error) {
+      exit_reason = 0;
+      break;
+    }
     bool degen = false;
     for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
       if ((all_bits & bit) && y[i].x == w.x && y[i].y == w.y && y[i].z == w.z) degen = true;
-    if (degen) break;
+    if (degen) {
+      exit_reason = 1;
+      break;
+    }
     y[last] = w;
     all_bits = bits | last_bit;
-    if (!gjk_closest(bits, last, last_bit, all_bits, y, g, v)) break;
+    if (!gjk_closest(bits, last, last_bit, all_bits, y, g, v)) {
+      exit_reason = 2;
+      break;
+    }
     dist = norm(v);
   }
   GjkResult<T> r;
@@ -292,13 +311,16 @@ GG_HD GjkResult<T> gjk_distance(const LocalBody<T>& A, const LocalBody<T>& B, T 
   r.pb = lb_apply(B, sc(pb, s));
   r.dist = dist;
   r.iters = num;
+  r.exit = exit_reason;
+  r.lower = lower;
   return r;
 }
 
 // RigidBodyWithCrust::ClosestPoint general case (RigidBodyWithCrust.cpp:278-348).
 // status: 0 = features valid, 1 = ContactError, 2 = bounding spheres apart.
 template <typename T>
-GG_HD ContactGeom convex_closest_point_t(const BodyRef& A, const BodyRef& B, double tol, int* iters) {
+GG_HD ContactGeom convex_closest_point_t(const BodyRef& A, const BodyRef& B, double tol, int* iters,
+                                        int* exit_out = nullptr, double* lower_out = nullptr) {
   ContactGeom c = no_contact();
   D3 g = xsub3(A.origin, B.origin);
   if (!(xnorm(g) < xadd(A.radius, B.radius))) {
@@ -310,6 +332,8 @@ GG_HD ContactGeom convex_closest_point_t(const BodyRef& A, const BodyRef& B, dou
   LocalBody<T> lb = local_body<T>(B, shift, B.scaling);
   GjkResult<T> r = gjk_distance(la, lb, T(tol));
   *iters = r.iters;
+  if (exit_out) *exit_out = r.exit;
+  if (lower_out) *lower_out = double(r.lower);
   double distance = double(r.dist);
   if (distance < kEpsilon) {
     c.status = 1;

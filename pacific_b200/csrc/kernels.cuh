@@ -434,19 +434,28 @@ __device__ __forceinline__ void make_obstacle_ref(const StepArgs<R>& a, int oidx
   for (int i = 0; i < 3; ++i) b.lext[i] = sh.scaling_ext[i];
 }
 
-// Closest point of a general pair: FP32 GJK in the mixed path with a double
-// re-run when the FP32 overlap distance is inside a guard band around zero;
-// double GJK in the FP64 path.  Error handling (crust x10) on ContactError.
+// Closest point of a general pair.  FP64 path: double GJK.  Mixed path: an
+// FP32 GJK is a separation filter.  Its largest support-plane separation is a
+// lower bound of the shrunk bodies' distance (up to FP32 rounding, a few 1e-10
+// m at particle scale); when that bound clears the crust sum by more than
+// 1e-5 (R_A + R_B) the pair is certainly apart.  Every other pair (contacts
+// and near misses) is re-run in double from the reference's start point, so
+// contact decisions and contact geometry equal the FP64 path's.  The FP32
+// distance itself is not used for contacts: on curved bodies FP32 GJK often
+// stops in Johnson's backup procedure with an error far above the overlaps.
+// Error handling (crust x10) on ContactError.
 template <typename R>
 __device__ ContactGeom convex_closest_point(const StepArgs<R>& a, const BodyRef& A, const BodyRef& B, int& iters,
                                             int& handled) {
   ContactGeom c;
   handled = 0;
   if (sizeof(R) == 4) {
-    c = convex_closest_point_t<float>(A, B, fmax(a.gjk_tol, 1.e-6), &iters);
+    double lower = 0.;
+    c = convex_closest_point_t<float>(A, B, fmax(a.gjk_tol, 1.e-6), &iters, nullptr, &lower);
     if (c.status != 2) {
       const double guard = 1.e-5 * (A.radius + B.radius);
-      if (c.status == 1 || fabs(c.overlap) < guard) c = convex_closest_point_t<double>(A, B, a.gjk_tol, &iters);
+      if (c.status == 1 || !(lower - xadd(A.crust, B.crust) > guard))
+        c = convex_closest_point_t<double>(A, B, a.gjk_tol, &iters);
     }
   } else {
     c = convex_closest_point_t<double>(A, B, a.gjk_tol, &iters);
@@ -642,6 +651,11 @@ __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
             if (slot < (unsigned long long)a.pairs_cap) {
               a.pairs[2 * slot] = mi.x;
               a.pairs[2 * slot + 1] = idj;
+              if (a.pair_force) {
+                a.pair_force[3 * slot] = double(res.force.x);
+                a.pair_force[3 * slot + 1] = double(res.force.y);
+                a.pair_force[3 * slot + 2] = double(res.force.z);
+              }
             }
           }
         }
@@ -708,11 +722,10 @@ __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
       b0.pos_minus_contact = from_d3<R>(xsub3(Xi, g.point));
       b0.mass = R(mdi.x);
       b0.req = R(mdi.z);
+      // the law adds w x lever to the centre velocity (velocity_at)
       const D3 olev = xsub3(g.point, oo);
-      const V3<double> ow = v3<double>(O.omega[0], O.omega[1], O.omega[2]);
-      const V3<double> ovp = v3<double>(O.vel[0], O.vel[1], O.vel[2]) + cross(ow, v3<double>(olev.x, olev.y, olev.z));
-      b1.v = v3<R>(R(ovp.x), R(ovp.y), R(ovp.z));
-      b1.w = v3<R>(R(ow.x), R(ow.y), R(ow.z));
+      b1.v = v3<R>(R(O.vel[0]), R(O.vel[1]), R(O.vel[2]));
+      b1.w = v3<R>(R(O.omega[0]), R(O.omega[1]), R(O.omega[2]));
       b1.lever = from_d3<R>(olev);
       b1.pos_minus_contact = from_d3<R>(xsub3(oo, g.point));
       b1.mass = R(kObstacleMass);

@@ -1,7 +1,18 @@
 """The CUDA path against the reference's own results (golden fixtures made by
 the reference Grains3D built from its sources, tests/golden/make_golden.py).
 Pair sets and coordination exact; plain FP64 forces within 1e-12 relative,
-mixed precision within 1e-5 (force floor: the particle weight)."""
+mixed precision within 1e-5 (force floor: the particle weight).
+
+Fixtures with polyhedra are the exception.  The reference's Polyhedron::support
+hill-climbs from a warm-start vertex that each body keeps between GJK calls
+(Polyhedron.cpp:265-293) and stops unless a neighbour gains more than 1e-16, so
+on flat-face contacts, where the face vertices tie within that margin, its
+witness points (hence the contact point) depend on the order of all earlier
+GJK calls of the body.  The CUDA path evaluates pairs in parallel and uses the
+order-independent arg-max.  For those fixtures the CUDA path is held to the
+oracle run with the same arg-max support at the usual bars, and to the
+reference at the level that contact-point choice explains (pair sets and
+coordination still exact)."""
 import glob
 import os
 import sys
@@ -11,7 +22,7 @@ import pytest
 
 from pacific_b200.abi import FP64, MIXED
 
-from helpers import make, pair_set, rel_err
+from helpers import check_contact_forces, make, pair_set, rel_err
 
 pytestmark = pytest.mark.gpu
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -19,12 +30,21 @@ sys.path.insert(0, os.path.join(HERE, "golden"))
 CASES = sorted(glob.glob(os.path.join(HERE, "golden", "*.npz")))
 
 
+def has_polyhedra(sc):
+    return any(sh[0] == 3 for sh in sc.shapes)
+
+
+def convex(sc):
+    return any(sc.shapes[k][0] != 0 for k in set(np.asarray(sc.particles["shape"]).tolist()))
+
+
 @pytest.mark.parametrize("precision", [FP64, MIXED], ids=["fp64", "mixed"])
 @pytest.mark.parametrize("path", CASES, ids=[os.path.basename(c)[:-4] for c in CASES])
-def test_gpu_matches_reference_fixture(gpu_lib, path, precision):
+def test_gpu_matches_reference_fixture(oracle_lib, gpu_lib, path, precision):
     import golden_io as G
     z = np.load(path)
     sc = G.scenario_from_npz(z)
+    poly = has_polyhedra(sc)
     sim = make(gpu_lib, sc, precision)
     sim.upload_contact_memory(G.memory_from(z, "mem_in_"))
     t = float(z["time"])
@@ -35,13 +55,38 @@ def test_gpu_matches_reference_fixture(gpu_lib, path, precision):
     assert np.array_equal(sim.candidate_pairs(), z["candidate_pairs"])
     if bool(z["has_contact_pairs"]):
         assert pair_set(sim.contact_pairs()) == pair_set(z["contact_pairs"])
-    tol = 1e-12 if precision == FP64 else 1e-5
-    assert rel_err(d["force"], z["force"], weight) < tol
-    assert rel_err(d["torque"], z["torque"], weight * 1e-3) < (1e-10 if precision == FP64 else 1e-5)
+    # per-particle sums: FP64 at rounding level; in mixed precision the FP32
+    # rounding of each contact force (~1e-7 of it) is amplified where several
+    # large face contacts of a convex body nearly cancel, so the sums get 1e-4
+    # and the individual contact forces are held to 1e-5 below
+    tol = 1e-12 if precision == FP64 else (1e-5 if not convex(sc) else 1e-4)
+    ttol = 1e-10 if precision == FP64 else (1e-5 if not convex(sc) else 1e-4)
+    o = make(oracle_lib, sc)
+    o.set_polyhedron_support(True)
+    o.upload_contact_memory(G.memory_from(z, "mem_in_"))
+    o.compute_forces(t, sc.dt)
+    if poly:
+        # the reference's order-dependent support choice on flat faces
+        assert rel_err(d["force"], z["force"], weight) < 2e-3
+        ref_force, ref_torque = o.download()["force"], o.download()["torque"]
+    else:
+        ref_force, ref_torque = z["force"], z["torque"]
+    assert rel_err(d["force"], ref_force, weight) < tol
+    assert rel_err(d["torque"], ref_torque, weight * 1e-3) < ttol
+    # every particle-particle contact force
+    pg, fg = sim.contact_forces()
+    po, fo = o.contact_forces()
+    assert np.array_equal(pg, po)
+    check_contact_forces(fg, fo, weight, precision)
     # 20-40 further steps: FP64 stays at rounding level; in mixed precision the
     # FP32 rounding of forces is amplified by the chaotic dense-packing
     # dynamics (observed up to 3e-8 m after 20 steps of a dense cluster)
     steps = int(z["after_steps"])
     sim.step(steps, t, sc.dt)
     d = sim.download()
-    assert np.max(np.abs(d["position"] - z["after_position"])) < (1e-13 if precision == FP64 else 2e-7)
+    if poly:
+        o.step(steps, t, sc.dt)
+        after = o.download()["position"]
+    else:
+        after = z["after_position"]
+    assert np.max(np.abs(d["position"] - after)) < (1e-13 if precision == FP64 else 2e-7)
