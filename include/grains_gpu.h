@@ -298,6 +298,53 @@ int grains_gpu_sphere_contacts_noalloc(int32_t n, const double* position, const 
                                        int32_t* pairs, int64_t cap, int64_t* n_pairs, int32_t* status,
                                        void* stream);
 
+/* ---- gradients: differentiable run and its adjoint ------------------------ */
+/* No counterpart in the reference (Grains3D has no gradients).  A handle on a
+ * context whose particles are uploaded: spheres with static box walls, Hooke
+ * or HookeMemory laws, one or more systems.
+ *
+ * grains_gpu_adjoint_forward runs the leapfrog of Grains::Simulation
+ * (Grains.cpp:169-174, 344-364) for n_steps from the context's current state,
+ * with the context's contact laws: the leapfrog start (one force evaluation,
+ * then kdelta and rolling springs of new memory entries zeroed), n_steps
+ * kick-drift-kick steps and the final half kick.  The context's own state is
+ * not changed.  The contact memory starts empty.  It keeps a checkpoint (state
+ * and contact rows) every 'checkpoint_every' force evaluations and a tape of
+ * one segment; the final positions, velocities and angular velocities (world
+ * frame) are written to the host arrays (3n doubles each, upload order; any
+ * may be NULL).  Contact pairs are owned by the lower upload index.
+ *
+ * grains_gpu_adjoint_backward takes dL/d(final position, velocity, angular
+ * velocity) (3n doubles each, upload order, NULL = zero) and returns
+ * dL/d(initial position, velocity, angular velocity) and, in grad_laws, 4
+ * doubles per law-table slot: dL/d(kn, en, muc, kt).  Slot of the law used by
+ * a contact whose owner has material a and partner material b (a wall's
+ * material for walls) in system s: (s * M + a) * M + b, M = max_materials of
+ * the context; a law set for (a, b) with a != b is used through both (a, b)
+ * and (b, a), so its gradient is the sum of the two slots.  Gradients are of
+ * the discrete map (exact up to the precision of the context: FP32 adjoint in
+ * mixed precision), valid away from contact onset / release events.
+ * Errors of the run (ContactError, MotionError, out of grid, more contacts
+ * than history_capacity) fail the call. */
+typedef struct grains_gpu_adjoint grains_gpu_adjoint;
+int grains_gpu_adjoint_create(grains_gpu_ctx* ctx, int32_t checkpoint_every, grains_gpu_adjoint** out);
+int grains_gpu_adjoint_destroy(grains_gpu_adjoint* adj);
+int grains_gpu_adjoint_last_error(const grains_gpu_adjoint* adj, char* buf, size_t len);
+int grains_gpu_adjoint_law_slots(const grains_gpu_adjoint* adj, int32_t* n_slots);
+int grains_gpu_adjoint_forward(grains_gpu_adjoint* adj, int32_t n_steps, double dt, double* position,
+                               double* velocity, double* omega);
+/* Signature of the contact sets of the last forward run: the xor of a 64-bit
+ * hash of every (force evaluation, owner, partner, branch of the contact law)
+ * contact, and the number of contacts summed over the evaluations.  Two runs
+ * with equal signatures met the same contacts at the same steps, each in the
+ * same case of the law (tangential direction from the velocity or from the
+ * spring; stick or Coulomb slip): the condition under which the run is smooth
+ * between them and finite differences approximate its gradient. */
+int grains_gpu_adjoint_contact_signature(const grains_gpu_adjoint* adj, uint64_t* signature, int64_t* n_contacts);
+int grains_gpu_adjoint_backward(grains_gpu_adjoint* adj, const double* dl_dposition, const double* dl_dvelocity,
+                                const double* dl_domega, double* grad_position, double* grad_velocity,
+                                double* grad_omega, double* grad_laws, int32_t n_grad_laws);
+
 /* ---- shape helpers (reference geometry formulas, host only) -------------- */
 /* volume, circumscribed radius and body-frame principal inertia per unit
  * density: Sphere.cpp:61-81,152-155; Box.cpp:181-210; Cylinder.cpp:61-85;

@@ -136,6 +136,13 @@ _GPU_ONLY = {
     "profile_kernels": [_VP, C.c_int32, _P_F64, C.c_double, C.c_char_p, C.c_size_t, _P_F64,
                         C.POINTER(C.c_int64), C.c_int32, _P_I32],
     "shape_properties": [C.c_int32, _P_F64, C.c_int32, _P_F64, _P_F64, _P_F64],
+    "adjoint_create": [_VP, C.c_int32, C.POINTER(_VP)],
+    "adjoint_destroy": [_VP],
+    "adjoint_last_error": [_VP, C.c_char_p, C.c_size_t],
+    "adjoint_law_slots": [_VP, _P_I32],
+    "adjoint_forward": [_VP, C.c_int32, C.c_double, _P_F64, _P_F64, _P_F64],
+    "adjoint_contact_signature": [_VP, C.POINTER(C.c_uint64), C.POINTER(C.c_int64)],
+    "adjoint_backward": [_VP, _P_F64, _P_F64, _P_F64, _P_F64, _P_F64, _P_F64, _P_F64, C.c_int32],
 }
 
 
@@ -457,3 +464,71 @@ class Simulation:
                                                    max_kernels, C.byref(nk)))
         keys = names.value.decode().split("\n")
         return t.value, {keys[i]: (ms[i], launches[i]) for i in range(nk.value)}
+
+
+class Adjoint:
+    """Differentiable run of a Simulation's current state (spheres, static box
+    walls) and its adjoint: grains_gpu_adjoint_* of the C ABI."""
+
+    def __init__(self, sim, checkpoint_every=100):
+        self.sim = sim
+        self.h = _VP()
+        rc = sim.lib.fn["adjoint_create"](sim.ctx, checkpoint_every, C.byref(self.h))
+        if rc:
+            msg = self.last_error() if self.h else "adjoint_create failed"
+            self.close()
+            raise error_for(rc, msg)
+        n = C.c_int32()
+        self._check(sim.lib.fn["adjoint_law_slots"](self.h, C.byref(n)))
+        self.n_law_slots = n.value
+
+    def close(self):
+        if self.h:
+            self.sim.lib.fn["adjoint_destroy"](self.h)
+            self.h = _VP()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def last_error(self):
+        buf = C.create_string_buffer(4096)
+        self.sim.lib.fn["adjoint_last_error"](self.h, buf, 4096)
+        return buf.value.decode(errors="replace")
+
+    def _check(self, rc):
+        if rc:
+            raise error_for(rc, self.last_error())
+
+    def forward(self, n_steps, dt):
+        """Final state {position, velocity, omega} (n, 3) in upload order."""
+        n = self.sim.n
+        x, v, w = (np.zeros(3 * n) for _ in range(3))
+        self._check(self.sim.lib.fn["adjoint_forward"](self.h, n_steps, dt, _ptr(x, C.c_double), _ptr(v, C.c_double),
+                                                       _ptr(w, C.c_double)))
+        return {"position": x.reshape(n, 3), "velocity": v.reshape(n, 3), "omega": w.reshape(n, 3)}
+
+    def signature(self):
+        """(hash of the contact sets of the last forward run, total contacts)."""
+        sig, cnt = C.c_uint64(), C.c_int64()
+        self._check(self.sim.lib.fn["adjoint_contact_signature"](self.h, C.byref(sig), C.byref(cnt)))
+        return sig.value, cnt.value
+
+    def backward(self, dposition=None, dvelocity=None, domega=None):
+        """Gradients of the loss w.r.t. the initial state and, in 'laws', an
+        (n_law_slots, 4) array of dL/d(kn, en, muc, kt) per law-table slot."""
+        n = self.sim.n
+
+        def arg(a):
+            return None if a is None else np.ascontiguousarray(a, dtype=np.float64).reshape(-1)
+        gx, gv, gw = arg(dposition), arg(dvelocity), arg(domega)
+        ox, ov, ow = (np.zeros(3 * n) for _ in range(3))
+        gl = np.zeros(4 * self.n_law_slots)
+        self._check(self.sim.lib.fn["adjoint_backward"](self.h, _ptr(gx, C.c_double), _ptr(gv, C.c_double),
+                                                        _ptr(gw, C.c_double), _ptr(ox, C.c_double),
+                                                        _ptr(ov, C.c_double), _ptr(ow, C.c_double),
+                                                        _ptr(gl, C.c_double), len(gl)))
+        return {"position": ox.reshape(n, 3), "velocity": ov.reshape(n, 3), "omega": ow.reshape(n, 3),
+                "laws": gl.reshape(-1, 4)}

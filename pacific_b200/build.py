@@ -23,10 +23,14 @@ NVCC = os.environ.get("NVCC", "nvcc")
 UNITS = [
     ("kernels_fp64.cu", ["-fmad=false"]),
     ("kernels_mixed.cu", ["-fmad=false"]),
+    ("adjoint_fp64.cu", ["-fmad=false"]),
+    ("adjoint_mixed.cu", ["-fmad=false"]),
+    ("adjoint_api.cu", []),
     ("api.cu", []),
     ("noalloc.cu", []),
 ]
-HEADERS = ["common.cuh", "sphere_contact.cuh", "contact_law.cuh", "gjk.cuh", "kernels.cuh", "device_state.h"]
+HEADERS = ["common.cuh", "sphere_contact.cuh", "contact_law.cuh", "gjk.cuh", "kernels.cuh", "device_state.h",
+           "dual.cuh", "adjoint.cuh", "adjoint.h"]
 
 
 def _newer(target, sources):

@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "../../include/grains_gpu.h"
+#include "adjoint.h"
 #include "device_state.h"
 #include "gjk.cuh"
 #include "sphere_contact.cuh"
@@ -1593,4 +1594,47 @@ int grains_gpu_shape_properties(int32_t type, const double* params, int32_t n, d
 
 namespace gg {
 int launches_per_fused_step() { return 8; }
+
+int context_view(grains_gpu_ctx* c, ContextView* v, std::string& err) {
+  if (!c || !v) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) {
+    err = "no particles uploaded";
+    return GRAINS_GPU_NOT_READY;
+  }
+  if (int rc = flush_kick(c)) {
+    err = c->err;
+    return rc;
+  }
+  const int maxmat = c->cfg.max_materials > 0 ? c->cfg.max_materials : 4;
+  *v = ContextView{};
+  v->precision = c->precision;
+  v->device = c->cfg.device;
+  v->stream = c->stream;
+  v->n = (int)c->n;
+  v->n_cells = c->n_cells;
+  v->n_sys = (int)c->sys.size();
+  v->n_laws = (int)c->sys.size() * maxmat * maxmat;
+  v->hist_cap = c->hist_cap;
+  v->spheres_only = c->has_basis ? 0 : 1;
+  v->box_walls_only = 1;
+  for (const auto& s : c->sys)
+    for (const auto& o : s.obs)
+      if (c->shapes[o.shape].type != GRAINS_GPU_BOX) v->box_walls_only = 0;
+  v->n_moving = c->n_moving;
+  v->sys = c->d_sys;
+  v->shapes = c->d_shapes;
+  v->obs = c->d_obs;
+  v->cell_obs_start = c->d_cell_obs_start;
+  v->cell_obs_idx = c->d_cell_obs_idx;
+  v->laws = c->d_laws;
+  const auto& b = c->buf[c->cur];
+  v->xr = b.xr;
+  v->md = b.md;
+  v->meta = b.meta;
+  v->orig = b.orig;
+  v->v = b.v;
+  v->w = b.w;
+  v->inertia = b.inertia;
+  return 0;
+}
 }  // namespace gg

@@ -84,6 +84,19 @@ GG_HD double xdot(D3 a, D3 b) { return xadd(xadd(xmul(a.x, b.x), xmul(a.y, b.y))
 GG_HD double xnorm(D3 a) { return xsqrt(xdot(a, a)); }
 GG_HD double xget(D3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
 
+// ---- generic scalar functions -------------------------------------------------
+// Unqualified gsqrt / gabs in the generic code below let a forward-mode dual
+// number (dual.cuh) overload them; for float and double they are std::sqrt
+// and std::fabs.
+template <typename R>
+GG_HD R gsqrt(R x) {
+  return std::sqrt(x);
+}
+template <typename R>
+GG_HD R gabs(R x) {
+  return std::fabs(x);
+}
+
 // ---- generic vectors -------------------------------------------------------
 template <typename R>
 struct V3 {
@@ -123,7 +136,7 @@ GG_HD V3<R> cross(V3<R> a, V3<R> b) {  // Vector3::operator^, Vector3.cpp:114-11
 }
 template <typename R>
 GG_HD R norm(V3<R> a) {
-  return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+  return gsqrt(a.x * a.x + a.y * a.y + a.z * a.z);
 }
 template <typename R>
 GG_HD R norm2(V3<R> a) {
@@ -132,8 +145,7 @@ GG_HD R norm2(V3<R> a) {
 template <typename R>
 GG_HD V3<R> round3(V3<R> a) {  // Group3::round(EPSILON), Group3.cpp:390-395
   const R tol = R(kEpsilon);
-  return v3<R>(std::fabs(a.x) < tol ? R(0) : a.x, std::fabs(a.y) < tol ? R(0) : a.y,
-               std::fabs(a.z) < tol ? R(0) : a.z);
+  return v3<R>(gabs(a.x) < tol ? R(0) : a.x, gabs(a.y) < tol ? R(0) : a.y, gabs(a.z) < tol ? R(0) : a.z);
 }
 template <typename R>
 GG_HD V3<R> from_d3(D3 a) {
@@ -172,7 +184,7 @@ GG_HD V3<R> qmult_to_v3(Qt<R> a, Qt<R> rhs) {  // Quaternion::multToVector3, :10
 }
 template <typename R>
 GG_HD R qnorm(Qt<R> q) {
-  return std::sqrt(q.v.x * q.v.x + q.v.y * q.v.y + q.v.z * q.v.z + q.w * q.w);
+  return gsqrt(q.v.x * q.v.x + q.v.y * q.v.y + q.v.z * q.v.z + q.w * q.w);
 }
 // q x [0,v] x conj(q) written as the reference composes it in
 // ParticleKinematics::Move (ParticleKinematics.cpp:79-80): q.multToVector3((v, conj(q)))
@@ -188,12 +200,12 @@ GG_HD V3<R> q_to_body(Qt<R> q, V3<R> v) {
 // Quaternion::setRotFromTwoVectors, Quaternion.cpp:263-289
 template <typename R>
 GG_HD Qt<R> q_rot_from_two(V3<R> u, V3<R> v) {
-  R nn = std::sqrt(dot(u, u) * dot(v, v));
+  R nn = gsqrt(dot(u, u) * dot(v, v));
   R real = nn + dot(u, v);
   V3<R> vect;
   if (real < R(1.e-6) * nn) {
     real = R(0);
-    vect = std::fabs(u.x) > std::fabs(u.z) ? v3<R>(-u.y, u.x, R(0)) : v3<R>(R(0), -u.z, u.y);
+    vect = gabs(u.x) > gabs(u.z) ? v3<R>(-u.y, u.x, R(0)) : v3<R>(R(0), -u.z, u.y);
   } else {
     vect = cross(u, v);
   }

@@ -49,12 +49,23 @@ GG_HD V3<R> velocity_at(const BodyAtContact<R>& b) {  // Particle.cpp:662-666
   return b.v + cross(b.w, b.lever);
 }
 
+// Branch flags of one law evaluation (optional output): which case of the
+// tangential direction and whether Coulomb's limit was reached.  The law is
+// smooth in its inputs between changes of these flags.
+enum { kLawTangentVelocity = 1, kLawTangentSpring = 2, kLawSlip = 4 };
+
 // computeTangentialVector (HookeMemoryContactForceModel.cpp:54-65)
 template <typename R>
-GG_HD V3<R> tangential_vector(R epst, R n_t, V3<R> ut, V3<R> kd) {
-  if (norm(ut) > R(0.001)) return dv(-ut, norm(ut));
+GG_HD V3<R> tangential_vector(R epst, R n_t, V3<R> ut, V3<R> kd, int* branch = nullptr) {
+  if (norm(ut) > R(0.001)) {
+    if (branch) *branch |= kLawTangentVelocity;
+    return dv(-ut, norm(ut));
+  }
   V3<R> s = kd + sc(ut, n_t);
-  if ((norm(kd) > epst || norm(sc(ut, n_t)) > epst) && norm(s) > epst) return dv(-s, norm(s));
+  if ((norm(kd) > epst || norm(sc(ut, n_t)) > epst) && norm(s) > epst) {
+    if (branch) *branch |= kLawTangentSpring;
+    return dv(-s, norm(s));
+  }
   return v3<R>(R(0), R(0), R(0));
 }
 
@@ -62,17 +73,18 @@ GG_HD V3<R> tangential_vector(R epst, R n_t, V3<R> ut, V3<R> kd) {
 // holds it on entry (when existed) and the updated entry on exit.
 template <typename R>
 GG_HD LawResult<R> hooke_memory(const LawParams<R>& L, R dt, V3<R> pen, const BodyAtContact<R>& b0,
-                                const BodyAtContact<R>& b1, bool existed, PairMemory<R>& mem) {
+                                const BodyAtContact<R>& b1, bool existed, PairMemory<R>& mem,
+                                int* branch = nullptr) {
   V3<R> normal = round3(dv(pen, norm(pen)));
   V3<R> tmpV = velocity_at(b0) - velocity_at(b1);
   V3<R> v_n = sc(normal, dot(tmpV, normal));
   V3<R> v_t = tmpV - v_n;
   V3<R> delFN = sc(pen, L.kn);
   R avmass = R(1) / (R(1) / b0.mass + R(1) / b1.mass);
-  R gamman = R(-2) * L.beta * std::sqrt(avmass * L.kn);
+  R gamman = R(-2) * L.beta * gsqrt(avmass * L.kn);
   delFN = delFN - sc(v_n, gamman);
   R normFN = norm(delFN);
-  R etat = L.etat == R(-1) ? -L.beta * std::sqrt(L.kn / avmass) : L.etat;
+  R etat = L.etat == R(-1) ? -L.beta * gsqrt(L.kn / avmass) : L.etat;
   R gammat = R(2) * etat * avmass;
   V3<R> viscousFT = sc(v_t, -gammat);
   Qt<R> qrot{v3<R>(R(0), R(0), R(0)), R(0)};
@@ -85,12 +97,13 @@ GG_HD LawResult<R> hooke_memory(const LawParams<R>& L, R dt, V3<R> pen, const Bo
   }
   mem.kdelta = mem.kdelta + sc(v_t, dt * L.kt);
   mem.prev_normal = normal;
-  V3<R> tij = tangential_vector(L.epst, gammat, v_t, mem.kdelta);
+  V3<R> tij = tangential_vector(L.epst, gammat, v_t, mem.kdelta, branch);
   R normFT = norm(-mem.kdelta + viscousFT);
   V3<R> delFT;
   if (normFT <= L.muc * normFN) {
     delFT = sc(tij, norm(-mem.kdelta + viscousFT));
   } else {
+    if (branch) *branch |= kLawSlip;
     if (L.kt != R(0)) mem.kdelta = dv(sc(tij, -L.muc * normFN) + viscousFT, L.kt);
     delFT = sc(tij, L.muc * normFN);
   }
@@ -115,22 +128,23 @@ GG_HD LawResult<R> hooke_memory(const LawParams<R>& L, R dt, V3<R> pen, const Bo
 // Hooke law (no memory)
 template <typename R>
 GG_HD LawResult<R> hooke(const LawParams<R>& L, V3<R> pen, const BodyAtContact<R>& b0,
-                         const BodyAtContact<R>& b1) {
+                         const BodyAtContact<R>& b1, int* branch = nullptr) {
   V3<R> normal = round3(dv(pen, norm(pen)));
   V3<R> tmpV = velocity_at(b0) - velocity_at(b1);
   V3<R> v_n = sc(normal, dot(tmpV, normal));
   V3<R> v_t = tmpV - v_n;
   V3<R> delFN = sc(pen, L.kn);
   R avmass = R(1) / (R(1) / b0.mass + R(1) / b1.mass);
-  R gamman = R(-2) * L.beta * std::sqrt(avmass * L.kn);
+  R gamman = R(-2) * L.beta * gsqrt(avmass * L.kn);
   delFN = delFN - sc(v_n, gamman);
   R normFN = norm(delFN);
-  R etat = L.etat == R(-1) ? -L.beta * std::sqrt(L.kn / avmass) : L.etat;
+  R etat = L.etat == R(-1) ? -L.beta * gsqrt(L.kn / avmass) : L.etat;
   R gammat = R(2) * etat * avmass;
   V3<R> delFT = sc(v_t, -gammat);
   R fn = L.muc * normFN;
   R ft = norm(delFT);
   if (fn < ft) {
+    if (branch) *branch |= kLawSlip;
     R nvt = norm(v_t);
     V3<R> tangent = v3<R>(R(0), R(0), R(0));
     if (nvt > R(kEpsilon)) tangent = dv(-v_t, nvt);

@@ -174,13 +174,13 @@ def ensemble_512(n_systems=512, seed=4, n_min=200, n_max=20000):
     return Scenario("ensemble_512", shapes, doms, laws, obstacles, p, 5.0e-6, 5000, meta=dict(sizes=ns))
 
 
-def adjoint_4k(seed=5, vseed=6, kn=1.0e5, en=0.9, mu=0.5):
+def adjoint_4k(seed=5, vseed=6, kn=1.0e5, en=0.9, mu=0.5, n=4096, kt_ratio=0.8):
     """4,096 spheres r = 1 mm on a 16^3 lattice (spacing 2.4 mm) in a
     40x40x60 mm box with floor + 4 walls, velocities N(0, 0.2 m/s); kn = 1e5,
-    en = 0.9, mu = 0.5, kt = 0.8 kn, dt = 1e-5 s, 2,000 steps."""
+    en = 0.9, mu = 0.5, kt = 0.8 kn, dt = 1e-5 s, 2,000 steps.  A smaller n
+    keeps the first n lattice sites (the lowest layers)."""
     rng = np.random.default_rng(seed)
     vrng = np.random.default_rng(vseed)
-    n = 4096
     crust = 0.05 * MM
     lo, hi = np.zeros(3), np.array([40.0, 40.0, 60.0]) * MM
     pos = lattice(n, lo, hi, 2.4 * MM, 1.2 * MM, 0.1 * MM, rng)
@@ -188,11 +188,11 @@ def adjoint_4k(seed=5, vseed=6, kn=1.0e5, en=0.9, mu=0.5):
     shapes = [(SPHERE, [1.0 * MM])]
     wshapes, obs = box_walls(lo, hi, "xXyYz", 0.5 * MM, crust, len(shapes), -1)
     shapes += wshapes
-    laws = [[(0, 0, HOOKE_MEMORY, hooke_memory_params(kn, en, mu, 0.8 * kn)),
-             (0, 1, HOOKE_MEMORY, hooke_memory_params(kn, en, mu, 0.8 * kn))]]
+    laws = [[(0, 0, HOOKE_MEMORY, hooke_memory_params(kn, en, mu, kt_ratio * kn)),
+             (0, 1, HOOKE_MEMORY, hooke_memory_params(kn, en, mu, kt_ratio * kn))]]
     dom = [dict(origin=lo, size=hi - lo, cell_size=2.0 * 1.0 * MM, gravity=(0.0, 0.0, -9.81))]
     p = _spheres(n, np.full(n, 1.0 * MM), 2500.0, pos, vel, crust)
-    return Scenario("adjoint_4k", shapes, dom, laws, [obs], p, 1.0e-5, 2000)
+    return Scenario("adjoint_4k" if n == 4096 else "adjoint_%d" % n, shapes, dom, laws, [obs], p, 1.0e-5, 2000)
 
 
 def small_box(n=64, seed=0, velocity_sigma=0.05, spacing=2.04, jitter=0.02, radius_range=(1.0, 1.0)):

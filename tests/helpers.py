@@ -50,3 +50,65 @@ def check_contact_forces(fg, fo, floor, precision):
     else:
         assert rel_err_quantile(fg, fo, floor, 0.99) < 1e-5
         assert rel_err(fg, fo, floor) < 1e-4
+
+
+TANGENT_SO = None
+
+
+def tangent_run(sc, n_steps, dir_v0=None, dir_laws=None, n_mat=4):
+    """The oracle's forward-mode run (oracle/tangent_oracle.cpp) of scenario
+    `sc` (spheres, one system, box walls): final state and, for each
+    direction, the derivative of the final state along (dir_v0[d] (n, 3),
+    dir_laws[d] (n_mat^2, 4) = d(kn, en, muc, kt) per law slot)."""
+    import ctypes as C
+    import os
+    from pacific_b200 import scenarios as S
+    global TANGENT_SO
+    if TANGENT_SO is None:
+        root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+        TANGENT_SO = C.CDLL(os.path.join(root, "oracle", "_build", "libgrains_tangent.so"))
+    p = sc.particles
+    n = len(p["id"])
+    d = sc.domains[0]
+    dom = np.concatenate([np.asarray(d["origin"], float), np.asarray(d["size"], float), [d["cell_size"]],
+                          np.asarray(d["gravity"], float)])
+    walls = []
+    for o in sc.obstacles[0]:
+        t, prm = sc.shapes[o["shape"]]
+        assert t == S.BOX
+        e = np.abs(np.asarray(prm, float)) / 2.0
+        vol = 8.0 * e[0] * e[1] * e[2]
+        walls.append(list(o["transform"]) + list(e) + [o["crust"], o["material"], (0.75 / np.pi * vol) ** (1.0 / 3.0)])
+    laws = np.zeros((n_mat * n_mat, 10))
+    laws[:, 0] = -1
+    for a, b, law, prm in sc.laws[0]:
+        if law == S.HOOKE_MEMORY:
+            row = [1, prm[0], prm[1], prm[2], prm[3], prm[4], prm[5], prm[6], prm[7], 0.0]
+        else:
+            row = [0, prm[0], prm[1], prm[2], prm[3], 0.0, 0.0, 0.0, 0.0, prm[4]]
+        laws[a * n_mat + b] = row
+        laws[b * n_mat + a] = row
+    nd = 0 if dir_v0 is None else len(dir_v0)
+
+    def f64(a):
+        return np.ascontiguousarray(a, dtype=np.float64)
+    x0, v0, w0 = f64(p["position"]), f64(p["velocity"]), f64(p["omega"])
+    rad, mass, inertia, crust = f64(p["radius"]), f64(p["mass"]), f64(np.asarray(p["inertia"])[:, 0]), f64(p["crust"])
+    mat = np.ascontiguousarray(p["material"], dtype=np.int32)
+    wl = f64(np.asarray(walls).reshape(-1))
+    dv = f64(np.zeros((max(nd, 1), n, 3)) if dir_v0 is None else dir_v0)
+    dl = f64(np.zeros((max(nd, 1), n_mat * n_mat, 4)) if dir_laws is None else dir_laws)
+    x, v, w = np.zeros(3 * n), np.zeros(3 * n), np.zeros(3 * n)
+    tx, tv, tw = (np.zeros(max(nd, 1) * 3 * n) for _ in range(3))
+    P = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    fn = TANGENT_SO.grains_tangent_run
+    fn.restype = C.c_int
+    rc = fn(C.c_int(n), P(x0), P(v0), P(w0), P(rad), P(mass), P(inertia), P(crust),
+            mat.ctypes.data_as(C.POINTER(C.c_int)), P(f64(dom)), C.c_int(len(walls)), P(wl), C.c_int(n_mat),
+            P(f64(laws)), C.c_int(n_steps), C.c_double(sc.dt), C.c_int(nd), P(dv), P(dl), P(x), P(v), P(w),
+            P(tx), P(tv), P(tw))
+    assert rc == 0, "tangent run failed (contact or motion error)"
+    fin = {"position": x.reshape(n, 3), "velocity": v.reshape(n, 3), "omega": w.reshape(n, 3)}
+    tan = {"position": tx.reshape(-1, n, 3)[:nd], "velocity": tv.reshape(-1, n, 3)[:nd],
+           "omega": tw.reshape(-1, n, 3)[:nd]}
+    return fin, tan
