@@ -66,13 +66,15 @@ def parse():
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--ref-dem-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
+    ap.add_argument("--adjoint", action="store_true", help="time the adjoint workload (4,096 spheres)")
     return ap.parse_args()
 
 
 def scenario(name):
     from pacific_b200 import scenarios as S
     return {"polydisperse_200k": S.polydisperse_200k, "settling_1k": S.settling_1k,
-            "adjoint_4k": S.adjoint_4k, "drum_100k": S.drum}[name]()
+            "adjoint_4k": S.adjoint_4k, "drum_100k": S.drum, "ensemble_512": S.ensemble_512}[name]()
 
 
 def measured_peaks():
@@ -219,6 +221,97 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def contact_force_error(lib, sc, state, mem, device):
+    """Per-contact relative error of the mixed-precision contact forces against
+    the plain FP64 path on identical states and contact memories: max and 99th
+    percentile of |f_mixed - f_fp64| / max(|f_fp64|, weight) over the
+    particle-particle contacts."""
+    from pacific_b200 import scenarios as S
+    from pacific_b200.abi import FP64, MIXED, Simulation
+    p = dict(sc.particles)
+    for k in ["position", "quaternion", "velocity", "omega"]:
+        p[k] = state[k]
+    if sc.particles.get("basis") is not None:
+        p["basis"] = state["basis"]
+    sc2 = S.Scenario(sc.name, sc.shapes, sc.domains, sc.laws, sc.obstacles, p, sc.dt, sc.n_steps)
+    res = {}
+    for name, prec in [("fp64", FP64), ("mixed", MIXED)]:
+        s = Simulation(lib, prec, max_particles=sc.n, n_systems=len(sc.domains), device=device)
+        S.apply(s, sc2)
+        s.upload_contact_memory(mem)
+        s.compute_forces(0.0, sc.dt)
+        res[name] = s.contact_forces()
+        s.close()
+    (p64, f64_), (pm, fm) = res["fp64"], res["mixed"]
+    if len(p64) == 0 or not np.array_equal(p64, pm):
+        return {"n_contacts": int(len(p64)), "pairs_equal": bool(np.array_equal(p64, pm))}
+    w = float(np.min(sc.particles["mass"])) * 9.81
+    rel = np.linalg.norm(fm - f64_, axis=1) / np.maximum(np.linalg.norm(f64_, axis=1), w)
+    return {"max": float(rel.max()), "p99": float(np.quantile(rel, 0.99)), "median": float(np.median(rel)),
+            "n_contacts": int(len(rel)), "pairs_equal": True, "floor": "particle weight",
+            "state": "end of the timed run, same state and contact memory in both precisions"}
+
+
+def run_adjoint(args, rank, world, local):
+    """The adjoint workload (4,096 spheres, 2,000 steps, a checkpoint every 100
+    force evaluations): device time of a differentiable forward run plus its
+    adjoint, in both precisions.  (Gradient accuracy against the FP64
+    dual-number oracle: tests/test_adjoint_gpu.py and
+    tests/measure_adjoint_accuracy.py.)"""
+    import torch
+    import pacific_b200
+    from pacific_b200 import scenarios as S
+    from pacific_b200.abi import FP64, MIXED, Adjoint, Simulation
+    torch.cuda.set_device(local)
+    lib = pacific_b200.load_library()
+    sc = S.adjoint_4k()
+    n, steps, every = sc.n, sc.n_steps, 100
+
+    def loss_grads(final):
+        m = sc.particles["mass"]
+        inertia = np.asarray(sc.particles["inertia"])[:, 0]
+        v, w = final["velocity"], final["omega"]
+        zc = final["position"][:, 2].mean()
+        ke = np.mean(0.5 * m * (v * v).sum(1) + 0.5 * inertia * (w * w).sum(1))
+        z0, k0 = 0.9 * zc, 0.5 * ke
+        gx = np.zeros_like(v)
+        gx[:, 2] = 2.0 * (zc - z0) / n
+        return (gx, 2.0 * (ke - k0) * (m[:, None] * v) / n, 2.0 * (ke - k0) * (inertia[:, None] * w) / n)
+
+    out = {}
+    for name, prec in [("mixed", MIXED), ("fp64", FP64)]:
+        sim = Simulation(lib, prec, max_particles=n, device=local)
+        S.apply(sim, sc)
+        adj = Adjoint(sim, every)
+        stream = torch.cuda.ExternalStream(sim.stream_handle(), device=local)
+        for _ in range(args.warmup):
+            adj.backward(*loss_grads(adj.forward(steps, sc.dt)))
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        fwd = bwd = 0.0
+        for _ in range(args.steps):
+            e[0].record(stream)
+            fin = adj.forward(steps, sc.dt)
+            e[1].record(stream)
+            adj.backward(*loss_grads(fin))
+            e[2].record(stream)
+            torch.cuda.synchronize()
+            fwd += e[0].elapsed_time(e[1])
+            bwd += e[1].elapsed_time(e[2])
+        out[name] = {"forward_ms": fwd / args.steps, "backward_ms": bwd / args.steps,
+                     "value": n * steps * args.steps / ((fwd + bwd) / 1e3), "contacts": adj.signature()[1]}
+        adj.close()
+        sim.close()
+    line = {"metric": "particle-steps/s (differentiable forward + adjoint)", "value": out["mixed"]["value"],
+            "unit": "particle-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": out["mixed"]["forward_ms"] + out["mixed"]["backward_ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": "adjoint_4k", "particles": n, "dem_steps": steps, "checkpoint_every": every,
+                       "loss": "(z_com - 0.9 z_com0)^2 + (KE - 0.5 KE0)^2"},
+            "mixed": out["mixed"], "fp64": out["fp64"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -226,6 +319,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.adjoint:
+        return run_adjoint(args, rank, world, local)
 
     import torch
     import torch.distributed as dist
@@ -240,28 +335,30 @@ def main():
     lib = pacific_b200.load_library()
     prec = MIXED if args.precision == "mixed" else FP64
     sc = scenario(args.workload)
-    sim = Simulation(lib, prec, max_particles=sc.n, n_systems=len(sc.domains), device=local)
-    S.apply(sim, sc)
-    sim.initialize_leapfrog(0.0, sc.dt)
-    stream = torch.cuda.ExternalStream(sim.stream_handle(), device=local)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda:%d" % local)
 
-    t = 0.0
-    for _ in range(args.warmup):
-        t = sim.step(args.chunk, t, sc.dt)
-    sim.synchronize()
-    # the timed run starts again from the initial state: K chunks of the
-    # workload's run (20 x 1000 = the whole 20,000-step run by default)
-    sim.update(sc.particles)
-    sim.reset_stats()
-    sim.initialize_leapfrog(0.0, sc.dt)
-    t = 0.0
-
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
+    def timed_run(precision, sample_clocks):
+        """W warm-up chunks, then K timed chunks from the initial state (the
+        whole 20,000-step run by default); device time in ms over the K chunks."""
+        sim = Simulation(lib, precision, max_particles=sc.n, n_systems=len(sc.domains), device=local)
+        S.apply(sim, sc)
+        sim.initialize_leapfrog(0.0, sc.dt)
+        stream = torch.cuda.ExternalStream(sim.stream_handle(), device=local)
+        t = 0.0
+        for _ in range(args.warmup):
+            t = sim.step(args.chunk, t, sc.dt)
+        sim.synchronize()
+        sim.update(sc.particles)
+        sim.reset_stats()
+        sim.initialize_leapfrog(0.0, sc.dt)
+        t = 0.0
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        clk = ClockSampler(local) if sample_clocks else None
+        if clk:
+            clk.__enter__()
         for k in range(args.steps):
             with torch.cuda.stream(stream):
                 flush.fill_(k & 0xFF)          # L2 flush between timed chunks (untimed)
@@ -270,7 +367,12 @@ def main():
             ev[k][1].record(stream)
         torch.cuda.synchronize()
         sim.synchronize()
-    ms = sum(a.elapsed_time(b) for a, b in ev)
+        if clk:
+            clk.__exit__()
+        return sim, stream, t, sum(a.elapsed_time(b) for a, b in ev), clk
+
+    sim, stream, t, ms, clk = timed_run(prec, True)
+    st_end, mem_end = sim.download(), sim.contact_memory()   # state at the end of the timed run
     if world > 1:
         tt = torch.tensor([ms], device="cuda:%d" % local, dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
@@ -348,6 +450,22 @@ def main():
         "status": st["status"],
         "clocks": clk.summary(),
     }
+    if prec == MIXED and not args.no_fp64:
+        # the plain FP64 path on the same run, and the mixed-precision contact
+        # force error against it on identical states (the end of the run)
+        sim64, _, _, ms64, _ = timed_run(FP64, False)
+        if world > 1:
+            tt = torch.tensor([ms64], device="cuda:%d" % local, dtype=torch.float64)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms64 = float(tt.item())
+        sim64.close()
+        v64 = total_particles * args.chunk * args.steps / (ms64 / 1e3)
+        line["fp64"] = {"value": v64, "unit": "particle-steps/s", "ms_per_step": ms64 / args.steps,
+                        "mixed_over_fp64": value / v64}
+        if len(sc.domains) == 1:
+            line["contact_force_error"] = contact_force_error(lib, sc, st_end, mem_end, local)
+        else:  # contact-memory ids are per system; the comparison is run on single systems
+            line["contact_force_error"] = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scenario(args.workload), args.cpu_steps)
     if rank == 0:

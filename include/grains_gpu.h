@@ -257,6 +257,35 @@ int grains_gpu_get_stats(grains_gpu_ctx* ctx, grains_gpu_stats* st);
 /* Reset the accumulated status bits and statistics. */
 int grains_gpu_reset_stats(grains_gpu_ctx* ctx);
 
+/* ---- tuning ---------------------------------------------------------------- */
+/* No counterpart in the reference (its grid is fixed by CellSizeFactor and it
+ * has no launch shapes).  Launch and grid choices of a context, none of which
+ * changes contacts or forces beyond the order of floating-point sums:
+ *   cell_factor    linked-cell edge = cell_factor x the domain's cell_size
+ *                  (1 = LinkedCell::set's grid; 1 .. 4).  Candidate pairs
+ *                  (a diagnostic) follow the grid.
+ *   contacts_block threads per block of the broadphase kernel (32 .. 256)
+ *   forces_block   threads per block of the contact-law kernel (32 .. 128)
+ *   list_capacity  contact-list slots per particle (8 .. 256; 0 = 32 for
+ *                  spheres, 64 when other shapes are present); a particle
+ *                  with more contacts fails the step with GRAINS_GPU_PAIR_OVERFLOW */
+typedef struct grains_gpu_tuning {
+  double  cell_factor;
+  int32_t contacts_block;
+  int32_t forces_block;
+  int32_t list_capacity;
+  int32_t reserved[5];
+} grains_gpu_tuning;
+int grains_gpu_get_tuning(const grains_gpu_ctx* ctx, grains_gpu_tuning* tuning);
+int grains_gpu_set_tuning(grains_gpu_ctx* ctx, const grains_gpu_tuning* tuning);
+/* Autotuner: times trial_steps fused steps from the context's current state
+ * for candidate tunings (coordinate descent over list capacity, force block,
+ * broadphase block, cell factor), keeps the fastest that completed without
+ * error, applies it and restores the state exactly (particles, contact
+ * memory, obstacle poses).  time = the current simulation time. */
+int grains_gpu_autotune(grains_gpu_ctx* ctx, double time, double dt, int32_t trial_steps,
+                        grains_gpu_tuning* best, double* best_ms);
+
 /* ---- timing helpers for benchmarks ---------------------------------------- */
 /* Times each kernel of n_steps uncaptured steps with CUDA events on the
  * context stream.  names: '\n'-separated kernel names (cap bytes); ms[k]:

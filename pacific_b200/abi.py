@@ -82,6 +82,11 @@ _P_I32 = C.POINTER(C.c_int32)
 _P_F64 = C.POINTER(C.c_double)
 
 
+class Tuning(C.Structure):
+    _fields_ = [("cell_factor", C.c_double), ("contacts_block", C.c_int32), ("forces_block", C.c_int32),
+                ("list_capacity", C.c_int32), ("reserved", C.c_int32 * 5)]
+
+
 class Particles(C.Structure):
     _fields_ = [("n", C.c_int64), ("id", _P_I32), ("system", _P_I32), ("shape", _P_I32), ("material", _P_I32),
                 ("radius", _P_F64), ("crust", _P_F64), ("mass", _P_F64), ("inertia", _P_F64),
@@ -129,6 +134,8 @@ _SIGS = {
     "get_stats": [_VP, C.POINTER(Stats)],
     "reset_stats": [_VP],
 }
+# diagnostics that the reference built from its sources (oracle/_ref) lacks
+_OPTIONAL = {"get_contact_forces"}
 _GPU_ONLY = {
     "get_stream": [_VP, C.POINTER(_VP)],
     "synchronize": [_VP],
@@ -136,6 +143,9 @@ _GPU_ONLY = {
     "profile_kernels": [_VP, C.c_int32, _P_F64, C.c_double, C.c_char_p, C.c_size_t, _P_F64,
                         C.POINTER(C.c_int64), C.c_int32, _P_I32],
     "shape_properties": [C.c_int32, _P_F64, C.c_int32, _P_F64, _P_F64, _P_F64],
+    "get_tuning": [_VP, C.POINTER(Tuning)],
+    "set_tuning": [_VP, C.POINTER(Tuning)],
+    "autotune": [_VP, C.c_double, C.c_double, C.c_int32, C.POINTER(Tuning), _P_F64],
     "adjoint_create": [_VP, C.c_int32, C.POINTER(_VP)],
     "adjoint_destroy": [_VP],
     "adjoint_last_error": [_VP, C.c_char_p, C.c_size_t],
@@ -159,7 +169,7 @@ class GrainsLib:
         for name, args in list(_SIGS.items()) + list(_GPU_ONLY.items()):
             sym = prefix + name
             if not hasattr(self.dll, sym):
-                if name in _GPU_ONLY:
+                if name in _GPU_ONLY or name in _OPTIONAL:
                     continue
                 raise AttributeError("%s does not export %s" % (path, sym))
             f = getattr(self.dll, sym)
@@ -442,6 +452,24 @@ class Simulation:
         order-independent arg-max of the CUDA path instead of the reference's
         warm-started hill climb."""
         self._check(self.lib.fn["set_polyhedron_support"](self.ctx, 1 if stateless else 0))
+
+    # ---- tuning (CUDA implementation only) ----
+    def tuning(self):
+        t = Tuning()
+        self._check(self.lib.fn["get_tuning"](self.ctx, C.byref(t)))
+        return {"cell_factor": t.cell_factor, "contacts_block": t.contacts_block, "forces_block": t.forces_block,
+                "list_capacity": t.list_capacity}
+
+    def set_tuning(self, cell_factor=1.0, contacts_block=256, forces_block=128, list_capacity=0):
+        t = Tuning(cell_factor, contacts_block, forces_block, list_capacity)
+        self._check(self.lib.fn["set_tuning"](self.ctx, C.byref(t)))
+
+    def autotune(self, time, dt, trial_steps=100):
+        """Picks and applies the fastest tuning; returns (tuning dict, ms of trial_steps)."""
+        t, ms = Tuning(), C.c_double()
+        self._check(self.lib.fn["autotune"](self.ctx, time, dt, trial_steps, C.byref(t), C.byref(ms)))
+        return ({"cell_factor": t.cell_factor, "contacts_block": t.contacts_block, "forces_block": t.forces_block,
+                 "list_capacity": t.list_capacity}, ms.value)
 
     # ---- benchmark helpers (CUDA implementation only) ----
     def stream_handle(self):

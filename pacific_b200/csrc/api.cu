@@ -132,6 +132,11 @@ struct grains_gpu_ctx {
   double graph_dt[4] = {0, 0, 0, 0};
   int64_t steps_done = 0;
   double gjk_tol = kEpsilon;
+  // launch and grid tuning (grains_gpu_set_tuning / grains_gpu_autotune)
+  double cell_factor = 1.0;
+  int contacts_block = 256;
+  int forces_block = 128;
+  int list_capacity = 0;  // 0: 32 slots for spheres, 64 when other shapes are present
 };
 
 namespace {
@@ -444,6 +449,8 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   a.pairs_n = c->pairs_n;
   a.pair_force = c->pair_force;
   a.gjk_tol = c->gjk_tol;
+  a.contacts_block = c->contacts_block;
+  a.forces_block = c->forces_block;
   return a;
 }
 
@@ -569,6 +576,30 @@ int last_step(grains_gpu_ctx* c, double dt) {
   return 0;
 }
 
+// LinkedCell::set (LinkedCell.cpp:69-98) with the cell edge scaled by the
+// context's cell factor (1 = the reference's grid)
+int apply_grid(grains_gpu_ctx* c, SysHost& s) {
+  const grains_gpu_domain* d = &s.dom;
+  const double cs = d->cell_size * c->cell_factor;
+  if (cs > kEpsilon) {
+    s.nbi = (int)((d->size[0] + kEpsilon) / cs);
+    if (!s.nbi) s.nbi = 1;
+    s.ex = d->size[0] / s.nbi;
+    s.nbj = (int)((d->size[1] + kEpsilon) / cs);
+    if (!s.nbj) s.nbj = 1;
+    s.ey = d->size[1] / s.nbj;
+    s.nbk = (int)((d->size[2] + kEpsilon) / cs);
+    if (!s.nbk) s.nbk = 1;
+    s.ez = d->size[2] / s.nbk;
+  } else {
+    s.nbi = s.nbj = s.nbk = 1;
+    s.ex = d->size[0];
+    s.ey = d->size[1];
+    s.ez = d->size[2];
+  }
+  if ((double)s.nbi * s.nbj * s.nbk > 2.0e9) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "too many cells");
+  return 0;
+}
 }  // namespace
 
 // ===========================================================================
@@ -682,25 +713,7 @@ int grains_gpu_set_domain(grains_gpu_ctx* c, int32_t system, const grains_gpu_do
     if (!(d->size[i] > 0)) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "domain size must be positive");
   SysHost& s = c->sys[system];
   s.dom = *d;
-  const double cs = d->cell_size;
-  // LinkedCell::set (LinkedCell.cpp:69-98)
-  if (cs > kEpsilon) {
-    s.nbi = (int)((d->size[0] + kEpsilon) / cs);
-    if (!s.nbi) s.nbi = 1;
-    s.ex = d->size[0] / s.nbi;
-    s.nbj = (int)((d->size[1] + kEpsilon) / cs);
-    if (!s.nbj) s.nbj = 1;
-    s.ey = d->size[1] / s.nbj;
-    s.nbk = (int)((d->size[2] + kEpsilon) / cs);
-    if (!s.nbk) s.nbk = 1;
-    s.ez = d->size[2] / s.nbk;
-  } else {
-    s.nbi = s.nbj = s.nbk = 1;
-    s.ex = d->size[0];
-    s.ey = d->size[1];
-    s.ez = d->size[2];
-  }
-  if ((double)s.nbi * s.nbj * s.nbk > 2.0e9) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "too many cells");
+  if (int rc = apply_grid(c, s)) return rc;
   s.has_domain = true;
   c->uploaded = false;
   c->tables_dirty = true;
@@ -933,7 +946,7 @@ int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
   {
     // contact lists: 32 slots per particle for spheres, 64 when bounding
     // spheres of other shapes are listed
-    const int cap_per = c->has_convex ? 64 : 32;
+    const int cap_per = c->list_capacity > 0 ? c->list_capacity : (c->has_convex ? 64 : 32);
     const int64_t need = (int64_t)c->cap * cap_per;
     if (need > c->clist_alloc) {
       if (c->clist) cudaFree(c->clist);
@@ -1587,6 +1600,216 @@ int grains_gpu_shape_properties(int32_t type, const double* params, int32_t n, d
   *volume = s.volume;
   *circ = s.circ;
   for (int i = 0; i < 3; ++i) inertia[i] = s.inertia[i];
+  return 0;
+}
+
+
+// ---- tuning ------------------------------------------------------------------
+int grains_gpu_get_tuning(const grains_gpu_ctx* c, grains_gpu_tuning* t) {
+  if (!c || !t) return GRAINS_GPU_INVALID_ARGUMENT;
+  std::memset(t, 0, sizeof(*t));
+  t->cell_factor = c->cell_factor;
+  t->contacts_block = c->contacts_block;
+  t->forces_block = c->forces_block;
+  t->list_capacity = c->list_capacity > 0 ? c->list_capacity : c->clist_cap;
+  return 0;
+}
+
+int grains_gpu_set_tuning(grains_gpu_ctx* c, const grains_gpu_tuning* t) {
+  if (!c || !t) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!(t->cell_factor >= 1.0 && t->cell_factor <= 4.0) || t->contacts_block < 32 || t->contacts_block > 256 ||
+      t->contacts_block % 32 || t->forces_block < 32 || t->forces_block > 128 || t->forces_block % 32 ||
+      (t->list_capacity != 0 && (t->list_capacity < 8 || t->list_capacity > 256)))
+    return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "tuning out of range");
+  const bool regrid = t->cell_factor != c->cell_factor;
+  c->cell_factor = t->cell_factor;
+  c->contacts_block = t->contacts_block;
+  c->forces_block = t->forces_block;
+  c->list_capacity = t->list_capacity;
+  for (int k = 0; k < 4; ++k)  // launch shapes are baked into the step graphs
+    if (c->graph[k]) {
+      cudaGraphExecDestroy(c->graph[k]);
+      c->graph[k] = nullptr;
+    }
+  for (auto& s : c->sys)
+    if (s.has_domain)
+      if (int rc = apply_grid(c, s)) return rc;
+  if (!c->uploaded) {
+    c->tables_dirty = true;
+    return 0;
+  }
+  if (regrid) {
+    // rebuild the cell tables for the new grid; moving obstacles keep their
+    // current poses and velocities
+    std::vector<ObstacleDev> live(c->h_obs.size());
+    if (!live.empty()) {
+      CK(cudaMemcpyAsync(live.data(), c->d_obs, live.size() * sizeof(ObstacleDev), cudaMemcpyDeviceToHost,
+                         c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
+    if (int rc = build_tables(c)) return rc;
+    if (!live.empty())
+      CK(cudaMemcpyAsync(c->d_obs, live.data(), live.size() * sizeof(ObstacleDev), cudaMemcpyHostToDevice,
+                         c->stream));
+    c->sorted = false;
+    c->keys_valid = false;
+  }
+  const int cap_per = c->list_capacity > 0 ? c->list_capacity : (c->has_convex ? 64 : 32);
+  const int64_t need = (int64_t)c->cap * cap_per;
+  if (need > c->clist_alloc) {
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->clist) cudaFree(c->clist);
+    void* q = nullptr;
+    CK(cudaMalloc(&q, (size_t)need * sizeof(int)));
+    c->clist = (int*)q;
+    c->clist_alloc = need;
+  }
+  c->clist_cap = cap_per;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+namespace {
+// exact device copy of the dynamic state of a context (particles, contact
+// memory, obstacle poses, clock), for trials that must start from it
+struct Snapshot {
+  std::vector<std::pair<void*, size_t>> bufs;  // (device copy, bytes), in the order of fields()
+  int cur = 0, hcur = 0;
+  bool pending = false;
+  double pending_dt = 0.;
+  int64_t steps_done = 0;
+};
+
+std::vector<std::pair<void*, size_t>> snapshot_fields(grains_gpu_ctx* c, int cur, int hcur) {
+  const size_t n = (size_t)c->n, r4 = 4 * c->rsize;
+  auto& b = c->buf[cur];
+  const size_t hsz = c->precision == GRAINS_GPU_FP64 ? sizeof(HistEntry<double>) : sizeof(HistEntry<float>);
+  std::vector<std::pair<void*, size_t>> f = {
+      {b.xr, n * sizeof(double4)}, {b.q, n * sizeof(double4)}, {b.v, n * r4}, {b.w, n * r4},
+      {b.wbf, n * r4}, {b.F, n * r4}, {b.T, n * r4}, {b.inertia, n * r4},
+      {b.md, n * sizeof(double4)}, {b.meta, n * sizeof(int4)}, {b.orig, n * sizeof(int)},
+      {c->hist[hcur], n * c->hist_cap * hsz}, {c->hist_n[hcur], n * sizeof(int)},
+      {c->clock, sizeof(double)}};
+  if (c->has_basis) f.push_back({b.basis, 9 * n * sizeof(double)});
+  if (!c->h_obs.empty()) f.push_back({c->d_obs, c->h_obs.size() * sizeof(ObstacleDev)});
+  return f;
+}
+
+int take_snapshot(grains_gpu_ctx* c, Snapshot& s) {
+  s.cur = c->cur;
+  s.hcur = c->hcur;
+  s.pending = c->pending_kick2;
+  s.pending_dt = c->pending_dt;
+  s.steps_done = c->steps_done;
+  for (auto& f : snapshot_fields(c, c->cur, c->hcur)) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, f.second) != cudaSuccess) return GRAINS_GPU_CUDA_ERROR;
+    s.bufs.push_back({q, f.second});
+    if (cudaMemcpyAsync(q, f.first, f.second, cudaMemcpyDeviceToDevice, c->stream) != cudaSuccess)
+      return GRAINS_GPU_CUDA_ERROR;
+  }
+  return cudaStreamSynchronize(c->stream) == cudaSuccess ? 0 : GRAINS_GPU_CUDA_ERROR;
+}
+
+int restore_snapshot(grains_gpu_ctx* c, const Snapshot& s) {
+  auto f = snapshot_fields(c, s.cur, s.hcur);
+  for (size_t k = 0; k < f.size() && k < s.bufs.size(); ++k)
+    if (cudaMemcpyAsync(f[k].first, s.bufs[k].first, f[k].second, cudaMemcpyDeviceToDevice, c->stream) !=
+        cudaSuccess)
+      return GRAINS_GPU_CUDA_ERROR;
+  c->cur = s.cur;
+  c->hcur = s.hcur;
+  c->pending_kick2 = s.pending;
+  c->pending_dt = s.pending_dt;
+  c->steps_done = s.steps_done;
+  c->sorted = false;
+  c->keys_valid = false;
+  if (cudaMemsetAsync(c->stats, 0, sizeof(StatsDev), c->stream) != cudaSuccess) return GRAINS_GPU_CUDA_ERROR;
+  return cudaStreamSynchronize(c->stream) == cudaSuccess ? 0 : GRAINS_GPU_CUDA_ERROR;
+}
+
+void free_snapshot(Snapshot& s) {
+  for (auto& b : s.bufs) cudaFree(b.first);
+  s.bufs.clear();
+}
+}  // namespace
+
+int grains_gpu_autotune(grains_gpu_ctx* c, double time, double dt, int32_t trial_steps, grains_gpu_tuning* best,
+                        double* best_ms) {
+  if (!c || !best || trial_steps < 1 || !(dt > 0.)) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  if (int rc = flush_kick(c)) return rc;
+  Snapshot snap;
+  if (take_snapshot(c, snap)) {
+    free_snapshot(snap);
+    return fail(c, GRAINS_GPU_CUDA_ERROR, "autotune: snapshot failed");
+  }
+  grains_gpu_tuning cur;
+  grains_gpu_get_tuning(c, &cur);
+  cur.list_capacity = c->clist_cap;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  // time of trial_steps fused steps from the snapshot (after one untimed run
+  // that builds the step graphs); < 0 when the tuning fails (list overflow)
+  auto trial = [&](const grains_gpu_tuning& t) -> double {
+    if (grains_gpu_set_tuning(c, &t)) return -1.;
+    double ms_best = -1.;
+    for (int rep = 0; rep < 2; ++rep) {
+      if (restore_snapshot(c, snap)) return -1.;
+      double tt = time;
+      cudaEventRecord(e0, c->stream);
+      int rc = grains_gpu_step(c, trial_steps, &tt, dt);
+      cudaEventRecord(e1, c->stream);
+      if (rc || cudaEventSynchronize(e1) != cudaSuccess) return -1.;
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep == 1) ms_best = ms;
+    }
+    return ms_best;
+  };
+  double t_best = trial(cur);
+  grains_gpu_tuning b = cur;
+  // coordinate descent: list capacity, force block, broadphase block, cell factor
+  const int caps_sphere[] = {16, 24, 32}, caps_convex[] = {32, 48, 64};
+  const int* caps = c->has_convex ? caps_convex : caps_sphere;
+  for (int k = 0; k < 3; ++k) {
+    grains_gpu_tuning t = b;
+    t.list_capacity = caps[k];
+    if (t.list_capacity == b.list_capacity) continue;
+    const double ms = trial(t);
+    if (ms > 0. && (t_best < 0. || ms < t_best)) { t_best = ms; b = t; }
+  }
+  for (int fb : {64, 128}) {
+    grains_gpu_tuning t = b;
+    t.forces_block = fb;
+    if (fb == b.forces_block) continue;
+    const double ms = trial(t);
+    if (ms > 0. && (t_best < 0. || ms < t_best)) { t_best = ms; b = t; }
+  }
+  for (int cb : {128, 256}) {
+    grains_gpu_tuning t = b;
+    t.contacts_block = cb;
+    if (cb == b.contacts_block) continue;
+    const double ms = trial(t);
+    if (ms > 0. && (t_best < 0. || ms < t_best)) { t_best = ms; b = t; }
+  }
+  for (double cf : {1.0, 1.25, 1.5}) {
+    grains_gpu_tuning t = b;
+    t.cell_factor = cf;
+    if (cf == b.cell_factor) continue;
+    const double ms = trial(t);
+    if (ms > 0. && (t_best < 0. || ms < t_best)) { t_best = ms; b = t; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  int rc = grains_gpu_set_tuning(c, &b);
+  if (!rc) rc = restore_snapshot(c, snap) ? GRAINS_GPU_CUDA_ERROR : 0;
+  free_snapshot(snap);
+  if (rc) return fail(c, rc, "autotune: restoring the state failed");
+  if (t_best < 0.) return fail(c, GRAINS_GPU_CUDA_ERROR, "autotune: no tuning completed a trial");
+  *best = b;
+  if (best_ms) *best_ms = t_best;
   return 0;
 }
 

@@ -159,6 +159,8 @@ struct StepArgs {
   double* pair_force;    // diagnostic: force on the lower id of each contact pair (3 doubles) or null
   double gjk_tol;
   double dt_disp;        // drift time step of the fused force kernel
+  int contacts_block;    // threads per block of contacts_kernel (<= 256)
+  int forces_block;      // threads per block of forces_kernel (<= 128)
 };
 
 // kernel launchers, instantiated for float and double

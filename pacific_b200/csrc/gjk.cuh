@@ -16,11 +16,11 @@
 // that margin (flat-face contacts): the distance is the same, the witness
 // points, hence the contact point, may not be.
 //
-// Precision: the iteration runs in T.  With T = float the two bodies are
-// expressed relative to body A's origin (the translation difference is formed
-// in double) so that FP32 keeps the body-size scale.  The FP32 run only
-// certifies separation (GjkResult::lower); pairs it cannot rule out are run
-// again in double.
+// Precision: the iteration runs in T; the step kernels of both precisions use
+// T = double (an FP32 run is too inaccurate for contact features and was
+// slower on B200, see convex_closest_point in kernels.cuh).  With T = float
+// the two bodies are expressed relative to body A's origin so that FP32 keeps
+// the body-size scale; GjkResult::lower is a lower bound of the distance.
 #pragma once
 
 #include "common.cuh"

@@ -434,32 +434,19 @@ __device__ __forceinline__ void make_obstacle_ref(const StepArgs<R>& a, int oidx
   for (int i = 0; i < 3; ++i) b.lext[i] = sh.scaling_ext[i];
 }
 
-// Closest point of a general pair.  FP64 path: double GJK.  Mixed path: an
-// FP32 GJK is a separation filter.  Its largest support-plane separation is a
-// lower bound of the shrunk bodies' distance (up to FP32 rounding, a few 1e-10
-// m at particle scale); when that bound clears the crust sum by more than
-// 1e-5 (R_A + R_B) the pair is certainly apart.  Every other pair (contacts
-// and near misses) is re-run in double from the reference's start point, so
-// contact decisions and contact geometry equal the FP64 path's.  The FP32
-// distance itself is not used for contacts: on curved bodies FP32 GJK often
-// stops in Johnson's backup procedure with an error far above the overlaps.
-// Error handling (crust x10) on ContactError.
+// Closest point of a general pair: the double GJK in both precisions (the
+// mixed path keeps FP32 for the contact law only).  An FP32 GJK is not used:
+// on curved bodies it often stops in Johnson's backup procedure with distance
+// errors up to 2e-5 m, far above typical overlaps, and even as a separation
+// filter (certified by its support-plane lower bound) it made the drum's
+// force kernel 3x slower than the double GJK alone on B200 (0.67 vs 0.22 ms
+// per step, 100,000 convex bodies).  Error handling (crust x10) on
+// ContactError.
 template <typename R>
 __device__ ContactGeom convex_closest_point(const StepArgs<R>& a, const BodyRef& A, const BodyRef& B, int& iters,
                                             int& handled) {
-  ContactGeom c;
   handled = 0;
-  if (sizeof(R) == 4) {
-    double lower = 0.;
-    c = convex_closest_point_t<float>(A, B, fmax(a.gjk_tol, 1.e-6), &iters, nullptr, &lower);
-    if (c.status != 2) {
-      const double guard = 1.e-5 * (A.radius + B.radius);
-      if (c.status == 1 || !(lower - xadd(A.crust, B.crust) > guard))
-        c = convex_closest_point_t<double>(A, B, a.gjk_tol, &iters);
-    }
-  } else {
-    c = convex_closest_point_t<double>(A, B, a.gjk_tol, &iters);
-  }
+  ContactGeom c = convex_closest_point_t<double>(A, B, a.gjk_tol, &iters);
   if (c.status == 1) {
     c = convex_error_handling(A, B, A.lext, B.lext, 10., a.gjk_tol);
     handled = 1;
@@ -1004,23 +991,25 @@ int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forc
 template <typename R>
 int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int fused, int phases) {
   if (a.n == 0) return 0;
-  if (phases & 1) contacts_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
+  const int cb = (a.contacts_block >= 32 && a.contacts_block <= 256) ? a.contacts_block : 256;
+  const int fb = (a.forces_block >= 32 && a.forces_block <= 128) ? a.forces_block : 128;
+  if (phases & 1) contacts_kernel<R><<<grid_for(a.n, cb), cb, 0, s>>>(a);
   if (!(phases & 2)) return check_launch();
-  const int g = grid_for(a.n, 128);
+  const int g = grid_for(a.n, fb);
   if (a.has_convex) {
     if (diag)
-      forces_kernel<R, true, true, false><<<g, 128, 0, s>>>(a, R(dt));
+      forces_kernel<R, true, true, false><<<g, fb, 0, s>>>(a, R(dt));
     else if (fused)
-      forces_kernel<R, false, true, true><<<g, 128, 0, s>>>(a, R(dt));
+      forces_kernel<R, false, true, true><<<g, fb, 0, s>>>(a, R(dt));
     else
-      forces_kernel<R, false, true, false><<<g, 128, 0, s>>>(a, R(dt));
+      forces_kernel<R, false, true, false><<<g, fb, 0, s>>>(a, R(dt));
   } else {
     if (diag)
-      forces_kernel<R, true, false, false><<<g, 128, 0, s>>>(a, R(dt));
+      forces_kernel<R, true, false, false><<<g, fb, 0, s>>>(a, R(dt));
     else if (fused)
-      forces_kernel<R, false, false, true><<<g, 128, 0, s>>>(a, R(dt));
+      forces_kernel<R, false, false, true><<<g, fb, 0, s>>>(a, R(dt));
     else
-      forces_kernel<R, false, false, false><<<g, 128, 0, s>>>(a, R(dt));
+      forces_kernel<R, false, false, false><<<g, fb, 0, s>>>(a, R(dt));
   }
   return check_launch();
 }

@@ -193,3 +193,67 @@ def test_adjoint_rejects_unsupported_scenes(gpu_lib):
     with pytest.raises(Exception):
         Adjoint(sim, 10).forward(5, sc.dt)
     sim.close()
+
+
+class GrainsRun:
+    """torch.autograd.Function over the differentiable run (test harness only):
+    inputs the initial velocities (n, 3) and theta = (kn, en, muc, kt) of both
+    laws; outputs the final positions, velocities and angular velocities."""
+
+    @staticmethod
+    def make(gpu_lib, precision):
+        import torch
+
+        class Fn(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, v0, theta):
+                sc = S.adjoint_4k(n=N)
+                kn, en, muc, kt = [float(x) for x in theta]
+                sc.laws = [[(a, b, law, S.hooke_memory_params(kn, en, muc, kt)) for a, b, law, _ in sc.laws[0]]]
+                sc.particles = dict(sc.particles)
+                sc.particles["velocity"] = v0.detach().cpu().numpy().astype(np.float64)
+                sim = make(gpu_lib, sc, precision)
+                adj = Adjoint(sim, CHECKPOINT)
+                fin = adj.forward(STEPS, sc.dt)
+                ctx.keep = (sim, adj)
+                as_t = lambda a: torch.tensor(a, dtype=torch.float64)  # noqa: E731
+                return as_t(fin["position"]), as_t(fin["velocity"]), as_t(fin["omega"])
+
+            @staticmethod
+            def backward(ctx, gx, gv, gw):
+                sim, adj = ctx.keep
+                g = adj.backward(gx.numpy(), gv.numpy(), gw.numpy())
+                laws = g["laws"][SLOTS].sum(0)
+                adj.close()
+                sim.close()
+                return torch.tensor(g["velocity"]), torch.tensor(laws)
+
+        return Fn
+
+
+def test_autograd_function_wrapper(gpu_lib):
+    """The adjoint through torch.autograd: L.backward() gives the gradients of
+    the C ABI, equal to the dual-number oracle's derivatives."""
+    import torch
+    Fn = GrainsRun.make(gpu_lib, FP64)
+    sc = scenario()
+    prm = sc.laws[0][0][3]
+    v0 = torch.tensor(sc.particles["velocity"], dtype=torch.float64, requires_grad=True)
+    theta = torch.tensor([prm[0], prm[1], prm[3], prm[4]], dtype=torch.float64, requires_grad=True)
+    x, v, w = Fn.apply(v0, theta)
+    m = torch.tensor(sc.particles["mass"])
+    inertia = torch.tensor(np.asarray(sc.particles["inertia"])[:, 0])
+    zc = x[:, 2].mean()
+    ke = (0.5 * m * (v * v).sum(1) + 0.5 * inertia * (w * w).sum(1)).mean()
+    targets = (float(zc) - 1e-4, 0.6 * float(ke))
+    L = (zc - targets[0]) ** 2 + (ke - targets[1]) ** 2
+    L.backward()
+    dv, dl = directions()
+    fin, tan = tangent_run(sc, STEPS, dv, dl)
+    _, gx, gv, gw = loss(sc, fin, targets)
+    dual = np.array([(gx * tan["position"][d]).sum() + (gv * tan["velocity"][d]).sum() +
+                     (gw * tan["omega"][d]).sum() for d in range(len(dv))])
+    # theta's gradient is summed over the law slots; the directions move all slots together
+    via_torch = np.array([(v0.grad.numpy() * dv[d]).sum() + (theta.grad.numpy() * dl[d][0]).sum()
+                          for d in range(len(dv))])
+    assert np.all(np.abs(via_torch - dual) <= 1e-6 * np.abs(dual)), (via_torch, dual)

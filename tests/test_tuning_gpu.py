@@ -1,0 +1,50 @@
+"""Launch and grid tuning (grains_gpu_set_tuning, grains_gpu_autotune): no
+tuning changes contacts or forces beyond the order of floating-point sums, and
+the autotuner restores the state it started from exactly."""
+import numpy as np
+import pytest
+
+from pacific_b200 import scenarios as S
+from pacific_b200.abi import FP64, MIXED
+
+from helpers import make, pair_set, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def evolved_box():
+    sc = S.small_box(343, seed=4, velocity_sigma=0.2)
+    return sc
+
+
+@pytest.mark.parametrize("tuning", [dict(cell_factor=1.5), dict(contacts_block=128, forces_block=64),
+                                    dict(list_capacity=16)])
+def test_tuning_keeps_the_physics(gpu_lib, tuning):
+    sc = evolved_box()
+    a, b = make(gpu_lib, sc, FP64), make(gpu_lib, sc, FP64)
+    b.set_tuning(**{**dict(cell_factor=1.0, contacts_block=256, forces_block=128, list_capacity=0), **tuning})
+    for s in (a, b):
+        s.initialize_leapfrog(0.0, sc.dt)
+        s.step(50, 0.0, sc.dt)
+        s.compute_forces(50 * sc.dt, sc.dt)
+    da, db = a.download(), b.download()
+    assert pair_set(a.contact_pairs()) == pair_set(b.contact_pairs())
+    weight = sc.particles["mass"][0] * 9.81
+    assert rel_err(db["force"], da["force"], weight) < 1e-9
+    assert np.max(np.abs(db["position"] - da["position"])) < 1e-12
+
+
+@pytest.mark.parametrize("precision", [FP64, MIXED])
+def test_autotune_restores_the_state(gpu_lib, precision):
+    sc = evolved_box()
+    sim = make(gpu_lib, sc, precision)
+    sim.initialize_leapfrog(0.0, sc.dt)
+    t = sim.step(20, 0.0, sc.dt)
+    before, mem_before = sim.download(), sim.contact_memory()
+    best, ms = sim.autotune(t, sc.dt, trial_steps=20)
+    after, mem_after = sim.download(), sim.contact_memory()
+    for k in ["position", "quaternion", "velocity", "omega"]:
+        assert np.array_equal(before[k], after[k]), k
+    assert set(zip(mem_before["owner"], mem_before["other"])) == set(zip(mem_after["owner"], mem_after["other"]))
+    assert ms > 0 and best["cell_factor"] >= 1.0 and sim.tuning() == best
+    sim.step(10, t, sc.dt)   # the tuned context keeps running
