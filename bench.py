@@ -32,25 +32,27 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Algorithmic HBM bytes per particle of the two force kernels of a middle step
-# (z = mean coordination number, contacts per particle incl. walls).
+# Algorithmic HBM bytes per particle of the per-step kernels (z = mean
+# coordination number, contacts per particle incl. walls; R4 = 16 B in mixed
+# precision, 32 B in FP64; a contact-memory entry is 44 B / 80 B):
 #  contacts_kernel: own position+radius (32) and meta (16) in, the 9 cell-row
 #   ranges (72), list length (4) and z list entries (4 z) out; the neighbours'
 #   positions are re-read from L1/L2 and not counted.
-#  forces_kernel (fused with the move): own state in (xr 32, q 32, meta 16,
-#   md 32, v, w, wbf, inertia, upload index 4, list length 4, z list entries),
-#   the moved state out (xr, q, md 32 each, meta 16, index 4, v, w, wbf, F, T,
-#   inertia, cell key 4, rank 4, coordination 4, memory count 4), and the
-#   contact memory: z entries looked up + z/2 owned entries written.  Bodies
-#   that are not spheres also carry their rotation matrix (72 B in and out).
+#  forces_kernel: own xr, meta, md (32 + 16 + 32), v, w (2 R4), upload index,
+#   list length, cell obstacle range (4 + 4 + 8) and z list entries in, the z
+#   memory entries looked up; F, T (2 R4), coordination and memory count (8)
+#   and the z/2 owned memory entries out.
+#  kick_move_kernel: xr, q, meta, md (32 + 32 + 16 + 32), v, w, wbf, inertia,
+#   F, T (6 R4) in; xr, q (64), v, w, wbf (3 R4), cell key and count (8) out.
+#   Bodies that are not spheres also carry their rotation matrix (72 B in and out).
 def kernel_bytes(kernel, precision, z, basis=False):
     r4 = 16 if precision == "mixed" else 32
     entry = 44 if precision == "mixed" else 80
     if kernel == "contacts":
         return 32 + 16 + 72 + 4 + 4 * z
-    reads = 32 + 32 + 16 + 32 + 4 * r4 + 4 + 4 + 4 * z + z * entry
-    writes = 32 + 32 + 32 + 16 + 4 + 6 * r4 + 4 * 4 + (z / 2.0) * entry
-    return reads + writes + (144 if basis else 0)
+    if kernel == "forces":
+        return (32 + 16 + 32 + 2 * r4 + 16 + 4 * z + z * entry) + (2 * r4 + 8 + (z / 2.0) * entry)
+    return (32 + 32 + 16 + 32 + 6 * r4) + (64 + 3 * r4 + 8) + (144 if basis else 0)
 
 
 def parse():
@@ -400,7 +402,7 @@ def main():
         st3 = sim.stats()
         zs.append((2.0 * st3["n_contacts"] + st3["n_obstacle_contacts"]) / sc.n)
     z = float(np.mean(zs))
-    dom = max(["contacts", "forces"], key=lambda k: prof_tot[k][0])
+    dom = max(["contacts", "forces", "kick_move"], key=lambda k: prof_tot[k][0])
     fk_ms, fk_n = prof_tot[dom]
     basis = any(sc.shapes[k][0] != S.SPHERE for k in set(np.asarray(sc.particles["shape"]).tolist()))
     alg_bytes = sc.n * kernel_bytes(dom, args.precision, z, basis)

@@ -1,6 +1,6 @@
 // api.cu -- the C ABI of include/grains_gpu.h: context, device memory, set-up
 // tables (shapes, domains, contact laws, obstacles, obstacle-cell links) and
-// the orchestration of the DEM step kernels, with the fused step loop
+// the orchestration of the DEM step kernels, with the step loop
 // replayed from CUDA graphs.
 #include <cuda_runtime.h>
 
@@ -80,7 +80,7 @@ struct grains_gpu_ctx {
   double* stage = nullptr;        // host-ordered staging of the kinematic state (13 doubles / particle)
   double* stage_basis = nullptr;  // 9 doubles / particle
   bool sorted = false;      // cur arrays are in cell order for the current positions
-  bool keys_valid = false;  // key/rank hold the cells of the current positions
+  bool keys_valid = false;  // key and cell counts hold the cells of the current positions
   bool pending_kick2 = false;
   double pending_dt = 0;
   bool has_basis = false;
@@ -101,9 +101,9 @@ struct grains_gpu_ctx {
   int* hist_n[2] = {nullptr, nullptr};
   int hcur = 0;  // hist[hcur] = latest memory (prev for the next force evaluation)
   int* coord = nullptr;
-  unsigned *key = nullptr, *rank = nullptr;
+  unsigned* key = nullptr;
   int* perm = nullptr;
-  int *cell_count = nullptr, *cell_start = nullptr, *block_sums = nullptr;
+  int *cell_count = nullptr, *cell_start = nullptr, *cell_cursor = nullptr, *block_sums = nullptr;
   StatsDev* stats = nullptr;
   double* clock = nullptr;  // the reference's m_time, advanced by the obstacle moves
   int* clist = nullptr;   // contact lists (scratch of the force evaluation)
@@ -127,7 +127,7 @@ struct grains_gpu_ctx {
   std::vector<SysDev> h_sys;
   std::vector<ObstacleDev> h_obs;
   int n_moving = 0;  // moving obstacles over all systems
-  // graphs of two fused steps, by the starting (cur, hcur) buffer selection
+  // graphs of two middle steps, by the starting (cur, hcur) buffer selection
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   double graph_dt[4] = {0, 0, 0, 0};
   int64_t steps_done = 0;
@@ -431,9 +431,9 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   fill_arrays<R>(c, a.alt, 1 - c->cur);
   a.coord = c->coord;
   a.key = c->key;
-  a.rank = c->rank;
   a.cell_count = c->cell_count;
   a.cell_start = c->cell_start;
+  a.cell_cursor = c->cell_cursor;
   a.block_sums = c->block_sums;
   a.perm = c->perm;
   a.hist_prev = (HistEntry<R>*)c->hist[c->hcur];
@@ -515,23 +515,13 @@ int flush_kick(grains_gpu_ctx* c) {
   return rc ? fail(c, rc, "advance-velocity launch failed") : 0;
 }
 
-int forces_now(grains_gpu_ctx* c, double dt, int diag, int fused = 0, int phases = 3) {
+int forces_now(grains_gpu_ctx* c, double dt, int diag, int phases = 3) {
   if (!c->sorted) {
     if (int rc = sort_now(c, 1)) return rc;
   }
-  int rc = with_args(c, [&](auto& a) {
-    a.dt_disp = dt;
-    return launch_forces(a, c->stream, dt, diag, fused, phases);
-  });
+  int rc = with_args(c, [&](auto& a) { return launch_forces(a, c->stream, dt, diag, phases); });
   if (rc) return fail(c, rc, "force kernel launch failed");
-  if (phases & 2) {
-    c->hcur = 1 - c->hcur;
-    if (fused) {  // the moved state is in the other buffer, keys computed
-      c->cur = 1 - c->cur;
-      c->keys_valid = true;
-      c->sorted = false;
-    }
-  }
+  if (phases & 2) c->hcur = 1 - c->hcur;
   return 0;
 }
 
@@ -559,18 +549,26 @@ int first_move(grains_gpu_ctx* c, double dt, double time) {
   return move_obstacles(c, dt, 1, time + dt);
 }
 
-// A middle step: sort, contact lists, forces fused with the rest of the step
-// and the next step's first half kick and drift
-int fused_middle_step(grains_gpu_ctx* c, double dt) {
+// A middle step: sort, contact lists, contact law, then the rest of the step
+// (second half kick) with the next step's first half kick and drift in one
+// kernel, which also bins the moved particles.  (Folding that kick into the
+// contact-law kernel was measured 14-15 % slower per step on 200,000 spheres:
+// the combined kernel's registers and serial memory chain cost more than the
+// extra pass over the state.)
+int middle_step(grains_gpu_ctx* c, double dt) {
   if (int rc = sort_now(c, 0)) return rc;
-  if (int rc = forces_now(c, dt, 0, 1)) return rc;
+  if (int rc = forces_now(c, dt, 0)) return rc;
+  int rc = with_args(c, [&](auto& a) { return launch_kick_move(a, c->stream, 1, 0.5 * dt, 1, 0.5 * dt, dt); });
+  if (rc) return fail(c, rc, "kick/move launch failed");
+  c->keys_valid = true;
+  c->sorted = false;
   return move_obstacles(c, dt);
 }
 
 // The last step of a run: sort and forces; the second half kick stays pending
 int last_step(grains_gpu_ctx* c, double dt) {
   if (int rc = sort_now(c, 0)) return rc;
-  if (int rc = forces_now(c, dt, 0, 0)) return rc;
+  if (int rc = forces_now(c, dt, 0)) return rc;
   c->pending_kick2 = true;
   c->pending_dt = 0.5 * dt;
   return 0;
@@ -653,7 +651,6 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
   if (ok) {
     c->coord = dalloc<int>(N, c->pool);
     c->key = dalloc<unsigned>(N, c->pool);
-    c->rank = dalloc<unsigned>(N, c->pool);
     c->perm = dalloc<int>(N, c->pool);
     c->stats = dalloc<StatsDev>(1, c->pool);
     c->pairs_cap = (int)std::min<size_t>(16 * N + 1024, (size_t)1 << 30);
@@ -661,7 +658,7 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
     c->pairs_n = dalloc<unsigned long long>(1, c->pool);
     c->pair_force = dalloc<double>(3 * (size_t)c->pairs_cap, c->pool);
     c->clock = dalloc<double>(1, c->pool);
-    ok = c->coord && c->key && c->rank && c->perm && c->stats && c->pairs && c->pairs_n && c->pair_force && c->clock;
+    ok = c->coord && c->key && c->perm && c->stats && c->pairs && c->pairs_n && c->pair_force && c->clock;
   }
   if (!ok) {
     c->err = "cudaMalloc failed for the requested capacity";
@@ -902,6 +899,9 @@ int build_tables(grains_gpu_ctx* c) {
   CK(cudaMalloc(&p, ((size_t)cells + 1) * sizeof(int)));
   c->table_pool.push_back(p);
   c->cell_start = (int*)p;
+  CK(cudaMalloc(&p, ((size_t)cells + 1) * sizeof(int)));
+  c->table_pool.push_back(p);
+  c->cell_cursor = (int*)p;
   CK(cudaMalloc(&p, ((size_t)cells / 4096 + 2) * sizeof(int)));
   c->table_pool.push_back(p);
   c->block_sums = (int*)p;
@@ -1359,9 +1359,9 @@ int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt)
   if (n_steps == 0) return 0;
   if (!c->sorted)
     if (int rc = sort_now(c, 1)) return rc;
-  // step 1 moves (finishing any pending half kick); steps 1..n-1 end with the
-  // fused force kernel, which already moves to the next step; step n ends
-  // with a plain force evaluation and leaves its second half kick pending
+  // step 1 moves (finishing any pending half kick); steps 1..n-1 end with
+  // the kick that also moves to the next step; step n ends with a force
+  // evaluation and leaves its second half kick pending
   if (int rc = first_move(c, dt, *time)) return rc;
   int middle = n_steps - 1;
   while (middle >= 2) {
@@ -1374,8 +1374,8 @@ int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt)
       const int cur0 = c->cur, h0 = c->hcur;
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      int rc = fused_middle_step(c, dt);
-      if (!rc) rc = fused_middle_step(c, dt);
+      int rc = middle_step(c, dt);
+      if (!rc) rc = middle_step(c, dt);
       cudaError_t e = cudaStreamEndCapture(c->stream, &g);
       c->cur = cur0;  // capturing does not execute: restore the buffer selection
       c->hcur = h0;
@@ -1392,7 +1392,7 @@ int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt)
     middle -= 2;
   }
   if (middle == 1)
-    if (int rc = fused_middle_step(c, dt)) return rc;
+    if (int rc = middle_step(c, dt)) return rc;
   if (int rc = last_step(c, dt)) return rc;
   for (int k = 0; k < n_steps; ++k) *time += dt;  // Grains::Simulation's clock
   c->steps_done += n_steps;
@@ -1528,8 +1528,8 @@ int grains_gpu_reset_stats(grains_gpu_ctx* c) {
 
 int grains_gpu_launches_per_step(grains_gpu_ctx* c, int64_t* launches) {
   if (!c || !launches) return GRAINS_GPU_INVALID_ARGUMENT;
-  // middle steps: scan (3), scatter, cell_sort, gather, contacts, forces (fused move)
-  *launches = 8;
+  // middle steps: scan (3), scatter, cell_sort, gather, contacts, forces, kick_move
+  *launches = launches_per_middle_step();
   return 0;
 }
 
@@ -1542,10 +1542,10 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time,
   if (!c->sorted)
     if (int rc = sort_now(c, 1)) return rc;
   // same schedule as grains_gpu_step, uncaptured, with events around each phase
-  cudaEvent_t ev[5];
+  cudaEvent_t ev[6];
   for (auto& e : ev) CK(cudaEventCreate(&e));
-  double acc[4] = {0, 0, 0, 0};  // first move, sort+gather, contact lists, contact law (+fused move)
-  int64_t cnt[4] = {0, 0, 0, 0};
+  double acc[5] = {0, 0, 0, 0, 0};  // first move, sort+gather, contact lists, contact law, kick/move
+  int64_t cnt[5] = {0, 0, 0, 0, 0};
   CK(cudaEventRecord(ev[0], c->stream));
   if (int rc = first_move(c, dt, *time)) return rc;
   CK(cudaEventRecord(ev[1], c->stream));
@@ -1559,35 +1559,39 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time,
     CK(cudaEventRecord(ev[1], c->stream));
     if (int rc = sort_now(c, 0)) return rc;
     CK(cudaEventRecord(ev[2], c->stream));
-    if (int rc = forces_now(c, dt, 0, last ? 0 : 1, 1)) return rc;
+    if (int rc = forces_now(c, dt, 0, 1)) return rc;
     CK(cudaEventRecord(ev[3], c->stream));
-    if (int rc = forces_now(c, dt, 0, last ? 0 : 1, 2)) return rc;
-    if (!last)
-      if (int rc = move_obstacles(c, dt)) return rc;
+    if (int rc = forces_now(c, dt, 0, 2)) return rc;
     CK(cudaEventRecord(ev[4], c->stream));
-    CK(cudaEventSynchronize(ev[4]));
-    float a = 0, b = 0, d = 0;
-    cudaEventElapsedTime(&a, ev[1], ev[2]);
-    cudaEventElapsedTime(&b, ev[2], ev[3]);
-    cudaEventElapsedTime(&d, ev[3], ev[4]);
-    acc[1] += a;
-    acc[2] += b;
-    acc[3] += d;
+    if (!last) {
+      int rc = with_args(c, [&](auto& a) { return launch_kick_move(a, c->stream, 1, 0.5 * dt, 1, 0.5 * dt, dt); });
+      if (rc) return fail(c, rc, "kick/move launch failed");
+      c->keys_valid = true;
+      c->sorted = false;
+      if (int rc2 = move_obstacles(c, dt)) return rc2;
+    }
+    CK(cudaEventRecord(ev[5], c->stream));
+    CK(cudaEventSynchronize(ev[5]));
+    float t[4] = {0, 0, 0, 0};
+    for (int q = 0; q < 4; ++q) cudaEventElapsedTime(&t[q], ev[1 + q], ev[2 + q]);
+    for (int q = 0; q < 4; ++q) acc[1 + q] += t[q];
     cnt[1] += 6;
     cnt[2] += 1;
     cnt[3] += 1;
+    if (!last) cnt[4] += 1;
   }
   c->pending_kick2 = true;
   c->pending_dt = 0.5 * dt;
   for (auto& e : ev) cudaEventDestroy(e);
   for (int k = 0; k < n_steps; ++k) *time += dt;
   c->steps_done += n_steps;
-  std::snprintf(names, cap, "kick_move\nsort_gather\ncontacts\nforces");
-  for (int k = 0; k < 4; ++k) {
+  std::snprintf(names, cap, "first_move\nsort_gather\ncontacts\nforces\nkick_move");
+  const int nk = max_kernels < 5 ? max_kernels : 5;
+  for (int k = 0; k < nk; ++k) {
     ms[k] = acc[k];
     launches[k] = cnt[k];
   }
-  *n_kernels = 4;
+  *n_kernels = nk;
   return finish_call(c);
 }
 
@@ -1750,7 +1754,7 @@ int grains_gpu_autotune(grains_gpu_ctx* c, double time, double dt, int32_t trial
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
-  // time of trial_steps fused steps from the snapshot (after one untimed run
+  // time of trial_steps steps from the snapshot (after one untimed run
   // that builds the step graphs); < 0 when the tuning fails (list overflow)
   auto trial = [&](const grains_gpu_tuning& t) -> double {
     if (grains_gpu_set_tuning(c, &t)) return -1.;
@@ -1816,7 +1820,7 @@ int grains_gpu_autotune(grains_gpu_ctx* c, double time, double dt, int32_t trial
 }  // extern "C"
 
 namespace gg {
-int launches_per_fused_step() { return 8; }
+int launches_per_middle_step() { return 9; }
 
 int context_view(grains_gpu_ctx* c, ContextView* v, std::string& err) {
   if (!c || !v) return GRAINS_GPU_INVALID_ARGUMENT;

@@ -140,8 +140,8 @@ struct StepArgs {
   ParticleArrays<R> alt;
   int* coord;            // coordination number (sorted order)
   unsigned* key;
-  unsigned* rank;
   int* cell_count;
+  int* cell_cursor;      // fill cursor of each cell (scatter)
   int* cell_start;
   int* block_sums;
   int* perm;
@@ -158,7 +158,6 @@ struct StepArgs {
   unsigned long long* pairs_n;
   double* pair_force;    // diagnostic: force on the lower id of each contact pair (3 doubles) or null
   double gjk_tol;
-  double dt_disp;        // drift time step of the fused force kernel
   int contacts_block;    // threads per block of contacts_kernel (<= 256)
   int forces_block;      // threads per block of forces_kernel (<= 128)
 };
@@ -171,11 +170,9 @@ template <typename R>
 int launch_bin(const StepArgs<R>& a, cudaStream_t s);
 template <typename R>
 int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forces);
-// fused != 0: forces + the rest of the step + the next step's first half kick
-// and drift, into the alternate buffer (then swap cur/alt)
 // phases: 1 = contact lists, 2 = contact law, 3 = both
 template <typename R>
-int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int fused, int phases = 3);
+int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int phases = 3);
 template <typename R>
 int launch_zero_kdelta(const StepArgs<R>& a, cudaStream_t s);
 // stage: 13 doubles per particle in upload order (position 3, quaternion 4,
@@ -189,7 +186,7 @@ int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int in
 int launch_obstacle_move(ObstacleDev* obs, const int* moving_idx, int n_moving, const ShapeDev* shapes,
                          const double* verts, double dt, double* clock, double host_time, int use_host_time,
                          cudaStream_t s);
-// number of kernel launches issued by one fused step
-int launches_per_fused_step();
+// number of kernel launches issued by one middle step of grains_gpu_step
+int launches_per_middle_step();
 
 }  // namespace gg

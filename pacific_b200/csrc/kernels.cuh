@@ -6,9 +6,9 @@
 // One DEM step (KDK leapfrog, Grains.cpp:344-364) is:
 //   kick_move      second half kick of the previous step (when pending),
 //                  first half kick + drift + rotation (SecondOrderLeapFrog),
-//                  new cell key and in-cell arrival rank (atomic)
+//                  new cell key and per-cell count (fire-and-forget atomic)
 //   scan x3        exclusive scan of the per-cell counts -> cell ranges
-//   scatter        slot = start[cell] + rank
+//   scatter        slot = atomic fill cursor of the cell
 //   cell_sort      each cell's particles ordered by id (deterministic order)
 //   gather         every per-particle array permuted into the new order
 //   forces         broadphase over the 27 surrounding cells, sphere/box
@@ -133,13 +133,13 @@ __device__ __forceinline__ void integrate(const StepArgs<R>& a, const ParticleAr
       for (int t = 0; t < 9; ++t) dst.basis[9 * (size_t)s + t] = b.m[t];
     }
     if (norm(tm) > md.y) set_status(a.stats, GRAINS_GPU_MOTION_ERROR);
-    // new cell key and arrival rank
+    // new cell key, counted in its cell
     const SysDev& S = a.sys[meta.w];
     int ci, cj, ck;
     if (!cell_of(S, xr.x, xr.y, xr.z, ci, cj, ck)) set_status(a.stats, GRAINS_GPU_OUT_OF_GRID);
     unsigned key = (unsigned)cell_index(S, ci, cj, ck);
     a.key[s] = key;
-    a.rank[s] = (unsigned)atomicAdd(&a.cell_count[key], 1);
+    atomicAdd(&a.cell_count[key], 1);  // result unused: a fire-and-forget reduction
   } else if (a.has_basis && !sphere && dst.basis != src.basis) {
     for (int t = 0; t < 9; ++t) dst.basis[9 * (size_t)s + t] = src.basis[9 * (size_t)s + t];
   }
@@ -172,7 +172,7 @@ __global__ void bin_kernel(StepArgs<R> a) {
   if (!cell_of(S, xr.x, xr.y, xr.z, ci, cj, ck)) set_status(a.stats, GRAINS_GPU_OUT_OF_GRID);
   unsigned key = (unsigned)cell_index(S, ci, cj, ck);
   a.key[s] = key;
-  a.rank[s] = (unsigned)atomicAdd(&a.cell_count[key], 1);
+  atomicAdd(&a.cell_count[key], 1);
 }
 
 // ---------------------------------------------------------------------------
@@ -248,17 +248,25 @@ static __global__ void __launch_bounds__(kScanThreads) scan_block_sums_kernel(in
   if (threadIdx.x == 0) out[n] = total;
 }
 
-static __global__ void scan_add_kernel(int* out, const int* block_sums, int n) {
+// finishes the scan and sets each cell's fill cursor to its start
+static __global__ void scan_add_kernel(int* out, int* cursor, const int* block_sums, int n) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) out[i] += block_sums[i / kScanTile];
+  if (i < n) {
+    const int v = out[i] + block_sums[i / kScanTile];
+    out[i] = v;
+    cursor[i] = v;
+  }
 }
 
+// slot of each particle in its cell's range; the order inside a cell is
+// fixed afterwards by cell_sort_kernel (by id), so the atomic order does not
+// matter
 template <typename R>
 __global__ void scatter_kernel(StepArgs<R> a) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const unsigned key = a.key[s];
-  const long long slot = (key < (unsigned)a.n_cells) ? (long long)a.cell_start[key] + a.rank[s] : -1;
+  const long long slot = (key < (unsigned)a.n_cells) ? (long long)atomicAdd(&a.cell_cursor[key], 1) : -1;
   if (slot < 0 || slot >= a.n) {
     set_status(a.stats, GRAINS_GPU_CUDA_ERROR);
     return;
@@ -523,7 +531,7 @@ __global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
 // by both of its particles; both evaluate the same contact law with the lower
 // id as p0 (same inputs, same instructions -> bit-identical forces of
 // opposite sign) and the lower id owns the pair's contact memory.
-template <typename R, bool DIAG, bool CONVEX, bool FUSED>
+template <typename R, bool DIAG, bool CONVEX>
 __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
@@ -739,20 +747,6 @@ __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
   P.T[s] = st3<R>(T);
   a.coord[s] = ncontact;
   a.hist_n_next[oi] = nnext;
-  if (FUSED) {
-    // the rest of this step (second half kick) and the next step's first half
-    // kick + drift, written to the other buffer in this slot: neighbours still
-    // read the unmoved state of `cur` in this kernel
-    const ParticleArrays<R>& D = a.alt;
-    integrate(a, P, D, s, F, T, 1, R(0.5) * dt, 1, R(0.5) * dt, a.dt_disp);
-    D.F[s] = st3<R>(F);
-    D.T[s] = st3<R>(T);
-    D.inertia[s] = P.inertia[s];
-    D.md[s] = mdi;
-    D.meta[s] = mi;
-    D.orig[s] = oi;
-  }
-
   // statistics: warp reduction then one atomic per warp
   const unsigned full = 0xffffffffu;
 #pragma unroll
@@ -981,7 +975,7 @@ int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forc
   const int nb = grid_for(C, kScanTile);
   scan_tiles_kernel<<<nb, kScanThreads, 0, s>>>(a.cell_count, a.cell_start, a.block_sums, C);
   scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(a.block_sums, nb, a.cell_start, C);
-  scan_add_kernel<<<grid_for(C, 256), 256, 0, s>>>(a.cell_start, a.block_sums, C);
+  scan_add_kernel<<<grid_for(C, 256), 256, 0, s>>>(a.cell_start, a.cell_cursor, a.block_sums, C);
   if (a.n > 0) scatter_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
   cell_sort_kernel<R><<<grid_for(C, 256), 256, 0, s>>>(a);
   if (a.n > 0) gather_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, gather_forces);
@@ -989,7 +983,7 @@ int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forc
 }
 
 template <typename R>
-int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int fused, int phases) {
+int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int phases) {
   if (a.n == 0) return 0;
   const int cb = (a.contacts_block >= 32 && a.contacts_block <= 256) ? a.contacts_block : 256;
   const int fb = (a.forces_block >= 32 && a.forces_block <= 128) ? a.forces_block : 128;
@@ -998,18 +992,14 @@ int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int
   const int g = grid_for(a.n, fb);
   if (a.has_convex) {
     if (diag)
-      forces_kernel<R, true, true, false><<<g, fb, 0, s>>>(a, R(dt));
-    else if (fused)
-      forces_kernel<R, false, true, true><<<g, fb, 0, s>>>(a, R(dt));
+      forces_kernel<R, true, true><<<g, fb, 0, s>>>(a, R(dt));
     else
-      forces_kernel<R, false, true, false><<<g, fb, 0, s>>>(a, R(dt));
+      forces_kernel<R, false, true><<<g, fb, 0, s>>>(a, R(dt));
   } else {
     if (diag)
-      forces_kernel<R, true, false, false><<<g, fb, 0, s>>>(a, R(dt));
-    else if (fused)
-      forces_kernel<R, false, false, true><<<g, fb, 0, s>>>(a, R(dt));
+      forces_kernel<R, true, false><<<g, fb, 0, s>>>(a, R(dt));
     else
-      forces_kernel<R, false, false, false><<<g, fb, 0, s>>>(a, R(dt));
+      forces_kernel<R, false, false><<<g, fb, 0, s>>>(a, R(dt));
   }
   return check_launch();
 }
@@ -1051,7 +1041,7 @@ int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int in
   template int launch_kick_move<R>(const StepArgs<R>&, cudaStream_t, int, double, int, double, double);    \
   template int launch_bin<R>(const StepArgs<R>&, cudaStream_t);                                            \
   template int launch_sort_and_gather<R>(const StepArgs<R>&, cudaStream_t, int);                           \
-  template int launch_forces<R>(const StepArgs<R>&, cudaStream_t, double, int, int, int);                  \
+  template int launch_forces<R>(const StepArgs<R>&, cudaStream_t, double, int, int);                       \
   template int launch_zero_kdelta<R>(const StepArgs<R>&, cudaStream_t);                                    \
   template int launch_update_dynamic<R>(const StepArgs<R>&, cudaStream_t, const double*, const double*);     \
   template int launch_candidate_pairs<R>(const StepArgs<R>&, cudaStream_t, int, int, int*, int,           \
