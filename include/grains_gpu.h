@@ -268,13 +268,19 @@ int grains_gpu_reset_stats(grains_gpu_ctx* ctx);
  *   forces_block   threads per block of the contact-law kernel (32 .. 128)
  *   list_capacity  contact-list slots per particle (8 .. 256; 0 = 32 for
  *                  spheres, 64 when other shapes are present); a particle
- *                  with more contacts fails the step with GRAINS_GPU_PAIR_OVERFLOW */
+ *                  with more contacts fails the step with GRAINS_GPU_PAIR_OVERFLOW
+ *   gather_every   steps between two permutations of the particle arrays
+ *                  into cell order (1 .. 64); in between the cell lists are
+ *                  rebuilt every step and reached through a permutation.
+ *                  Results do not depend on it: every sum runs in cell order,
+ *                  then id order inside a cell. */
 typedef struct grains_gpu_tuning {
   double  cell_factor;
   int32_t contacts_block;
   int32_t forces_block;
   int32_t list_capacity;
-  int32_t reserved[5];
+  int32_t gather_every;
+  int32_t reserved[4];
 } grains_gpu_tuning;
 int grains_gpu_get_tuning(const grains_gpu_ctx* ctx, grains_gpu_tuning* tuning);
 int grains_gpu_set_tuning(grains_gpu_ctx* ctx, const grains_gpu_tuning* tuning);
@@ -282,7 +288,9 @@ int grains_gpu_set_tuning(grains_gpu_ctx* ctx, const grains_gpu_tuning* tuning);
  * for candidate tunings (coordinate descent over list capacity, force block,
  * broadphase block, cell factor), keeps the fastest that completed without
  * error, applies it and restores the state exactly (particles, contact
- * memory, obstacle poses).  time = the current simulation time. */
+ * memory, obstacle poses).  The candidates cover the list capacity, the two
+ * block shapes, the gather period and the cell factor (coordinate descent).
+ * time = the current simulation time. */
 int grains_gpu_autotune(grains_gpu_ctx* ctx, double time, double dt, int32_t trial_steps,
                         grains_gpu_tuning* best, double* best_ms);
 

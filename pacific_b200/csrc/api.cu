@@ -137,6 +137,8 @@ struct grains_gpu_ctx {
   int contacts_block = 256;
   int forces_block = 128;
   int list_capacity = 0;  // 0: 32 slots for spheres, 64 when other shapes are present
+  int gather_every = 16;  // steps between two gathers of the arrays into cell order
+  int since_gather = 0;   // sorts without a gather since the last one
 };
 
 namespace {
@@ -465,20 +467,30 @@ int with_args(grains_gpu_ctx* c, F f) {
   return f(a);
 }
 
-int sort_now(grains_gpu_ctx* c, int gather_forces) {
+// Cell ranges and permutation of the current positions; with gather the
+// particle arrays are also permuted into cell order (other buffer).
+int sort_now(grains_gpu_ctx* c, int gather_forces, bool gather = true) {
   int rc = 0;
   if (!c->keys_valid) {
     CK(cudaMemsetAsync(c->cell_count, 0, (size_t)c->n_cells * sizeof(int), c->stream));
     rc = with_args(c, [&](auto& a) { return launch_bin(a, c->stream); });
     if (rc) return fail(c, rc, "bin kernel launch failed");
   }
-  rc = with_args(c, [&](auto& a) { return launch_sort_and_gather(a, c->stream, gather_forces); });
+  rc = with_args(c, [&](auto& a) { return launch_sort_and_gather(a, c->stream, gather ? 1 : 0, gather_forces); });
   if (rc) return fail(c, rc, "sort kernels launch failed");
-  c->cur = 1 - c->cur;
+  if (gather) {
+    c->cur = 1 - c->cur;
+    c->since_gather = 0;
+  } else {
+    ++c->since_gather;
+  }
   c->sorted = true;
   c->keys_valid = false;
   return 0;
 }
+
+// the sort of a middle step: the arrays are gathered every gather_every steps
+int sort_for_step(grains_gpu_ctx* c) { return sort_now(c, 0, c->since_gather + 1 >= c->gather_every); }
 
 int read_status(grains_gpu_ctx* c) {
   int st = 0;
@@ -556,7 +568,7 @@ int first_move(grains_gpu_ctx* c, double dt, double time) {
 // the combined kernel's registers and serial memory chain cost more than the
 // extra pass over the state.)
 int middle_step(grains_gpu_ctx* c, double dt) {
-  if (int rc = sort_now(c, 0)) return rc;
+  if (int rc = sort_for_step(c)) return rc;
   if (int rc = forces_now(c, dt, 0)) return rc;
   int rc = with_args(c, [&](auto& a) { return launch_kick_move(a, c->stream, 1, 0.5 * dt, 1, 0.5 * dt, dt); });
   if (rc) return fail(c, rc, "kick/move launch failed");
@@ -1364,8 +1376,16 @@ int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt)
   // evaluation and leaves its second half kick pending
   if (int rc = first_move(c, dt, *time)) return rc;
   int middle = n_steps - 1;
-  while (middle >= 2) {
-    const int slot = 2 * c->cur + c->hcur;  // two middle steps restore (cur, hcur)
+  // a graph holds G middle steps starting right after a gather: G = the gather
+  // period, doubled when odd, so that the contact-memory buffers (swapped every
+  // step) come back; (cur, hcur) then select the graph
+  const int G = c->gather_every % 2 ? 2 * c->gather_every : c->gather_every;
+  while (middle > 0 && c->since_gather % c->gather_every != 0) {
+    if (int rc = middle_step(c, dt)) return rc;
+    --middle;
+  }
+  while (middle >= G) {
+    const int slot = 2 * c->cur + c->hcur;
     if (!c->graph[slot] || c->graph_dt[slot] != dt) {
       if (c->graph[slot]) {
         cudaGraphExecDestroy(c->graph[slot]);
@@ -1374,11 +1394,13 @@ int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt)
       const int cur0 = c->cur, h0 = c->hcur;
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-      int rc = middle_step(c, dt);
-      if (!rc) rc = middle_step(c, dt);
+      const int sg0 = c->since_gather;
+      int rc = 0;
+      for (int k = 0; k < G && !rc; ++k) rc = middle_step(c, dt);
       cudaError_t e = cudaStreamEndCapture(c->stream, &g);
       c->cur = cur0;  // capturing does not execute: restore the buffer selection
       c->hcur = h0;
+      c->since_gather = sg0;
       c->keys_valid = true;
       c->sorted = false;
       if (rc) return rc;
@@ -1389,9 +1411,18 @@ int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt)
       c->graph_dt[slot] = dt;
     }
     CK(cudaGraphLaunch(c->graph[slot], c->stream));
-    middle -= 2;
+    for (int k = 0; k < G; ++k) {  // the buffer selection the graph leaves
+      if (c->since_gather + 1 >= c->gather_every) {
+        c->cur = 1 - c->cur;
+        c->since_gather = 0;
+      } else {
+        ++c->since_gather;
+      }
+      c->hcur = 1 - c->hcur;
+    }
+    middle -= G;
   }
-  if (middle == 1)
+  while (middle-- > 0)
     if (int rc = middle_step(c, dt)) return rc;
   if (int rc = last_step(c, dt)) return rc;
   for (int k = 0; k < n_steps; ++k) *time += dt;  // Grains::Simulation's clock
@@ -1557,7 +1588,7 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time,
   for (int k = 0; k < n_steps; ++k) {
     const bool last = (k == n_steps - 1);
     CK(cudaEventRecord(ev[1], c->stream));
-    if (int rc = sort_now(c, 0)) return rc;
+    if (int rc = last ? sort_now(c, 0) : sort_for_step(c)) return rc;
     CK(cudaEventRecord(ev[2], c->stream));
     if (int rc = forces_now(c, dt, 0, 1)) return rc;
     CK(cudaEventRecord(ev[3], c->stream));
@@ -1616,6 +1647,7 @@ int grains_gpu_get_tuning(const grains_gpu_ctx* c, grains_gpu_tuning* t) {
   t->contacts_block = c->contacts_block;
   t->forces_block = c->forces_block;
   t->list_capacity = c->list_capacity > 0 ? c->list_capacity : c->clist_cap;
+  t->gather_every = c->gather_every;
   return 0;
 }
 
@@ -1623,14 +1655,16 @@ int grains_gpu_set_tuning(grains_gpu_ctx* c, const grains_gpu_tuning* t) {
   if (!c || !t) return GRAINS_GPU_INVALID_ARGUMENT;
   if (!(t->cell_factor >= 1.0 && t->cell_factor <= 4.0) || t->contacts_block < 32 || t->contacts_block > 256 ||
       t->contacts_block % 32 || t->forces_block < 32 || t->forces_block > 128 || t->forces_block % 32 ||
-      (t->list_capacity != 0 && (t->list_capacity < 8 || t->list_capacity > 256)))
+      (t->list_capacity != 0 && (t->list_capacity < 8 || t->list_capacity > 256)) || t->gather_every < 1 ||
+      t->gather_every > 64)
     return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "tuning out of range");
   const bool regrid = t->cell_factor != c->cell_factor;
   c->cell_factor = t->cell_factor;
   c->contacts_block = t->contacts_block;
   c->forces_block = t->forces_block;
   c->list_capacity = t->list_capacity;
-  for (int k = 0; k < 4; ++k)  // launch shapes are baked into the step graphs
+  c->gather_every = t->gather_every;
+  for (int k = 0; k < 4; ++k)  // launch shapes and the gather period are baked into the step graphs
     if (c->graph[k]) {
       cudaGraphExecDestroy(c->graph[k]);
       c->graph[k] = nullptr;
@@ -1678,7 +1712,7 @@ namespace {
 // memory, obstacle poses, clock), for trials that must start from it
 struct Snapshot {
   std::vector<std::pair<void*, size_t>> bufs;  // (device copy, bytes), in the order of fields()
-  int cur = 0, hcur = 0;
+  int cur = 0, hcur = 0, since_gather = 0;
   bool pending = false;
   double pending_dt = 0.;
   int64_t steps_done = 0;
@@ -1702,6 +1736,7 @@ std::vector<std::pair<void*, size_t>> snapshot_fields(grains_gpu_ctx* c, int cur
 int take_snapshot(grains_gpu_ctx* c, Snapshot& s) {
   s.cur = c->cur;
   s.hcur = c->hcur;
+  s.since_gather = c->since_gather;
   s.pending = c->pending_kick2;
   s.pending_dt = c->pending_dt;
   s.steps_done = c->steps_done;
@@ -1723,6 +1758,7 @@ int restore_snapshot(grains_gpu_ctx* c, const Snapshot& s) {
       return GRAINS_GPU_CUDA_ERROR;
   c->cur = s.cur;
   c->hcur = s.hcur;
+  c->since_gather = s.since_gather;
   c->pending_kick2 = s.pending;
   c->pending_dt = s.pending_dt;
   c->steps_done = s.steps_done;
@@ -1795,6 +1831,13 @@ int grains_gpu_autotune(grains_gpu_ctx* c, double time, double dt, int32_t trial
     grains_gpu_tuning t = b;
     t.contacts_block = cb;
     if (cb == b.contacts_block) continue;
+    const double ms = trial(t);
+    if (ms > 0. && (t_best < 0. || ms < t_best)) { t_best = ms; b = t; }
+  }
+  for (int ge : {1, 2, 4, 8, 16}) {
+    grains_gpu_tuning t = b;
+    t.gather_every = ge;
+    if (ge == b.gather_every) continue;
     const double ms = trial(t);
     if (ms > 0. && (t_best < 0. || ms < t_best)) { t_best = ms; b = t; }
   }

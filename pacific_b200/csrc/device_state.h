@@ -13,7 +13,8 @@
 //     md     double4 (mass, crust, equivalent radius, 0)
 //     meta   int4    (id, material, shape, system)
 //     orig   int     upload index (history row, download order)
-//   cells: count[C], start[C+1] (exclusive scan), perm[N]
+//   cells: count[C], start[C+1] (exclusive scan), perm[N] (cell slot ->
+//     particle; the identity right after the arrays are gathered in cell order)
 //   contact memory: rows of H entries per particle, indexed by upload
 //     index, double buffered (prev -> next each force evaluation).
 #pragma once
@@ -168,8 +169,11 @@ int launch_kick_move(const StepArgs<R>& a, cudaStream_t s, int do_kick2, double 
                      double dt_v, double dt_x);
 template <typename R>
 int launch_bin(const StepArgs<R>& a, cudaStream_t s);
+// cell ranges and the slot -> particle permutation of the current positions;
+// gather != 0 also permutes the particle arrays into cell order (into the
+// other buffer; the permutation becomes the identity)
 template <typename R>
-int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forces);
+int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather, int gather_forces);
 // phases: 1 = contact lists, 2 = contact law, 3 = both
 template <typename R>
 int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int phases = 3);

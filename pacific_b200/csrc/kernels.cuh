@@ -11,6 +11,8 @@
 //   scatter        slot = atomic fill cursor of the cell
 //   cell_sort      each cell's particles ordered by id (deterministic order)
 //   gather         every per-particle array permuted into the new order
+//                  (every few steps only: between gathers the kernels reach
+//                  a cell's particles through the permutation)
 //   forces         broadphase over the 27 surrounding cells, sphere/box
 //                  narrowphase, contact law + memory, per-particle sums,
 //                  static and moving obstacles
@@ -294,6 +296,8 @@ __global__ void cell_sort_kernel(StepArgs<R> a) {
   }
 }
 
+// permutes every per-particle array into cell order; the permutation then
+// becomes the identity (each thread resets its own entry after reading it)
 template <typename R>
 __global__ void __launch_bounds__(256) gather_kernel(StepArgs<R> a, int gather_forces) {
   int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -303,6 +307,7 @@ __global__ void __launch_bounds__(256) gather_kernel(StepArgs<R> a, int gather_f
     set_status(a.stats, GRAINS_GPU_CUDA_ERROR);
     return;
   }
+  a.perm[t] = t;
   const ParticleArrays<R>& C = a.cur;
   const ParticleArrays<R>& D = a.alt;
   D.xr[t] = C.xr[s];
@@ -496,7 +501,8 @@ __global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
       const int t1 = a.cell_start[cell_index(S, i1, j, k) + 1];
       ncand += (unsigned long long)(t1 - t0);
       for (int t = t0; t < t1; ++t) {
-        const double4 xj = P.xr[t];
+        const int j = a.perm[t];  // cell slot -> particle (identity right after a gather)
+        const double4 xj = P.xr[j];
         // cheap rejection of far candidates: the squared distance against the
         // squared radius sum with a 1e-12 relative margin (rounding of either
         // side is below 1e-15 relative)
@@ -508,8 +514,8 @@ __global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
         // |AB| and r_A + r_B are symmetric in IEEE arithmetic, so the test
         // gives the same bits whichever body is A
         const double dist = sphere_sphere_overlap(Xi, xi.w, d3(xj.x, xj.y, xj.z), xj.w, &ab, &nab);
-        if (dist < 0. && t != s) {
-          if (cnt < a.clist_cap) list[cnt] = t;
+        if (dist < 0. && j != s) {
+          if (cnt < a.clist_cap) list[cnt] = j;
           ++cnt;
         }
       }
@@ -910,8 +916,9 @@ __global__ void candidate_pairs_kernel(StepArgs<R> a, int sys, int include_obsta
       const int t0 = a.cell_start[cell_index(S, i0, j, k)];
       const int t1 = a.cell_start[cell_index(S, i1, j, k) + 1];
       for (int t = t0; t < t1; ++t) {
-        int idj = P.meta[t].x;
-        if (t == s || !(mi.x < idj)) continue;
+        const int j = a.perm[t];
+        int idj = P.meta[j].x;
+        if (j == s || !(mi.x < idj)) continue;
         unsigned long long slot = atomicAdd(count, 1ull);
         if (slot < (unsigned long long)cap) {
           out[2 * slot] = mi.x;
@@ -970,7 +977,7 @@ int launch_bin(const StepArgs<R>& a, cudaStream_t s) {
 }
 
 template <typename R>
-int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forces) {
+int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather, int gather_forces) {
   const int C = a.n_cells;
   const int nb = grid_for(C, kScanTile);
   scan_tiles_kernel<<<nb, kScanThreads, 0, s>>>(a.cell_count, a.cell_start, a.block_sums, C);
@@ -978,7 +985,7 @@ int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather_forc
   scan_add_kernel<<<grid_for(C, 256), 256, 0, s>>>(a.cell_start, a.cell_cursor, a.block_sums, C);
   if (a.n > 0) scatter_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
   cell_sort_kernel<R><<<grid_for(C, 256), 256, 0, s>>>(a);
-  if (a.n > 0) gather_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, gather_forces);
+  if (a.n > 0 && gather) gather_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, gather_forces);
   return check_launch();
 }
 
@@ -1040,7 +1047,7 @@ int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int in
 #define GG_INSTANTIATE(R)                                                                                  \
   template int launch_kick_move<R>(const StepArgs<R>&, cudaStream_t, int, double, int, double, double);    \
   template int launch_bin<R>(const StepArgs<R>&, cudaStream_t);                                            \
-  template int launch_sort_and_gather<R>(const StepArgs<R>&, cudaStream_t, int);                           \
+  template int launch_sort_and_gather<R>(const StepArgs<R>&, cudaStream_t, int, int);                      \
   template int launch_forces<R>(const StepArgs<R>&, cudaStream_t, double, int, int);                       \
   template int launch_zero_kdelta<R>(const StepArgs<R>&, cudaStream_t);                                    \
   template int launch_update_dynamic<R>(const StepArgs<R>&, cudaStream_t, const double*, const double*);     \
