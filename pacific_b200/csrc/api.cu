@@ -95,13 +95,13 @@ struct grains_gpu_ctx {
     double4* md;
     int4* meta;
     int* orig;
+    unsigned* key;  // cell key of the current positions
   } buf[2]{};
   int cur = 0;  // which copy is current
   void* hist[2] = {nullptr, nullptr};
   int* hist_n[2] = {nullptr, nullptr};
   int hcur = 0;  // hist[hcur] = latest memory (prev for the next force evaluation)
   int* coord = nullptr;
-  unsigned* key = nullptr;
   int* perm = nullptr;
   int *cell_count = nullptr, *cell_start = nullptr, *cell_cursor = nullptr, *block_sums = nullptr;
   StatsDev* stats = nullptr;
@@ -410,6 +410,7 @@ void fill_arrays(grains_gpu_ctx* c, ParticleArrays<R>& P, int which) {
   P.md = b.md;
   P.meta = b.meta;
   P.orig = b.orig;
+  P.key = b.key;
 }
 
 template <typename R>
@@ -432,7 +433,6 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   fill_arrays<R>(c, a.cur, c->cur);
   fill_arrays<R>(c, a.alt, 1 - c->cur);
   a.coord = c->coord;
-  a.key = c->key;
   a.cell_count = c->cell_count;
   a.cell_start = c->cell_start;
   a.cell_cursor = c->cell_cursor;
@@ -652,7 +652,8 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
     b.md = dalloc<double4>(N, c->pool);
     b.meta = dalloc<int4>(N, c->pool);
     b.orig = dalloc<int>(N, c->pool);
-    ok = b.xr && b.q && b.v && b.w && b.wbf && b.F && b.T && b.inertia && b.md && b.meta && b.orig;
+    b.key = dalloc<unsigned>(N, c->pool);
+    ok = b.xr && b.q && b.v && b.w && b.wbf && b.F && b.T && b.inertia && b.md && b.meta && b.orig && b.key;
   }
   const size_t hsz = c->precision == GRAINS_GPU_FP64 ? sizeof(HistEntry<double>) : sizeof(HistEntry<float>);
   for (int k = 0; k < 2 && ok; ++k) {
@@ -662,7 +663,6 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
   }
   if (ok) {
     c->coord = dalloc<int>(N, c->pool);
-    c->key = dalloc<unsigned>(N, c->pool);
     c->perm = dalloc<int>(N, c->pool);
     c->stats = dalloc<StatsDev>(1, c->pool);
     c->pairs_cap = (int)std::min<size_t>(16 * N + 1024, (size_t)1 << 30);
@@ -670,7 +670,7 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
     c->pairs_n = dalloc<unsigned long long>(1, c->pool);
     c->pair_force = dalloc<double>(3 * (size_t)c->pairs_cap, c->pool);
     c->clock = dalloc<double>(1, c->pool);
-    ok = c->coord && c->key && c->perm && c->stats && c->pairs && c->pairs_n && c->pair_force && c->clock;
+    ok = c->coord && c->perm && c->stats && c->pairs && c->pairs_n && c->pair_force && c->clock;
   }
   if (!ok) {
     c->err = "cudaMalloc failed for the requested capacity";

@@ -119,6 +119,7 @@ struct ParticleArrays {
   double4* md;
   int4* meta;
   int* orig;
+  unsigned* key;  // cell key of the current positions (written by the kick / bin kernels)
 };
 
 template <typename R>
@@ -140,7 +141,6 @@ struct StepArgs {
   ParticleArrays<R> cur;
   ParticleArrays<R> alt;
   int* coord;            // coordination number (sorted order)
-  unsigned* key;
   int* cell_count;
   int* cell_cursor;      // fill cursor of each cell (scatter)
   int* cell_start;

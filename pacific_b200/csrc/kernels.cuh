@@ -140,7 +140,7 @@ __device__ __forceinline__ void integrate(const StepArgs<R>& a, const ParticleAr
     int ci, cj, ck;
     if (!cell_of(S, xr.x, xr.y, xr.z, ci, cj, ck)) set_status(a.stats, GRAINS_GPU_OUT_OF_GRID);
     unsigned key = (unsigned)cell_index(S, ci, cj, ck);
-    a.key[s] = key;
+    dst.key[s] = key;
     atomicAdd(&a.cell_count[key], 1);  // result unused: a fire-and-forget reduction
   } else if (a.has_basis && !sphere && dst.basis != src.basis) {
     for (int t = 0; t < 9; ++t) dst.basis[9 * (size_t)s + t] = src.basis[9 * (size_t)s + t];
@@ -173,7 +173,7 @@ __global__ void bin_kernel(StepArgs<R> a) {
   int ci, cj, ck;
   if (!cell_of(S, xr.x, xr.y, xr.z, ci, cj, ck)) set_status(a.stats, GRAINS_GPU_OUT_OF_GRID);
   unsigned key = (unsigned)cell_index(S, ci, cj, ck);
-  a.key[s] = key;
+  a.cur.key[s] = key;
   atomicAdd(&a.cell_count[key], 1);
 }
 
@@ -267,7 +267,7 @@ template <typename R>
 __global__ void scatter_kernel(StepArgs<R> a) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
-  const unsigned key = a.key[s];
+  const unsigned key = a.cur.key[s];
   const long long slot = (key < (unsigned)a.n_cells) ? (long long)atomicAdd(&a.cell_cursor[key], 1) : -1;
   if (slot < 0 || slot >= a.n) {
     set_status(a.stats, GRAINS_GPU_CUDA_ERROR);
@@ -319,6 +319,7 @@ __global__ void __launch_bounds__(256) gather_kernel(StepArgs<R> a, int gather_f
   D.md[t] = C.md[s];
   D.meta[t] = C.meta[s];
   D.orig[t] = C.orig[s];
+  D.key[t] = C.key[s];
   if (gather_forces) {
     D.F[t] = C.F[s];
     D.T[t] = C.T[s];
@@ -485,39 +486,43 @@ __global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
   const double4 xi = P.xr[s];
   const SysDev& S = a.sys[P.meta[s].w];
   const D3 Xi = d3(xi.x, xi.y, xi.z);
-  int ci, cj, ck;
-  cell_of(S, xi.x, xi.y, xi.z, ci, cj, ck);
+  // the particle's cell from the key of the current positions (the cell lists
+  // were built from it): key = offset + j nbk nbi + k nbi + i
+  const int local = (int)P.key[s] - S.cell_offset;
+  const int ci = local % S.nbi, ck = (local / S.nbi) % S.nbk, cj = local / (S.nbi * S.nbk);
   const int i0 = max(ci - 1, 0), i1 = min(ci + 1, S.nbi - 1);
+  // the slot ranges of the 9 cell rows, loaded before any candidate
+  int r0[9], r1[9];
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+    const int j = cj + r / 3 - 1, k = ck + r % 3 - 1;
+    const bool ok = j >= 0 && j < S.nbj && k >= 0 && k < S.nbk;
+    r0[r] = ok ? a.cell_start[cell_index(S, i0, j, k)] : 0;
+    r1[r] = ok ? a.cell_start[cell_index(S, i1, j, k) + 1] : 0;
+  }
   int* list = a.clist + (size_t)s * a.clist_cap;
   int cnt = 0;
   unsigned long long ncand = 0;
-  for (int dj = -1; dj <= 1; ++dj) {
-    const int j = cj + dj;
-    if (j < 0 || j >= S.nbj) continue;
-    for (int dk = -1; dk <= 1; ++dk) {
-      const int k = ck + dk;
-      if (k < 0 || k >= S.nbk) continue;
-      const int t0 = a.cell_start[cell_index(S, i0, j, k)];
-      const int t1 = a.cell_start[cell_index(S, i1, j, k) + 1];
-      ncand += (unsigned long long)(t1 - t0);
-      for (int t = t0; t < t1; ++t) {
-        const int j = a.perm[t];  // cell slot -> particle (identity right after a gather)
-        const double4 xj = P.xr[j];
-        // cheap rejection of far candidates: the squared distance against the
-        // squared radius sum with a 1e-12 relative margin (rounding of either
-        // side is below 1e-15 relative)
-        const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-        const double rs = xi.w + xj.w;
-        if (dx * dx + dy * dy + dz * dz > rs * rs * (1. + 1.e-12)) continue;
-        D3 ab;
-        double nab;
-        // |AB| and r_A + r_B are symmetric in IEEE arithmetic, so the test
-        // gives the same bits whichever body is A
-        const double dist = sphere_sphere_overlap(Xi, xi.w, d3(xj.x, xj.y, xj.z), xj.w, &ab, &nab);
-        if (dist < 0. && j != s) {
-          if (cnt < a.clist_cap) list[cnt] = j;
-          ++cnt;
-        }
+#pragma unroll
+  for (int r = 0; r < 9; ++r) {
+    ncand += (unsigned long long)(r1[r] - r0[r]);
+    for (int t = r0[r]; t < r1[r]; ++t) {
+      const int p = a.perm[t];  // cell slot -> particle (identity right after a gather)
+      const double4 xj = P.xr[p];
+      // cheap rejection of far candidates: the squared distance against the
+      // squared radius sum with a 1e-12 relative margin (rounding of either
+      // side is below 1e-15 relative)
+      const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+      const double rs = xi.w + xj.w;
+      if (dx * dx + dy * dy + dz * dz > rs * rs * (1. + 1.e-12)) continue;
+      D3 ab;
+      double nab;
+      // |AB| and r_A + r_B are symmetric in IEEE arithmetic, so the test
+      // gives the same bits whichever body is A
+      const double dist = sphere_sphere_overlap(Xi, xi.w, d3(xj.x, xj.y, xj.z), xj.w, &ab, &nab);
+      if (dist < 0. && p != s) {
+        if (cnt < a.clist_cap) list[cnt] = p;
+        ++cnt;
       }
     }
   }
