@@ -273,14 +273,20 @@ int grains_gpu_reset_stats(grains_gpu_ctx* ctx);
  *                  into cell order (1 .. 64); in between the cell lists are
  *                  rebuilt every step and reached through a permutation.
  *                  Results do not depend on it: every sum runs in cell order,
- *                  then id order inside a cell. */
+ *                  then id order inside a cell.
+ *   persistent     1: the middle steps of grains_gpu_step run in one
+ *                  cooperative launch (every block resident, the phases
+ *                  separated by a grid barrier with a bounded wait) instead of
+ *                  9 launches per step replayed from graphs; same results.
+ *                  Pays where launch gaps dominate (small systems). */
 typedef struct grains_gpu_tuning {
   double  cell_factor;
   int32_t contacts_block;
   int32_t forces_block;
   int32_t list_capacity;
   int32_t gather_every;
-  int32_t reserved[4];
+  int32_t persistent;
+  int32_t reserved[3];
 } grains_gpu_tuning;
 int grains_gpu_get_tuning(const grains_gpu_ctx* ctx, grains_gpu_tuning* tuning);
 int grains_gpu_set_tuning(grains_gpu_ctx* ctx, const grains_gpu_tuning* tuning);

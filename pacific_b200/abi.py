@@ -84,7 +84,8 @@ _P_F64 = C.POINTER(C.c_double)
 
 class Tuning(C.Structure):
     _fields_ = [("cell_factor", C.c_double), ("contacts_block", C.c_int32), ("forces_block", C.c_int32),
-                ("list_capacity", C.c_int32), ("gather_every", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("list_capacity", C.c_int32), ("gather_every", C.c_int32), ("persistent", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
 
 
 class Particles(C.Structure):
@@ -458,10 +459,11 @@ class Simulation:
         t = Tuning()
         self._check(self.lib.fn["get_tuning"](self.ctx, C.byref(t)))
         return {"cell_factor": t.cell_factor, "contacts_block": t.contacts_block, "forces_block": t.forces_block,
-                "list_capacity": t.list_capacity, "gather_every": t.gather_every}
+                "list_capacity": t.list_capacity, "gather_every": t.gather_every, "persistent": t.persistent}
 
-    def set_tuning(self, cell_factor=1.0, contacts_block=256, forces_block=128, list_capacity=0, gather_every=16):
-        t = Tuning(cell_factor, contacts_block, forces_block, list_capacity, gather_every)
+    def set_tuning(self, cell_factor=1.0, contacts_block=256, forces_block=128, list_capacity=0, gather_every=16,
+                   persistent=0):
+        t = Tuning(cell_factor, contacts_block, forces_block, list_capacity, gather_every, persistent)
         self._check(self.lib.fn["set_tuning"](self.ctx, C.byref(t)))
 
     def autotune(self, time, dt, trial_steps=100):
@@ -469,7 +471,8 @@ class Simulation:
         t, ms = Tuning(), C.c_double()
         self._check(self.lib.fn["autotune"](self.ctx, time, dt, trial_steps, C.byref(t), C.byref(ms)))
         return ({"cell_factor": t.cell_factor, "contacts_block": t.contacts_block, "forces_block": t.forces_block,
-                 "list_capacity": t.list_capacity, "gather_every": t.gather_every}, ms.value)
+                 "list_capacity": t.list_capacity, "gather_every": t.gather_every, "persistent": t.persistent},
+                ms.value)
 
     # ---- benchmark helpers (CUDA implementation only) ----
     def stream_handle(self):

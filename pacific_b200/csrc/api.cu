@@ -139,6 +139,10 @@ struct grains_gpu_ctx {
   int list_capacity = 0;  // 0: 32 slots for spheres, 64 when other shapes are present
   int gather_every = 16;  // steps between two gathers of the arrays into cell order
   int since_gather = 0;   // sorts without a gather since the last one
+  int persistent = 0;     // middle steps in one cooperative launch instead of graphs
+  unsigned* pbar = nullptr;  // grid-barrier state of the persistent launch
+  int* psums = nullptr;      // its scan scratch (one int per block)
+  int pblocks = 0;
 };
 
 namespace {
@@ -577,6 +581,41 @@ int middle_step(grains_gpu_ctx* c, double dt) {
   return move_obstacles(c, dt);
 }
 
+// n middle steps in one cooperative launch (persistent_steps_kernel); the
+// host then follows the buffer selection the launch leaves
+int persistent_middle_steps(grains_gpu_ctx* c, int n, double dt) {
+  if (!c->pbar) {
+    void* q = nullptr;
+    CK(cudaMalloc(&q, 2 * sizeof(unsigned)));
+    c->pbar = (unsigned*)q;
+  }
+  if (!c->pblocks) {
+    c->pblocks = with_args(c, [&](auto& a) { return persistent_blocks(a); });
+    if (c->pblocks <= 0) return fail(c, GRAINS_GPU_CUDA_ERROR, "persistent launch: occupancy query failed");
+    void* q = nullptr;
+    CK(cudaMalloc(&q, (size_t)c->pblocks * sizeof(int)));
+    c->psums = (int*)q;
+  }
+  CK(cudaMemsetAsync(c->pbar, 0, 2 * sizeof(unsigned), c->stream));
+  int rc = with_args(c, [&](auto& a) {
+    return launch_persistent_steps(a, c->stream, n, dt, c->gather_every, c->since_gather, c->n_moving, c->clock,
+                                   c->pbar, c->psums, c->pblocks);
+  });
+  if (rc) return fail(c, rc, "persistent launch failed (cooperative launch refused?)");
+  for (int k = 0; k < n; ++k) {
+    if (c->since_gather + 1 >= c->gather_every) {
+      c->cur = 1 - c->cur;
+      c->since_gather = 0;
+    } else {
+      ++c->since_gather;
+    }
+    c->hcur = 1 - c->hcur;
+  }
+  c->keys_valid = true;
+  c->sorted = false;
+  return 0;
+}
+
 // The last step of a run: sort and forces; the second half kick stays pending
 int last_step(grains_gpu_ctx* c, double dt) {
   if (int rc = sort_now(c, 0)) return rc;
@@ -698,6 +737,8 @@ int grains_gpu_destroy(grains_gpu_ctx* c) {
   if (c->clist) cudaFree(c->clist);
   if (c->ccount) cudaFree(c->ccount);
   if (c->stage_basis) cudaFree(c->stage_basis);
+  if (c->pbar) cudaFree(c->pbar);
+  if (c->psums) cudaFree(c->psums);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -1376,6 +1417,10 @@ int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt)
   // evaluation and leaves its second half kick pending
   if (int rc = first_move(c, dt, *time)) return rc;
   int middle = n_steps - 1;
+  if (c->persistent && middle > 0) {
+    if (int rc = persistent_middle_steps(c, middle, dt)) return rc;
+    middle = 0;
+  }
   // a graph holds G middle steps starting right after a gather: G = the gather
   // period, doubled when odd, so that the contact-memory buffers (swapped every
   // step) come back; (cur, hcur) then select the graph
@@ -1648,6 +1693,7 @@ int grains_gpu_get_tuning(const grains_gpu_ctx* c, grains_gpu_tuning* t) {
   t->forces_block = c->forces_block;
   t->list_capacity = c->list_capacity > 0 ? c->list_capacity : c->clist_cap;
   t->gather_every = c->gather_every;
+  t->persistent = c->persistent;
   return 0;
 }
 
@@ -1664,6 +1710,12 @@ int grains_gpu_set_tuning(grains_gpu_ctx* c, const grains_gpu_tuning* t) {
   c->forces_block = t->forces_block;
   c->list_capacity = t->list_capacity;
   c->gather_every = t->gather_every;
+  c->persistent = t->persistent ? 1 : 0;
+  c->pblocks = 0;  // the block count follows the kernel variant (convex or not)
+  if (c->psums) {
+    cudaFree(c->psums);
+    c->psums = nullptr;
+  }
   for (int k = 0; k < 4; ++k)  // launch shapes and the gather period are baked into the step graphs
     if (c->graph[k]) {
       cudaGraphExecDestroy(c->graph[k]);
@@ -1838,6 +1890,13 @@ int grains_gpu_autotune(grains_gpu_ctx* c, double time, double dt, int32_t trial
     grains_gpu_tuning t = b;
     t.gather_every = ge;
     if (ge == b.gather_every) continue;
+    const double ms = trial(t);
+    if (ms > 0. && (t_best < 0. || ms < t_best)) { t_best = ms; b = t; }
+  }
+  for (int ps : {0, 1}) {
+    grains_gpu_tuning t = b;
+    t.persistent = ps;
+    if (ps == b.persistent) continue;
     const double ms = trial(t);
     if (ms > 0. && (t_best < 0. || ms < t_best)) { t_best = ms; b = t; }
   }

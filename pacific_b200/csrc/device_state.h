@@ -190,6 +190,14 @@ int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int in
 int launch_obstacle_move(ObstacleDev* obs, const int* moving_idx, int n_moving, const ShapeDev* shapes,
                          const double* verts, double dt, double* clock, double host_time, int use_host_time,
                          cudaStream_t s);
+// n middle steps of grains_gpu_step in one cooperative launch of `blocks`
+// blocks (persistent_blocks: all resident); bar: 2 zeroed unsigned of grid
+// barrier state, sums: `blocks` ints of scan scratch
+template <typename R>
+int persistent_blocks(const StepArgs<R>& a);
+template <typename R>
+int launch_persistent_steps(const StepArgs<R>& a, cudaStream_t s, int n_steps, double dt, int gather_every,
+                            int since_gather, int n_moving, double* clock, unsigned* bar, int* sums, int blocks);
 // number of kernel launches issued by one middle step of grains_gpu_step
 int launches_per_middle_step();
 

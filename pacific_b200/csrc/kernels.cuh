@@ -20,6 +20,8 @@
 // do_move = 0.
 #pragma once
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "contact_law.cuh"
 #include "device_state.h"
@@ -264,9 +266,7 @@ static __global__ void scan_add_kernel(int* out, int* cursor, const int* block_s
 // fixed afterwards by cell_sort_kernel (by id), so the atomic order does not
 // matter
 template <typename R>
-__global__ void scatter_kernel(StepArgs<R> a) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n) return;
+__device__ __forceinline__ void scatter_one(const StepArgs<R>& a, int s) {
   const unsigned key = a.cur.key[s];
   const long long slot = (key < (unsigned)a.n_cells) ? (long long)atomicAdd(&a.cell_cursor[key], 1) : -1;
   if (slot < 0 || slot >= a.n) {
@@ -276,11 +276,15 @@ __global__ void scatter_kernel(StepArgs<R> a) {
   a.perm[slot] = s;
 }
 
+template <typename R>
+__global__ void scatter_kernel(StepArgs<R> a) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < a.n) scatter_one(a, s);
+}
+
 // order each cell's slots by particle id; resets the count for the next step
 template <typename R>
-__global__ void cell_sort_kernel(StepArgs<R> a) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= a.n_cells) return;
+__device__ __forceinline__ void cell_sort_one(const StepArgs<R>& a, int c) {
   int b = a.cell_start[c], e = a.cell_start[c + 1];
   a.cell_count[c] = 0;
   if (b < 0 || e > a.n || b > e) return;
@@ -296,12 +300,16 @@ __global__ void cell_sort_kernel(StepArgs<R> a) {
   }
 }
 
+template <typename R>
+__global__ void cell_sort_kernel(StepArgs<R> a) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c < a.n_cells) cell_sort_one(a, c);
+}
+
 // permutes every per-particle array into cell order; the permutation then
 // becomes the identity (each thread resets its own entry after reading it)
 template <typename R>
-__global__ void __launch_bounds__(256) gather_kernel(StepArgs<R> a, int gather_forces) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= a.n) return;
+__device__ __forceinline__ void gather_one(const StepArgs<R>& a, int t, int gather_forces) {
   int s = a.perm[t];
   if (s < 0 || s >= a.n) {
     set_status(a.stats, GRAINS_GPU_CUDA_ERROR);
@@ -327,6 +335,12 @@ __global__ void __launch_bounds__(256) gather_kernel(StepArgs<R> a, int gather_f
   if (a.has_basis) {
     for (int k = 0; k < 9; ++k) D.basis[9 * (size_t)t + k] = C.basis[9 * (size_t)s + k];
   }
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) gather_kernel(StepArgs<R> a, int gather_forces) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < a.n) gather_one(a, t, gather_forces);
 }
 
 // ---------------------------------------------------------------------------
@@ -479,9 +493,7 @@ __device__ ContactGeom convex_closest_point(const StepArgs<R>& a, const BodyRef&
 // appends j's slot to the particle's contact list.  Few live registers: the
 // contact law runs in forces_kernel over the lists only.
 template <typename R>
-__global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n) return;
+__device__ __forceinline__ void contacts_one(const StepArgs<R>& a, int s, unsigned long long& ncand) {
   const ParticleArrays<R>& P = a.cur;
   const double4 xi = P.xr[s];
   const SysDev& S = a.sys[P.meta[s].w];
@@ -502,7 +514,6 @@ __global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
   }
   int* list = a.clist + (size_t)s * a.clist_cap;
   int cnt = 0;
-  unsigned long long ncand = 0;
 #pragma unroll
   for (int r = 0; r < 9; ++r) {
     ncand += (unsigned long long)(r1[r] - r0[r]);
@@ -532,9 +543,22 @@ __global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
   }
   a.ccount[s] = cnt;
   ncand -= 1;  // the particle itself
+}
+
+// warp sum of a per-thread count into a statistics counter (every lane of the
+// warp calls it)
+__device__ __forceinline__ void warp_add(unsigned long long* dst, unsigned long long v) {
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) ncand += __shfl_down_sync(0xffffffffu, ncand, o);
-  if ((threadIdx.x & 31) == 0 && ncand) atomicAdd(&a.stats->n_cand, ncand);
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  unsigned long long ncand = 0;
+  if (s < a.n) contacts_one(a, s, ncand);
+  warp_add(&a.stats->n_cand, ncand);
 }
 
 // ---------------------------------------------------------------------------
@@ -542,10 +566,37 @@ __global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
 // by both of its particles; both evaluate the same contact law with the lower
 // id as p0 (same inputs, same instructions -> bit-identical forces of
 // opposite sign) and the lower id owns the pair's contact memory.
+// statistics of the force evaluation, summed per thread then per warp
+struct ForceStats {
+  unsigned long long nobs_cand, ncont_own, nobs_cont, ngjk, ngjk_it;
+  double ov_sum, ov_max;
+};
+
+__device__ __forceinline__ void flush_force_stats(StatsDev* st, ForceStats& f) {
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    f.nobs_cand += __shfl_down_sync(full, f.nobs_cand, o);
+    f.ncont_own += __shfl_down_sync(full, f.ncont_own, o);
+    f.nobs_cont += __shfl_down_sync(full, f.nobs_cont, o);
+    f.ngjk += __shfl_down_sync(full, f.ngjk, o);
+    f.ngjk_it += __shfl_down_sync(full, f.ngjk_it, o);
+    f.ov_sum += __shfl_down_sync(full, f.ov_sum, o);
+    f.ov_max = fmax(f.ov_max, __shfl_down_sync(full, f.ov_max, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (f.nobs_cand) atomicAdd(&st->n_obs_cand, f.nobs_cand);
+    if (f.ncont_own) atomicAdd(&st->n_contacts, f.ncont_own);
+    if (f.nobs_cont) atomicAdd(&st->n_obs_contacts, f.nobs_cont);
+    if (f.ngjk) atomicAdd(&st->n_gjk_calls, f.ngjk);
+    if (f.ngjk_it) atomicAdd(&st->n_gjk_iters, f.ngjk_it);
+    if (f.ov_sum > 0.) atomicAdd(&st->overlap_sum, f.ov_sum);
+    if (f.ov_max > 0.) atomic_max_pos_double(&st->overlap_max_bits, f.ov_max);
+  }
+}
+
 template <typename R, bool DIAG, bool CONVEX>
-__global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n) return;
+__device__ __forceinline__ void forces_one(const StepArgs<R>& a, int s, R dt, ForceStats& fs) {
   const ParticleArrays<R>& P = a.cur;
   const double4 xi = P.xr[s];
   const int4 mi = P.meta[s];
@@ -561,8 +612,9 @@ __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
   V3<R> F = v3<R>(R(S.gx * mdi.x), R(S.gy * mdi.x), R(S.gz * mdi.x));
   V3<R> T = v3<R>(R(0), R(0), R(0));
   int ncontact = 0, nnext = 0;
-  unsigned long long nobs_cand = 0, ncont_own = 0, nobs_cont = 0, ngjk = 0, ngjk_it = 0;
-  double ov_max = 0., ov_sum = 0.;
+  unsigned long long &nobs_cand = fs.nobs_cand, &ncont_own = fs.ncont_own, &nobs_cont = fs.nobs_cont,
+                     &ngjk = fs.ngjk, &ngjk_it = fs.ngjk_it;
+  double &ov_max = fs.ov_max, &ov_sum = fs.ov_sum;
 
   int ci, cj, ck;
   cell_of(S, xi.x, xi.y, xi.z, ci, cj, ck);
@@ -758,27 +810,14 @@ __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
   P.T[s] = st3<R>(T);
   a.coord[s] = ncontact;
   a.hist_n_next[oi] = nnext;
-  // statistics: warp reduction then one atomic per warp
-  const unsigned full = 0xffffffffu;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    nobs_cand += __shfl_down_sync(full, nobs_cand, o);
-    ncont_own += __shfl_down_sync(full, ncont_own, o);
-    nobs_cont += __shfl_down_sync(full, nobs_cont, o);
-    ngjk += __shfl_down_sync(full, ngjk, o);
-    ngjk_it += __shfl_down_sync(full, ngjk_it, o);
-    ov_sum += __shfl_down_sync(full, ov_sum, o);
-    ov_max = fmax(ov_max, __shfl_down_sync(full, ov_max, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    if (nobs_cand) atomicAdd(&a.stats->n_obs_cand, nobs_cand);
-    if (ncont_own) atomicAdd(&a.stats->n_contacts, ncont_own);
-    if (nobs_cont) atomicAdd(&a.stats->n_obs_contacts, nobs_cont);
-    if (ngjk) atomicAdd(&a.stats->n_gjk_calls, ngjk);
-    if (ngjk_it) atomicAdd(&a.stats->n_gjk_iters, ngjk_it);
-    if (ov_sum > 0.) atomicAdd(&a.stats->overlap_sum, ov_sum);
-    if (ov_max > 0.) atomic_max_pos_double(&a.stats->overlap_max_bits, ov_max);
-  }
+}
+
+template <typename R, bool DIAG, bool CONVEX>
+__global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  ForceStats fs{0, 0, 0, 0, 0, 0., 0.};
+  if (s < a.n) forces_one<R, DIAG, CONVEX>(a, s, dt, fs);
+  flush_force_stats(a.stats, fs);
 }
 
 template <typename R>
@@ -818,13 +857,13 @@ __global__ void update_dynamic_kernel(StepArgs<R> a, const double* st, const dou
     for (int k = 0; k < 9; ++k) P.basis[9 * (size_t)s + k] = sb[9 * i + k];
 }
 
-#ifdef GG_DEFINE_SHARED_KERNELS
 // moving obstacles: constant rotation about a centre over one step
 // (ObstacleImposedVelocity ConstantRotation, ObstacleImposedVelocity.cpp:
 // 332-370, 389-455; ObstacleKinematicsVelocity::ImposedMotion, :86-122;
 // SimpleObstacle::Move, SimpleObstacle.cpp:119-170), then the world AABB
 // (Convex::bbox, Convex.cpp:29-41 -> BBox::setValue, BBox.cpp:235-239).
-__device__ void obstacle_move_one(ObstacleDev& O, const ShapeDev* shapes, const double* verts, double sub) {
+static __device__ __noinline__ void obstacle_move_one(ObstacleDev& O, const ShapeDev* shapes, const double* verts,
+                                                      double sub) {
   const V3<double> om = v3<double>(O.iomega[0], O.iomega[1], O.iomega[2]);
   const V3<double> cg = v3<double>(O.o[0], O.o[1], O.o[2]);
   M3 b;
@@ -880,6 +919,19 @@ __device__ void obstacle_move_one(ObstacleDev& O, const ShapeDev* shapes, const 
 }
 
 
+// Imposed motion of every moving obstacle over one step, by one block: every
+// thread reads the clock before thread 0 advances it.
+static __device__ __forceinline__ void obstacle_move_block(ObstacleDev* obs, const int* moving_idx, int n_moving,
+                                                           const ShapeDev* shapes, const double* verts, double dt,
+                                                           double* clock, double host_time, int use_host_time) {
+  const double T = use_host_time ? host_time : xadd(*clock, dt);
+  const double sub = xsub(T, xsub(T, dt));
+  __syncthreads();
+  if (threadIdx.x == 0) *clock = T;
+  for (int u = threadIdx.x; u < n_moving; u += blockDim.x) obstacle_move_one(obs[moving_idx[u]], shapes, verts, sub);
+}
+
+#ifdef GG_DEFINE_SHARED_KERNELS
 // Imposed obstacle motion of one step (ObstacleKinematicsVelocity::ImposedMotion,
 // ObstacleKinematicsVelocity.cpp:86-122; ObstacleImposedVelocity.cpp:388-445).
 // The clock is the reference's m_time: T = clock + dt, and the motion acts over
@@ -889,11 +941,7 @@ __device__ void obstacle_move_one(ObstacleDev& O, const ShapeDev* shapes, const 
 __global__ void obstacle_move_kernel(ObstacleDev* obs, const int* moving_idx, int n_moving, const ShapeDev* shapes,
                                      const double* verts, double dt, double* clock, double host_time,
                                      int use_host_time) {
-  const double T = use_host_time ? host_time : xadd(*clock, dt);
-  const double sub = xsub(T, xsub(T, dt));
-  __syncthreads();
-  if (threadIdx.x == 0) *clock = T;
-  for (int u = threadIdx.x; u < n_moving; u += blockDim.x) obstacle_move_one(obs[moving_idx[u]], shapes, verts, sub);
+  obstacle_move_block(obs, moving_idx, n_moving, shapes, verts, dt, clock, host_time, use_host_time);
 }
 
 #endif  // GG_DEFINE_SHARED_KERNELS
@@ -1049,6 +1097,171 @@ int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int in
   return check_launch();
 }
 
+// ---------------------------------------------------------------------------
+// Persistent step: n middle steps of grains_gpu_step in ONE cooperative launch
+// (every block resident), the phases separated by a grid barrier.  The same
+// device bodies as the per-phase kernels run in grid-stride loops, so the
+// results are bit-identical to the launched pipeline.  Measured on B200 it is
+// slower than the graph-replayed launches at every size tried (1,000 spheres:
+// 35.4 vs 30.9 us per step; 200,000: 127 vs 78 us): each phase is a chain of
+// dependent L2 round trips whose latency a barrier does not hide any better
+// than a launch boundary, and for large systems every phase runs at the
+// occupancy of the heaviest (the contact law).  Kept as a tuning choice.
+
+constexpr int kPersistentThreads = 128;
+constexpr long long kBarrierSpinLimit = 1ll << 24;  // x 64 ns sleep: about a second
+
+// Grid barrier with a bounded wait: bar[0] counts arrivals, bar[1] is the
+// generation.  A wait that runs out sets GRAINS_GPU_TIMEOUT and returns false;
+// the kernel then returns, and the others run out at their next barrier.
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status) {
+  __shared__ int ok_s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    int ok = 1;
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      long long it = 0;
+      while (*gen == g) {
+        if (++it > kBarrierSpinLimit || (*((volatile int*)status) & GRAINS_GPU_TIMEOUT)) {
+          ok = 0;
+          atomicOr(status, GRAINS_GPU_TIMEOUT);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    ok_s = ok;
+  }
+  __syncthreads();
+  return ok_s != 0;
+}
+
+template <typename R, bool CONVEX>
+__global__ void __launch_bounds__(kPersistentThreads) persistent_steps_kernel(
+    StepArgs<R> a0, int n_steps, R dt_r, double dt, int gather_every, int since_gather, int n_moving,
+    double* clock, unsigned* bar, int* sums) {
+  StepArgs<R> a = a0;  // the buffer roles change from step to step
+  const int nthreads = gridDim.x * blockDim.x;
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int n = a.n, C = a.n_cells;
+  const int n_pad = (n + nthreads - 1) / nthreads * nthreads;  // uniform trip counts for warp reductions
+  int* status = &a.stats->status;
+  __shared__ int offset_s;
+  for (int step = 0; step < n_steps; ++step) {
+    // exclusive scan of the cell counts: a chunk per block, then the offsets
+    {
+      const int chunk = (C + gridDim.x - 1) / gridDim.x;
+      const int c0 = min(C, (int)blockIdx.x * chunk), c1 = min(C, c0 + chunk);
+      int run = 0;
+      for (int base = c0; base < c1; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < c1 ? a.cell_count[i] : 0;
+        int total;
+        const int pre = block_exclusive_scan(v, &total);
+        if (i < c1) a.cell_start[i] = run + pre;
+        run += total;
+      }
+      if (threadIdx.x == 0) sums[blockIdx.x] = run;
+      if (!grid_barrier(bar, status)) return;
+      if (threadIdx.x == 0) {
+        int o = 0;
+        for (int b = 0; b < (int)blockIdx.x; ++b) o += sums[b];
+        offset_s = o;
+        if (blockIdx.x == gridDim.x - 1) a.cell_start[C] = o + run;
+      }
+      __syncthreads();
+      for (int i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+        const int v = a.cell_start[i] + offset_s;
+        a.cell_start[i] = v;
+        a.cell_cursor[i] = v;
+      }
+      if (!grid_barrier(bar, status)) return;
+    }
+    for (int s = tid; s < n; s += nthreads) scatter_one(a, s);
+    if (!grid_barrier(bar, status)) return;
+    for (int c = tid; c < C; c += nthreads) cell_sort_one(a, c);
+    if (!grid_barrier(bar, status)) return;
+    if (since_gather + 1 >= gather_every) {
+      for (int t = tid; t < n; t += nthreads) gather_one(a, t, 0);
+      const ParticleArrays<R> tmp = a.cur;
+      a.cur = a.alt;
+      a.alt = tmp;
+      since_gather = 0;
+      if (!grid_barrier(bar, status)) return;
+    } else {
+      ++since_gather;
+    }
+    {
+      unsigned long long ncand = 0;
+      for (int s = tid; s < n_pad; s += nthreads)
+        if (s < n) contacts_one(a, s, ncand);
+      warp_add(&a.stats->n_cand, ncand);
+    }
+    if (!grid_barrier(bar, status)) return;
+    {
+      ForceStats fs{0, 0, 0, 0, 0, 0., 0.};
+      for (int s = tid; s < n_pad; s += nthreads)
+        if (s < n) forces_one<R, false, CONVEX>(a, s, dt_r, fs);
+      flush_force_stats(a.stats, fs);
+    }
+    {
+      HistEntry<R>* h = a.hist_prev;
+      a.hist_prev = a.hist_next;
+      a.hist_next = h;
+      int* hn = a.hist_n_prev;
+      a.hist_n_prev = a.hist_n_next;
+      a.hist_n_next = hn;
+    }
+    if (!grid_barrier(bar, status)) return;
+    for (int s = tid; s < n; s += nthreads)
+      integrate(a, a.cur, a.cur, s, ld3<R>(a.cur.F[s]), ld3<R>(a.cur.T[s]), 1, R(0.5) * dt_r, 1, R(0.5) * dt_r, dt);
+    if (blockIdx.x == 0 && n_moving > 0)
+      obstacle_move_block(const_cast<ObstacleDev*>(a.obs), a.moving_idx, n_moving, a.shapes, a.verts, dt, clock, 0.,
+                          0);
+    if (!grid_barrier(bar, status)) return;
+  }
+}
+
+// blocks of the persistent launch: every SM filled to its residency, no more
+// than the work needs
+template <typename R>
+int persistent_blocks(const StepArgs<R>& a) {
+  int dev = 0, sms = 0, per_sm = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+  cudaError_t e = a.has_convex
+                      ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_steps_kernel<R, true>,
+                                                                      kPersistentThreads, 0)
+                      : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, persistent_steps_kernel<R, false>,
+                                                                      kPersistentThreads, 0);
+  if (e != cudaSuccess || per_sm < 1) return 0;
+  const long long need = ((long long)a.n + kPersistentThreads - 1) / kPersistentThreads;
+  return (int)std::max(1ll, std::min((long long)sms * per_sm, need));
+}
+
+template <typename R>
+int launch_persistent_steps(const StepArgs<R>& a, cudaStream_t s, int n_steps, double dt, int gather_every,
+                            int since_gather, int n_moving, double* clock, unsigned* bar, int* sums, int blocks) {
+  if (n_steps <= 0 || a.n == 0) return 0;
+  StepArgs<R> a0 = a;
+  R dt_r = R(dt);
+  void* args[] = {&a0, &n_steps, &dt_r, &dt, &gather_every, &since_gather, &n_moving, &clock, &bar, &sums};
+  cudaError_t e = a.has_convex
+                      ? cudaLaunchCooperativeKernel((const void*)persistent_steps_kernel<R, true>, dim3(blocks),
+                                                    dim3(kPersistentThreads), args, 0, s)
+                      : cudaLaunchCooperativeKernel((const void*)persistent_steps_kernel<R, false>, dim3(blocks),
+                                                    dim3(kPersistentThreads), args, 0, s);
+  return e == cudaSuccess ? 0 : GRAINS_GPU_CUDA_ERROR;
+}
+
 #define GG_INSTANTIATE(R)                                                                                  \
   template int launch_kick_move<R>(const StepArgs<R>&, cudaStream_t, int, double, int, double, double);    \
   template int launch_bin<R>(const StepArgs<R>&, cudaStream_t);                                            \
@@ -1057,6 +1270,9 @@ int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int in
   template int launch_zero_kdelta<R>(const StepArgs<R>&, cudaStream_t);                                    \
   template int launch_update_dynamic<R>(const StepArgs<R>&, cudaStream_t, const double*, const double*);     \
   template int launch_candidate_pairs<R>(const StepArgs<R>&, cudaStream_t, int, int, int*, int,           \
-                                         unsigned long long*);
+                                         unsigned long long*);                                            \
+  template int persistent_blocks<R>(const StepArgs<R>&);                                                   \
+  template int launch_persistent_steps<R>(const StepArgs<R>&, cudaStream_t, int, double, int, int, int, double*, \
+                                          unsigned*, int*, int);
 
 }  // namespace gg
