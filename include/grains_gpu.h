@@ -62,8 +62,11 @@ enum grains_gpu_shape_type {   /* Grains/Geometry/include/Convex.hh ConvexType *
 
 enum grains_gpu_contact_law {
   GRAINS_GPU_HOOKE        = 0, /* params: kn, en, etat, muc, kr            (HookeContactForceModel.cpp:170-199) */
-  GRAINS_GPU_HOOKE_MEMORY = 1  /* params: kn, en, etat, muc, kt, mur, etarpf, epst
+  GRAINS_GPU_HOOKE_MEMORY = 1, /* params: kn, en, etat, muc, kt, mur, etarpf, epst
                                                                      (HookeMemoryContactForceModel.cpp:11-29) */
+  GRAINS_GPU_HERTZ        = 2, /* params: Es, en, muc, kr, Gs            (HertzContactForceModel.cpp:12-21, 236-276) */
+  GRAINS_GPU_HERTZ_MEMORY = 3  /* params: Es, en, muc, Gs, mur, etarpf, epst
+                                                               (HertzMemoryContactForceModel.cpp:12-32, 261-309) */
 };
 
 /* ---- configuration ------------------------------------------------------ */

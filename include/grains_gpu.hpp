@@ -5,7 +5,8 @@
 //   Convex (Geometry/include/Convex.hh:88-123)      -> grains_gpu::Convex, Sphere, Box, Cylinder, Polyhedron
 //   ContactForceModel (Component/include/ContactForceModel.hh:43-68)
 //                                                    -> grains_gpu::ContactForceModel, HookeContactForceModel,
-//                                                       HookeMemoryContactForceModel
+//                                                       HookeMemoryContactForceModel, HertzContactForceModel,
+//                                                       HertzMemoryContactForceModel
 //   App / AppCollision (Base/include/App.hh:38-39, AppCollision.hh:79-100)
 //                                                    -> grains_gpu::App, AppCollision, LinkedCellGPU
 //   TimeIntegrator::Move / advanceVelocity (TimeIntegration/include/TimeIntegrator.hh:47-66)
@@ -181,6 +182,34 @@ class HookeMemoryContactForceModel : public ContactForceModel {
 
  private:
   double p_[8];
+};
+
+// HertzContactForceModel (HertzContactForceModel.cpp:12-21, 236-276); Gs
+// defaults to Es / 4 as when the XML omits it
+class HertzContactForceModel : public ContactForceModel {
+ public:
+  HertzContactForceModel(double Es, double en, double muc, double kr, double Gs = -1.)
+      : p_{Es, en, muc, kr, Gs < 0. ? Es / 4. : Gs} {}
+  std::string name() const override { return "HertzContactForceModel"; }
+  int law() const override { return GRAINS_GPU_HERTZ; }
+  std::vector<double> parameters() const override { return std::vector<double>(p_, p_ + 5); }
+
+ private:
+  double p_[5];
+};
+
+// HertzMemoryContactForceModel (HertzMemoryContactForceModel.cpp:12-32, 261-309)
+class HertzMemoryContactForceModel : public ContactForceModel {
+ public:
+  HertzMemoryContactForceModel(double Es, double en, double muc, double Gs = -1., double mur = 0.,
+                               double etarpf = 0., double epst = 0.)
+      : p_{Es, en, muc, Gs < 0. ? Es / 4. : Gs, mur, etarpf, epst} {}
+  std::string name() const override { return "HertzMemoryContactForceModel"; }
+  int law() const override { return GRAINS_GPU_HERTZ_MEMORY; }
+  std::vector<double> parameters() const override { return std::vector<double>(p_, p_ + 7); }
+
+ private:
+  double p_[7];
 };
 
 // ---- the host image of the particles (AllComponents' active particles) -------

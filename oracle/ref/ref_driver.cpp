@@ -318,6 +318,14 @@ int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
         << num(q[6]) << "</etarpf>";
       if (q[7] != 0.) x << "<epst>" << num(q[7]) << "</epst>";
       x << "</HookeMemory>";
+    } else if (kv.second.first == GRAINS_GPU_HERTZ) {
+      x << "<Hertz><Es>" << num(q[0]) << "</Es><en>" << num(q[1]) << "</en><muc>" << num(q[2]) << "</muc><kr>"
+        << num(q[3]) << "</kr><Gs>" << num(q[4]) << "</Gs></Hertz>";
+    } else if (kv.second.first == GRAINS_GPU_HERTZ_MEMORY) {
+      x << "<HertzMemory><Es>" << num(q[0]) << "</Es><en>" << num(q[1]) << "</en><muc>" << num(q[2]) << "</muc><Gs>"
+        << num(q[3]) << "</Gs><mur>" << num(q[4]) << "</mur><etarpf>" << num(q[5]) << "</etarpf>";
+      if (q[6] != 0.) x << "<epst>" << num(q[6]) << "</epst>";
+      x << "</HertzMemory>";
     } else {
       x << "<Hooke><kn>" << num(q[0]) << "</kn><en>" << num(q[1]) << "</en><etat>" << num(q[2]) << "</etat><muc>"
         << num(q[3]) << "</muc><kr>" << num(q[4]) << "</kr></Hooke>";

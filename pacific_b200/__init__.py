@@ -7,7 +7,7 @@ missing or no CUDA device is usable.
 """
 import os
 
-from .abi import (BOX, CYLINDER, FP64, HOOKE, HOOKE_MEMORY, MIXED, POLYHEDRON, SPHERE, ContactError,  # noqa: F401
+from .abi import (BOX, CYLINDER, FP64, HERTZ, HERTZ_MEMORY, HOOKE, HOOKE_MEMORY, MIXED, POLYHEDRON, SPHERE, ContactError,  # noqa: F401
                   GrainsError, GrainsLib, MotionError, Simulation, SimulationError)
 
 __version__ = "0.1.0"

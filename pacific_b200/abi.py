@@ -29,7 +29,7 @@ FP64 = 0
 MIXED = 1
 
 SPHERE, BOX, CYLINDER, POLYHEDRON = 0, 1, 2, 3
-HOOKE, HOOKE_MEMORY = 0, 1
+HOOKE, HOOKE_MEMORY, HERTZ, HERTZ_MEMORY = 0, 1, 2, 3
 
 
 class GrainsError(RuntimeError):

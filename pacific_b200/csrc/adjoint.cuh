@@ -929,6 +929,10 @@ class AdjEngineT : public AdjointEngine {
       err = "the differentiable run supports spheres with static box walls only";
       return GRAINS_GPU_INVALID_ARGUMENT;
     }
+    if (!v.hooke_laws_only) {
+      err = "the differentiable run supports the Hooke and HookeMemory laws only";
+      return GRAINS_GPU_INVALID_ARGUMENT;
+    }
     if (K < 0 || !(dt > 0.)) {
       err = "n_steps must be >= 0 and dt > 0";
       return GRAINS_GPU_INVALID_ARGUMENT;

@@ -26,6 +26,7 @@ struct ContextView {
   int hist_cap;
   int spheres_only;     // every particle is a sphere
   int box_walls_only;   // every obstacle is a box
+  int hooke_laws_only;  // every contact law is Hooke or HookeMemory
   int n_moving;
   const SysDev* sys;
   const ShapeDev* shapes;

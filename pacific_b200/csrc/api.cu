@@ -36,7 +36,7 @@ struct ShapeHost {
 
 struct LawHost {
   int type = -1;
-  double p[10] = {0};  // kn, en, etat, muc, kt, mur, etarpf, epst, kr
+  double p[11] = {0};  // kn, en, etat, muc, kt, mur, etarpf, epst, kr, Es, Gs
   double beta = 0;
 };
 
@@ -800,9 +800,29 @@ int grains_gpu_set_contact_law(grains_gpu_ctx* c, int32_t system, int32_t a, int
     L.p[2] = p[2];
     L.p[3] = p[3];
     L.p[8] = p[4];
+  } else if (law == GRAINS_GPU_HERTZ) {
+    // HertzContactForceModel::defineParameters (HertzContactForceModel.cpp:236-276)
+    if (n < 5) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "Hertz needs Es, en, muc, kr, Gs");
+    L.p[9] = p[0];
+    L.p[1] = p[1];
+    L.p[3] = p[2];
+    L.p[8] = p[3];
+    L.p[10] = p[4];
+  } else if (law == GRAINS_GPU_HERTZ_MEMORY) {
+    // HertzMemoryContactForceModel::defineParameters (HertzMemoryContactForceModel.cpp:261-309)
+    if (n < 7) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "HertzMemory needs Es, en, muc, Gs, mur, etarpf, epst");
+    L.p[9] = p[0];
+    L.p[1] = p[1];
+    L.p[3] = p[2];
+    L.p[10] = p[3];
+    L.p[5] = p[4];
+    L.p[6] = p[5];
+    L.p[7] = p[6];
   } else {
     return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "unknown contact law");
   }
+  if ((law == GRAINS_GPU_HERTZ || law == GRAINS_GPU_HERTZ_MEMORY) && !(L.p[9] > 0 && L.p[10] > 0))
+    return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "Hertz laws need Es > 0 and Gs > 0");
   if (!(L.p[1] > 0 && L.p[1] <= 1)) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "restitution must be in (0, 1]");
   // m_beta, HookeMemoryContactForceModel.cpp:28 / HookeContactForceModel.cpp:17
   L.beta = std::log(L.p[1]) / std::sqrt(kPi * kPi + std::log(L.p[1]) * std::log(L.p[1]));
@@ -905,8 +925,10 @@ int build_tables(grains_gpu_ctx* c) {
         P.etarpf = L.p[6];
         P.epst = L.p[7];
         P.kr = L.p[8];
+        P.Es = L.p[9];
+        P.Gs = L.p[10];
         P.beta = L.beta;
-        P.rolling = (L.type == GRAINS_GPU_HOOKE_MEMORY && P.mur != 0.) ? 1 : 0;
+        P.rolling = (law_has_memory(L.type) && P.mur != 0.) ? 1 : 0;
         ld[k] = P;
         LawParams<float> Q{};
         Q.type = P.type;
@@ -914,6 +936,7 @@ int build_tables(grains_gpu_ctx* c) {
         Q.kn = (float)P.kn; Q.en = (float)P.en; Q.etat = (float)P.etat; Q.muc = (float)P.muc;
         Q.kt = (float)P.kt; Q.mur = (float)P.mur; Q.etarpf = (float)P.etarpf; Q.epst = (float)P.epst;
         Q.kr = (float)P.kr; Q.beta = (float)P.beta;
+        Q.Es = (float)P.Es; Q.Gs = (float)P.Gs;
         lf[k] = Q;
       }
   // shapes
@@ -1946,9 +1969,13 @@ int context_view(grains_gpu_ctx* c, ContextView* v, std::string& err) {
   v->hist_cap = c->hist_cap;
   v->spheres_only = c->has_basis ? 0 : 1;
   v->box_walls_only = 1;
-  for (const auto& s : c->sys)
+  v->hooke_laws_only = 1;
+  for (const auto& s : c->sys) {
     for (const auto& o : s.obs)
       if (c->shapes[o.shape].type != GRAINS_GPU_BOX) v->box_walls_only = 0;
+    for (const auto& kv : s.laws)
+      if (kv.second.type != GRAINS_GPU_HOOKE && kv.second.type != GRAINS_GPU_HOOKE_MEMORY) v->hooke_laws_only = 0;
+  }
   v->n_moving = c->n_moving;
   v->sys = c->d_sys;
   v->shapes = c->d_shapes;

@@ -389,9 +389,7 @@ template <typename R>
 __device__ __forceinline__ LawResult<R> pair_law(const StepArgs<R>& a, const LawParams<R>& L, R dt,
                                                  const ContactGeom& g, const BodyAtContact<R>& b0,
                                                  const BodyAtContact<R>& b1, bool existed, PairMemory<R>& mem) {
-  V3<R> pen = from_d3<R>(g.overlap_vector);
-  if (L.type == GRAINS_GPU_HOOKE_MEMORY) return hooke_memory(L, dt, pen, b0, b1, existed, mem);
-  return hooke(L, pen, b0, b1);
+  return apply_contact_law(L, dt, from_d3<R>(g.overlap_vector), R(-g.overlap), b0, b1, existed, mem);
 }
 
 // Contact with a pair error: RigidBodyWithCrust::ClosestPoint_ErreurHandling
@@ -690,14 +688,14 @@ __device__ __forceinline__ void forces_one(const StepArgs<R>& a, int s, R dt, Fo
         const int row0 = own ? oi : P.orig[t];
         const int other = own ? idj : mi.x;
         bool existed = false;
-        if (L.type == GRAINS_GPU_HOOKE_MEMORY) existed = find_memory(a, row0, other, 0, mem);
+        if (law_has_memory(L.type)) existed = find_memory(a, row0, other, 0, mem);
         LawResult<R> res = pair_law(a, L, dt, g, b0, b1, existed, mem);
-        if (own && L.type == GRAINS_GPU_HOOKE_MEMORY) store_memory(a, oi, nnext, other, 0, mem);
+        if (own && law_has_memory(L.type)) store_memory(a, oi, nnext, other, 0, mem);
         // Torsor::addForce (Torsor.cpp:184-189); p1 gets -delFN - delFT
         const V3<R> f = own ? res.force : -res.force;
         F = F + f;
         T = T + cross(own ? b0.lever : b1.lever, f);
-        if (L.rolling || L.kr != R(0)) T = T + (own ? res.torque : -res.torque);
+        if (law_has_torque(L)) T = T + (own ? res.torque : -res.torque);
         ++ncontact;
         if (own) {
           ++ncont_own;
@@ -792,12 +790,12 @@ __device__ __forceinline__ void forces_one(const StepArgs<R>& a, int s, R dt, Fo
       PairMemory<R> mem;
       const int oloc = oidx - S.obs_offset;
       bool existed = false;
-      if (L.type == GRAINS_GPU_HOOKE_MEMORY) existed = find_memory(a, oi, oloc, 1, mem);
+      if (law_has_memory(L.type)) existed = find_memory(a, oi, oloc, 1, mem);
       LawResult<R> res = pair_law(a, L, dt, g, b0, b1, existed, mem);
-      if (L.type == GRAINS_GPU_HOOKE_MEMORY) store_memory(a, oi, nnext, oloc, 1, mem);
+      if (law_has_memory(L.type)) store_memory(a, oi, nnext, oloc, 1, mem);
       F = F + res.force;
       T = T + cross(b0.lever, res.force);
-      if (L.rolling || L.kr != R(0)) T = T + res.torque;
+      if (law_has_torque(L)) T = T + res.torque;
       ++ncontact;
       ++nobs_cont;
       const double o = fabs(g.overlap);

@@ -14,7 +14,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .abi import BOX, CYLINDER, HOOKE_MEMORY, POLYHEDRON, SPHERE
+from .abi import BOX, CYLINDER, HERTZ, HERTZ_MEMORY, HOOKE_MEMORY, POLYHEDRON, SPHERE  # noqa: F401
 
 MM = 1.0e-3
 PI = 3.14159265358979323846

@@ -37,6 +37,8 @@ CASES = {
     "convex216": ("S.convex_box(216, seed=0, converge_time=0.004, velocity_sigma=0.05)", 900, 5),
     "drum300": ("converge(S.drum(n=300, radius=25e-3, length=30e-3, n_boxes=32), (0.0, -25e-3, 15e-3), 0.006)",
                 1500, 3),
+    "hertz_dense125": ("hertz(S.dense_cluster(125, seed=5, velocity_sigma=0.1), memory=False)", 10, 30),
+    "hertz_memory216_rolling": ("hertz(S.dense_cluster(216, seed=6, velocity_sigma=0.1), memory=True)", 10, 30),
 }
 
 
@@ -61,6 +63,20 @@ def rolling(sc):
 def hooke(sc):
     from pacific_b200.abi import HOOKE
     sc.laws = [[(a, b, HOOKE, [prm[0], prm[1], prm[2], prm[3], 1.0e-3]) for a, b, law, prm in sc.laws[0]]]
+    return sc
+
+
+def hertz(sc, memory):
+    """Hertz (Es = 1 GPa, Gs = 0.3 GPa, en = 0.8, muc = 0.4, kr = 1e-3) or
+    HertzMemory (same moduli, mur = 0.05, etarpf = 0.3) on every pair;
+    dt = 2e-6 s, a twentieth of the Hertz contact time at 0.1 m/s."""
+    from pacific_b200.abi import HERTZ, HERTZ_MEMORY
+    Es, Gs = 1.0e9, 0.3e9
+    if memory:
+        sc.laws = [[(a, b, HERTZ_MEMORY, [Es, 0.8, 0.4, Gs, 0.05, 0.3, 0.0]) for a, b, law, prm in sc.laws[0]]]
+    else:
+        sc.laws = [[(a, b, HERTZ, [Es, 0.8, 0.4, 1.0e-3, Gs]) for a, b, law, prm in sc.laws[0]]]
+    sc.dt = 2.0e-6
     return sc
 
 
@@ -115,8 +131,8 @@ def replay_case(name):
     out["torque"] = d["torque"]
     out["coordination"] = d["coordination"]
     # contact pairs are read from the reference's contact-memory maps, which
-    # only the HookeMemory law fills
-    out["has_contact_pairs"] = np.array(all(l[2] == 1 for l in sc.laws[0]))
+    # only the memory laws (HookeMemory, HertzMemory) fill
+    out["has_contact_pairs"] = np.array(all(l[2] in (1, 3) for l in sc.laws[0]))
     out["contact_pairs"] = sim.contact_pairs()
     out["candidate_pairs"] = sim.candidate_pairs()
     out.update(G.memory_arrays(sim.contact_memory(), "mem_out_"))

@@ -31,6 +31,29 @@ def test_header_declares_entry_points():
         assert n in names
 
 
+def test_header_enums_match_the_python_binding():
+    """Contact-law and shape codes of the header are the ones abi.py passes."""
+    from pacific_b200 import abi
+    txt = open(HEADER).read()
+    for name in ["HOOKE", "HOOKE_MEMORY", "HERTZ", "HERTZ_MEMORY", "SPHERE", "BOX", "CYLINDER", "POLYHEDRON"]:
+        m = re.search(r"\bGRAINS_GPU_%s\s*=\s*(\d+)" % name, txt)
+        assert m and int(m.group(1)) == getattr(abi, name), name
+
+
+def test_oracle_checks_hertz_parameters(oracle_lib):
+    from pacific_b200.abi import GrainsError, HERTZ, HERTZ_MEMORY, FP64, Simulation
+    sc = S.dense_cluster(8, seed=0)
+    sim = Simulation(oracle_lib, FP64, max_particles=8)
+    S.apply(sim, sc)
+    sim.set_contact_law(0, 0, 0, HERTZ, [1e9, 0.8, 0.4, 1e-3, 0.3e9])
+    sim.set_contact_law(0, 0, 0, HERTZ_MEMORY, [1e9, 0.8, 0.4, 0.3e9, 0.05, 0.3, 0.0])
+    with pytest.raises(GrainsError):
+        sim.set_contact_law(0, 0, 0, HERTZ, [1e9, 0.8, 0.4, 1e-3])
+    with pytest.raises(GrainsError):
+        sim.set_contact_law(0, 0, 0, HERTZ_MEMORY, [1e9, 0.8, 0.4, 0.3e9, 0.05, 0.3])
+    sim.close()
+
+
 def test_cuda_library_exports_every_declared_symbol():
     import ctypes
     import pacific_b200

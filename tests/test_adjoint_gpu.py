@@ -186,12 +186,19 @@ def test_adjoint_is_deterministic(gpu_lib):
 
 
 def test_adjoint_rejects_unsupported_scenes(gpu_lib):
-    """Non-spherical particles are outside the differentiable run's scope: the
-    call fails with a message instead of returning wrong gradients."""
+    """Non-spherical particles and the Hertz laws are outside the
+    differentiable run's scope: the call fails with a message instead of
+    returning wrong gradients."""
     sc = S.convex_box(27, seed=1)
     sim = make(gpu_lib, sc, MIXED)
-    with pytest.raises(Exception):
+    with pytest.raises(Exception, match="spheres"):
         Adjoint(sim, 10).forward(5, sc.dt)
+    sim.close()
+    sc = S.dense_cluster(27, seed=1)
+    sc.laws = [[(a, b, S.HERTZ_MEMORY, [1.0e9, 0.8, 0.4, 0.3e9, 0.0, 0.0, 0.0]) for a, b, _, _ in sc.laws[0]]]
+    sim = make(gpu_lib, sc, MIXED)
+    with pytest.raises(Exception, match="Hooke"):
+        Adjoint(sim, 10).forward(5, 2.0e-6)
     sim.close()
 
 

@@ -60,12 +60,17 @@ def test_oracle_matches_reference_fixture(oracle_lib, path):
 
 def test_fixtures_exercise_the_path():
     """The fixture set covers particle-particle and wall contacts, memory,
-    rolling friction, the memory-less Hooke law, polydispersity, boxes,
-cylinders and polyhedra through the GJK narrowphase, and a rotating drum."""
+    rolling friction, the memory-less Hooke law, the Hertz and HertzMemory
+    laws, polydispersity, boxes, cylinders and polyhedra through the GJK
+    narrowphase, and a rotating drum."""
     names = [os.path.basename(c)[:-4] for c in CASES]
     for n in ["dense125", "dense216_rolling", "poly_box200", "hooke_dense125", "settling_1k", "convex216",
-              "drum300"]:
+              "drum300", "hertz_dense125", "hertz_memory216_rolling"]:
         assert n in names
+    for n, law in [("hertz_dense125", 2), ("hertz_memory216_rolling", 3)]:
+        z = np.load(os.path.join(HERE, "golden", n + ".npz"))
+        assert {l[2] for l in json.loads(str(z["spec"]))["laws"][0]} == {law}
+        assert int(z["coordination"].sum()) > 400 and np.abs(z["torque"]).max() > 0
     z = np.load(os.path.join(HERE, "golden", "dense125.npz"))
     assert len(z["contact_pairs"]) > 100 and len(z["mem_in_owner"]) > 100
     z = np.load(os.path.join(HERE, "golden", "convex216.npz"))
