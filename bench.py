@@ -70,6 +70,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--adjoint", action="store_true", help="time the adjoint workload (4,096 spheres)")
+    ap.add_argument("--no-io", action="store_true", help="skip the reload / RawData file writers")
     return ap.parse_args()
 
 
@@ -179,7 +180,7 @@ def cpu_context(sc):
     return sim, kind, sc
 
 
-def cpu_baseline(sc, steps):
+def cpu_baseline(sc, steps, keep=False):
     """Times `steps` DEM steps of the CPU implementation (serial, one core)
     from the initial state of the same workload."""
     sim, kind, sc = cpu_context(sc)
@@ -189,7 +190,60 @@ def cpu_baseline(sc, steps):
     sample = "%s, %d DEM steps after the leapfrog start, serial" % (sc.name, steps)
     if "radius_classes" in sc.meta:
         sample += ", sphere radii rounded to 64 classes (one reference particle class each)"
-    return {"value": sc.n * steps / el, "unit": "particle-steps/s", "cores": 1, "kind": kind, "sample": sample}
+    res = {"value": sc.n * steps / el, "unit": "particle-steps/s", "cores": 1, "kind": kind, "sample": sample}
+    if keep:
+        return res, sim
+    sim.close()
+    return res
+
+
+def io_measure(lib, sim, t, cpu=None, reps=3):
+    """Output files of the reference's formats from the device state (the end
+    of the timed run): the particle file of a reload (text and hybrid binary),
+    read back, and one RawData output (text and binary); host wall time per
+    call, files in a temporary directory.  `cpu`: (context, kind) of the CPU
+    implementation, whose writers are timed once on its own state."""
+    import tempfile
+    from pacific_b200.abi import read_reload_particles
+    out = {}
+
+    def timed(fn, n_reps):
+        ts, nb = [], 0
+        for _ in range(n_reps):
+            t0 = time.perf_counter()
+            nb = fn()
+            ts.append(time.perf_counter() - t0)
+        return float(np.median(ts)), int(nb)
+
+    def entry(s, nb, n):
+        return {"ms": s * 1e3, "bytes": nb, "GB_per_s": nb / s / 1e9, "particles_per_s": n / s}
+
+    with tempfile.TemporaryDirectory(prefix="gg_bench_io") as d:
+        for binary in (False, True):
+            key = "hybrid" if binary else "text"
+            path = os.path.join(d, "save_" + key)
+            s, nb = timed(lambda: sim.write_reload_particles(path, binary), reps)
+            out["reload_write_" + key] = entry(s, nb, sim.n)
+            s, nb = timed(lambda: (read_reload_particles(lib, path, binary), os.path.getsize(path))[1], reps)
+            out["reload_read_" + key] = entry(s, nb, sim.n)
+            rkey = "binary" if binary else "text"
+            root = os.path.join(d, "raw_" + rkey)
+            s, nb = timed(lambda: sim.write_rawdata(root, t, binary=binary, truncate=True), reps)
+            out["rawdata_write_" + rkey] = entry(s, nb, sim.n)
+        if cpu is not None:
+            csim, kind = cpu
+            base = {}
+            for name, fn in [("reload_write_text", lambda: csim.write_reload_particles(os.path.join(d, "c.txt"))),
+                             ("rawdata_write_text", lambda: csim.write_rawdata(os.path.join(d, "craw"), t,
+                                                                               truncate=True))]:
+                s, nb = timed(fn, 1)
+                base[name] = entry(s, nb if nb else sum(os.path.getsize(os.path.join(d, f)) for f in os.listdir(d)
+                                                        if f.startswith("craw")), csim.n)
+            base["kind"] = kind
+            base["cores"] = 1
+            base["sample"] = "the CPU implementation's writers, serial, on its own state of the same workload"
+            out["cpu_baseline"] = base
+    return out
 
 
 def run_reference(args, rank, world):
@@ -468,8 +522,14 @@ def main():
             line["contact_force_error"] = contact_force_error(lib, sc, st_end, mem_end, local)
         else:  # contact-memory ids are per system; the comparison is run on single systems
             line["contact_force_error"] = None
+    cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(scenario(args.workload), args.cpu_steps)
+        line["cpu_baseline"], cpu_sim = cpu_baseline(scenario(args.workload), args.cpu_steps, keep=True)
+        cpu = (cpu_sim, line["cpu_baseline"]["kind"])
+    if rank == 0 and not args.no_io:
+        line["io"] = io_measure(lib, sim, t, cpu)
+    if cpu is not None:
+        cpu[0].close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     sim.close()

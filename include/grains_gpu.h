@@ -113,6 +113,34 @@ typedef struct grains_gpu_obstacle {
   double  rotation_center[3];
 } grains_gpu_obstacle;
 
+/* Imposed obstacle motions (ObstacleImposedVelocity, Component/src/
+ * ObstacleImposedVelocity.cpp:60-262 for the XML, 306-455 for the motion):
+ * each is active on [t_start, t_end]; over a step ending at time T the active
+ * part of [T - dt, T] is integrated analytically, the velocities are those at
+ * T, and the motions of all loadings of an obstacle add up
+ * (ObstacleKinematicsVelocity::ImposedMotion, ObstacleKinematicsVelocity.cpp:
+ * 86-122), in the order of their start times. */
+enum grains_gpu_motion {
+  GRAINS_GPU_CONSTANT_TRANSLATION = 0,  /* vector = velocity */
+  GRAINS_GPU_SIN_TRANSLATION      = 1,  /* vector = direction; amplitude[0] (velocity), period[0], phase_deg[0] */
+  GRAINS_GPU_CRENEL_TRANSLATION   = 2,  /* vector = direction; amplitude[0] (velocity), period[0] (half cycle) */
+  GRAINS_GPU_CONSTANT_ROTATION    = 3,  /* vector = angular velocity; about center when has_center, else
+                                           about the obstacle's own centre */
+  GRAINS_GPU_MULTISIN_TRANSLATION = 4   /* vector = direction; per axis amplitude, period, phase_deg */
+};
+typedef struct grains_gpu_obstacle_loading {
+  int32_t obstacle_id;
+  int32_t type;          /* grains_gpu_motion */
+  double  t_start, t_end;
+  double  vector[3];
+  double  center[3];
+  int32_t has_center;
+  int32_t reserved;
+  double  amplitude[3];
+  double  period[3];
+  double  phase_deg[3];
+} grains_gpu_obstacle_loading;
+
 /* Particle state, structure of arrays, n entries each.  Static fields are
  * read by upload only; dynamic fields are read by upload and written by
  * download.  'basis' may be NULL on upload (then basis = R(q)). */
@@ -192,6 +220,13 @@ int grains_gpu_set_contact_law(grains_gpu_ctx* ctx, int32_t system, int32_t mat_
  * (LinkedCell.cpp:1371-1445) */
 int grains_gpu_set_obstacles(grains_gpu_ctx* ctx, int32_t system, int32_t n,
                              const grains_gpu_obstacle* obstacles);
+/* replaces: ObstacleImposedVelocity loadings of Grains::Construction
+ * (<ObstacleLoadings>, ObstacleImposedVelocity.cpp:60-262).  Sets every loading
+ * of the system's obstacles (after grains_gpu_set_obstacles); an obstacle with
+ * loadings moves by them, one without by its 'moving' / velocity / omega
+ * fields (as a single loading from 0 on). */
+int grains_gpu_set_obstacle_loadings(grains_gpu_ctx* ctx, int32_t system, int32_t n,
+                                     const grains_gpu_obstacle_loading* loadings);
 /* replaces: LinkedCell::Link(Particle*) for all active particles
  * (LinkedCell.cpp:1330-1365) + AllComponents state upload */
 int grains_gpu_upload_particles(grains_gpu_ctx* ctx, const grains_gpu_particles* p);
@@ -390,6 +425,81 @@ int grains_gpu_adjoint_contact_signature(const grains_gpu_adjoint* adj, uint64_t
 int grains_gpu_adjoint_backward(grains_gpu_adjoint* adj, const double* dl_dposition, const double* dl_dvelocity,
                                 const double* dl_domega, double* grad_position, double* grad_velocity,
                                 double* grad_omega, double* grad_laws, int32_t n_grad_laws);
+
+/* ---- reload and RawData files --------------------------------------------- */
+/* Attributes that the reference's reload files carry per particle and the step
+ * does not use (Particle::write2014, Particle.cpp:1146-1157), in upload order:
+ * m_GeomType (index of the particle's reference type), tag (0 interior,
+ * 1 buffer zone, 2 periodic clone), activity (1 = COMPUTE) and the transform
+ * type bits of Transform.hh:246-260.  Any array may be NULL (kept).  An upload
+ * sets the shape id, 0, 1 and TRANSLATION (1); a move adds ROTATION and
+ * TRANSLATION, as Transform::composeLeftByRotation / setOrigin do. */
+int grains_gpu_set_record_attributes(grains_gpu_ctx* ctx, int64_t n, const int32_t* geom_type, const int32_t* tag,
+                                     const int32_t* active, const int32_t* transform_type);
+
+/* The particle file of a __Format2024__ reload (AllComponents::write,
+ * AllComponents.cpp:1148-1180; Grains::saveReload, Base/src/Grains.cpp:2541-2580
+ * writes the header file that names it): binary = 0 writes "Text" mode, one
+ * Particle::write2014 line per particle (Particle.cpp:1146-1157); binary = 1
+ * writes "Hybrid" mode, per particle its byte count (size_t) then
+ * Particle::write2014_binary (Particle.cpp:1183-1195).  Particles in upload
+ * order; each carries its contact map (Component::writeContactMemory2014,
+ * Component.cpp:776-835) with both sides of every pair, as the reference keeps
+ * them (Component.cpp:675-684), sorted by neighbour id.  Numbers are formatted
+ * on the device exactly as GrainsExec::doubleToString(ios::scientific, 16, x)
+ * prints them (Base/src/GrainsExec.cpp:213-225).  *bytes = file size. */
+int grains_gpu_write_reload_particles(grains_gpu_ctx* ctx, const char* path, int32_t binary, int64_t* bytes);
+
+/* One output time of RawDataPostProcessingWriter::one_output_Standard
+ * (PostProcessing/src/RawDataPostProcessingWriter.cpp:369-600) for one system:
+ * appends (truncate = 0) or starts (truncate = 1, the reference's "new" run)
+ * <root>_position_{x,y,z}.dat, _translational_velocity_{x,y,z}.dat,
+ * _angular_velocity_{x,y,z}.dat, _coordinationNumber.dat, and rewrites
+ * <root>_particleType.dat.  Columns are particle ids 1..n_total; absent ids
+ * and periodic clones get the reference's inactive values.  Text (6 digits)
+ * or binary (WritingMode="Binary"). *bytes = bytes written. */
+int grains_gpu_write_rawdata(grains_gpu_ctx* ctx, const char* root, double time, int32_t system, int32_t n_total,
+                             int32_t binary, int32_t truncate, int64_t* bytes);
+
+/* A particle file read back (Particle::read2014 / read2014_binary,
+ * Particle.cpp:972-1072; AllComponents::read_particles).  The parse is done
+ * at grains_gpu_reload_open; grains_gpu_reload_get reports the counts and copies
+ * the arrays that are not NULL (capacity n_particles / n_memory entries).
+ * Quaternions are xyzw.  Memory entries: every contact-map entry with its
+ * holder's id as owner (both sides of each pair, as in the file);
+ * grains_gpu_upload_contact_memory keeps the side it needs. */
+typedef struct grains_gpu_reload grains_gpu_reload;
+typedef struct grains_gpu_reload_data {
+  int64_t  n_particles;
+  int64_t  n_memory;
+  int32_t* geom_type;
+  int32_t* id;
+  int32_t* tag;
+  int32_t* active;
+  int32_t* transform_type;
+  double*  position;      /* 3n */
+  double*  basis;         /* 9n, row-major */
+  double*  velocity;      /* 3n */
+  double*  quaternion;    /* 4n */
+  double*  omega;         /* 3n */
+  double*  force;         /* 3n */
+  double*  torque;        /* 3n */
+  grains_gpu_contact_memory memory;
+} grains_gpu_reload_data;
+int grains_gpu_reload_open(const char* path, int32_t binary, grains_gpu_reload** out);  /* *out set even on failure */
+int grains_gpu_reload_last_error(const grains_gpu_reload* r, char* buf, size_t len);
+int grains_gpu_reload_get(const grains_gpu_reload* r, grains_gpu_reload_data* out);
+int grains_gpu_reload_close(grains_gpu_reload* r);
+
+/* GrainsExec::doubleToString(ios::scientific, digits, x) (Base/src/GrainsExec.cpp:
+ * 213-225) on the host, with the device writers' formatter: writes the text
+ * and a NUL into out; *length = its length.  0 <= digits <= 16. */
+int grains_gpu_format_double(double x, int32_t digits, char* out, size_t cap, int32_t* length);
+
+/* The same formatter on the device: the n values, each followed by '\n',
+ * formatted on the current device; *length = bytes written to out (host). */
+int grains_gpu_format_doubles(const double* x, int64_t n, int32_t digits, char* out, int64_t cap,
+                              int64_t* length);
 
 /* ---- shape helpers (reference geometry formulas, host only) -------------- */
 /* volume, circumscribed radius and body-frame principal inertia per unit

@@ -358,6 +358,21 @@ class LinkedCellGPU : public AppCollision {
     v.basis = p->basis.data();
     check(grains_gpu_download_particles(ctx_.get(), &v), ctx_.get());
   }
+  // the particle file of Grains::saveReload (AllComponents::write, text or hybrid)
+  int64_t saveReloadParticles(const std::string& path, bool hybrid = false) {
+    int64_t bytes = 0;
+    check(grains_gpu_write_reload_particles(ctx_.get(), path.c_str(), hybrid ? 1 : 0, &bytes), ctx_.get());
+    return bytes;
+  }
+  // RawDataPostProcessingWriter::PostProcessing_start (start = true) / PostProcessing
+  int64_t writeRawData(const std::string& root, double time, int n_total, bool binary, bool start,
+                       int system = 0) {
+    int64_t bytes = 0;
+    check(grains_gpu_write_rawdata(ctx_.get(), root.c_str(), time, system, n_total, binary ? 1 : 0, start ? 1 : 0,
+                                   &bytes),
+          ctx_.get());
+    return bytes;
+  }
 
  private:
   struct Del {

@@ -44,6 +44,7 @@
 #include "Quaternion.hh"
 #include "ReaderXML.hh"
 #include "RigidBodyWithCrust.hh"
+#include "RawDataPostProcessingWriter.hh"
 #include "SimpleObstacle.hh"
 #include "Transform.hh"
 
@@ -78,6 +79,7 @@ class OracleGrains : public Grains {
   }
   double& time() { return m_time; }
   double& dt() { return m_dt; }
+  AllInsertionWindows const& windows() const { return m_insertion_windows; }
 };
 
 struct ShapeSpec {
@@ -100,6 +102,7 @@ struct grains_gpu_ctx {
   bool has_dom = false;
   std::map<std::pair<int, int>, std::pair<int, std::vector<double>>> laws;
   std::vector<grains_gpu_obstacle> obs;
+  std::vector<grains_gpu_obstacle_loading> loads;  // explicit imposed motions
   OracleGrains* g = nullptr;
   std::string dir;
   std::string err;
@@ -249,6 +252,13 @@ int grains_ref_set_obstacles(grains_gpu_ctx* c, int32_t system, int32_t n, const
   return 0;
 }
 
+int grains_ref_set_obstacle_loadings(grains_gpu_ctx* c, int32_t system, int32_t n,
+                                     const grains_gpu_obstacle_loading* l) {
+  (void)system;
+  c->loads.assign(l, l + n);
+  return 0;
+}
+
 int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p) {
   if (!c->has_dom) return fail(c, GRAINS_GPU_NOT_READY, "no domain");
   if (c->g) return fail(c, GRAINS_GPU_NOT_READY, "one upload per context");
@@ -371,13 +381,20 @@ int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
   // imposed obstacle motion (Grains::AdditionalFeatures, Base/src/Grains.cpp:1719-1745;
   // ObstacleImposedVelocity.cpp:38-260): a constant rotation about the
   // obstacle's rotation centre, or a constant translation
-  bool any_moving = false;
+  // explicit loadings (<ObstacleLoading> per motion, ObstacleImposedVelocity.cpp:60-262) replace an
+  // obstacle's legacy motion fields
+  auto has_explicit = [&](int id) {
+    for (auto& l : c->loads)
+      if (l.obstacle_id == id) return true;
+    return false;
+  };
+  bool any_moving = !c->loads.empty();
   for (auto& o : c->obs) any_moving = any_moving || o.moving;
   if (any_moving) {
     x << "<ObstacleLoadings>\n";
     for (size_t k = 0; k < c->obs.size(); ++k) {
       const grains_gpu_obstacle& o = c->obs[k];
-      if (!o.moving) continue;
+      if (!o.moving || has_explicit(o.id)) continue;
       x << "<ObstacleLoading Type=\"Velocity\" ObstacleName=\"o" << k
         << "\"><TimeInterval Start=\"0.\" End=\"1.e9\"/>";
       if (o.omega[0] != 0. || o.omega[1] != 0. || o.omega[2] != 0.)
@@ -387,6 +404,49 @@ int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
       else
         x << "<ConstantTranslation><TranslationalVelocity VX=\"" << num(o.velocity[0]) << "\" VY=\""
           << num(o.velocity[1]) << "\" VZ=\"" << num(o.velocity[2]) << "\"/></ConstantTranslation>";
+      x << "</ObstacleLoading>\n";
+    }
+    for (const auto& l : c->loads) {
+      size_t k = 0;
+      while (k < c->obs.size() && c->obs[k].id != l.obstacle_id) ++k;
+      if (k == c->obs.size()) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "loading of an unknown obstacle");
+      x << "<ObstacleLoading Type=\"Velocity\" ObstacleName=\"o" << k << "\"><TimeInterval Start=\""
+        << num(l.t_start) << "\" End=\"" << num(l.t_end) << "\"/>";
+      auto vec = [&](const char* tag, const char* a, const char* b, const char* cc, const double* v) {
+        x << "<" << tag << " " << a << "=\"" << num(v[0]) << "\" " << b << "=\"" << num(v[1]) << "\" " << cc
+          << "=\"" << num(v[2]) << "\"/>";
+      };
+      switch (l.type) {
+        case GRAINS_GPU_CONSTANT_TRANSLATION:
+          x << "<ConstantTranslation>";
+          vec("TranslationalVelocity", "VX", "VY", "VZ", l.vector);
+          x << "</ConstantTranslation>";
+          break;
+        case GRAINS_GPU_SIN_TRANSLATION:
+        case GRAINS_GPU_CRENEL_TRANSLATION:
+          x << (l.type == GRAINS_GPU_SIN_TRANSLATION ? "<SinTranslation>" : "<CrenelTranslation>");
+          vec("Direction", "VX", "VY", "VZ", l.vector);
+          x << "<Parameters Amplitude=\"" << num(l.amplitude[0]) << "\" Period=\"" << num(l.period[0]) << "\"";
+          if (l.type == GRAINS_GPU_SIN_TRANSLATION) x << " PhaseShift=\"" << num(l.phase_deg[0]) << "\"";
+          x << "/>" << (l.type == GRAINS_GPU_SIN_TRANSLATION ? "</SinTranslation>" : "</CrenelTranslation>");
+          break;
+        case GRAINS_GPU_CONSTANT_ROTATION:
+          x << "<ConstantRotation>";
+          vec("AngularVelocity", "WX", "WY", "WZ", l.vector);
+          if (l.has_center) vec("RotationCenter", "CX", "CY", "CZ", l.center);
+          x << "</ConstantRotation>";
+          break;
+        case GRAINS_GPU_MULTISIN_TRANSLATION:
+          x << "<MultiSinTranslation>";
+          vec("Direction", "VX", "VY", "VZ", l.vector);
+          vec("Period", "PX", "PY", "PZ", l.period);
+          vec("PhaseShift", "PhiX", "PhiY", "PhiZ", l.phase_deg);
+          vec("Amplitude", "AX", "AY", "AZ", l.amplitude);
+          x << "</MultiSinTranslation>";
+          break;
+        default:
+          return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "unknown loading type");
+      }
       x << "</ObstacleLoading>\n";
     }
     x << "</ObstacleLoadings>\n";
@@ -667,6 +727,59 @@ int grains_ref_get_stats(grains_gpu_ctx* c, grains_gpu_stats* st) {
 
 int grains_ref_reset_stats(grains_gpu_ctx* c) {
   c->status = 0;
+  return 0;
+}
+
+// The reference's own writers on the reference state, for the I/O fixtures:
+// AllComponents::write (AllComponents.cpp:1062-1181) writes the particle file
+// <root>_Particles.result (".bin" appended in Hybrid mode), moved to `path`.
+int grains_ref_write_reload_particles(grains_gpu_ctx* c, const char* path, int32_t binary, int64_t* bytes) {
+  if (!c || !c->g || !path) return GRAINS_GPU_INVALID_ARGUMENT;
+  const std::string root = c->dir + "/refsave";
+  GrainsExec::m_writingModeHybrid = binary != 0;
+  std::ostringstream head;
+  std::vector<Point3> known;
+  c->g->comps().write(head, root + ".x", &known, CIR_NONE, c->g->lc(), 0, 1, nullptr);
+  GrainsExec::m_writingModeHybrid = false;
+  const std::string pfile = root + "_Particles.result" + (binary ? ".bin" : "");
+  if (std::rename(pfile.c_str(), path) != 0) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "cannot move " + pfile);
+  if (bytes) {
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    *bytes = (int64_t)f.tellg();
+  }
+  return 0;
+}
+
+// RawDataPostProcessingWriter (PostProcessing/src/RawDataPostProcessingWriter.cpp)
+// for one output time: a writer built from <RawData Name=root WritingMode=...>,
+// started in "new" mode (truncating) or appending, then closed.  The
+// reference numbers the columns 1..GrainsExec::getTotalNumberPhysicalParticles
+// itself; n_total is not used.
+int grains_ref_write_rawdata(grains_gpu_ctx* c, const char* root, double time, int32_t system, int32_t n_total,
+                             int32_t binary, int32_t truncate, int64_t* bytes) {
+  (void)system;
+  (void)n_total;
+  if (!c || !c->g || !root) return GRAINS_GPU_INVALID_ARGUMENT;
+  const std::string xml = c->dir + "/rawdata.xml";
+  {
+    std::ofstream f(xml.c_str());
+    f << "<RawData Name=\"" << root << "\" WritingMode=\"" << (binary ? "Binary" : "Text") << "\"/>\n";
+  }
+  DOMElement* node = ReaderXML::getRoot(xml);
+  const std::string saved = GrainsExec::m_ReloadType;
+  GrainsExec::m_ReloadType = truncate ? "new" : "same";
+  std::streambuf* old = std::cout.rdbuf();
+  std::ostringstream quiet;
+  std::cout.rdbuf(quiet.rdbuf());
+  RawDataPostProcessingWriter* w = new RawDataPostProcessingWriter(node, 0, 1, false);
+  AllComponents& a = c->g->comps();
+  w->PostProcessing_start(time, c->g->dt(), a.getActiveParticles(), nullptr, nullptr, a.getReferenceParticles(),
+                          a.getObstacles(), c->g->lc(), c->g->windows());
+  w->PostProcessing_end();
+  delete w;
+  std::cout.rdbuf(old);
+  GrainsExec::m_ReloadType = saved;
+  if (bytes) *bytes = 0;
   return 0;
 }
 

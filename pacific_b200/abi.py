@@ -134,9 +134,13 @@ _SIGS = {
     "get_contact_forces": [_VP, C.c_int32, C.c_int64, _P_I32, _P_F64, C.POINTER(C.c_int64)],
     "get_stats": [_VP, C.POINTER(Stats)],
     "reset_stats": [_VP],
+    "set_record_attributes": [_VP, C.c_int64, _P_I32, _P_I32, _P_I32, _P_I32],
+    "write_reload_particles": [_VP, C.c_char_p, C.c_int32, C.POINTER(C.c_int64)],
+    "write_rawdata": [_VP, C.c_char_p, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
+                      C.POINTER(C.c_int64)],
 }
 # diagnostics that the reference built from its sources (oracle/_ref) lacks
-_OPTIONAL = {"get_contact_forces"}
+_OPTIONAL = {"get_contact_forces", "set_record_attributes"}
 _GPU_ONLY = {
     "get_stream": [_VP, C.POINTER(_VP)],
     "synchronize": [_VP],
@@ -154,7 +158,82 @@ _GPU_ONLY = {
     "adjoint_forward": [_VP, C.c_int32, C.c_double, _P_F64, _P_F64, _P_F64],
     "adjoint_contact_signature": [_VP, C.POINTER(C.c_uint64), C.POINTER(C.c_int64)],
     "adjoint_backward": [_VP, _P_F64, _P_F64, _P_F64, _P_F64, _P_F64, _P_F64, _P_F64, C.c_int32],
+    "reload_open": [C.c_char_p, C.c_int32, C.POINTER(_VP)],
+    "reload_last_error": [_VP, C.c_char_p, C.c_size_t],
+    "reload_get": [_VP, C.c_void_p],
+    "reload_close": [_VP],
+    "format_double": [C.c_double, C.c_int32, C.c_char_p, C.c_size_t, _P_I32],
+    "format_doubles": [_P_F64, C.c_int64, C.c_int32, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)],
 }
+
+
+class ReloadData(C.Structure):
+    _fields_ = [("n_particles", C.c_int64), ("n_memory", C.c_int64), ("geom_type", _P_I32), ("id", _P_I32),
+                ("tag", _P_I32), ("active", _P_I32), ("transform_type", _P_I32), ("position", _P_F64),
+                ("basis", _P_F64), ("velocity", _P_F64), ("quaternion", _P_F64), ("omega", _P_F64),
+                ("force", _P_F64), ("torque", _P_F64), ("memory", ContactMemory)]
+
+
+def read_reload_particles(lib, path, binary=False):
+    """Parses a particle file of a reload (text or hybrid binary) with
+    grains_gpu_reload_open / _get: a dict of per-particle arrays (file order)
+    and 'memory' with every contact-map entry (owner = holder id)."""
+    h = C.c_void_p()
+    rc = lib.fn["reload_open"](os.fsencode(path), 1 if binary else 0, C.byref(h))
+    try:
+        if rc:
+            buf = C.create_string_buffer(4096)
+            if h:
+                lib.fn["reload_last_error"](h, buf, 4096)
+            raise error_for(rc, buf.value.decode(errors="replace"))
+        d = ReloadData()
+        lib.fn["reload_get"](h, C.byref(d))
+        n, m = d.n_particles, d.n_memory
+        out = {k: np.zeros(n, np.int32) for k in ["geom_type", "id", "tag", "active", "transform_type"]}
+        for k, w in [("position", 3), ("basis", 9), ("velocity", 3), ("quaternion", 4), ("omega", 3),
+                     ("force", 3), ("torque", 3)]:
+            out[k] = np.zeros((n, w))
+        mem = {"owner": np.zeros(m, np.int32), "other": np.zeros(m, np.int32), "kdelta": np.zeros((m, 3)),
+               "prev_normal": np.zeros((m, 3)), "spring_torque": np.zeros((m, 3))}
+        for k in ["geom_type", "id", "tag", "active", "transform_type"]:
+            setattr(d, k, _ptr(out[k], C.c_int32))
+        for k in ["position", "basis", "velocity", "quaternion", "omega", "force", "torque"]:
+            setattr(d, k, _ptr(out[k], C.c_double))
+        d.memory.n = m
+        d.memory.owner, d.memory.other = _ptr(mem["owner"], C.c_int32), _ptr(mem["other"], C.c_int32)
+        d.memory.kdelta = _ptr(mem["kdelta"], C.c_double)
+        d.memory.prev_normal = _ptr(mem["prev_normal"], C.c_double)
+        d.memory.spring_torque = _ptr(mem["spring_torque"], C.c_double)
+        rc = lib.fn["reload_get"](h, C.byref(d))
+        if rc:
+            raise error_for(rc, "reload_get failed")
+        out["memory"] = mem
+        return out
+    finally:
+        if h:
+            lib.fn["reload_close"](h)
+
+
+def format_double(lib, x, digits):
+    """GrainsExec::doubleToString(ios::scientific, digits, x) with the library's formatter (host)."""
+    buf = C.create_string_buffer(64)
+    n = C.c_int32()
+    rc = lib.fn["format_double"](float(x), digits, buf, 64, C.byref(n))
+    if rc:
+        raise error_for(rc, "format_double failed")
+    return buf.value.decode()
+
+
+def format_doubles_on_device(lib, values, digits):
+    """The same formatter run on the device over an array: one value per line."""
+    x = np.ascontiguousarray(values, dtype=np.float64)
+    cap = 32 * len(x) + 64
+    buf = C.create_string_buffer(cap)
+    n = C.c_int64()
+    rc = lib.fn["format_doubles"](_ptr(x, C.c_double), len(x), digits, buf, cap, C.byref(n))
+    if rc:
+        raise error_for(rc, "format_doubles failed")
+    return buf.raw[:n.value].decode()
 
 
 class GrainsLib:
@@ -315,6 +394,8 @@ class Simulation:
             "basis": f64(p["basis"]) if p.get("basis") is not None else None,
             "velocity": f64(p["velocity"]),
             "omega": f64(p["omega"]),
+            "force": f64(p["force"]) if p.get("force") is not None else None,
+            "torque": f64(p["torque"]) if p.get("torque") is not None else None,
         }
         s = Particles()
         s.n = n
@@ -436,6 +517,28 @@ class Simulation:
         self._check(self.lib.fn["get_contact_forces"](self.ctx, system, cap, _ptr(buf, C.c_int32),
                                                       _ptr(f, C.c_double), C.byref(n)))
         return buf[: 2 * n.value].reshape(-1, 2), f[: 3 * n.value].reshape(-1, 3)
+
+    # ---- reload and RawData files ----
+    def set_record_attributes(self, geom_type=None, tag=None, active=None, transform_type=None):
+        """Reload-file attributes per particle (upload order); None keeps them."""
+        arrs = [None if a is None else i32(a) for a in (geom_type, tag, active, transform_type)]
+        ptrs = [_ptr(a, C.c_int32) for a in arrs]
+        self._check(self.lib.fn["set_record_attributes"](self.ctx, self.n, *ptrs))
+
+    def write_reload_particles(self, path, binary=False):
+        """The particle file of a reload (text, or hybrid binary); returns its size."""
+        nb = C.c_int64()
+        self._check(self.lib.fn["write_reload_particles"](self.ctx, os.fsencode(path), 1 if binary else 0,
+                                                          C.byref(nb)))
+        return nb.value
+
+    def write_rawdata(self, root, time, n_total=None, binary=False, truncate=False, system=0):
+        """One RawData output time (the ten time-series files and the type file)."""
+        nb = C.c_int64()
+        n_total = self.n if n_total is None else n_total
+        self._check(self.lib.fn["write_rawdata"](self.ctx, os.fsencode(root), float(time), system, n_total,
+                                                 1 if binary else 0, 1 if truncate else 0, C.byref(nb)))
+        return nb.value
 
     def stats(self):
         st = Stats()

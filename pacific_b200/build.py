@@ -28,9 +28,10 @@ UNITS = [
     ("adjoint_api.cu", []),
     ("api.cu", []),
     ("noalloc.cu", []),
+    ("io.cu", ["-fmad=false"]),
 ]
 HEADERS = ["common.cuh", "sphere_contact.cuh", "contact_law.cuh", "gjk.cuh", "kernels.cuh", "device_state.h",
-           "dual.cuh", "adjoint.cuh", "adjoint.h"]
+           "dual.cuh", "adjoint.cuh", "adjoint.h", "format.cuh", "io.h"]
 
 
 def _newer(target, sources):

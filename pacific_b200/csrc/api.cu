@@ -15,6 +15,8 @@
 #include "../../include/grains_gpu.h"
 #include "adjoint.h"
 #include "device_state.h"
+#include "format.cuh"
+#include "io.h"
 #include "gjk.cuh"
 #include "sphere_contact.cuh"
 
@@ -83,7 +85,8 @@ struct grains_gpu_ctx {
   bool keys_valid = false;  // key and cell counts hold the cells of the current positions
   bool pending_kick2 = false;
   double pending_dt = 0;
-  bool has_basis = false;
+  bool has_basis = false;    // a basis per particle is kept (non-spheres, or given at upload)
+  bool all_spheres = true;   // every particle is a sphere
   bool has_convex = false;
   StepArgs<float> af{};
   StepArgs<double> ad{};
@@ -143,6 +146,17 @@ struct grains_gpu_ctx {
   unsigned* pbar = nullptr;  // grid-barrier state of the persistent launch
   int* psums = nullptr;      // its scan scratch (one int per block)
   int pblocks = 0;
+  // reload and RawData files (io.cu): particle names by upload index, sorted
+  // (system, id) keys, obstacle ids, per-particle record attributes
+  int* d_row_id = nullptr;
+  int* d_row_sys = nullptr;
+  unsigned long long* d_row_keys = nullptr;
+  int* d_key_rows = nullptr;
+  RecordAttr* d_attr = nullptr;
+  int* d_obs_id = nullptr;
+  int* d_sys_obs_offset = nullptr;
+  int moved = 0;  // a move since the upload: transform types gain ROTATION | TRANSLATION
+  IoScratch io;
 };
 
 namespace {
@@ -739,6 +753,9 @@ int grains_gpu_destroy(grains_gpu_ctx* c) {
   if (c->stage_basis) cudaFree(c->stage_basis);
   if (c->pbar) cudaFree(c->pbar);
   if (c->psums) cudaFree(c->psums);
+  for (void* p : {(void*)c->d_row_id, (void*)c->d_row_sys, (void*)c->d_row_keys, (void*)c->d_key_rows,
+                  (void*)c->d_attr})
+    if (p) cudaFree(p);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
   return 0;
@@ -962,6 +979,16 @@ int build_tables(grains_gpu_ctx* c) {
   rc |= up(cstart.data(), cstart.size() * sizeof(int), (void**)&c->d_cell_obs_start);
   rc |= up(cidx.data(), cidx.size() * sizeof(int), (void**)&c->d_cell_obs_idx);
   rc |= up(moving.data(), moving.size() * sizeof(int), (void**)&c->d_moving);
+  {
+    // obstacle ids by global obstacle index, and each system's first index
+    std::vector<int> oid, ooff;
+    for (const auto& sy : c->sys) {
+      ooff.push_back((int)oid.size());
+      for (const auto& o : sy.obs) oid.push_back(o.id);
+    }
+    rc |= up(oid.data(), oid.size() * sizeof(int), (void**)&c->d_obs_id);
+    rc |= up(ooff.data(), ooff.size() * sizeof(int), (void**)&c->d_sys_obs_offset);
+  }
   if (c->precision == GRAINS_GPU_FP64)
     rc |= up(ld.data(), ld.size() * sizeof(LawParams<double>), &c->d_laws);
   else
@@ -1010,12 +1037,27 @@ int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
     if (si < 0 || si >= (int)c->sys.size()) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "particle system out of range");
     if (c->shapes[p->shape[i]].type != GRAINS_GPU_SPHERE) basis_needed = true;
   }
+  const bool nonsphere = basis_needed;
+  // a basis given for spheres is kept and turned with them, as the
+  // reference's transforms are (RigidBody::composeLeftByRotation)
+  if (p->basis) basis_needed = true;
+  // names of the particles: sorted (system, id) keys; an id appears once per system
+  std::vector<std::pair<unsigned long long, int>> keyed((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    const int si = p->system ? p->system[i] : 0;
+    keyed[i] = {((unsigned long long)(unsigned)si << 32) | (unsigned)(p->id[i] ^ (int)0x80000000), (int)i};
+  }
+  std::sort(keyed.begin(), keyed.end());
+  for (int64_t i = 1; i < n; ++i)
+    if (keyed[i].first == keyed[i - 1].first)
+      return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "a particle id appears twice in one system");
   if (c->tables_dirty) {
     if (int rc = build_tables(c)) return rc;
     c->tables_dirty = false;
   }
   c->has_basis = basis_needed;
-  c->has_convex = basis_needed;
+  c->has_convex = nonsphere;
+  c->all_spheres = !nonsphere;
   for (auto& s : c->sys)
     for (auto& o : s.obs)
       if (c->shapes[o.shape].type != GRAINS_GPU_BOX) c->has_convex = true;
@@ -1112,9 +1154,58 @@ int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
     srcs[0] = vf.data(); srcs[1] = wf.data(); srcs[2] = wbff.data(); srcs[3] = zf.data(); srcs[4] = zf.data();
     srcs[5] = If.data();
   }
+  // a given torsor (a reload's force and torque) stands until the next force evaluation
+  std::vector<double> Fd, Td;
+  std::vector<float> Ff, Tf;
+  if (p->force && p->torque) {
+    if (dbl) { Fd.assign(4 * n, 0.); Td.assign(4 * n, 0.); }
+    else { Ff.assign(4 * n, 0.f); Tf.assign(4 * n, 0.f); }
+    for (int64_t i = 0; i < n; ++i) {
+      put(Fd, Ff, i, p->force[3 * i], p->force[3 * i + 1], p->force[3 * i + 2]);
+      put(Td, Tf, i, p->torque[3 * i], p->torque[3 * i + 1], p->torque[3 * i + 2]);
+    }
+    srcs[3] = dbl ? (const void*)Fd.data() : (const void*)Ff.data();
+    srcs[4] = dbl ? (const void*)Td.data() : (const void*)Tf.data();
+  }
   void* dsts[6] = {b.v, b.w, b.wbf, b.F, b.T, b.inertia};
   for (int k = 0; k < 6; ++k) rc |= cp(dsts[k], srcs[k], n * r4);
   if (rc) return rc;
+  CK(cudaMemsetAsync(c->coord, 0, (size_t)c->cap * sizeof(int), c->stream));
+  // tables of the reload and RawData writers
+  if (!c->d_row_id) {
+    void* q0 = nullptr;
+    CK(cudaMalloc(&q0, (size_t)c->cap * sizeof(int)));
+    c->d_row_id = (int*)q0;
+    CK(cudaMalloc(&q0, (size_t)c->cap * sizeof(int)));
+    c->d_row_sys = (int*)q0;
+    CK(cudaMalloc(&q0, (size_t)c->cap * sizeof(unsigned long long)));
+    c->d_row_keys = (unsigned long long*)q0;
+    CK(cudaMalloc(&q0, (size_t)c->cap * sizeof(int)));
+    c->d_key_rows = (int*)q0;
+    CK(cudaMalloc(&q0, (size_t)c->cap * sizeof(RecordAttr)));
+    c->d_attr = (RecordAttr*)q0;
+  }
+  {
+    std::vector<int> rid(n), rsys(n), krow(n);
+    std::vector<unsigned long long> keys(n);
+    std::vector<RecordAttr> attr(n);
+    for (int64_t i = 0; i < n; ++i) {
+      rid[i] = p->id[i];
+      rsys[i] = p->system ? p->system[i] : 0;
+      keys[i] = keyed[i].first;
+      krow[i] = keyed[i].second;
+      // defaults: the shape's type, interior, active, a translated transform
+      attr[i] = RecordAttr{p->shape[i], 0, 1, 1};
+    }
+    rc |= cp(c->d_row_id, rid.data(), n * sizeof(int));
+    rc |= cp(c->d_row_sys, rsys.data(), n * sizeof(int));
+    rc |= cp(c->d_row_keys, keys.data(), n * sizeof(unsigned long long));
+    rc |= cp(c->d_key_rows, krow.data(), n * sizeof(int));
+    rc |= cp(c->d_attr, attr.data(), n * sizeof(RecordAttr));
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(c->stream));  // the host vectors above are pageable
+  }
+  c->moved = 0;
   for (int k = 0; k < 2; ++k) CK(cudaMemsetAsync(c->hist_n[k], 0, (size_t)c->cap * sizeof(int), c->stream));
   CK(cudaMemsetAsync(c->stats, 0, sizeof(StatsDev), c->stream));
   c->keys_valid = false;
@@ -1396,6 +1487,7 @@ int grains_gpu_move(grains_gpu_ctx* c, double time, double dt_v, double dt_x) {
   }
   int rc = with_args(c, [&](auto& a) { return launch_kick_move(a, c->stream, 0, 0., 1, dt_v, dt_x); });
   if (rc) return fail(c, rc, "move launch failed");
+  c->moved = 1;
   c->keys_valid = true;
   c->sorted = false;
   if ((rc = move_obstacles(c, dt_x, 1, time))) return rc;
@@ -1433,6 +1525,7 @@ int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt)
   if (!c || !time || n_steps < 0 || !(dt > 0)) return GRAINS_GPU_INVALID_ARGUMENT;
   if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
   if (n_steps == 0) return 0;
+  c->moved = 1;
   if (!c->sorted)
     if (int rc = sort_now(c, 1)) return rc;
   // step 1 moves (finishing any pending half kick); steps 1..n-1 end with
@@ -1967,7 +2060,7 @@ int context_view(grains_gpu_ctx* c, ContextView* v, std::string& err) {
   v->n_sys = (int)c->sys.size();
   v->n_laws = (int)c->sys.size() * maxmat * maxmat;
   v->hist_cap = c->hist_cap;
-  v->spheres_only = c->has_basis ? 0 : 1;
+  v->spheres_only = c->all_spheres ? 1 : 0;
   v->box_walls_only = 1;
   v->hooke_laws_only = 1;
   for (const auto& s : c->sys) {
@@ -1994,3 +2087,155 @@ int context_view(grains_gpu_ctx* c, ContextView* v, std::string& err) {
   return 0;
 }
 }  // namespace gg
+
+// ---- reload and RawData files ---------------------------------------------------
+namespace {
+
+int io_view(grains_gpu_ctx* c, IoView& v) {
+  if (int rc = flush_kick(c)) return rc;
+  const auto& b = c->buf[c->cur];
+  v = IoView{};
+  v.precision = c->precision;
+  v.stream = c->stream;
+  v.n = (int)c->n;
+  v.xr = b.xr;
+  v.q = b.q;
+  v.basis = c->has_basis ? b.basis : nullptr;
+  v.v = b.v;
+  v.w = b.w;
+  v.F = b.F;
+  v.T = b.T;
+  v.meta = b.meta;
+  v.orig = b.orig;
+  v.coord = c->coord;
+  v.hist = c->hist[c->hcur];
+  v.hist_n = c->hist_n[c->hcur];
+  v.hist_cap = c->hist_cap;
+  v.row_id = c->d_row_id;
+  v.row_sys = c->d_row_sys;
+  v.row_keys = c->d_row_keys;
+  v.key_rows = c->d_key_rows;
+  v.obs_id = c->d_obs_id;
+  v.sys_obs_offset = c->d_sys_obs_offset;
+  v.attr = c->d_attr;
+  v.moved = c->moved;
+  return 0;
+}
+
+}  // namespace
+
+struct grains_gpu_reload {
+  ReloadData d;
+  std::string err;
+  int status = 0;
+};
+
+int grains_gpu_set_record_attributes(grains_gpu_ctx* c, int64_t n, const int32_t* geom_type, const int32_t* tag,
+                                     const int32_t* active, const int32_t* transform_type) {
+  if (!c || n < 0) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "upload particles first");
+  if (n != c->n) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "attributes must cover every uploaded particle");
+  std::vector<RecordAttr> a((size_t)n);
+  CK(cudaMemcpyAsync(a.data(), c->d_attr, (size_t)n * sizeof(RecordAttr), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int64_t i = 0; i < n; ++i) {
+    if (geom_type) a[i].geom_type = geom_type[i];
+    if (tag) a[i].tag = tag[i];
+    if (active) a[i].active = active[i] ? 1 : 0;
+    if (transform_type) a[i].transform_type = transform_type[i];
+  }
+  CK(cudaMemcpyAsync(c->d_attr, a.data(), (size_t)n * sizeof(RecordAttr), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int grains_gpu_write_reload_particles(grains_gpu_ctx* c, const char* path, int32_t binary, int64_t* bytes) {
+  if (!c || !path) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  IoView v;
+  if (int rc = io_view(c, v)) return rc;
+  int64_t nb = 0;
+  std::string err;
+  if (int rc = write_reload_particles(v, c->io, path, binary ? 1 : 0, &nb, err)) return fail(c, rc, err);
+  if (bytes) *bytes = nb;
+  return 0;
+}
+
+int grains_gpu_write_rawdata(grains_gpu_ctx* c, const char* root, double time, int32_t system, int32_t n_total,
+                             int32_t binary, int32_t truncate, int64_t* bytes) {
+  if (!c || !root || n_total < 0) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (system < 0 || system >= (int)c->sys.size()) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "bad system index");
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
+  IoView v;
+  if (int rc = io_view(c, v)) return rc;
+  int64_t nb = 0;
+  std::string err;
+  if (int rc = write_rawdata(v, c->io, root, time, system, n_total, binary ? 1 : 0, truncate ? 1 : 0, &nb, err))
+    return fail(c, rc, err);
+  if (bytes) *bytes = nb;
+  return 0;
+}
+
+int grains_gpu_reload_open(const char* path, int32_t binary, grains_gpu_reload** out) {
+  if (!path || !out) return GRAINS_GPU_INVALID_ARGUMENT;
+  grains_gpu_reload* r = new grains_gpu_reload;
+  r->status = read_reload_particles(path, binary ? 1 : 0, r->d, r->err);
+  *out = r;  // returned even on failure, so that the message can be read
+  return r->status;
+}
+
+int grains_gpu_reload_last_error(const grains_gpu_reload* r, char* buf, size_t len) {
+  if (!r || !buf || !len) return GRAINS_GPU_INVALID_ARGUMENT;
+  std::snprintf(buf, len, "%s", r->err.c_str());
+  return 0;
+}
+
+int grains_gpu_reload_get(const grains_gpu_reload* r, grains_gpu_reload_data* o) {
+  if (!r || !o) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (r->status) return r->status;
+  const ReloadData& d = r->d;
+  const size_t n = d.id.size(), m = d.owner.size();
+  o->n_particles = (int64_t)n;
+  o->n_memory = (int64_t)m;
+  auto put = [](auto* dst, const auto& src) {
+    if (dst && !src.empty()) std::memcpy(dst, src.data(), src.size() * sizeof(src[0]));
+  };
+  put(o->geom_type, d.geom_type);
+  put(o->id, d.id);
+  put(o->tag, d.tag);
+  put(o->active, d.active);
+  put(o->transform_type, d.transform_type);
+  put(o->position, d.position);
+  put(o->basis, d.basis);
+  put(o->velocity, d.velocity);
+  put(o->quaternion, d.quaternion);
+  put(o->omega, d.omega);
+  put(o->force, d.force);
+  put(o->torque, d.torque);
+  o->memory.n = (int64_t)m;
+  put(o->memory.owner, d.owner);
+  put(o->memory.other, d.other);
+  put(o->memory.kdelta, d.kdelta);
+  put(o->memory.prev_normal, d.prev_normal);
+  put(o->memory.spring_torque, d.spring_torque);
+  return 0;
+}
+
+int grains_gpu_reload_close(grains_gpu_reload* r) {
+  delete r;
+  return 0;
+}
+
+int grains_gpu_format_double(double x, int32_t digits, char* out, size_t cap, int32_t* length) {
+  if (!out || digits < 0 || digits > 16) return GRAINS_GPU_INVALID_ARGUMENT;
+  const int n = gg::fmt::grains_double_host(x, digits, out, cap);
+  if (n < 0) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (length) *length = n;
+  return 0;
+}
+
+int grains_gpu_format_doubles(const double* x, int64_t n, int32_t digits, char* out, int64_t cap, int64_t* length) {
+  if ((!x && n) || !out || n < 0 || digits < 0 || digits > 16 || !length) return GRAINS_GPU_INVALID_ARGUMENT;
+  std::string err;
+  return format_doubles(x, n, digits, out, cap, length, err);
+}

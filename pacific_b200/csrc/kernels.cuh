@@ -130,7 +130,7 @@ __device__ __forceinline__ void integrate(const StepArgs<R>& a, const ParticleAr
       dq = Qt<double>{sc(mw, sn * 1. / nom), c};
     }
     q = qmul(dq, q);
-    if (a.has_basis && !sphere) {
+    if (a.has_basis) {
       M3 b;
       for (int t = 0; t < 9; ++t) b.m[t] = src.basis[9 * (size_t)s + t];
       mrotate_left(b, dq);
@@ -144,7 +144,7 @@ __device__ __forceinline__ void integrate(const StepArgs<R>& a, const ParticleAr
     unsigned key = (unsigned)cell_index(S, ci, cj, ck);
     dst.key[s] = key;
     atomicAdd(&a.cell_count[key], 1);  // result unused: a fire-and-forget reduction
-  } else if (a.has_basis && !sphere && dst.basis != src.basis) {
+  } else if (a.has_basis && dst.basis != src.basis) {
     for (int t = 0; t < 9; ++t) dst.basis[9 * (size_t)s + t] = src.basis[9 * (size_t)s + t];
   }
   dst.xr[s] = xr;

@@ -51,3 +51,11 @@ def gpu_lib(oracle_lib):
         return oracle_lib
     import pacific_b200
     return pacific_b200.load_library()
+
+
+@pytest.fixture(scope="session")
+def reader_lib():
+    """The CUDA library for its host-only entry points (reload reader, host
+    formatter): loading it needs no device."""
+    import pacific_b200
+    return pacific_b200.load_library()

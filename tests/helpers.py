@@ -1,5 +1,7 @@
 """Shared helpers of the parity tests: run the same scenario through the CUDA
 library and the CPU oracle and compare."""
+import os
+
 import numpy as np
 
 from pacific_b200 import scenarios as S
@@ -112,3 +114,45 @@ def tangent_run(sc, n_steps, dir_v0=None, dir_laws=None, n_mat=4):
     tan = {"position": tx.reshape(-1, n, 3)[:nd], "velocity": tv.reshape(-1, n, 3)[:nd],
            "omega": tw.reshape(-1, n, 3)[:nd]}
     return fin, tan
+
+
+# ---- reload / RawData fixtures (tests/golden/io_*.npz) ----
+RAW_FILES = ["_position_x.dat", "_position_y.dat", "_position_z.dat", "_translational_velocity_x.dat",
+             "_translational_velocity_y.dat", "_translational_velocity_z.dat", "_angular_velocity_x.dat",
+             "_angular_velocity_y.dat", "_angular_velocity_z.dat", "_coordinationNumber.dat", "_particleType.dat"]
+
+
+def read_fixture_reload(reader_lib, z, tmpdir, binary=False):
+    """The reference's particle file of fixture z, parsed by the library's reader."""
+    from pacific_b200.abi import read_reload_particles
+    path = os.path.join(str(tmpdir), "ref_reload" + (".bin" if binary else ".txt"))
+    with open(path, "wb") as f:
+        f.write(bytes(z["reload_bin" if binary else "reload_text"]))
+    return read_reload_particles(reader_lib, path, binary)
+
+
+def fixture_scenario(z, r):
+    """The fixture's scenario with the particles of the parsed file r (file
+    order) and the static data the fixture recorded for them."""
+    import json
+    spec = json.loads(str(z["spec"]))
+    doms = [dict(origin=np.array(d["origin"]), size=np.array(d["size"]), cell_size=d["cell_size"],
+                 gravity=tuple(d["gravity"])) for d in spec["domains"]]
+    laws = [[(l[0], l[1], l[2], l[3]) for l in ls] for ls in spec["laws"]]
+    p = dict(id=r["id"], system=None, shape=z["static_shape"], material=z["static_material"],
+             radius=z["static_radius"], crust=z["static_crust"], mass=z["static_mass"], inertia=z["static_inertia"],
+             position=r["position"], quaternion=r["quaternion"], basis=r["basis"], velocity=r["velocity"],
+             omega=r["omega"], force=r["force"], torque=r["torque"])
+    return S.Scenario(spec["name"], [tuple(s) for s in spec["shapes"]], doms, laws, spec["obstacles"], p,
+                      spec["dt"], spec["n_steps"])
+
+
+def load_fixture_state(lib, z, r, precision=FP64):
+    """A context holding exactly the state the reference wrote: particles,
+    torsors, bases, both sides of every contact memory and the record
+    attributes."""
+    sc = fixture_scenario(z, r)
+    sim = make(lib, sc, precision)
+    sim.upload_contact_memory(r["memory"])
+    sim.set_record_attributes(r["geom_type"], r["tag"], r["active"], r["transform_type"])
+    return sc, sim
