@@ -78,6 +78,16 @@ class Obstacle(C.Structure):
                 ("omega", C.c_double * 3), ("rotation_center", C.c_double * 3)]
 
 
+class ObstacleLoading(C.Structure):
+    _fields_ = [("obstacle_id", C.c_int32), ("type", C.c_int32), ("t_start", C.c_double), ("t_end", C.c_double),
+                ("vector", C.c_double * 3), ("center", C.c_double * 3), ("has_center", C.c_int32),
+                ("reserved", C.c_int32), ("amplitude", C.c_double * 3), ("period", C.c_double * 3),
+                ("phase_deg", C.c_double * 3)]
+
+
+# imposed obstacle motions (grains_gpu_motion)
+CONSTANT_TRANSLATION, SIN_TRANSLATION, CRENEL_TRANSLATION, CONSTANT_ROTATION, MULTISIN_TRANSLATION = 0, 1, 2, 3, 4
+
 _P_I32 = C.POINTER(C.c_int32)
 _P_F64 = C.POINTER(C.c_double)
 
@@ -117,6 +127,7 @@ _SIGS = {
     "add_shape": [_VP, C.c_int32, _P_F64, C.c_int32, _P_I32],
     "set_contact_law": [_VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P_F64, C.c_int32],
     "set_obstacles": [_VP, C.c_int32, C.c_int32, C.POINTER(Obstacle)],
+    "set_obstacle_loadings": [_VP, C.c_int32, C.c_int32, C.POINTER(ObstacleLoading)],
     "upload_particles": [_VP, C.POINTER(Particles)],
     "download_particles": [_VP, C.POINTER(Particles)],
     "update_particles": [_VP, C.POINTER(Particles)],
@@ -376,6 +387,29 @@ class Simulation:
             ob.omega[:] = list(o.get("omega", (0.0, 0.0, 0.0)))
             ob.rotation_center[:] = list(o.get("rotation_center", (0.0, 0.0, 0.0)))
         self._check(self.lib.fn["set_obstacles"](self.ctx, system, len(obstacles), arr))
+
+    def set_obstacle_loadings(self, system, loadings):
+        """Imposed obstacle motions: dicts with obstacle_id, type, t_start,
+        t_end and the type's fields (vector, center, amplitude, period,
+        phase_deg as 3-sequences or scalars)."""
+        arr = (ObstacleLoading * max(1, len(loadings)))()
+
+        def three(v):
+            v = np.atleast_1d(np.asarray(v, dtype=float))
+            return list(v) + [0.0] * (3 - len(v))
+        for k, l in enumerate(loadings):
+            g = arr[k]
+            g.obstacle_id = l["obstacle_id"]
+            g.type = l["type"]
+            g.t_start = l.get("t_start", 0.0)
+            g.t_end = l.get("t_end", 1.0e9)
+            g.vector[:] = three(l.get("vector", 0.0))
+            g.center[:] = three(l.get("center", 0.0))
+            g.has_center = 1 if "center" in l else 0
+            g.amplitude[:] = three(l.get("amplitude", 0.0))
+            g.period[:] = three(l.get("period", 0.0))
+            g.phase_deg[:] = three(l.get("phase_deg", 0.0))
+        self._check(self.lib.fn["set_obstacle_loadings"](self.ctx, system, len(loadings), arr))
 
     # ---- state ----
     def upload(self, p):

@@ -49,6 +49,7 @@ struct SysHost {
   double ex = 0, ey = 0, ez = 0;
   std::map<std::pair<int, int>, LawHost> laws;
   std::vector<grains_gpu_obstacle> obs;
+  std::vector<grains_gpu_obstacle_loading> loads;  // explicit imposed motions
 };
 
 template <typename T>
@@ -125,6 +126,8 @@ struct grains_gpu_ctx {
   ShapeDev* d_shapes = nullptr;
   double* d_verts = nullptr;
   ObstacleDev* d_obs = nullptr;
+  LoadingDev* d_loads = nullptr;
+  int* d_load_flags = nullptr;  // per system: a loading active over this step, over the previous one
   int *d_cell_obs_start = nullptr, *d_cell_obs_idx = nullptr, *d_moving = nullptr;
   void* d_laws = nullptr;
   std::vector<SysDev> h_sys;
@@ -303,6 +306,74 @@ ShapeDev shape_dev(const ShapeHost& s, int vert_offset) {
 }
 
 // ---- obstacles ----------------------------------------------------------------
+// ObstacleImposedVelocity's XML constructor (ObstacleImposedVelocity.cpp:60-262):
+// directions normalised (Vector3::normalize), phases to radians, multi-sin
+// amplitudes times the direction
+LoadingDev loading_dev(const grains_gpu_obstacle_loading& g) {
+  LoadingDev L{};
+  L.type = g.type;
+  L.has_center = g.has_center ? 1 : 0;
+  L.ts = g.t_start;
+  L.te = g.t_end;
+  for (int i = 0; i < 3; ++i) L.center[i] = g.center[i];
+  if (g.type == GRAINS_GPU_CONSTANT_TRANSLATION)
+    for (int i = 0; i < 3; ++i) L.vel[i] = g.vector[i];
+  if (g.type == GRAINS_GPU_CONSTANT_ROTATION)
+    for (int i = 0; i < 3; ++i) L.omega[i] = g.vector[i];
+  if (g.type == GRAINS_GPU_SIN_TRANSLATION || g.type == GRAINS_GPU_CRENEL_TRANSLATION ||
+      g.type == GRAINS_GPU_MULTISIN_TRANSLATION) {
+    const double nv = std::sqrt(g.vector[0] * g.vector[0] + g.vector[1] * g.vector[1] + g.vector[2] * g.vector[2]);
+    for (int i = 0; i < 3; ++i) L.unit[i] = g.vector[i] / nv;
+    L.amp = g.amplitude[0];
+    L.period = g.period[0];
+    L.phase = g.phase_deg[0] * kPi / 180.;
+    for (int i = 0; i < 3; ++i) {
+      L.mper[i] = g.period[i];
+      L.mphase[i] = g.phase_deg[i] * kPi / 180.;
+      L.mamp[i] = g.amplitude[i] * L.unit[i];
+    }
+  }
+  return L;
+}
+
+// an obstacle's legacy motion fields as one loading over [0, 1e9]
+grains_gpu_obstacle_loading legacy_loading(const grains_gpu_obstacle& o) {
+  grains_gpu_obstacle_loading g{};
+  g.obstacle_id = o.id;
+  g.t_start = 0.;
+  g.t_end = 1.e9;
+  if (o.omega[0] != 0. || o.omega[1] != 0. || o.omega[2] != 0.) {
+    g.type = GRAINS_GPU_CONSTANT_ROTATION;
+    for (int i = 0; i < 3; ++i) {
+      g.vector[i] = o.omega[i];
+      g.center[i] = o.rotation_center[i];
+    }
+    g.has_center = 1;
+  } else {
+    g.type = GRAINS_GPU_CONSTANT_TRANSLATION;
+    for (int i = 0; i < 3; ++i) g.vector[i] = o.velocity[i];
+  }
+  return g;
+}
+
+// the loadings of one obstacle in ObstacleKinematicsVelocity's order
+// (ObstacleKinematicsVelocity.cpp:28-40): by start time, a later-given
+// loading before those starting at the same time
+std::vector<LoadingDev> obstacle_loadings(const SysHost& s, const grains_gpu_obstacle& o) {
+  std::vector<grains_gpu_obstacle_loading> v;
+  auto insert = [&](const grains_gpu_obstacle_loading& g) {
+    size_t k = 0;
+    while (k < v.size() && v[k].t_start < g.t_start) ++k;
+    v.insert(v.begin() + (long)k, g);
+  };
+  for (const auto& g : s.loads)
+    if (g.obstacle_id == o.id) insert(g);
+  if (v.empty() && o.moving) v.push_back(legacy_loading(o));
+  std::vector<LoadingDev> out;
+  for (const auto& g : v) out.push_back(loading_dev(g));
+  return out;
+}
+
 ObstacleDev obstacle_dev(const grains_gpu_obstacle& o, const ShapeHost& sh) {
   ObstacleDev d{};
   for (int i = 0; i < 9; ++i) d.b[i] = o.transform[i];
@@ -312,9 +383,6 @@ ObstacleDev obstacle_dev(const grains_gpu_obstacle& o, const ShapeHost& sh) {
     // the start time, when an imposed motion starting then is not active yet)
     d.vel[i] = 0.;
     d.omega[i] = 0.;
-    d.ivel[i] = o.velocity[i];
-    d.iomega[i] = o.omega[i];
-    d.rot_center[i] = o.rotation_center[i];
   }
   d.crust = o.crust;
   d.circ = sh.circ;
@@ -322,7 +390,7 @@ ObstacleDev obstacle_dev(const grains_gpu_obstacle& o, const ShapeHost& sh) {
   d.id = o.id;
   d.material = o.material;
   d.shape = o.shape;
-  d.moving = o.moving;
+  d.moving = 0;  // set with its loadings
   // world AABB: Convex::bbox (Convex.cpp:29-41) -> BBox centre / extent (BBox.cpp:235-239)
   M3 b;
   for (int i = 0; i < 9; ++i) b.m[i] = d.b[i];
@@ -447,6 +515,8 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   a.cell_obs_start = c->d_cell_obs_start;
   a.cell_obs_idx = c->d_cell_obs_idx;
   a.moving_idx = c->d_moving;
+  a.loads = c->d_loads;
+  a.load_flags = c->d_load_flags;
   a.laws = (const LawParams<R>*)c->d_laws;
   fill_arrays<R>(c, a.cur, c->cur);
   fill_arrays<R>(c, a.alt, 1 - c->cur);
@@ -562,8 +632,9 @@ int forces_now(grains_gpu_ctx* c, double dt, int diag, int phases = 3) {
 // by dt, as Grains::Simulation advances m_time
 int move_obstacles(grains_gpu_ctx* c, double dt, int from_host = 0, double time = 0.) {
   if (c->n_moving == 0) return 0;
-  int rc = launch_obstacle_move(c->d_obs, c->d_moving, c->n_moving, c->d_shapes, c->d_verts, dt, c->clock,
-                                time, from_host, c->stream);
+  int rc = launch_obstacle_move(c->d_obs, c->d_moving, c->n_moving, c->d_loads, c->d_load_flags,
+                                (int)c->sys.size(), c->d_shapes, c->d_verts, dt, c->clock, time, from_host,
+                                c->stream);
   return rc ? fail(c, rc, "obstacle move launch failed") : 0;
 }
 
@@ -865,6 +936,30 @@ int grains_gpu_set_obstacles(grains_gpu_ctx* c, int32_t system, int32_t n, const
   return 0;
 }
 
+int grains_gpu_set_obstacle_loadings(grains_gpu_ctx* c, int32_t system, int32_t n,
+                                     const grains_gpu_obstacle_loading* l) {
+  if (!c || n < 0 || (n && !l)) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (system < 0 || system >= (int)c->sys.size()) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "bad system index");
+  SysHost& s = c->sys[system];
+  for (int k = 0; k < n; ++k) {
+    bool found = false;
+    for (const auto& o : s.obs) found = found || o.id == l[k].obstacle_id;
+    if (!found) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "loading of an unknown obstacle");
+    if (l[k].type < GRAINS_GPU_CONSTANT_TRANSLATION || l[k].type > GRAINS_GPU_MULTISIN_TRANSLATION)
+      return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "unknown loading type");
+    if ((l[k].type == GRAINS_GPU_SIN_TRANSLATION || l[k].type == GRAINS_GPU_CRENEL_TRANSLATION) &&
+        !(l[k].period[0] > 0.))
+      return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "a periodic loading needs a positive period");
+    if (l[k].type == GRAINS_GPU_MULTISIN_TRANSLATION &&
+        !(l[k].period[0] > 0. && l[k].period[1] > 0. && l[k].period[2] > 0.))
+      return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "a periodic loading needs a positive period");
+  }
+  s.loads.assign(l, l + n);
+  c->uploaded = false;
+  c->tables_dirty = true;
+  return 0;
+}
+
 namespace {
 // Builds the device tables and the per-cell obstacle links (set-up time)
 int build_tables(grains_gpu_ctx* c) {
@@ -873,6 +968,7 @@ int build_tables(grains_gpu_ctx* c) {
   const int maxmat = c->cfg.max_materials > 0 ? c->cfg.max_materials : 4;
   std::vector<SysDev> hs;
   std::vector<ObstacleDev> ho;
+  std::vector<LoadingDev> hl;
   std::vector<int> moving;
   std::vector<int> cstart;
   std::vector<int> cidx;
@@ -900,8 +996,15 @@ int build_tables(grains_gpu_ctx* c) {
     d.n_obs = (int)s.obs.size();
     d.moving_offset = (int)moving.size();
     for (size_t k = 0; k < s.obs.size(); ++k) {
-      ho.push_back(obstacle_dev(s.obs[k], c->shapes[s.obs[k].shape]));
-      if (s.obs[k].moving) moving.push_back(d.obs_offset + (int)k);
+      ObstacleDev od = obstacle_dev(s.obs[k], c->shapes[s.obs[k].shape]);
+      const std::vector<LoadingDev> ls = obstacle_loadings(s, s.obs[k]);
+      od.load_first = (int)hl.size();
+      od.load_count = (int)ls.size();
+      od.moving = ls.empty() ? 0 : 1;
+      od.sys = (int)si;
+      hl.insert(hl.end(), ls.begin(), ls.end());
+      ho.push_back(od);
+      if (od.moving) moving.push_back(d.obs_offset + (int)k);
     }
     d.n_moving = (int)moving.size() - d.moving_offset;
     const int nb = s.nbi * s.nbj * s.nbk;
@@ -979,6 +1082,11 @@ int build_tables(grains_gpu_ctx* c) {
   rc |= up(cstart.data(), cstart.size() * sizeof(int), (void**)&c->d_cell_obs_start);
   rc |= up(cidx.data(), cidx.size() * sizeof(int), (void**)&c->d_cell_obs_idx);
   rc |= up(moving.data(), moving.size() * sizeof(int), (void**)&c->d_moving);
+  rc |= up(hl.data(), hl.size() * sizeof(LoadingDev), (void**)&c->d_loads);
+  {
+    std::vector<int> flags(2 * c->sys.size(), 0);  // no loading active before the first step
+    rc |= up(flags.data(), flags.size() * sizeof(int), (void**)&c->d_load_flags);
+  }
   {
     // obstacle ids by global obstacle index, and each system's first index
     std::vector<int> oid, ooff;
@@ -1848,15 +1956,22 @@ int grains_gpu_set_tuning(grains_gpu_ctx* c, const grains_gpu_tuning* t) {
     // rebuild the cell tables for the new grid; moving obstacles keep their
     // current poses and velocities
     std::vector<ObstacleDev> live(c->h_obs.size());
+    std::vector<int> flags(2 * c->sys.size());
     if (!live.empty()) {
       CK(cudaMemcpyAsync(live.data(), c->d_obs, live.size() * sizeof(ObstacleDev), cudaMemcpyDeviceToHost,
+                         c->stream));
+      CK(cudaMemcpyAsync(flags.data(), c->d_load_flags, flags.size() * sizeof(int), cudaMemcpyDeviceToHost,
                          c->stream));
       CK(cudaStreamSynchronize(c->stream));
     }
     if (int rc = build_tables(c)) return rc;
-    if (!live.empty())
+    if (!live.empty()) {
       CK(cudaMemcpyAsync(c->d_obs, live.data(), live.size() * sizeof(ObstacleDev), cudaMemcpyHostToDevice,
                          c->stream));
+      CK(cudaMemcpyAsync(c->d_load_flags, flags.data(), flags.size() * sizeof(int), cudaMemcpyHostToDevice,
+                         c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+    }
     c->sorted = false;
     c->keys_valid = false;
   }
@@ -1898,6 +2013,7 @@ std::vector<std::pair<void*, size_t>> snapshot_fields(grains_gpu_ctx* c, int cur
       {c->clock, sizeof(double)}};
   if (c->has_basis) f.push_back({b.basis, 9 * n * sizeof(double)});
   if (!c->h_obs.empty()) f.push_back({c->d_obs, c->h_obs.size() * sizeof(ObstacleDev)});
+  if (!c->h_obs.empty()) f.push_back({c->d_load_flags, 2 * c->sys.size() * sizeof(int)});
   return f;
 }
 

@@ -72,8 +72,8 @@ struct ObstacleDev {
   double o[3];   // origin
   double bbc[3], bbe[3];  // world AABB centre / half extent
   double vel[3], omega[3];  // current velocity of the centre and angular velocity (zero until the first move)
-  double ivel[3], iomega[3];  // imposed motion: translation velocity, or angular velocity about rot_center
-  double rot_center[3];
+  int load_first, load_count;  // its imposed motions in the loading table
+  int sys;
   double crust;
   double circ;
   double scaling[3];
@@ -81,6 +81,17 @@ struct ObstacleDev {
   int material;
   int shape;
   int moving;
+};
+
+// One imposed motion of an obstacle (ObstacleImposedVelocity), directions
+// normalised and phases in radians as its XML constructor leaves them
+// (ObstacleImposedVelocity.cpp:60-262)
+struct LoadingDev {
+  int type, has_center;
+  double ts, te;
+  double vel[3], unit[3], omega[3], center[3];
+  double amp, period, phase;
+  double mamp[3], mper[3], mphase[3];
 };
 
 template <typename R>
@@ -137,6 +148,8 @@ struct StepArgs {
   const int* cell_obs_start;  // static obstacle CSR per cell (C+1)
   const int* cell_obs_idx;
   const int* moving_idx;
+  const LoadingDev* loads;    // imposed obstacle motions
+  int* load_flags;            // per system: a loading active over this step, over the previous one
   const LawParams<R>* laws;
   ParticleArrays<R> cur;
   ParticleArrays<R> alt;
@@ -187,9 +200,9 @@ template <typename R>
 int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int include_obstacles, int* out,
                            int cap, unsigned long long* count);
 // moves every moving obstacle over dt (defined in kernels_mixed.cu)
-int launch_obstacle_move(ObstacleDev* obs, const int* moving_idx, int n_moving, const ShapeDev* shapes,
-                         const double* verts, double dt, double* clock, double host_time, int use_host_time,
-                         cudaStream_t s);
+int launch_obstacle_move(ObstacleDev* obs, const int* moving_idx, int n_moving, const LoadingDev* loads,
+                         int* load_flags, int n_sys, const ShapeDev* shapes, const double* verts, double dt,
+                         double* clock, double host_time, int use_host_time, cudaStream_t s);
 // n middle steps of grains_gpu_step in one cooperative launch of `blocks`
 // blocks (persistent_blocks: all resident); bar: 2 zeroed unsigned of grid
 // barrier state, sums: `blocks` ints of scan scratch

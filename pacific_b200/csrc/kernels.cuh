@@ -855,44 +855,112 @@ __global__ void update_dynamic_kernel(StepArgs<R> a, const double* st, const dou
     for (int k = 0; k < 9; ++k) P.basis[9 * (size_t)s + k] = sb[9 * i + k];
 }
 
-// moving obstacles: constant rotation about a centre over one step
-// (ObstacleImposedVelocity ConstantRotation, ObstacleImposedVelocity.cpp:
-// 332-370, 389-455; ObstacleKinematicsVelocity::ImposedMotion, :86-122;
-// SimpleObstacle::Move, SimpleObstacle.cpp:119-170), then the world AABB
-// (Convex::bbox, Convex.cpp:29-41 -> BBox::setValue, BBox.cpp:235-239).
-static __device__ __noinline__ void obstacle_move_one(ObstacleDev& O, const ShapeDev* shapes, const double* verts,
-                                                      double sub) {
-  const V3<double> om = v3<double>(O.iomega[0], O.iomega[1], O.iomega[2]);
+// Imposed motion of one obstacle over the step ending at T
+// (ObstacleKinematicsVelocity::ImposedMotion, ObstacleKinematicsVelocity.cpp:
+// 86-122, with ObstacleImposedVelocity::isActif / isCompleted /
+// translationalMotion / angularMotion / translationalVelocity / angularVelocity,
+// ObstacleImposedVelocity.cpp:306-455), then SimpleObstacle::Move
+// (SimpleObstacle.cpp:119-170): the active loadings' motions add up; an
+// obstacle that did not move keeps its velocities and its box.  Then the
+// world AABB (Convex::bbox, Convex.cpp:29-41 -> BBox::setValue, BBox.cpp:235-239).
+static __device__ V3<double> loading_motion(const LoadingDev& L, double T, double dt, double sub, V3<double> cg) {
+  const double td = xsub(T, dt);
+  const double ti = td < L.ts ? L.ts : td;
+  const double te = T > L.te ? L.te : T;
+  const V3<double> u = v3<double>(L.unit[0], L.unit[1], L.unit[2]);
+  switch (L.type) {
+    case GRAINS_GPU_CONSTANT_TRANSLATION:
+      return v3<double>(L.vel[0] * sub, L.vel[1] * sub, L.vel[2] * sub);
+    case GRAINS_GPU_CRENEL_TRANSLATION:
+      return sc(u, L.amp * (int((0.5 * (ti + te) - L.ts) / L.period) % 2 == 0 ? 1 : -1) * sub);
+    case GRAINS_GPU_SIN_TRANSLATION:
+      return sc(u, (L.amp * L.period / (2. * kPi)) * (cos(2. * kPi * (ti - L.ts) / L.period + L.phase) -
+                                                       cos(2. * kPi * (te - L.ts) / L.period + L.phase)));
+    case GRAINS_GPU_MULTISIN_TRANSLATION: {
+      double m[3];
+      for (int i = 0; i < 3; ++i)
+        m[i] = (L.mamp[i] * L.mper[i] / (2. * kPi)) * (cos(2. * kPi * (ti - L.ts) / L.mper[i] + L.mphase[i]) -
+                                                        cos(2. * kPi * (te - L.ts) / L.mper[i] + L.mphase[i])) *
+               L.unit[i];
+      return v3<double>(m[0], m[1], m[2]);
+    }
+    case GRAINS_GPU_CONSTANT_ROTATION: {
+      if (!L.has_center) return v3<double>(0., 0., 0.);
+      const V3<double> rota = sc(v3<double>(L.omega[0], L.omega[1], L.omega[2]), sub);
+      const double d = norm(rota);
+      Qt<double> q{v3<double>(0., 0., 0.), 1.};
+      if (d != 0.) q = Qt<double>{sc(rota, sin(d / 2.) / d), cos(d / 2.)};
+      const V3<double> rel = cg - v3<double>(L.center[0], L.center[1], L.center[2]);
+      return q_rotate(q, rel) - rel;
+    }
+  }
+  return v3<double>(0., 0., 0.);
+}
+
+static __device__ V3<double> loading_velocity(const LoadingDev& L, double T, double dt, V3<double> cg) {
+  if (T > L.te + dt * 1.e-5) return v3<double>(0., 0., 0.);  // isCompleted
+  const V3<double> u = v3<double>(L.unit[0], L.unit[1], L.unit[2]);
+  switch (L.type) {
+    case GRAINS_GPU_CONSTANT_TRANSLATION:
+      return v3<double>(L.vel[0], L.vel[1], L.vel[2]);
+    case GRAINS_GPU_SIN_TRANSLATION:
+      return sc(u, L.amp * sin(2. * kPi * (T - L.ts) / L.period + L.phase));
+    case GRAINS_GPU_CRENEL_TRANSLATION:
+      return sc(u, L.amp * (int((T - L.ts) / L.period) % 2 == 0 ? 1 : -1));
+    case GRAINS_GPU_MULTISIN_TRANSLATION: {
+      double v[3];
+      for (int i = 0; i < 3; ++i) v[i] = L.mamp[i] * sin(2. * kPi * (T - L.ts) / L.mper[i] + L.mphase[i]) * L.unit[i];
+      return v3<double>(v[0], v[1], v[2]);
+    }
+    case GRAINS_GPU_CONSTANT_ROTATION:
+      return L.has_center ? cross(v3<double>(L.omega[0], L.omega[1], L.omega[2]),
+                                  cg - v3<double>(L.center[0], L.center[1], L.center[2]))
+                          : v3<double>(0., 0., 0.);
+  }
+  return v3<double>(0., 0., 0.);
+}
+
+// ObstacleImposedVelocity::isActif (ObstacleImposedVelocity.cpp:306-315) over [T - dt, T]
+static __device__ __forceinline__ bool loading_active(const LoadingDev& L, double T, double dt, double& sub) {
+  const double td = xsub(T, dt);
+  sub = xsub(T, td);
+  if (td < L.ts) sub = xsub(sub, xsub(L.ts, td));
+  if (L.te < T) sub = xsub(sub, xsub(T, L.te));
+  return sub > dt * 1.e-5;
+}
+
+static __device__ __noinline__ void obstacle_move_one(ObstacleDev& O, const LoadingDev* loads, const ShapeDev* shapes,
+                                                      const double* verts, double T, double dt) {
   const V3<double> cg = v3<double>(O.o[0], O.o[1], O.o[2]);
+  V3<double> depl = v3<double>(0., 0., 0.), rota = depl, vt = depl, vr = depl;
+  for (int k = O.load_first; k < O.load_first + O.load_count; ++k) {
+    const LoadingDev& L = loads[k];
+    double sub;
+    if (!loading_active(L, T, dt, sub)) continue;
+    depl = depl + loading_motion(L, T, dt, sub, cg);
+    const V3<double> om = v3<double>(L.omega[0], L.omega[1], L.omega[2]);
+    if (L.type == GRAINS_GPU_CONSTANT_ROTATION) rota = rota + sc(om, sub);
+    vt = vt + loading_velocity(L, T, dt, cg);
+    if (L.type == GRAINS_GPU_CONSTANT_ROTATION && !(T > L.te + dt * 1.e-5)) vr = vr + om;
+  }
+  const double d = norm(rota);
+  if (!(norm(depl) != 0. || d != 0.)) return;
+  Qt<double> qrot{v3<double>(0., 0., 0.), 1.};
+  if (d != 0.) qrot = Qt<double>{sc(rota, sin(d / 2.) / d), cos(d / 2.)};
+  const Qt<double> qdt = qmul(qrot, Qt<double>{v3<double>(0., 0., 0.), 1.});
   M3 b;
   for (int t = 0; t < 9; ++t) b.m[t] = O.b[t];
-  if (om.x == 0. && om.y == 0. && om.z == 0.) {
-    // ConstantTranslation: velocity x sub-interval, basis unchanged
-    for (int i = 0; i < 3; ++i) {
-      O.o[i] = xadd(O.o[i], xmul(O.ivel[i], sub));
-      O.vel[i] = O.ivel[i];
-      O.omega[i] = 0.;
-    }
-  } else {
-    const V3<double> c = v3<double>(O.rot_center[0], O.rot_center[1], O.rot_center[2]);
-    const V3<double> rota = sc(om, sub);
-    const double d = norm(rota);
-    Qt<double> q{v3<double>(0., 0., 0.), 1.};
-    if (d != 0.) q = Qt<double>{sc(rota, sin(d / 2.) / d), cos(d / 2.)};
-    const V3<double> rel = cg - c;
-    const V3<double> tr = q_rotate(q, rel) - rel;
-    const V3<double> vt = cross(om, cg - c);
-    const Qt<double> qdt = qmul(q, Qt<double>{v3<double>(0., 0., 0.), 1.});
-    O.o[0] = cg.x + tr.x;
-    O.o[1] = cg.y + tr.y;
-    O.o[2] = cg.z + tr.z;
-    mrotate_left(b, qdt);
-    for (int t = 0; t < 9; ++t) O.b[t] = b.m[t];
-    O.vel[0] = vt.x;
-    O.vel[1] = vt.y;
-    O.vel[2] = vt.z;
-    for (int i = 0; i < 3; ++i) O.omega[i] = O.iomega[i];
-  }
+  O.o[0] = cg.x + depl.x;
+  O.o[1] = cg.y + depl.y;
+  O.o[2] = cg.z + depl.z;
+  mrotate_left(b, qdt);
+  for (int t = 0; t < 9; ++t) O.b[t] = b.m[t];
+  O.vel[0] = vt.x;
+  O.vel[1] = vt.y;
+  O.vel[2] = vt.z;
+  O.omega[0] = vr.x;
+  O.omega[1] = vr.y;
+  O.omega[2] = vr.z;
   const ShapeDev& sh = shapes[O.shape];
   LocalBody<double> L{};
   L.type = sh.type;
@@ -919,14 +987,42 @@ static __device__ __noinline__ void obstacle_move_one(ObstacleDev& O, const Shap
 
 // Imposed motion of every moving obstacle over one step, by one block: every
 // thread reads the clock before thread 0 advances it.
+// AllComponents::Move (AllComponents.cpp:168-213): when a loading of a system
+// is active over [T - dt, T], or was over the previous step, the velocities of
+// the system's obstacles are reset (Obstacle::resetKinematics, Obstacle.cpp:
+// 160-167); when one is active, its obstacles move.  Global flags per system:
+// [2 s] active now, [2 s + 1] active over the previous step.
 static __device__ __forceinline__ void obstacle_move_block(ObstacleDev* obs, const int* moving_idx, int n_moving,
+                                                           const LoadingDev* loads, int* flags, int n_sys,
                                                            const ShapeDev* shapes, const double* verts, double dt,
                                                            double* clock, double host_time, int use_host_time) {
   const double T = use_host_time ? host_time : xadd(*clock, dt);
-  const double sub = xsub(T, xsub(T, dt));
   __syncthreads();
   if (threadIdx.x == 0) *clock = T;
-  for (int u = threadIdx.x; u < n_moving; u += blockDim.x) obstacle_move_one(obs[moving_idx[u]], shapes, verts, sub);
+  for (int s = threadIdx.x; s < n_sys; s += blockDim.x) flags[2 * s] = 0;
+  __syncthreads();
+  for (int u = threadIdx.x; u < n_moving; u += blockDim.x) {
+    const ObstacleDev& O = obs[moving_idx[u]];
+    bool any = false;
+    for (int k = O.load_first; k < O.load_first + O.load_count && !any; ++k) {
+      double sub;
+      any = loading_active(loads[k], T, dt, sub);
+    }
+    if (any) flags[2 * O.sys] = 1;
+  }
+  __syncthreads();
+  for (int u = threadIdx.x; u < n_moving; u += blockDim.x) {
+    ObstacleDev& O = obs[moving_idx[u]];
+    const int now = flags[2 * O.sys], before = flags[2 * O.sys + 1];
+    if (now || before)
+      for (int i = 0; i < 3; ++i) {
+        O.vel[i] = 0.;
+        O.omega[i] = 0.;
+      }
+    if (now) obstacle_move_one(O, loads, shapes, verts, T, dt);
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < n_sys; s += blockDim.x) flags[2 * s + 1] = flags[2 * s];
 }
 
 #ifdef GG_DEFINE_SHARED_KERNELS
@@ -936,10 +1032,11 @@ static __device__ __forceinline__ void obstacle_move_block(ObstacleDev* obs, con
 // the sub-interval T - (T - dt) (ObstacleImposedVelocity::isActif, :306-315).
 // With use_host_time the caller gives T directly.  One block: every thread
 // reads the clock before thread 0 advances it.
-__global__ void obstacle_move_kernel(ObstacleDev* obs, const int* moving_idx, int n_moving, const ShapeDev* shapes,
-                                     const double* verts, double dt, double* clock, double host_time,
-                                     int use_host_time) {
-  obstacle_move_block(obs, moving_idx, n_moving, shapes, verts, dt, clock, host_time, use_host_time);
+__global__ void obstacle_move_kernel(ObstacleDev* obs, const int* moving_idx, int n_moving, const LoadingDev* loads,
+                                     int* flags, int n_sys, const ShapeDev* shapes, const double* verts, double dt,
+                                     double* clock, double host_time, int use_host_time) {
+  obstacle_move_block(obs, moving_idx, n_moving, loads, flags, n_sys, shapes, verts, dt, clock, host_time,
+                      use_host_time);
 }
 
 #endif  // GG_DEFINE_SHARED_KERNELS
@@ -1070,12 +1167,12 @@ int launch_zero_kdelta(const StepArgs<R>& a, cudaStream_t s) {
 }
 
 #ifdef GG_DEFINE_SHARED_KERNELS
-int launch_obstacle_move(ObstacleDev* obs, const int* moving_idx, int n_moving, const ShapeDev* shapes,
-                         const double* verts, double dt, double* clock, double host_time, int use_host_time,
-                         cudaStream_t s) {
+int launch_obstacle_move(ObstacleDev* obs, const int* moving_idx, int n_moving, const LoadingDev* loads,
+                         int* load_flags, int n_sys, const ShapeDev* shapes, const double* verts, double dt,
+                         double* clock, double host_time, int use_host_time, cudaStream_t s) {
   if (n_moving <= 0) return 0;
-  obstacle_move_kernel<<<1, 256, 0, s>>>(obs, moving_idx, n_moving, shapes, verts, dt, clock, host_time,
-                                         use_host_time);
+  obstacle_move_kernel<<<1, 256, 0, s>>>(obs, moving_idx, n_moving, loads, load_flags, n_sys, shapes, verts, dt, clock,
+                                         host_time, use_host_time);
   return check_launch();
 }
 #endif
@@ -1222,8 +1319,8 @@ __global__ void __launch_bounds__(kPersistentThreads) persistent_steps_kernel(
     for (int s = tid; s < n; s += nthreads)
       integrate(a, a.cur, a.cur, s, ld3<R>(a.cur.F[s]), ld3<R>(a.cur.T[s]), 1, R(0.5) * dt_r, 1, R(0.5) * dt_r, dt);
     if (blockIdx.x == 0 && n_moving > 0)
-      obstacle_move_block(const_cast<ObstacleDev*>(a.obs), a.moving_idx, n_moving, a.shapes, a.verts, dt, clock, 0.,
-                          0);
+      obstacle_move_block(const_cast<ObstacleDev*>(a.obs), a.moving_idx, n_moving, a.loads, a.load_flags, a.n_sys,
+                          a.shapes, a.verts, dt, clock, 0., 0);
     if (!grid_barrier(bar, status)) return;
   }
 }

@@ -459,6 +459,9 @@ def apply(sim, sc):
             o2["shape"] = ids[o["shape"]]
             obs.append(o2)
         sim.set_obstacles(s, obs)
+        loads = sc.meta.get("loadings")
+        if loads and loads[s]:
+            sim.set_obstacle_loadings(s, loads[s])
     p = dict(sc.particles)
     p["shape"] = np.asarray(ids, np.int32)[np.asarray(p["shape"])]
     sim.upload(p)

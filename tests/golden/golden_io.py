@@ -16,6 +16,9 @@ def scenario_to_npz_dict(sc, prefix="in_"):
                 laws=[[list(l[:3]) + [list(l[3])] for l in ls] for ls in sc.laws],
                 obstacles=[[{k: (list(v) if isinstance(v, (list, tuple, np.ndarray)) else v) for k, v in o.items()}
                             for o in obs] for obs in sc.obstacles])
+    if sc.meta.get("loadings"):
+        spec["loadings"] = [[{k: (list(v) if isinstance(v, (list, tuple, np.ndarray)) else v) for k, v in l.items()}
+                             for l in ls] for ls in sc.meta["loadings"]]
     out = {"spec": np.array(json.dumps(spec))}
     for k in STATIC_KEYS + STATE_KEYS:
         out[prefix + k] = np.asarray(sc.particles[k])
@@ -35,8 +38,11 @@ def scenario_from_npz(z, prefix="in_"):
     doms = [dict(origin=np.array(d["origin"]), size=np.array(d["size"]), cell_size=d["cell_size"],
                  gravity=tuple(d["gravity"])) for d in spec["domains"]]
     laws = [[(l[0], l[1], l[2], l[3]) for l in ls] for ls in spec["laws"]]
-    return S.Scenario(spec["name"], [tuple(s) for s in spec["shapes"]], doms, laws, spec["obstacles"], p,
-                      spec["dt"], spec["n_steps"])
+    sc = S.Scenario(spec["name"], [tuple(s) for s in spec["shapes"]], doms, laws, spec["obstacles"], p,
+                    spec["dt"], spec["n_steps"])
+    if spec.get("loadings"):
+        sc.meta["loadings"] = spec["loadings"]
+    return sc
 
 
 def memory_arrays(mem, prefix):

@@ -39,6 +39,7 @@ CASES = {
                 1500, 3),
     "hertz_dense125": ("hertz(S.dense_cluster(125, seed=5, velocity_sigma=0.1), memory=False)", 10, 30),
     "hertz_memory216_rolling": ("hertz(S.dense_cluster(216, seed=6, velocity_sigma=0.1), memory=True)", 10, 30),
+    "loadings125": ("loaded(S.dense_cluster(125, seed=7, velocity_sigma=0.05))", 10, 18),
 }
 
 
@@ -77,6 +78,33 @@ def hertz(sc, memory):
     else:
         sc.laws = [[(a, b, HERTZ, [Es, 0.8, 0.4, 1.0e-3, Gs]) for a, b, law, prm in sc.laws[0]]]
     sc.dt = 2.0e-6
+    return sc
+
+
+def loaded(sc):
+    """Imposed motions of every kind on the six walls (ids -1..-6 = x, X, y, Y,
+    z, Z), with time windows that open and close during the replayed steps
+    (t = 1e-4 .. 2.8e-4 s): a sinusoidal floor, a crenel on x [1e-4, 3e-4], a
+    multi-sinusoid on y, a translation plus a rotation about its own centre
+    starting at 2e-4 on the top, a rotation about the box centre on X
+    [5e-5, 2.5e-4], and a translation on Y that ends at 2e-4."""
+    from pacific_b200.abi import (CONSTANT_ROTATION, CONSTANT_TRANSLATION, CRENEL_TRANSLATION,
+                                  MULTISIN_TRANSLATION, SIN_TRANSLATION)
+    d = sc.domains[0]
+    centre = list(np.asarray(d["origin"]) + np.asarray(d["size"]) / 2.0)
+    sc.meta["loadings"] = [[
+        dict(obstacle_id=-5, type=SIN_TRANSLATION, vector=(0, 0, 1), amplitude=0.05, period=2e-3, phase_deg=30.0),
+        dict(obstacle_id=-1, type=CRENEL_TRANSLATION, t_start=1e-4, t_end=3e-4, vector=(1, 0, 0), amplitude=0.02,
+             period=5e-5),
+        dict(obstacle_id=-3, type=MULTISIN_TRANSLATION, vector=(1, 1, 0), amplitude=(0.01, 0.02, 0.0),
+             period=(1e-3, 1.3e-3, 1.0), phase_deg=(0.0, 90.0, 0.0)),
+        dict(obstacle_id=-6, type=CONSTANT_TRANSLATION, vector=(0, 0, -0.01)),
+        dict(obstacle_id=-6, type=CONSTANT_ROTATION, t_start=2e-4, vector=(0, 0, 20.0)),
+        dict(obstacle_id=-2, type=CONSTANT_ROTATION, t_start=5e-5, t_end=2.5e-4, vector=(0, 5.0, 0), center=centre),
+        dict(obstacle_id=-4, type=CONSTANT_TRANSLATION, t_end=2e-4, vector=(0, -0.02, 0)),
+    ]]
+    for o in sc.obstacles[0]:
+        o["moving"] = 1
     return sc
 
 
@@ -144,6 +172,8 @@ def replay_case(name):
     if "in_basis" in out:
         out["after_basis"] = d["basis"]
     out.update(G.memory_arrays(sim.contact_memory(), "mem_after_"))
+    if sc.meta.get("loadings"):
+        out["after_obstacles"] = sim.obstacles(0, len(sc.obstacles[0]))
     np.savez_compressed(path, **out)
     print("%s: %d particles, %d contacts, %d candidates" % (name, sc.n, len(out["contact_pairs"]),
                                                            len(out["candidate_pairs"])))

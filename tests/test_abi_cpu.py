@@ -123,3 +123,17 @@ def test_polydisperse_lattice_has_no_initial_overlap():
     if len(pairs):
         d = np.linalg.norm(p["position"][pairs[:, 0]] - p["position"][pairs[:, 1]], axis=1)
         assert np.all(d > p["radius"][pairs[:, 0]] + p["radius"][pairs[:, 1]])
+
+
+def test_obstacle_loadings_are_checked(oracle_lib):
+    from pacific_b200.abi import FP64, GrainsError, SIN_TRANSLATION, Simulation
+    sc = S.dense_cluster(8, seed=0)
+    sim = Simulation(oracle_lib, FP64, max_particles=8)
+    S.apply(sim, sc)
+    sim.set_obstacle_loadings(0, [dict(obstacle_id=-1, type=SIN_TRANSLATION, vector=(1, 0, 0), amplitude=0.1,
+                                       period=1e-3)])
+    with pytest.raises(GrainsError):
+        sim.set_obstacle_loadings(0, [dict(obstacle_id=-99, type=SIN_TRANSLATION, vector=(1, 0, 0))])
+    with pytest.raises(GrainsError):
+        sim.set_obstacle_loadings(0, [dict(obstacle_id=-1, type=17, vector=(1, 0, 0))])
+    sim.close()

@@ -92,3 +92,8 @@ def test_gpu_matches_reference_fixture(oracle_lib, gpu_lib, path, precision):
     else:
         after = z["after_position"]
     assert np.max(np.abs(d["position"] - after)) < (1e-13 if precision == FP64 else 2e-7)
+    if "after_obstacles" in z.files:
+        # imposed obstacle motions: poses (basis, centre) after the steps; the
+        # device's sin / cos may differ from the host's in the last bit
+        poses = sim.obstacles(0, len(sc.obstacles[0]))
+        assert np.max(np.abs(poses - z["after_obstacles"])) < 1e-14

@@ -57,6 +57,8 @@ def test_oracle_matches_reference_fixture(oracle_lib, path):
     assert np.max(np.abs(d["position"] - z["after_position"])) < 1e-14
     assert np.max(np.abs(d["velocity"] - z["after_velocity"])) < 1e-10
     assert np.max(np.abs(d["quaternion"] - z["after_quaternion"])) < 1e-11
+    if "after_obstacles" in z.files:  # imposed obstacle motions (every kind, time windows)
+        assert np.max(np.abs(sim.obstacles(0, len(sc.obstacles[0])) - z["after_obstacles"])) < 1e-15
     assert rel_err(d["force"], z["after_force"], weight) < 1e-8
 
 
@@ -67,8 +69,11 @@ def test_fixtures_exercise_the_path():
     narrowphase, and a rotating drum."""
     names = [os.path.basename(c)[:-4] for c in CASES]
     for n in ["dense125", "dense216_rolling", "poly_box200", "hooke_dense125", "settling_1k", "convex216",
-              "drum300", "hertz_dense125", "hertz_memory216_rolling"]:
+              "drum300", "hertz_dense125", "hertz_memory216_rolling", "loadings125"]:
         assert n in names
+    z = np.load(os.path.join(HERE, "golden", "loadings125.npz"))
+    types = {l["type"] for l in json.loads(str(z["spec"]))["loadings"][0]}
+    assert types == {0, 1, 2, 3, 4}
     for n, law in [("hertz_dense125", 2), ("hertz_memory216_rolling", 3)]:
         z = np.load(os.path.join(HERE, "golden", n + ".npz"))
         assert {l[2] for l in json.loads(str(z["spec"]))["laws"][0]} == {law}
