@@ -227,6 +227,14 @@ int grains_gpu_set_obstacles(grains_gpu_ctx* ctx, int32_t system, int32_t n,
  * fields (as a single loading from 0 on). */
 int grains_gpu_set_obstacle_loadings(grains_gpu_ctx* ctx, int32_t system, int32_t n,
                                      const grains_gpu_obstacle_loading* loadings);
+/* replaces: <CollisionDetectionAlgorithm><CollisionDetection Type="GJK" | "GJK_SV">
+ * (Base/src/Grains.cpp:640-670, GrainsExec::m_colDetGJK_SV): the distance
+ * algorithm of RigidBodyWithCrust::ClosestPoint (RigidBodyWithCrust.cpp:299-312)
+ * for pairs of non-spherical bodies, Johnson's (Convex.cpp:536-627, the
+ * default) or the signed-volume one (GJK_SV.cpp:428-525).  The crust-x10 retry
+ * and the obstacle-cell links use Johnson's, as in the reference. */
+enum grains_gpu_collision_algorithm { GRAINS_GPU_GJK = 0, GRAINS_GPU_GJK_SV = 1 };
+int grains_gpu_set_collision_algorithm(grains_gpu_ctx* ctx, int32_t algorithm);
 /* replaces: LinkedCell::Link(Particle*) for all active particles
  * (LinkedCell.cpp:1330-1365) + AllComponents state upload */
 int grains_gpu_upload_particles(grains_gpu_ctx* ctx, const grains_gpu_particles* p);

@@ -318,6 +318,10 @@ class LinkedCellGPU : public AppCollision {
   void LinkObstacles(const std::vector<grains_gpu_obstacle>& obs, int system = 0) {
     check(grains_gpu_set_obstacles(ctx_.get(), system, (int32_t)obs.size(), obs.data()), ctx_.get());
   }
+  // <CollisionDetection Type="GJK" | "GJK_SV">
+  void setCollisionAlgorithm(int algorithm) {
+    check(grains_gpu_set_collision_algorithm(ctx_.get(), algorithm), ctx_.get());
+  }
   // the <ObstacleLoadings> of the input file (ObstacleImposedVelocity)
   void setObstacleLoadings(const std::vector<grains_gpu_obstacle_loading>& loads, int system = 0) {
     check(grains_gpu_set_obstacle_loadings(ctx_.get(), system, (int32_t)loads.size(), loads.data()), ctx_.get());

@@ -103,6 +103,7 @@ struct grains_gpu_ctx {
   std::map<std::pair<int, int>, std::pair<int, std::vector<double>>> laws;
   std::vector<grains_gpu_obstacle> obs;
   std::vector<grains_gpu_obstacle_loading> loads;  // explicit imposed motions
+  int collision = GRAINS_GPU_GJK;                   // <CollisionDetection Type=...>
   OracleGrains* g = nullptr;
   std::string dir;
   std::string err;
@@ -252,6 +253,12 @@ int grains_ref_set_obstacles(grains_gpu_ctx* c, int32_t system, int32_t n, const
   return 0;
 }
 
+int grains_ref_set_collision_algorithm(grains_gpu_ctx* c, int32_t algorithm) {
+  if (algorithm != GRAINS_GPU_GJK && algorithm != GRAINS_GPU_GJK_SV) return GRAINS_GPU_INVALID_ARGUMENT;
+  c->collision = algorithm;
+  return 0;
+}
+
 int grains_ref_set_obstacle_loadings(grains_gpu_ctx* c, int32_t system, int32_t n,
                                      const grains_gpu_obstacle_loading* l) {
   (void)system;
@@ -313,6 +320,8 @@ int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
       m = std::nextafter(m, m - d.origin[a] < d.size[a] ? 1e300 : -1e300);
     mxyz[a] = m;
   }
+  if (c->collision == GRAINS_GPU_GJK_SV)
+    x << "<CollisionDetectionAlgorithm><CollisionDetection Type=\"GJK_SV\"/></CollisionDetectionAlgorithm>\n";
   x << "<LinkedCell MX=\"" << num(mxyz[0]) << "\" MY=\"" << num(mxyz[1]) << "\" MZ=\"" << num(mxyz[2])
     << "\" CellSizeFactor=\"" << num(d.cell_size / (2. * rmax)) << "\"/>\n";
   x << "<Origin OX=\"" << num(d.origin[0]) << "\" OY=\"" << num(d.origin[1]) << "\" OZ=\"" << num(d.origin[2])

@@ -29,6 +29,7 @@ FP64 = 0
 MIXED = 1
 
 SPHERE, BOX, CYLINDER, POLYHEDRON = 0, 1, 2, 3
+GJK, GJK_SV = 0, 1
 HOOKE, HOOKE_MEMORY, HERTZ, HERTZ_MEMORY = 0, 1, 2, 3
 
 
@@ -128,6 +129,7 @@ _SIGS = {
     "set_contact_law": [_VP, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _P_F64, C.c_int32],
     "set_obstacles": [_VP, C.c_int32, C.c_int32, C.POINTER(Obstacle)],
     "set_obstacle_loadings": [_VP, C.c_int32, C.c_int32, C.POINTER(ObstacleLoading)],
+    "set_collision_algorithm": [_VP, C.c_int32],
     "upload_particles": [_VP, C.POINTER(Particles)],
     "download_particles": [_VP, C.POINTER(Particles)],
     "update_particles": [_VP, C.POINTER(Particles)],
@@ -387,6 +389,10 @@ class Simulation:
             ob.omega[:] = list(o.get("omega", (0.0, 0.0, 0.0)))
             ob.rotation_center[:] = list(o.get("rotation_center", (0.0, 0.0, 0.0)))
         self._check(self.lib.fn["set_obstacles"](self.ctx, system, len(obstacles), arr))
+
+    def set_collision_algorithm(self, algorithm):
+        """GJK (0, Johnson's) or GJK_SV (1, signed volumes) for non-spherical pairs."""
+        self._check(self.lib.fn["set_collision_algorithm"](self.ctx, algorithm))
 
     def set_obstacle_loadings(self, system, loadings):
         """Imposed obstacle motions: dicts with obstacle_id, type, t_start,

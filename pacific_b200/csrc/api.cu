@@ -138,6 +138,7 @@ struct grains_gpu_ctx {
   double graph_dt[4] = {0, 0, 0, 0};
   int64_t steps_done = 0;
   double gjk_tol = kEpsilon;
+  int gjk_sv = 0;  // GrainsExec::m_colDetGJK_SV
   // launch and grid tuning (grains_gpu_set_tuning / grains_gpu_autotune)
   double cell_factor = 1.0;
   int contacts_block = 256;
@@ -539,6 +540,7 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   a.pairs_n = c->pairs_n;
   a.pair_force = c->pair_force;
   a.gjk_tol = c->gjk_tol;
+  a.gjk_sv = c->gjk_sv;
   a.contacts_block = c->contacts_block;
   a.forces_block = c->forces_block;
   return a;
@@ -933,6 +935,14 @@ int grains_gpu_set_obstacles(grains_gpu_ctx* c, int32_t system, int32_t n, const
   c->sys[system].obs.assign(o, o + n);
   c->uploaded = false;
   c->tables_dirty = true;
+  return 0;
+}
+
+int grains_gpu_set_collision_algorithm(grains_gpu_ctx* c, int32_t algorithm) {
+  if (!c) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (algorithm != GRAINS_GPU_GJK && algorithm != GRAINS_GPU_GJK_SV)
+    return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "unknown collision algorithm");
+  c->gjk_sv = algorithm == GRAINS_GPU_GJK_SV ? 1 : 0;
   return 0;
 }
 
@@ -1641,7 +1651,8 @@ int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt)
   // evaluation and leaves its second half kick pending
   if (int rc = first_move(c, dt, *time)) return rc;
   int middle = n_steps - 1;
-  if (c->persistent && middle > 0) {
+  // the persistent kernel carries Johnson's GJK only: the signed-volume one runs from the graphs
+  if (c->persistent && middle > 0 && !(c->gjk_sv && c->has_convex)) {
     if (int rc = persistent_middle_steps(c, middle, dt)) return rc;
     middle = 0;
   }

@@ -172,6 +172,7 @@ struct StepArgs {
   unsigned long long* pairs_n;
   double* pair_force;    // diagnostic: force on the lower id of each contact pair (3 doubles) or null
   double gjk_tol;
+  int gjk_sv;            // the signed-volume GJK for non-spherical pairs
   int contacts_block;    // threads per block of contacts_kernel (<= 256)
   int forces_block;      // threads per block of forces_kernel (<= 128)
 };

@@ -316,6 +316,226 @@ GG_HD GjkResult<T> gjk_distance(const LocalBody<T>& A, const LocalBody<T>& B, T 
   return r;
 }
 
+// ---- the signed-volume GJK ------------------------------------------------------
+// Montanari, Petrinic, Barbieri, "Improving the GJK algorithm for faster and more
+// reliable distance queries between convex objects", ACM TOG 36(3), 2017, in the
+// operation order of GJK_SV.cpp:9-525 (closest_points_GJK_SV, acceleration
+// off): the sub-algorithm compares the signed volumes of the simplex with those
+// where the origin replaces each vertex; a face or edge that does not contain
+// the origin's projection gives way to its best sub-simplex.
+GG_HD bool sv_same_sign(double a, double b) { return !((a > 0) ^ (b > 0)); }
+
+GG_HD double sv_comp(const V3<double>& v, unsigned i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+
+GG_HD void sv_edge(const V3<double> y[4], unsigned& bits, double lam[4]) {  // s1d
+  unsigned i1 = 0xffffffffu, i2 = 0xffffffffu;
+  bool first = false;
+  for (unsigned i = 0; i < 4; ++i)
+    if (bits & (1u << i)) {
+      if (first) {
+        i2 = i;
+        break;
+      }
+      i1 = i;
+      first = true;
+    }
+  const V3<double> t = y[i2] - y[i1];
+  unsigned I = 0;
+  double neg = -t.x;
+  if (fabs(t.y) > fabs(neg)) {
+    I = 1;
+    neg = -t.y;
+  }
+  if (fabs(t.z) > fabs(neg)) {
+    I = 2;
+    neg = -t.z;
+  }
+  const double pI = dot(y[i2], t) / dot(t, t) * neg + sv_comp(y[i2], I);
+  const double C0 = -sv_comp(y[i2], I) + pI, C1 = sv_comp(y[i1], I) - pI;
+  const bool s0 = sv_same_sign(neg, C0), s1 = sv_same_sign(neg, C1);
+  if (s0 && s1) {
+    lam[i1] = C0 / neg;
+    lam[i2] = C1 / neg;
+  } else if (s0) {
+    bits &= ~(1u << i2);
+    lam[i1] = 1.;
+  } else {
+    bits &= ~(1u << i1);
+    lam[i2] = 1.;
+  }
+}
+
+GG_HD void sv_face(const V3<double> y[4], unsigned& bits, double lam[4]) {  // s2d
+  unsigned cnt = 0, i0 = 0, i1 = 0, i2 = 0;
+  for (unsigned i = 0; i < 4; ++i)
+    if (bits & (1u << i)) {
+      if (cnt == 0) i0 = i;
+      else if (cnt == 1) i1 = i;
+      else i2 = i;
+      ++cnt;
+    }
+  const V3<double> n = cross(y[i1] - y[i0], y[i2] - y[i0]);
+  const V3<double> p0 = sc(n, dot(y[i0], n) / dot(n, n));
+  const V3<double>&a = y[i0], &b = y[i1], &c = y[i2];
+  unsigned ix = 1, iy = 2;
+  double mu_max = b.y * c.z + a.y * b.z + c.y * a.z - b.y * a.z - c.y * b.z - a.y * c.z;
+  double mu = b.z * a.x + c.z * b.x + a.z * c.x - b.z * c.x - a.z * b.x - c.z * a.x;
+  if (fabs(mu) > fabs(mu_max)) {
+    mu_max = mu;
+    ix = 0;
+  }
+  mu = b.x * c.y + a.x * b.y + c.x * a.y - b.x * a.y - c.x * b.y - a.x * c.y;
+  if (fabs(mu) > fabs(mu_max)) {
+    mu_max = mu;
+    ix = 0;
+    iy = 1;
+  }
+  const double px = sv_comp(p0, ix), py = sv_comp(p0, iy);
+  const double ax = sv_comp(a, ix), ay = sv_comp(a, iy), bx = sv_comp(b, ix), by = sv_comp(b, iy);
+  const double cx = sv_comp(c, ix), cy = sv_comp(c, iy);
+  double C[3];
+  C[0] = px * by + py * cx + bx * cy - px * cy - py * bx - cx * by;
+  C[1] = px * cy + py * ax + cx * ay - px * ay - py * cx - ax * cy;
+  C[2] = px * ay + py * bx + ax * by - px * by - py * ax - bx * ay;
+  const bool sg[3] = {sv_same_sign(mu_max, C[0]), sv_same_sign(mu_max, C[1]), sv_same_sign(mu_max, C[2])};
+  if (sg[0] && sg[1] && sg[2]) {
+    lam[i0] = C[0] / mu_max;
+    lam[i1] = C[1] / mu_max;
+    lam[i2] = C[2] / mu_max;
+    return;
+  }
+  double d = 1.e9;
+  unsigned nb = 0;
+  const unsigned idx[3] = {i0, i1, i2};
+  for (unsigned j = 0; j < 3; ++j) {
+    if (sg[j]) continue;
+    unsigned used = bits & ~(1u << idx[j]);
+    double nl[4] = {0., 0., 0., 0.};
+    sv_edge(y, used, nl);
+    V3<double> pt = v3<double>(0., 0., 0.);
+    for (unsigned i = 0; i < 4; ++i)
+      if (used & (1u << i)) pt = pt + sc(y[i], nl[i]);
+    const double ds = dot(pt, pt);
+    if (ds < d) {
+      nb = used;
+      d = ds;
+      for (int i = 0; i < 4; ++i) lam[i] = nl[i];
+    }
+  }
+  bits = nb;
+}
+
+GG_HD void sv_tetra(const V3<double> y[4], unsigned& bits, double lam[4]) {  // s3d
+  double C[4];
+  C[0] = y[3].x * y[2].y * y[1].z + y[2].x * y[1].y * y[3].z + y[1].x * y[3].y * y[2].z -
+         y[1].x * y[2].y * y[3].z - y[2].x * y[3].y * y[1].z - y[3].x * y[1].y * y[2].z;
+  C[1] = y[0].x * y[2].y * y[3].z + y[2].x * y[3].y * y[0].z + y[3].x * y[0].y * y[2].z -
+         y[3].x * y[2].y * y[0].z - y[2].x * y[0].y * y[3].z - y[0].x * y[3].y * y[2].z;
+  C[2] = y[3].x * y[1].y * y[0].z + y[1].x * y[0].y * y[3].z + y[0].x * y[3].y * y[1].z -
+         y[0].x * y[1].y * y[3].z - y[1].x * y[3].y * y[0].z - y[3].x * y[0].y * y[1].z;
+  C[3] = y[0].x * y[1].y * y[2].z + y[1].x * y[2].y * y[0].z + y[2].x * y[0].y * y[1].z -
+         y[2].x * y[1].y * y[0].z - y[1].x * y[0].y * y[2].z - y[0].x * y[2].y * y[1].z;
+  const double dM = C[0] + C[1] + C[2] + C[3];
+  bool sg[4];
+  int nsame = 0;
+  for (int i = 0; i < 4; ++i) {
+    sg[i] = sv_same_sign(dM, C[i]);
+    nsame += sg[i] ? 1 : 0;
+  }
+  if (nsame == 4) {
+    for (int i = 0; i < 4; ++i) lam[i] = C[i] / dM;
+    return;
+  }
+  double d = 1.e9;
+  unsigned nb = 0;
+  for (unsigned j = 0; j < 4; ++j) {
+    if (sg[j]) continue;
+    unsigned used = bits & ~(1u << j);
+    double nl[4] = {0., 0., 0., 0.};
+    sv_face(y, used, nl);
+    V3<double> pt = v3<double>(0., 0., 0.);
+    for (unsigned i = 0; i < 4; ++i)
+      if (used & (1u << i)) pt = pt + sc(y[i], nl[i]);
+    const double ds = dot(pt, pt);
+    if (ds < d) {
+      nb = used;
+      d = ds;
+      for (int i = 0; i < 4; ++i) lam[i] = nl[i];
+    }
+  }
+  bits = nb;
+}
+
+GG_HD GjkResult<double> gjk_sv_distance(const LocalBody<double>& A, const LocalBody<double>& B, double rel_error) {
+  unsigned bits = 0, last = 0;
+  V3<double> p[4], q[4], y[4];
+  double lam[4] = {0., 0., 0., 0.};
+  const V3<double> zero = v3<double>(0., 0., 0.);
+  for (int i = 0; i < 4; ++i) p[i] = q[i] = y[i] = zero;
+  const double abs_error = 1.e-4 * rel_error;
+  V3<double> v = lb_apply(A, support_local(A, zero)) - lb_apply(B, support_local(B, zero));
+  V3<double> w = v;
+  double dist = norm(v);
+  int num = 0, exit_reason = 3;
+  double lower = -dist;
+  while (bits < 15 && dist > kEpsilon2 && num < 1000) {
+    ++num;
+    for (unsigned k = 0; k < 4; ++k)
+      if (!(bits & (1u << k))) {
+        last = k;
+        break;
+      }
+    p[last] = support_local(A, lb_vecmat(-v, A));
+    q[last] = support_local(B, lb_vecmat(v, B));
+    w = lb_apply(A, p[last]) - lb_apply(B, q[last]);
+    const double sep = dot(v, w) / dist;
+    if (sep > lower) lower = sep;
+    const double mu = dist - sep;
+    if (mu < dist * rel_error || mu < abs_error) {
+      exit_reason = 0;
+      break;
+    }
+    bool degen = false;
+    for (unsigned i = 0; i < 4; ++i)
+      if ((bits & (1u << i)) && y[i].x == w.x && y[i].y == w.y && y[i].z == w.z) degen = true;
+    if (degen) {
+      exit_reason = 1;
+      break;
+    }
+    y[last] = w;
+    bits |= 1u << last;
+    const int used = (int)((bits & 1u) + ((bits >> 1) & 1u) + ((bits >> 2) & 1u) + ((bits >> 3) & 1u));
+    if (used == 1) {
+      for (unsigned i = 0; i < 4; ++i)
+        if (bits & (1u << i)) lam[i] = 1.;
+    } else if (used == 2) {
+      sv_edge(y, bits, lam);
+    } else if (used == 3) {
+      sv_face(y, bits, lam);
+    } else {
+      sv_tetra(y, bits, lam);
+    }
+    v = zero;
+    for (unsigned i = 0; i < 4; ++i)
+      if (bits & (1u << i)) v = v + sc(y[i], lam[i]);
+    dist = norm(v);
+  }
+  V3<double> pa = zero, pb = zero;
+  for (unsigned i = 0; i < 4; ++i)
+    if (bits & (1u << i)) {
+      pa = pa + sc(p[i], lam[i]);
+      pb = pb + sc(q[i], lam[i]);
+    }
+  GjkResult<double> r;
+  r.pa = lb_apply(A, pa);
+  r.pb = lb_apply(B, pb);
+  r.dist = dist;
+  r.iters = num;
+  r.exit = exit_reason;
+  r.lower = lower;
+  return r;
+}
+
 // RigidBodyWithCrust::ClosestPoint general case (RigidBodyWithCrust.cpp:278-348).
 // status: 0 = features valid, 1 = ContactError, 2 = bounding spheres apart.
 template <typename T>
@@ -347,6 +567,35 @@ GG_HD ContactGeom convex_closest_point_t(const BodyRef& A, const BodyRef& B, dou
   c.point = xadd3(d3(double(pc.x), double(pc.y), double(pc.z)), shift);
   c.overlap_vector = d3(double(ov.x), double(ov.y), double(ov.z));
   c.overlap = distance - crust_sum;
+  c.status = 0;
+  return c;
+}
+
+// RigidBodyWithCrust::ClosestPoint with the signed-volume GJK (the same
+// features as convex_closest_point_t)
+GG_HD ContactGeom convex_closest_point_sv(const BodyRef& A, const BodyRef& B, double tol, int* iters) {
+  ContactGeom c = no_contact();
+  D3 g = xsub3(A.origin, B.origin);
+  if (!(xnorm(g) < xadd(A.radius, B.radius))) {
+    c.status = 2;
+    return c;
+  }
+  LocalBody<double> la = local_body<double>(A, d3(0., 0., 0.), A.scaling);
+  LocalBody<double> lb = local_body<double>(B, d3(0., 0., 0.), B.scaling);
+  GjkResult<double> r = gjk_sv_distance(la, lb, tol);
+  *iters = r.iters;
+  if (r.dist < kEpsilon) {
+    c.status = 1;
+    return c;
+  }
+  V3<double> ba = r.pa - r.pb;
+  V3<double> pc = dv(r.pa, 2.) + dv(r.pb, 2.);
+  double crust_sum = xadd(A.crust, B.crust);
+  V3<double> ov = round3(dv(ba, r.dist));
+  ov = sc(ov, crust_sum - r.dist);
+  c.point = d3(pc.x, pc.y, pc.z);
+  c.overlap_vector = d3(ov.x, ov.y, ov.z);
+  c.overlap = r.dist - crust_sum;
   c.status = 0;
   return c;
 }

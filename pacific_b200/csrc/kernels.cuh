@@ -468,11 +468,12 @@ __device__ __forceinline__ void make_obstacle_ref(const StepArgs<R>& a, int oidx
 // force kernel 3x slower than the double GJK alone on B200 (0.67 vs 0.22 ms
 // per step, 100,000 convex bodies).  Error handling (crust x10) on
 // ContactError.
-template <typename R>
+template <typename R, bool SV = false>
 __device__ ContactGeom convex_closest_point(const StepArgs<R>& a, const BodyRef& A, const BodyRef& B, int& iters,
                                             int& handled) {
   handled = 0;
-  ContactGeom c = convex_closest_point_t<double>(A, B, a.gjk_tol, &iters);
+  ContactGeom c = SV ? convex_closest_point_sv(A, B, a.gjk_tol, &iters)
+                     : convex_closest_point_t<double>(A, B, a.gjk_tol, &iters);
   if (c.status == 1) {
     c = convex_error_handling(A, B, A.lext, B.lext, 10., a.gjk_tol);
     handled = 1;
@@ -593,7 +594,7 @@ __device__ __forceinline__ void flush_force_stats(StatsDev* st, ForceStats& f) {
   }
 }
 
-template <typename R, bool DIAG, bool CONVEX>
+template <typename R, bool DIAG, bool CONVEX, bool SV = false>
 __device__ __forceinline__ void forces_one(const StepArgs<R>& a, int s, R dt, ForceStats& fs) {
   const ParticleArrays<R>& P = a.cur;
   const double4 xi = P.xr[s];
@@ -654,7 +655,7 @@ __device__ __forceinline__ void forces_one(const StepArgs<R>& a, int s, R dt, Fo
           make_body_ref(a, own ? mi.z : mj.z, sa, own ? mdi.y : mdj.y, ba);
           make_body_ref(a, own ? mj.z : mi.z, sbx, own ? mdj.y : mdi.y, bb);
           int it = 0, handled = 0;
-          g = convex_closest_point(a, ba, bb, it, handled);
+          g = convex_closest_point<R, SV>(a, ba, bb, it, handled);
           if (own && g.status != 2) {
             ++ngjk;
             ngjk_it += it;
@@ -760,7 +761,7 @@ __device__ __forceinline__ void forces_one(const StepArgs<R>& a, int s, R dt, Fo
         make_body_ref(a, mi.z, s, mdi.y, ba);
         make_obstacle_ref(a, oidx, bb);
         int it = 0, handled = 0;
-        g = convex_closest_point(a, ba, bb, it, handled);
+        g = convex_closest_point<R, SV>(a, ba, bb, it, handled);
         if (g.status != 2) {
           ++ngjk;
           ngjk_it += it;
@@ -810,11 +811,11 @@ __device__ __forceinline__ void forces_one(const StepArgs<R>& a, int s, R dt, Fo
   a.hist_n_next[oi] = nnext;
 }
 
-template <typename R, bool DIAG, bool CONVEX>
+template <typename R, bool DIAG, bool CONVEX, bool SV = false>
 __global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   ForceStats fs{0, 0, 0, 0, 0, 0., 0.};
-  if (s < a.n) forces_one<R, DIAG, CONVEX>(a, s, dt, fs);
+  if (s < a.n) forces_one<R, DIAG, CONVEX, SV>(a, s, dt, fs);
   flush_force_stats(a.stats, fs);
 }
 
@@ -1145,7 +1146,12 @@ int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int
   if (phases & 1) contacts_kernel<R><<<grid_for(a.n, cb), cb, 0, s>>>(a);
   if (!(phases & 2)) return check_launch();
   const int g = grid_for(a.n, fb);
-  if (a.has_convex) {
+  if (a.has_convex && a.gjk_sv) {  // the signed-volume GJK: a kernel of its own
+    if (diag)
+      forces_kernel<R, true, true, true><<<g, fb, 0, s>>>(a, R(dt));
+    else
+      forces_kernel<R, false, true, true><<<g, fb, 0, s>>>(a, R(dt));
+  } else if (a.has_convex) {
     if (diag)
       forces_kernel<R, true, true><<<g, fb, 0, s>>>(a, R(dt));
     else

@@ -449,6 +449,8 @@ def apply(sim, sc):
     """Registers shapes, domains, laws and obstacles of `sc` on `sim` and
     uploads the particles.  Returns the shape-id map."""
     ids = [sim.add_shape(t, prm) for t, prm in sc.shapes]
+    if sc.meta.get("collision") is not None:
+        sim.set_collision_algorithm(sc.meta["collision"])
     for s, d in enumerate(sc.domains):
         sim.set_domain(s, d["origin"], d["size"], d["cell_size"], d["gravity"])
         for a, b, law, prm in sc.laws[s]:

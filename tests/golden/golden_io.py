@@ -16,6 +16,8 @@ def scenario_to_npz_dict(sc, prefix="in_"):
                 laws=[[list(l[:3]) + [list(l[3])] for l in ls] for ls in sc.laws],
                 obstacles=[[{k: (list(v) if isinstance(v, (list, tuple, np.ndarray)) else v) for k, v in o.items()}
                             for o in obs] for obs in sc.obstacles])
+    if sc.meta.get("collision") is not None:
+        spec["collision"] = sc.meta["collision"]
     if sc.meta.get("loadings"):
         spec["loadings"] = [[{k: (list(v) if isinstance(v, (list, tuple, np.ndarray)) else v) for k, v in l.items()}
                              for l in ls] for ls in sc.meta["loadings"]]
@@ -42,6 +44,8 @@ def scenario_from_npz(z, prefix="in_"):
                     spec["dt"], spec["n_steps"])
     if spec.get("loadings"):
         sc.meta["loadings"] = spec["loadings"]
+    if spec.get("collision") is not None:
+        sc.meta["collision"] = spec["collision"]
     return sc
 
 

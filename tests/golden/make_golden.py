@@ -40,6 +40,8 @@ CASES = {
     "hertz_dense125": ("hertz(S.dense_cluster(125, seed=5, velocity_sigma=0.1), memory=False)", 10, 30),
     "hertz_memory216_rolling": ("hertz(S.dense_cluster(216, seed=6, velocity_sigma=0.1), memory=True)", 10, 30),
     "loadings125": ("loaded(S.dense_cluster(125, seed=7, velocity_sigma=0.05))", 10, 18),
+    "convex216_gjk_sv": ("signed_volumes(S.convex_box(216, seed=8, converge_time=0.004, velocity_sigma=0.05))",
+                         900, 5),
 }
 
 
@@ -105,6 +107,14 @@ def loaded(sc):
     ]]
     for o in sc.obstacles[0]:
         o["moving"] = 1
+    return sc
+
+
+def signed_volumes(sc):
+    """The signed-volume GJK (<CollisionDetection Type="GJK_SV"/>) for the
+    pairs of non-spherical bodies."""
+    from pacific_b200.abi import GJK_SV
+    sc.meta["collision"] = GJK_SV
     return sc
 
 

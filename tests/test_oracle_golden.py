@@ -69,8 +69,10 @@ def test_fixtures_exercise_the_path():
     narrowphase, and a rotating drum."""
     names = [os.path.basename(c)[:-4] for c in CASES]
     for n in ["dense125", "dense216_rolling", "poly_box200", "hooke_dense125", "settling_1k", "convex216",
-              "drum300", "hertz_dense125", "hertz_memory216_rolling", "loadings125"]:
+              "drum300", "hertz_dense125", "hertz_memory216_rolling", "loadings125", "convex216_gjk_sv"]:
         assert n in names
+    z = np.load(os.path.join(HERE, "golden", "convex216_gjk_sv.npz"))
+    assert json.loads(str(z["spec"]))["collision"] == 1  # the signed-volume GJK
     z = np.load(os.path.join(HERE, "golden", "loadings125.npz"))
     types = {l["type"] for l in json.loads(str(z["spec"]))["loadings"][0]}
     assert types == {0, 1, 2, 3, 4}
