@@ -513,27 +513,38 @@ __device__ __forceinline__ void contacts_one(const StepArgs<R>& a, int s, unsign
   }
   int* list = a.clist + (size_t)s * a.clist_cap;
   int cnt = 0;
+  auto test = [&](int p, const double4& xj) {
+    // cheap rejection of far candidates: the squared distance against the
+    // squared radius sum with a 1e-12 relative margin (rounding of either
+    // side is below 1e-15 relative)
+    const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+    const double rs = xi.w + xj.w;
+    if (dx * dx + dy * dy + dz * dz > rs * rs * (1. + 1.e-12)) return;
+    D3 ab;
+    double nab;
+    // |AB| and r_A + r_B are symmetric in IEEE arithmetic, so the test
+    // gives the same bits whichever body is A
+    const double dist = sphere_sphere_overlap(Xi, xi.w, d3(xj.x, xj.y, xj.z), xj.w, &ab, &nab);
+    if (dist < 0. && p != s) {
+      if (cnt < a.clist_cap) list[cnt] = p;
+      ++cnt;
+    }
+  };
 #pragma unroll
   for (int r = 0; r < 9; ++r) {
     ncand += (unsigned long long)(r1[r] - r0[r]);
-    for (int t = r0[r]; t < r1[r]; ++t) {
-      const int p = a.perm[t];  // cell slot -> particle (identity right after a gather)
-      const double4 xj = P.xr[p];
-      // cheap rejection of far candidates: the squared distance against the
-      // squared radius sum with a 1e-12 relative margin (rounding of either
-      // side is below 1e-15 relative)
-      const double dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-      const double rs = xi.w + xj.w;
-      if (dx * dx + dy * dy + dz * dz > rs * rs * (1. + 1.e-12)) continue;
-      D3 ab;
-      double nab;
-      // |AB| and r_A + r_B are symmetric in IEEE arithmetic, so the test
-      // gives the same bits whichever body is A
-      const double dist = sphere_sphere_overlap(Xi, xi.w, d3(xj.x, xj.y, xj.z), xj.w, &ab, &nab);
-      if (dist < 0. && p != s) {
-        if (cnt < a.clist_cap) list[cnt] = p;
-        ++cnt;
-      }
+    // two candidates per iteration: their permutation and position loads are
+    // in flight together (the list order stays the slot order)
+    int t = r0[r];
+    for (; t + 1 < r1[r]; t += 2) {
+      const int pa = a.perm[t], pb = a.perm[t + 1];  // cell slot -> particle
+      const double4 xa = P.xr[pa], xb = P.xr[pb];
+      test(pa, xa);
+      test(pb, xb);
+    }
+    if (t < r1[r]) {
+      const int pa = a.perm[t];
+      test(pa, P.xr[pa]);
     }
   }
   if (cnt > a.clist_cap) {
