@@ -626,8 +626,10 @@ __device__ __forceinline__ void forces_one(const StepArgs<R>& a, int s, R dt, Fo
                      &ngjk = fs.ngjk, &ngjk_it = fs.ngjk_it;
   double &ov_max = fs.ov_max, &ov_sum = fs.ov_sum;
 
-  int ci, cj, ck;
-  cell_of(S, xi.x, xi.y, xi.z, ci, cj, ck);
+  // the particle's cell from the key of the current positions (the kick
+  // computed it with cell_of): no divisions here
+  const int local = (int)P.key[s] - S.cell_offset;
+  const int ci = local % S.nbi, ck = (local / S.nbi) % S.nbk, cj = local / (S.nbi * S.nbk);
 
   {
     const int nlist = a.ccount[s];
