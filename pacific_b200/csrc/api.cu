@@ -2165,7 +2165,7 @@ int grains_gpu_autotune(grains_gpu_ctx* c, double time, double dt, int32_t trial
 }  // extern "C"
 
 namespace gg {
-int launches_per_middle_step() { return 9; }
+int launches_per_middle_step() { return 8; }
 
 int context_view(grains_gpu_ctx* c, ContextView* v, std::string& err) {
   if (!c || !v) return GRAINS_GPU_INVALID_ARGUMENT;

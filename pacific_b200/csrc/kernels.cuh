@@ -7,7 +7,7 @@
 //   kick_move      second half kick of the previous step (when pending),
 //                  first half kick + drift + rotation (SecondOrderLeapFrog),
 //                  new cell key and per-cell count (fire-and-forget atomic)
-//   scan x3        exclusive scan of the per-cell counts -> cell ranges
+//   scan x2        exclusive scan of the per-cell counts -> cell ranges
 //   scatter        slot = atomic fill cursor of the cell
 //   cell_sort      each cell's particles ordered by id (deterministic order)
 //   gather         every per-particle array permuted into the new order
@@ -232,33 +232,31 @@ static __global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(const i
   if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
 }
 
-static __global__ void __launch_bounds__(kScanThreads) scan_block_sums_kernel(int* block_sums, int nb, int* out, int n) {
-  // single block: exclusive scan of up to kScanTile block sums
-  int base = threadIdx.x * kScanItems;
-  int vals[kScanItems];
-  int sum = 0;
+// finishes the scan and sets each cell's fill cursor to its start.  A block
+// of 256 cells lies in one tile; it sums the totals of the tiles before its
+// own itself (at most kScanTile of them), so that the tile totals need no
+// scan of their own.  The cell of index n - 1 also writes the grand total.
+constexpr int kScanAddThreads = 256;
+static_assert(kScanTile % kScanAddThreads == 0, "a scan-add block must lie in one tile");
+static __global__ void __launch_bounds__(kScanAddThreads)
+    scan_finish_kernel(int* out, int* cursor, const int* block_sums, const int* counts, int n) {
+  __shared__ int warp_part[kScanAddThreads / 32];
+  const int i = blockIdx.x * kScanAddThreads + threadIdx.x;
+  const int tile = (blockIdx.x * kScanAddThreads) / kScanTile;
+  int part = 0;
+  for (int b = threadIdx.x; b < tile; b += kScanAddThreads) part += block_sums[b];
 #pragma unroll
-  for (int t = 0; t < kScanItems; ++t) {
-    vals[t] = (base + t < nb) ? block_sums[base + t] : 0;
-    sum += vals[t];
-  }
-  int total;
-  int pre = block_exclusive_scan(sum, &total);
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+  if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = part;
+  __syncthreads();
+  int prefix = 0;
 #pragma unroll
-  for (int t = 0; t < kScanItems; ++t) {
-    if (base + t < nb) block_sums[base + t] = pre;
-    pre += vals[t];
-  }
-  if (threadIdx.x == 0) out[n] = total;
-}
-
-// finishes the scan and sets each cell's fill cursor to its start
-static __global__ void scan_add_kernel(int* out, int* cursor, const int* block_sums, int n) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int w = 0; w < kScanAddThreads / 32; ++w) prefix += warp_part[w];
   if (i < n) {
-    const int v = out[i] + block_sums[i / kScanTile];
+    const int v = out[i] + prefix;
     out[i] = v;
     cursor[i] = v;
+    if (i == n - 1) out[n] = v + counts[i];
   }
 }
 
@@ -1143,8 +1141,8 @@ int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather, int
   const int C = a.n_cells;
   const int nb = grid_for(C, kScanTile);
   scan_tiles_kernel<<<nb, kScanThreads, 0, s>>>(a.cell_count, a.cell_start, a.block_sums, C);
-  scan_block_sums_kernel<<<1, kScanThreads, 0, s>>>(a.block_sums, nb, a.cell_start, C);
-  scan_add_kernel<<<grid_for(C, 256), 256, 0, s>>>(a.cell_start, a.cell_cursor, a.block_sums, C);
+  scan_finish_kernel<<<grid_for(C, kScanAddThreads), kScanAddThreads, 0, s>>>(a.cell_start, a.cell_cursor,
+                                                                             a.block_sums, a.cell_count, C);
   if (a.n > 0) scatter_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
   cell_sort_kernel<R><<<grid_for(C, 256), 256, 0, s>>>(a);
   if (a.n > 0 && gather) gather_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, gather_forces);
