@@ -43,6 +43,7 @@ extern "C" {
 #define GRAINS_GPU_NOT_READY          (1 << 8) /* call order violated (e.g. step before upload) */
 #define GRAINS_GPU_GJK_NOT_CONVERGED  (1 << 9) /* GJK hit its iteration cap (Convex.cpp:566) */
 #define GRAINS_GPU_CONTACT_HANDLED    (1 << 10) /* informational: a contact went through the crust x10 retry */
+#define GRAINS_GPU_CELL_TOO_SMALL     (1 << 11) /* a sphere's diameter exceeds the cell edge: contacts may be missed */
 
 /* ---- enumerations ------------------------------------------------------- */
 enum grains_gpu_precision {
@@ -369,19 +370,28 @@ int grains_gpu_launches_per_step(grains_gpu_ctx* ctx, int64_t* launches);
  *   position (3n doubles), radius (n doubles): device arrays, current device
  *   pairs: device, 2*cap int32; *n_pairs (device int64) = pairs found (may
  *     exceed cap: only cap are written); *status (device int32) = status bits
- *     of this call (GRAINS_GPU_OUT_OF_GRID for a sphere outside the grid)
+ *     of this call: GRAINS_GPU_OUT_OF_GRID for a sphere outside the grid,
+ *     GRAINS_GPU_CELL_TOO_SMALL when a sphere's diameter exceeds the smallest
+ *     cell edge (only the 27 surrounding cells are searched, so contacts may
+ *     then be missed: pass a cell_size of at least the largest diameter)
  *   stream: cudaStream_t (NULL = legacy default stream); the call is
  *     asynchronous on it.
- * Limits: n <= 65,536 spheres and at most 262,144 cells; larger inputs return
- * GRAINS_GPU_INVALID_ARGUMENT without launching anything.  The scratch (about
- * 11.5 MB) is a file-scope device array present on every GPU that loads the
- * library until the process exits; every call on a device shares it, so calls
- * that overlap on the GPU (different streams, or several host threads) race
- * and must be serialised by the caller.  The first call on a device looks up
- * the array's device address (cudaGetSymbolAddress); make that first call
- * before any stream capture.  No cudaMalloc, cudaFree or allocating library
- * routine is called.  Nothing has to start at zero: each call clears *n_pairs,
- * *status and the part of the scratch it uses before it writes them. */
+ * Only the set of pairs is defined: their order in `pairs` comes from device
+ * atomics and changes from call to call.
+ * Limits: n <= 65,536 spheres and at most 262,144 cells; larger inputs, and
+ * non-finite or non-positive sizes, return GRAINS_GPU_INVALID_ARGUMENT without
+ * launching anything.  The scratch (4,980,752 bytes, about 5.0 MB) is a
+ * file-scope device array present on every GPU that loads the library until
+ * the process exits; every call on a device shares it, so calls that overlap
+ * on the GPU (different streams, or several host threads) race and must be
+ * serialised by the caller.  A call outside a stream capture looks up the
+ * array's device address (cudaGetSymbolAddress); a call inside a capture uses
+ * the address the last call outside one found, so make a first call on each
+ * device before any stream capture (a first call inside one returns
+ * GRAINS_GPU_NOT_READY), and again after a cudaDeviceReset.  No cudaMalloc,
+ * cudaFree or allocating library routine is called.  Nothing has to start at
+ * zero: each call clears *n_pairs, *status and the part of the scratch it uses
+ * before it writes them. */
 int grains_gpu_sphere_contacts_noalloc(int32_t n, const double* position, const double* radius,
                                        const double origin[3], const double size[3], double cell_size,
                                        int32_t* pairs, int64_t cap, int64_t* n_pairs, int32_t* status,

@@ -24,6 +24,7 @@ INVALID_ARGUMENT = 1 << 7
 NOT_READY = 1 << 8
 GJK_NOT_CONVERGED = 1 << 9
 CONTACT_HANDLED = 1 << 10
+CELL_TOO_SMALL = 1 << 11
 
 FP64 = 0
 MIXED = 1

@@ -1839,7 +1839,8 @@ int grains_gpu_reset_stats(grains_gpu_ctx* c) {
 
 int grains_gpu_launches_per_step(grains_gpu_ctx* c, int64_t* launches) {
   if (!c || !launches) return GRAINS_GPU_INVALID_ARGUMENT;
-  // middle steps: scan (3), scatter, cell_sort, gather, contacts, forces, kick_move
+  // middle steps: scan (2: scan_tiles, scan_finish), scatter, cell_sort,
+  // gather, contacts, forces, kick_move
   *launches = launches_per_middle_step();
   return 0;
 }

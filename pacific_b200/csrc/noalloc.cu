@@ -6,15 +6,20 @@
 // whose overlap distance |x_j - x_i| - (r_i + r_j) is negative, with the same
 // double-precision rounding as the context-based path.  All of its scratch
 // (cell counts and ranges, the cell-sorted copy of the spheres) lives in the
-// file-scope device arrays below, sized for at most kMaxSpheres spheres and
+// file-scope device array below, sized for at most kMaxSpheres spheres and
 // kMaxCells cells; the caller passes only its inputs and outputs.
 //
 // It exists for callers that cannot call cudaMalloc: code running inside a
 // stream capture that must not allocate, real-time loops where cudaMalloc's
 // implicit device synchronisation is not acceptable, and hosts (a fluid solver
 // coupling, a memory-budgeted service) that own every byte of device memory
-// through their own pool.  The arrays take about 11.5 MB on every GPU that
-// loads the library, for as long as the process lives.
+// through their own pool.  The array takes sizeof(NoallocScratch) =
+// 4,980,752 bytes (about 5.0 MB) on every GPU that loads the library, for as
+// long as the process lives.
+//
+// Only the SET of output pairs is defined: the slot of each pair comes from an
+// atomic counter, and the order of spheres inside a cell from atomic ranks, so
+// the order of the pairs changes from call to call.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -38,6 +43,7 @@ struct NoallocScratch {
   int perm[kMaxSpheres];        // sorted slot -> input index
   double4 sorted[kMaxSpheres];  // (x, y, z, r) in cell order
 };
+static_assert(sizeof(NoallocScratch) == 4980752, "documented scratch size");
 
 // Shared by every call on a device; keeps the last call's contents.
 static __device__ __align__(256) NoallocScratch g_noalloc_scratch;
@@ -71,11 +77,17 @@ __global__ void noalloc_clear(NoallocScratch* sc, int n_cells, unsigned long lon
   }
 }
 
-__global__ void noalloc_bin(NoallocScratch* sc, Grid g, int n, const double* pos, int* status) {
+// Bins sphere s.  Only the 27 cells around a sphere are searched, which finds
+// every contact when no two touching spheres are more than one cell apart,
+// i.e. when the smallest cell edge is at least the largest diameter: a sphere
+// whose diameter exceeds it sets GRAINS_GPU_CELL_TOO_SMALL.
+__global__ void noalloc_bin(NoallocScratch* sc, Grid g, int n, const double* pos, const double* radius,
+                            int* status) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= n) return;
   int i, j, k;
   if (!grid_cell(g, pos[3 * s], pos[3 * s + 1], pos[3 * s + 2], i, j, k)) atomicOr(status, GRAINS_GPU_OUT_OF_GRID);
+  if (2. * radius[s] > fmin(g.ex, fmin(g.ey, g.ez))) atomicOr(status, GRAINS_GPU_CELL_TOO_SMALL);
   const unsigned key = (unsigned)grid_index(g, i, j, k);
   sc->key[s] = key;
   sc->rank[s] = (unsigned)atomicAdd(&sc->cell_count[key], 1);
@@ -155,14 +167,23 @@ __global__ void __launch_bounds__(256) noalloc_contacts(NoallocScratch* sc, Grid
   }
 }
 
-// device address of the scratch, looked up once per device
+// Device address of the scratch, per device.  It is looked up again on every
+// call whose stream is not being captured (the lookup is cheap then), so a new
+// primary context after a cudaDeviceReset gets its own address; a call inside
+// a stream capture uses the address of the last call outside one.
 std::mutex g_addr_mutex;
 NoallocScratch* g_addr[128] = {nullptr};
 
-int scratch_address(int device, NoallocScratch** out) {
+int scratch_address(int device, cudaStream_t st, NoallocScratch** out) {
   if (device < 0 || device >= 128) return GRAINS_GPU_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(g_addr_mutex);
-  if (!g_addr[device]) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusActive;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+    cudaGetLastError();  // treat an unanswered query as a capture
+    cap = cudaStreamCaptureStatusActive;
+  }
+  if (cap == cudaStreamCaptureStatusNone || !g_addr[device]) {
+    if (cap != cudaStreamCaptureStatusNone) return GRAINS_GPU_NOT_READY;  // first call inside a capture
     void* p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess) return GRAINS_GPU_CUDA_ERROR;
     g_addr[device] = (NoallocScratch*)p;
@@ -184,32 +205,38 @@ extern "C" int grains_gpu_sphere_contacts_noalloc(int32_t n, const double* posit
   g.ox = origin[0];
   g.oy = origin[1];
   g.oz = origin[2];
-  // the linked-cell grid of LinkedCell::set (LinkedCell.cpp:69-98)
+  // the linked-cell grid of LinkedCell::set (LinkedCell.cpp:69-98); the cell
+  // counts are checked as doubles before any conversion to int
+  if (!(cell_size >= 0.) || !std::isfinite(cell_size)) return GRAINS_GPU_INVALID_ARGUMENT;
   double ext[3];
   int nb[3];
   for (int a = 0; a < 3; ++a) {
-    if (!(size[a] > 0.)) return GRAINS_GPU_INVALID_ARGUMENT;
-    nb[a] = cell_size > gg::kEpsilon ? (int)((size[a] + gg::kEpsilon) / cell_size) : 1;
+    if (!(size[a] > 0.) || !std::isfinite(size[a]) || !std::isfinite(origin[a])) return GRAINS_GPU_INVALID_ARGUMENT;
+    const double q = cell_size > gg::kEpsilon ? (size[a] + gg::kEpsilon) / cell_size : 1.;
+    if (!(q < (double)kMaxCells + 1.)) return GRAINS_GPU_INVALID_ARGUMENT;
+    nb[a] = (int)q;
     if (!nb[a]) nb[a] = 1;
     ext[a] = size[a] / nb[a];
   }
-  if ((long long)nb[0] * nb[1] * nb[2] > kMaxCells) return GRAINS_GPU_INVALID_ARGUMENT;
+  const long long cells = (long long)nb[0] * nb[1] * nb[2];
+  if (cells <= 0 || cells > kMaxCells) return GRAINS_GPU_INVALID_ARGUMENT;
   g.ex = ext[0];
   g.ey = ext[1];
   g.ez = ext[2];
   g.nbi = nb[0];
   g.nbj = nb[1];
   g.nbk = nb[2];
-  const int n_cells = nb[0] * nb[1] * nb[2];
+  const int n_cells = (int)cells;
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess) return GRAINS_GPU_CUDA_ERROR;
   NoallocScratch* sc = nullptr;
-  if (int rc = scratch_address(device, &sc)) return rc;
   cudaStream_t st = (cudaStream_t)stream;
+  if (int rc = scratch_address(device, st, &sc)) return rc;
   unsigned long long* cnt = (unsigned long long*)n_pairs;
   noalloc_clear<<<(n_cells + 255) / 256, 256, 0, st>>>(sc, n_cells, cnt, status);
+  if (cudaPeekAtLastError() != cudaSuccess) return GRAINS_GPU_CUDA_ERROR;
   if (n > 0) {
-    noalloc_bin<<<(n + 255) / 256, 256, 0, st>>>(sc, g, n, position, status);
+    noalloc_bin<<<(n + 255) / 256, 256, 0, st>>>(sc, g, n, position, radius, status);
     noalloc_scan<<<1, kScanThreads, 0, st>>>(sc, n_cells);
     noalloc_scatter<<<(n + 255) / 256, 256, 0, st>>>(sc, n, position, radius, status);
     noalloc_contacts<<<(n + 255) / 256, 256, 0, st>>>(sc, g, n, pairs, (long long)cap, cnt);

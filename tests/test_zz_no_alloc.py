@@ -25,7 +25,7 @@ from helpers import make, pair_set
 pytestmark = pytest.mark.gpu
 
 
-def noalloc_pairs(lib, sc, position, torch):
+def noalloc_pairs(lib, sc, position, torch, cell_size=None, expect_status=0):
     fn = lib.dll.grains_gpu_sphere_contacts_noalloc
     fn.restype = C.c_int
     fn.argtypes = [C.c_int32, C.c_void_p, C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
@@ -42,13 +42,14 @@ def noalloc_pairs(lib, sc, position, torch):
     origin = (C.c_double * 3)(*[float(x) for x in d["origin"]])
     size = (C.c_double * 3)(*[float(x) for x in d["size"]])
     stream = torch.cuda.current_stream(dev)
-    rc = fn(n, pos.data_ptr(), rad.data_ptr(), origin, size, float(d["cell_size"]), pairs.data_ptr(), cap,
+    cs = float(d["cell_size"]) if cell_size is None else cell_size
+    rc = fn(n, pos.data_ptr(), rad.data_ptr(), origin, size, cs, pairs.data_ptr(), cap,
             count.data_ptr(), status.data_ptr(), stream.cuda_stream)
     assert rc == 0
     torch.cuda.synchronize()
     k = int(count.item())
     assert 0 < k <= cap
-    assert int(status.item()) == 0
+    assert int(status.item()) == expect_status
     return pairs[: 2 * k].cpu().numpy().reshape(-1, 2)
 
 
@@ -83,3 +84,22 @@ def test_noalloc_rejects_oversized_input(gpu_lib):
     assert rc != 0
     rc = fn(C.c_int32(10), dummy, dummy, origin, size, C.c_double(1e-3), dummy, C.c_int64(1), dummy, dummy, None)
     assert rc != 0  # 1e9 cells > 262,144
+    # a cell count per axis above INT_MAX must be rejected before any
+    # conversion to int (it would wrap to a negative product of counts)
+    long_size = (C.c_double * 3)(1e4, 1e-6, 1e-6)
+    rc = fn(C.c_int32(10), dummy, dummy, origin, long_size, C.c_double(1e-6), dummy, C.c_int64(1), dummy, dummy,
+            None)
+    assert rc != 0
+    for bad in [float("nan"), float("inf"), -1.0]:
+        rc = fn(C.c_int32(10), dummy, dummy, origin, size, C.c_double(bad), dummy, C.c_int64(1), dummy, dummy, None)
+        assert rc != 0
+
+
+def test_noalloc_flags_cells_smaller_than_a_diameter(gpu_lib):
+    """A cell edge below the largest diameter can hide contacts two cells
+    apart: the call still runs and reports GRAINS_GPU_CELL_TOO_SMALL."""
+    torch = pytest.importorskip("torch")
+    from pacific_b200.abi import CELL_TOO_SMALL
+    sc = S.dense_cluster(343, seed=3, velocity_sigma=0.2)
+    r_max = float(np.max(sc.particles["radius"]))
+    noalloc_pairs(gpu_lib, sc, sc.particles["position"], torch, cell_size=1.0 * r_max, expect_status=CELL_TOO_SMALL)
