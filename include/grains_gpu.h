@@ -175,6 +175,9 @@ typedef struct grains_gpu_contact_memory {
   double*  kdelta;       /* 3n */
   double*  prev_normal;  /* 3n */
   double*  spring_torque;/* 3n */
+  int32_t* system;       /* n: the system of each entry (ids are per system); may be
+                            NULL: the download then omits it and an upload puts each
+                            entry in the first system that has its owner id */
 } grains_gpu_contact_memory;
 
 /* Counters and overlap statistics accumulate over the force evaluations since
@@ -289,11 +292,12 @@ int grains_gpu_synchronize(grains_gpu_ctx* ctx);
  * cap, then GRAINS_GPU_PAIR_OVERFLOW). */
 int grains_gpu_get_candidate_pairs(grains_gpu_ctx* ctx, int32_t system, int32_t include_obstacles,
                                    int64_t cap, int32_t* pairs, int64_t* n);
-/* Contact pairs (overlap distance < 0) of the last force evaluation, same layout. */
+/* Contact pairs (overlap distance < 0) of system `system` in the last force
+ * evaluation of grains_gpu_compute_forces, same layout (ids are per system). */
 int grains_gpu_get_contact_pairs(grains_gpu_ctx* ctx, int32_t system, int64_t cap,
                                  int32_t* pairs, int64_t* n);
-/* Contact pairs of the last force evaluation of grains_gpu_compute_forces
- * with the contact force (delFN + delFT of the contact law) on the lower id of
+/* Contact pairs of system `system` in the last force evaluation of
+ * grains_gpu_compute_forces with the contact force (delFN + delFT of the contact law) on the lower id of
  * each: forces[3k..3k+2] for pairs[2k], pairs[2k+1], same order as
  * grains_gpu_get_contact_pairs.  The reference applies the same force at the
  * contact point through Component::addForce (Component.cpp:67-71) inside
@@ -313,9 +317,11 @@ int grains_gpu_reset_stats(grains_gpu_ctx* ctx);
  *                  (a diagnostic) follow the grid.
  *   contacts_block threads per block of the broadphase kernel (32 .. 256)
  *   forces_block   threads per block of the contact-law kernel (32 .. 128)
- *   list_capacity  contact-list slots per particle (8 .. 256; 0 = 32 for
- *                  spheres, 64 when other shapes are present); a particle
- *                  with more contacts fails the step with GRAINS_GPU_PAIR_OVERFLOW
+ *   list_capacity  contact-list slots per particle (8 .. 256, a multiple
+ *                  of 4; 0 = 32 for spheres, 64 when other shapes are
+ *                  present): contacting particles and candidate obstacles of
+ *                  a force evaluation; a particle with more fails the step
+ *                  with GRAINS_GPU_PAIR_OVERFLOW
  *   gather_every   steps between two permutations of the particle arrays
  *                  into cell order (1 .. 64); in between the cell lists are
  *                  rebuilt every step and reached through a permutation.

@@ -109,7 +109,7 @@ class Particles(C.Structure):
 
 class ContactMemory(C.Structure):
     _fields_ = [("n", C.c_int64), ("owner", _P_I32), ("other", _P_I32), ("kdelta", _P_F64),
-                ("prev_normal", _P_F64), ("spring_torque", _P_F64)]
+                ("prev_normal", _P_F64), ("spring_torque", _P_F64), ("system", _P_I32)]
 
 
 class Stats(C.Structure):
@@ -486,20 +486,23 @@ class Simulation:
         m.n = n
         m.owner, m.other = _ptr(owner, C.c_int32), _ptr(other, C.c_int32)
         m.kdelta, m.prev_normal, m.spring_torque = _ptr(kd, C.c_double), _ptr(pn, C.c_double), _ptr(sp, C.c_double)
+        sy = i32(mem["system"]) if mem.get("system") is not None else None
+        m.system = _ptr(sy, C.c_int32) if sy is not None else None
         self._check(self.lib.fn["upload_contact_memory"](self.ctx, C.byref(m)))
 
     def contact_memory(self, cap=None):
         cap = cap or max(64, 32 * self.n)
-        owner, other = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
+        owner, other, sy = np.zeros(cap, np.int32), np.zeros(cap, np.int32), np.zeros(cap, np.int32)
         kd, pn, sp = np.zeros((cap, 3)), np.zeros((cap, 3)), np.zeros((cap, 3))
         m = ContactMemory()
         m.n = cap
         m.owner, m.other = _ptr(owner, C.c_int32), _ptr(other, C.c_int32)
         m.kdelta, m.prev_normal, m.spring_torque = _ptr(kd, C.c_double), _ptr(pn, C.c_double), _ptr(sp, C.c_double)
+        m.system = _ptr(sy, C.c_int32)
         self._check(self.lib.fn["download_contact_memory"](self.ctx, C.byref(m)))
         k = m.n
         return {"owner": owner[:k], "other": other[:k], "kdelta": kd[:k], "prev_normal": pn[:k],
-                "spring_torque": sp[:k]}
+                "spring_torque": sp[:k], "system": sy[:k]}
 
     def obstacles(self, system, n):
         """Poses of the first n obstacles of `system` after their imposed

@@ -112,12 +112,17 @@ struct grains_gpu_ctx {
   double* clock = nullptr;  // the reference's m_time, advanced by the obstacle moves
   int* clist = nullptr;   // contact lists (scratch of the force evaluation)
   int* ccount = nullptr;
+  void* res_f = nullptr;  // per list entry: force and contact flag, torque (R4 each)
+  void* res_t = nullptr;
+  int2* work = nullptr;   // owned list entries of an evaluation
+  int* work_n = nullptr;
   int clist_cap = 0;
   int64_t clist_alloc = 0;
   int* pairs = nullptr;  // contact pairs of the last compute_forces (diagnostic)
   int pairs_cap = 0;
   unsigned long long* pairs_n = nullptr;
   double* pair_force = nullptr;  // force on the lower id of each diagnostic contact pair
+  int* pair_sys = nullptr;       // system of each diagnostic contact pair
   int* cand = nullptr;   // candidate pairs (diagnostic, separate from the contact pairs)
   int cand_cap = 0;
   unsigned long long* cand_n = nullptr;
@@ -535,10 +540,15 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   a.clist = c->clist;
   a.ccount = c->ccount;
   a.clist_cap = c->clist_cap;
+  a.res_f = (typename Vec4<R>::type*)c->res_f;
+  a.res_t = (typename Vec4<R>::type*)c->res_t;
+  a.work = c->work;
+  a.work_n = c->work_n;
   a.pairs = c->pairs;
   a.pairs_cap = c->pairs_cap;
   a.pairs_n = c->pairs_n;
   a.pair_force = c->pair_force;
+  a.pair_sys = c->pair_sys;
   a.gjk_tol = c->gjk_tol;
   a.gjk_sv = c->gjk_sv;
   a.contacts_block = c->contacts_block;
@@ -712,6 +722,38 @@ int last_step(grains_gpu_ctx* c, double dt) {
   return 0;
 }
 
+// Contact-list scratch for cap_per entries per particle: the lists, the
+// result of each entry (two R4) and the work items; grown, never shrunk.
+int ensure_lists(grains_gpu_ctx* c, int cap_per) {
+  const int64_t need = (int64_t)c->cap * cap_per;
+  if (need > c->clist_alloc) {
+    for (void** p : {(void**)&c->clist, &c->res_f, &c->res_t, (void**)&c->work})
+      if (*p) {
+        cudaFree(*p);
+        *p = nullptr;
+      }
+    c->clist_alloc = 0;
+    const size_t r4 = 4 * c->rsize;
+    void* q = nullptr;
+    CK(cudaMalloc(&q, (size_t)need * sizeof(int)));
+    c->clist = (int*)q;
+    CK(cudaMalloc(&q, (size_t)need * r4));
+    c->res_f = q;
+    CK(cudaMalloc(&q, (size_t)need * r4));
+    c->res_t = q;
+    CK(cudaMalloc(&q, (size_t)need * sizeof(int2)));
+    c->work = (int2*)q;
+    c->clist_alloc = need;
+    for (int k = 0; k < 4; ++k)  // graphs hold the old pointers
+      if (c->graph[k]) {
+        cudaGraphExecDestroy(c->graph[k]);
+        c->graph[k] = nullptr;
+      }
+  }
+  c->clist_cap = cap_per;
+  return 0;
+}
+
 // LinkedCell::set (LinkedCell.cpp:69-98) with the cell edge scaled by the
 // context's cell factor (1 = the reference's grid)
 int apply_grid(grains_gpu_ctx* c, SysHost& s) {
@@ -795,8 +837,11 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
     c->pairs = dalloc<int>(2 * (size_t)c->pairs_cap, c->pool);
     c->pairs_n = dalloc<unsigned long long>(1, c->pool);
     c->pair_force = dalloc<double>(3 * (size_t)c->pairs_cap, c->pool);
+    c->pair_sys = dalloc<int>((size_t)c->pairs_cap, c->pool);
     c->clock = dalloc<double>(1, c->pool);
-    ok = c->coord && c->perm && c->stats && c->pairs && c->pairs_n && c->pair_force && c->clock;
+    c->work_n = dalloc<int>(1, c->pool);
+    ok = c->coord && c->perm && c->stats && c->pairs && c->pairs_n && c->pair_force && c->pair_sys && c->clock &&
+         c->work_n;
   }
   if (!ok) {
     c->err = "cudaMalloc failed for the requested capacity";
@@ -806,6 +851,7 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
   for (int k = 0; k < 2; ++k) cudaMemsetAsync(c->hist_n[k], 0, N * sizeof(int), c->stream);
   cudaMemsetAsync(c->perm, 0, N * sizeof(int), c->stream);
   cudaMemsetAsync(c->stats, 0, sizeof(StatsDev), c->stream);
+  cudaMemsetAsync(c->work_n, 0, sizeof(int), c->stream);
   cudaStreamSynchronize(c->stream);
   *out = c;
   return 0;
@@ -821,8 +867,8 @@ int grains_gpu_destroy(grains_gpu_ctx* c) {
   for (int k = 0; k < 2; ++k)
     if (c->buf[k].basis) cudaFree(c->buf[k].basis);
   if (c->stage) cudaFree(c->stage);
-  if (c->clist) cudaFree(c->clist);
-  if (c->ccount) cudaFree(c->ccount);
+  for (void* p : {(void*)c->clist, (void*)c->ccount, c->res_f, c->res_t, (void*)c->work})
+    if (p) cudaFree(p);
   if (c->stage_basis) cudaFree(c->stage_basis);
   if (c->pbar) cudaFree(c->pbar);
   if (c->psums) cudaFree(c->psums);
@@ -1059,6 +1105,11 @@ int build_tables(grains_gpu_ctx* c) {
         P.Gs = L.p[10];
         P.beta = L.beta;
         P.rolling = (law_has_memory(L.type) && P.mur != 0.) ? 1 : 0;
+        P.kn64 = P.kn;
+        P.beta64 = P.beta;
+        P.etat64 = P.etat;
+        P.Es64 = P.Es;
+        P.Gs64 = P.Gs;
         ld[k] = P;
         LawParams<float> Q{};
         Q.type = P.type;
@@ -1067,6 +1118,7 @@ int build_tables(grains_gpu_ctx* c) {
         Q.kt = (float)P.kt; Q.mur = (float)P.mur; Q.etarpf = (float)P.etarpf; Q.epst = (float)P.epst;
         Q.kr = (float)P.kr; Q.beta = (float)P.beta;
         Q.Es = (float)P.Es; Q.Gs = (float)P.Gs;
+        Q.kn64 = P.kn64; Q.beta64 = P.beta64; Q.etat64 = P.etat64; Q.Es64 = P.Es64; Q.Gs64 = P.Gs64;
         lf[k] = Q;
       }
   // shapes
@@ -1183,18 +1235,12 @@ int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
     // contact lists: 32 slots per particle for spheres, 64 when bounding
     // spheres of other shapes are listed
     const int cap_per = c->list_capacity > 0 ? c->list_capacity : (c->has_convex ? 64 : 32);
-    const int64_t need = (int64_t)c->cap * cap_per;
-    if (need > c->clist_alloc) {
-      if (c->clist) cudaFree(c->clist);
-      if (c->ccount) cudaFree(c->ccount);
+    if (!c->ccount) {
       void* q = nullptr;
-      CK(cudaMalloc(&q, (size_t)need * sizeof(int)));
-      c->clist = (int*)q;
       CK(cudaMalloc(&q, (size_t)c->cap * sizeof(int)));
       c->ccount = (int*)q;
-      c->clist_alloc = need;
     }
-    c->clist_cap = cap_per;
+    if (int rc = ensure_lists(c, cap_per)) return rc;
   }
   if (basis_needed) {
     for (int k = 0; k < 2; ++k)
@@ -1457,7 +1503,9 @@ int grains_gpu_upload_contact_memory(grains_gpu_ctx* c, const grains_gpu_contact
     // find the owner row in any system holding that id (ids are unique per system;
     // the owner's system decides)
     int owner = m->owner[k], other = m->other[k];
-    for (size_t si = 0; si < c->sys.size(); ++si) {
+    const size_t s0 = m->system ? (size_t)std::max(0, m->system[k]) : 0;
+    const size_t s1 = m->system ? std::min(s0 + 1, c->sys.size()) : c->sys.size();
+    for (size_t si = s0; si < s1; ++si) {
       auto it = row_of.find(std::make_pair((int)si, owner));
       if (it == row_of.end()) continue;
       int row = it->second;
@@ -1524,10 +1572,12 @@ int grains_gpu_download_contact_memory(grains_gpu_ctx* c, grains_gpu_contact_mem
     sys_of_row[orig[s]] = meta[s].w;
   }
   int64_t k = 0, cap = m->n;
+  int cur_sys = 0;
   auto emit = [&](int owner, int other, const double* kd, const double* nn, const double* sp, double sign) {
     if (k < cap) {
       m->owner[k] = owner;
       m->other[k] = other;
+      if (m->system) m->system[k] = cur_sys;
       for (int t = 0; t < 3; ++t) {
         m->kdelta[3 * k + t] = sign * kd[t];
         m->prev_normal[3 * k + t] = sign * nn[t];
@@ -1550,6 +1600,7 @@ int grains_gpu_download_contact_memory(grains_gpu_ctx* c, grains_gpu_contact_mem
         for (int t = 0; t < 3; ++t) { kd[t] = x.kd[t]; nn[t] = x.n[t]; sp[t] = x.sp[t]; }
       }
       int owner = id_of_row[row];
+      cur_sys = sys_of_row[row];
       if (flags & 1) {
         const SysHost& s = c->sys[sys_of_row[row]];
         int oid = (other >= 0 && other < (int)s.obs.size()) ? s.obs[other].id : other;
@@ -1760,52 +1811,61 @@ int grains_gpu_get_candidate_pairs(grains_gpu_ctx* c, int32_t system, int32_t in
   return (int64_t)pp.size() > cap ? fail(c, GRAINS_GPU_PAIR_OVERFLOW, "pair buffer too small") : 0;
 }
 
-int grains_gpu_get_contact_pairs(grains_gpu_ctx* c, int32_t system, int64_t cap, int32_t* pairs, int64_t* n) {
-  if (!c || !n || (cap > 0 && !pairs)) return GRAINS_GPU_INVALID_ARGUMENT;
-  (void)system;
+namespace {
+// The diagnostic contact pairs of `system` from the last force evaluation,
+// sorted by (id, id): indices into the device lists
+int system_pairs(grains_gpu_ctx* c, int32_t system, std::vector<int>& h, std::vector<double>* f,
+                 std::vector<size_t>& idx) {
+  if (system < 0 || system >= (int)c->sys.size()) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "bad system index");
   unsigned long long cnt = 0;
   CK(cudaMemcpyAsync(&cnt, c->pairs_n, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   if (cnt > (unsigned long long)c->pairs_cap) return fail(c, GRAINS_GPU_PAIR_OVERFLOW, "device pair buffer too small");
-  std::vector<int> h(2 * cnt);
-  if (cnt) CK(cudaMemcpy(h.data(), c->pairs, 2 * cnt * sizeof(int), cudaMemcpyDeviceToHost));
-  std::vector<std::pair<int, int>> pp;
-  for (size_t k = 0; k < cnt; ++k) pp.push_back(std::make_pair(h[2 * k], h[2 * k + 1]));
-  std::sort(pp.begin(), pp.end());
-  *n = (int64_t)pp.size();
-  for (int64_t k = 0; k < (int64_t)pp.size() && k < cap; ++k) {
-    pairs[2 * k] = pp[k].first;
-    pairs[2 * k + 1] = pp[k].second;
+  h.assign(2 * cnt, 0);
+  std::vector<int> sy(cnt);
+  if (f) f->assign(3 * cnt, 0.);
+  if (cnt) {
+    CK(cudaMemcpy(h.data(), c->pairs, 2 * cnt * sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(sy.data(), c->pair_sys, cnt * sizeof(int), cudaMemcpyDeviceToHost));
+    if (f) CK(cudaMemcpy(f->data(), c->pair_force, 3 * cnt * sizeof(double), cudaMemcpyDeviceToHost));
   }
-  return (int64_t)pp.size() > cap ? fail(c, GRAINS_GPU_PAIR_OVERFLOW, "pair buffer too small") : 0;
+  idx.clear();
+  for (size_t k = 0; k < cnt; ++k)
+    if (sy[k] == system) idx.push_back(k);
+  std::sort(idx.begin(), idx.end(), [&](size_t x, size_t y) {
+    return std::make_pair(h[2 * x], h[2 * x + 1]) < std::make_pair(h[2 * y], h[2 * y + 1]);
+  });
+  return 0;
+}
+}  // namespace
+
+int grains_gpu_get_contact_pairs(grains_gpu_ctx* c, int32_t system, int64_t cap, int32_t* pairs, int64_t* n) {
+  if (!c || !n || (cap > 0 && !pairs)) return GRAINS_GPU_INVALID_ARGUMENT;
+  std::vector<int> h;
+  std::vector<size_t> idx;
+  if (int rc = system_pairs(c, system, h, nullptr, idx)) return rc;
+  *n = (int64_t)idx.size();
+  for (int64_t k = 0; k < (int64_t)idx.size() && k < cap; ++k) {
+    pairs[2 * k] = h[2 * idx[k]];
+    pairs[2 * k + 1] = h[2 * idx[k] + 1];
+  }
+  return (int64_t)idx.size() > cap ? fail(c, GRAINS_GPU_PAIR_OVERFLOW, "pair buffer too small") : 0;
 }
 
 int grains_gpu_get_contact_forces(grains_gpu_ctx* c, int32_t system, int64_t cap, int32_t* pairs, double* forces,
                                   int64_t* n) {
   if (!c || !n || (cap > 0 && (!pairs || !forces))) return GRAINS_GPU_INVALID_ARGUMENT;
-  (void)system;
-  unsigned long long cnt = 0;
-  CK(cudaMemcpyAsync(&cnt, c->pairs_n, sizeof(cnt), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  if (cnt > (unsigned long long)c->pairs_cap) return fail(c, GRAINS_GPU_PAIR_OVERFLOW, "device pair buffer too small");
-  std::vector<int> h(2 * cnt);
-  std::vector<double> f(3 * cnt);
-  if (cnt) {
-    CK(cudaMemcpy(h.data(), c->pairs, 2 * cnt * sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(f.data(), c->pair_force, 3 * cnt * sizeof(double), cudaMemcpyDeviceToHost));
-  }
-  std::vector<size_t> idx(cnt);
-  for (size_t k = 0; k < cnt; ++k) idx[k] = k;
-  std::sort(idx.begin(), idx.end(), [&](size_t x, size_t y) {
-    return std::make_pair(h[2 * x], h[2 * x + 1]) < std::make_pair(h[2 * y], h[2 * y + 1]);
-  });
-  *n = (int64_t)cnt;
-  for (int64_t k = 0; k < (int64_t)cnt && k < cap; ++k) {
+  std::vector<int> h;
+  std::vector<double> f;
+  std::vector<size_t> idx;
+  if (int rc = system_pairs(c, system, h, &f, idx)) return rc;
+  *n = (int64_t)idx.size();
+  for (int64_t k = 0; k < (int64_t)idx.size() && k < cap; ++k) {
     pairs[2 * k] = h[2 * idx[k]];
     pairs[2 * k + 1] = h[2 * idx[k] + 1];
     for (int d = 0; d < 3; ++d) forces[3 * k + d] = f[3 * idx[k] + d];
   }
-  return (int64_t)cnt > cap ? fail(c, GRAINS_GPU_PAIR_OVERFLOW, "pair buffer too small") : 0;
+  return (int64_t)idx.size() > cap ? fail(c, GRAINS_GPU_PAIR_OVERFLOW, "pair buffer too small") : 0;
 }
 
 int grains_gpu_get_stats(grains_gpu_ctx* c, grains_gpu_stats* st) {
@@ -1937,7 +1997,7 @@ int grains_gpu_set_tuning(grains_gpu_ctx* c, const grains_gpu_tuning* t) {
   if (!c || !t) return GRAINS_GPU_INVALID_ARGUMENT;
   if (!(t->cell_factor >= 1.0 && t->cell_factor <= 4.0) || t->contacts_block < 32 || t->contacts_block > 256 ||
       t->contacts_block % 32 || t->forces_block < 32 || t->forces_block > 128 || t->forces_block % 32 ||
-      (t->list_capacity != 0 && (t->list_capacity < 8 || t->list_capacity > 256)) || t->gather_every < 1 ||
+      (t->list_capacity != 0 && (t->list_capacity < 8 || t->list_capacity > 256 || t->list_capacity % 4)) || t->gather_every < 1 ||
       t->gather_every > 64)
     return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "tuning out of range");
   const bool regrid = t->cell_factor != c->cell_factor;
@@ -1988,16 +2048,8 @@ int grains_gpu_set_tuning(grains_gpu_ctx* c, const grains_gpu_tuning* t) {
     c->keys_valid = false;
   }
   const int cap_per = c->list_capacity > 0 ? c->list_capacity : (c->has_convex ? 64 : 32);
-  const int64_t need = (int64_t)c->cap * cap_per;
-  if (need > c->clist_alloc) {
-    CK(cudaStreamSynchronize(c->stream));
-    if (c->clist) cudaFree(c->clist);
-    void* q = nullptr;
-    CK(cudaMalloc(&q, (size_t)need * sizeof(int)));
-    c->clist = (int*)q;
-    c->clist_alloc = need;
-  }
-  c->clist_cap = cap_per;
+  CK(cudaStreamSynchronize(c->stream));
+  if (int rc = ensure_lists(c, cap_per)) return rc;
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }

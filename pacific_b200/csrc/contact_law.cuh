@@ -25,6 +25,9 @@ struct LawParams {
   int rolling;  // memory law with a rolling spring (mur != 0)
   R kn, en, etat, muc, kt, mur, etarpf, epst, kr, beta;
   R Es, Gs;     // Hertz laws: Young-like and shear moduli
+  // the same parameters of the normal part in double, for the mixed path
+  // (normal_part_fp64): kn, beta, etat, Es, Gs
+  double kn64, beta64, etat64, Es64, Gs64;
 };
 
 // laws that keep a tangential (and rolling) spring per contact
@@ -56,8 +59,9 @@ struct BodyAtContact {
 
 template <typename R>
 struct LawResult {
-  V3<R> force;  // on p0
-  V3<R> torque; // extra torque on p0 (rolling), zero otherwise
+  V3<R> force;       // on p0
+  V3<R> torque;      // extra torque on p0 (rolling), zero otherwise
+  V3<R> tangential;  // the tangential part of `force` (delFT)
 };
 
 template <typename R>
@@ -121,6 +125,7 @@ GG_HD LawResult<R> memory_tangent_rolling(const LawParams<R>& L, R dt, V3<R> nor
   }
   LawResult<R> out;
   out.force = delFN + delFT;
+  out.tangential = delFT;
   out.torque = v3<R>(R(0), R(0), R(0));
   if (L.rolling) {
     R Req = R(1) / (R(1) / b0.req + R(1) / b1.req);
@@ -205,7 +210,8 @@ GG_HD LawResult<R> hooke(const LawParams<R>& L, V3<R> pen, const BodyAtContact<R
   R etat = L.etat == R(-1) ? -L.beta * gsqrt(L.kn / avmass) : L.etat;
   R gammat = R(2) * etat * avmass;
   LawResult<R> out;
-  out.force = delFN + coulomb_cap(sc(v_t, -gammat), v_t, L.muc * normFN, branch);
+  out.tangential = coulomb_cap(sc(v_t, -gammat), v_t, L.muc * normFN, branch);
+  out.force = delFN + out.tangential;
   out.torque = kr_rolling_torque(L.kr, normFN, b0, b1);
   return out;
 }
@@ -249,7 +255,8 @@ GG_HD LawResult<R> hertz(const LawParams<R>& L, V3<R> pen, R deltan, const BodyA
                          const BodyAtContact<R>& b1, int* branch = nullptr) {
   const HertzNormal<R> h = hertz_normal(L, pen, deltan, b0, b1);
   LawResult<R> out;
-  out.force = h.delFN + coulomb_cap(sc(h.v_t, -h.gammat), h.v_t, L.muc * h.normFN, branch);
+  out.tangential = coulomb_cap(sc(h.v_t, -h.gammat), h.v_t, L.muc * h.normFN, branch);
+  out.force = h.delFN + out.tangential;
   out.torque = kr_rolling_torque(L.kr, h.normFN, b0, b1);
   return out;
 }
@@ -264,6 +271,88 @@ GG_HD LawResult<R> hertz_memory(const LawParams<R>& L, R dt, V3<R> pen, R deltan
   const R kt = R(8) * L.Gs * h.sqrtReqdeltan;
   return memory_tangent_rolling(L, dt, h.normal, h.v_t, h.delFN, h.normFN, h.gammat, kt, h.kn, h.gamman, b0, b1,
                                 existed, mem, branch);
+}
+
+// ---- mixed precision: the normal part in double -----------------------------
+// In FP32 the normal force kn * overlap - gamman * v_n loses its leading digits
+// when the elastic and viscous terms nearly cancel (a contact about to open):
+// relative errors of 1e-5 and more against FP64 on a settling bed.  The mixed
+// path therefore forms the normal direction, the relative velocity at the
+// contact point, its normal and tangential parts, the normal force and its
+// norm, and the damping coefficients in double, from the double overlap
+// vector, lever arms and masses and the FP32 velocities widened exactly.  The
+// tangential spring, Coulomb's limit, the rolling terms, the contact memory and
+// the force sums stay in FP32.  The double expressions follow the FP32 ones
+// above term by term, so for R = double they would give the same bits.
+
+// Double-precision inputs of one contact: the bodies' velocities and angular
+// velocities, lever arms (contact point - centre), masses and equivalent
+// radii.
+struct PairFp64 {
+  V3<double> v0, w0, lev0, v1, w1, lev1;
+  double m0, m1, req0, req1;
+};
+
+// Normal part of a law evaluated in double, and its FP32 images for the rest.
+template <typename R>
+struct NormalFp64 {
+  V3<double> delFN64;  // the normal force in double (for its torque)
+  V3<R> normal, v_t, delFN;
+  R normFN, kn, gamman, gammat;
+  R kt;  // tangential stiffness: kt of HookeMemory, 8 Gs sqrt(Req deltan) of HertzMemory
+};
+
+template <typename R>
+GG_HD NormalFp64<R> normal_part_fp64(const LawParams<R>& L, V3<double> pen, double deltan, const PairFp64& p) {
+  const bool hertz = L.type == GRAINS_GPU_HERTZ || L.type == GRAINS_GPU_HERTZ_MEMORY;
+  const V3<double> normal = round3(dv(pen, norm(pen)));
+  const V3<double> tmpV = (p.v0 + cross(p.w0, p.lev0)) - (p.v1 + cross(p.w1, p.lev1));
+  const V3<double> v_n = sc(normal, dot(tmpV, normal));
+  const V3<double> v_t = tmpV - v_n;
+  const double avmass = 1. / (1. / p.m0 + 1. / p.m1);
+  double kn, gamman, gammat, kt = double(L.kt);
+  if (hertz) {  // HertzContactForceModel.cpp:48-84, HertzMemoryContactForceModel.cpp:141
+    const double Req = 1. / (1. / p.req0 + 1. / p.req1);
+    const double sq = std::sqrt(Req * deltan);
+    const double Sn = 2. * L.Es64 * sq, St = 8. * L.Gs64 * sq;
+    const double m2sqrt56 = -2. * 0.91287092917527690;
+    kn = (4. / 3.) * L.Es64 * sq;
+    gamman = m2sqrt56 * L.beta64 * std::sqrt(avmass * Sn);
+    gammat = m2sqrt56 * L.beta64 * std::sqrt(avmass * St);
+    kt = St;
+  } else {  // HookeMemoryContactForceModel.cpp:96-124, HookeContactForceModel.cpp:56-78
+    kn = L.kn64;
+    gamman = -2. * L.beta64 * std::sqrt(avmass * L.kn64);
+    const double etat = L.etat64 == -1. ? -L.beta64 * std::sqrt(L.kn64 / avmass) : L.etat64;
+    gammat = 2. * etat * avmass;
+  }
+  const V3<double> delFN = sc(pen, kn) - sc(v_n, gamman);
+  NormalFp64<R> o;
+  o.delFN64 = delFN;
+  o.normal = v3<R>(R(normal.x), R(normal.y), R(normal.z));
+  o.v_t = v3<R>(R(v_t.x), R(v_t.y), R(v_t.z));
+  o.delFN = v3<R>(R(delFN.x), R(delFN.y), R(delFN.z));
+  o.normFN = R(norm(delFN));
+  o.kn = R(kn);
+  o.gamman = R(gamman);
+  o.gammat = R(gammat);
+  o.kt = R(kt);
+  return o;
+}
+
+// Any of the four laws with the normal part of normal_part_fp64 (mixed path).
+template <typename R>
+GG_HD LawResult<R> apply_contact_law_fp64_normal(const LawParams<R>& L, R dt, const NormalFp64<R>& nd,
+                                                 const BodyAtContact<R>& b0, const BodyAtContact<R>& b1,
+                                                 bool existed, PairMemory<R>& mem) {
+  if (law_has_memory(L.type))
+    return memory_tangent_rolling(L, dt, nd.normal, nd.v_t, nd.delFN, nd.normFN, nd.gammat, nd.kt, nd.kn, nd.gamman,
+                                  b0, b1, existed, mem, (int*)nullptr);
+  LawResult<R> out;
+  out.tangential = coulomb_cap(sc(nd.v_t, -nd.gammat), nd.v_t, L.muc * nd.normFN, (int*)nullptr);
+  out.force = nd.delFN + out.tangential;
+  out.torque = kr_rolling_torque(L.kr, nd.normFN, b0, b1);
+  return out;
 }
 
 // Any of the four laws.  deltan = -overlap distance (Hertz laws only).

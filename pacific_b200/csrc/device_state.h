@@ -17,6 +17,9 @@
 //     particle; the identity right after the arrays are gathered in cell order)
 //   contact memory: rows of H entries per particle, indexed by upload
 //     index, double buffered (prev -> next each force evaluation).
+//   contact lists (scratch of a force evaluation): L entries per particle
+//     (clist), the result of each entry (res_f, res_t: R4 each) and the work
+//     items of the owned entries (work: int2 per entry at most).
 #pragma once
 
 #include <cstdint>
@@ -164,13 +167,20 @@ struct StepArgs {
   HistEntry<R>* hist_next;
   int* hist_n_next;
   StatsDev* stats;
-  int* clist;            // per-particle contact lists (slots), clist_cap entries each
+  int* clist;            // per-particle contact lists, clist_cap entries each: a contacting
+                         // particle's slot (| 1 << 30 when this particle owns the pair) or
+                         // -1 - obstacle index for a candidate obstacle
   int* ccount;
   int clist_cap;
+  typename Vec4<R>::type* res_f;  // per list entry: force on this particle, w = contact flag
+  typename Vec4<R>::type* res_t;  // per list entry: torque on this particle
+  int2* work;            // owned list entries of this evaluation: (particle, entry | memory rank << 9)
+  int* work_n;           // their count (cleared by the sums kernel)
   int* pairs;            // diagnostic contact pair output (2 ints per pair) or null
   int pairs_cap;
   unsigned long long* pairs_n;
   double* pair_force;    // diagnostic: force on the lower id of each contact pair (3 doubles) or null
+  int* pair_sys;         // diagnostic: system of each contact pair
   double gjk_tol;
   int gjk_sv;            // the signed-volume GJK for non-spherical pairs
   int contacts_block;    // threads per block of contacts_kernel (<= 256)

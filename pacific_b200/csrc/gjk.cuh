@@ -317,220 +317,196 @@ GG_HD GjkResult<T> gjk_distance(const LocalBody<T>& A, const LocalBody<T>& B, T 
 }
 
 // ---- the signed-volume GJK ------------------------------------------------------
-// Montanari, Petrinic, Barbieri, "Improving the GJK algorithm for faster and more
-// reliable distance queries between convex objects", ACM TOG 36(3), 2017, in the
-// operation order of GJK_SV.cpp:9-525 (closest_points_GJK_SV, acceleration
-// off): the sub-algorithm compares the signed volumes of the simplex with those
-// where the origin replaces each vertex; a face or edge that does not contain
-// the origin's projection gives way to its best sub-simplex.
-GG_HD bool sv_same_sign(double a, double b) { return !((a > 0) ^ (b > 0)); }
+// Montanari, Petrinic and Barbieri, "Improving the GJK algorithm for faster and
+// more reliable distance queries between convex objects", ACM Transactions on
+// Graphics 36(3), 2017.  Its distance sub-algorithm finds the point of a
+// simplex W = {y_k} closest to the origin from signed volumes: the barycentric
+// coordinate of y_k in the origin's projection onto aff(W) is the signed volume
+// of W with y_k replaced by that projection, over the signed volume of W.  When
+// every such volume has the sign of the whole, the projection lies inside W and
+// is the answer.  Otherwise each face of W opposite a vertex whose volume has
+// the wrong sign is searched in turn (one dimension lower), and the closest of
+// their answers is kept.
+//
+// Formulation used here (vector products over the full 3-vectors, no
+// projection onto a coordinate plane), with edge vectors taken between
+// vertices wherever possible: near convergence the simplex is far smaller than
+// its distance from the origin, and products of the vertices themselves would
+// cancel to rounding noise.
+//   segment (a, b):      t = b - a; the projection's signed length past a is
+//                        u = -a.t (in units of 1 / |t|); weights (t.t - u, u) / t.t
+//   triangle (a, b, c):  n = (b - a) x (c - a), p = the origin's projection onto
+//                        the plane; the signed areas measured along n are
+//                        n.((b - p) x (c - p)) and cyclically (total n.n)
+//   tetrahedron:         the volume with y_k replaced by the origin, e.g.
+//                        det[y1, y2 - y1, y3 - y1] for y0, with alternating
+//                        signs; the whole: det[y1 - y0, y2 - y0, y3 - y0]
+// A zero volume counts as a wrong sign, so a projection on the boundary of W is
+// answered by the smaller simplex.  The simplex is kept packed: vertices
+// 0 .. n-1, the newest last.
 
-GG_HD double sv_comp(const V3<double>& v, unsigned i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+// closest point of a sub-simplex: the vertices kept (bit k = vertex k) and
+// their weights, and the squared distance of the point from the origin
+struct SvPick {
+  unsigned keep;
+  double lam[4];
+  double d2;
+};
 
-GG_HD void sv_edge(const V3<double> y[4], unsigned& bits, double lam[4]) {  // s1d
-  unsigned i1 = 0xffffffffu, i2 = 0xffffffffu;
-  bool first = false;
-  for (unsigned i = 0; i < 4; ++i)
-    if (bits & (1u << i)) {
-      if (first) {
-        i2 = i;
-        break;
-      }
-      i1 = i;
-      first = true;
-    }
-  const V3<double> t = y[i2] - y[i1];
-  unsigned I = 0;
-  double neg = -t.x;
-  if (fabs(t.y) > fabs(neg)) {
-    I = 1;
-    neg = -t.y;
-  }
-  if (fabs(t.z) > fabs(neg)) {
-    I = 2;
-    neg = -t.z;
-  }
-  const double pI = dot(y[i2], t) / dot(t, t) * neg + sv_comp(y[i2], I);
-  const double C0 = -sv_comp(y[i2], I) + pI, C1 = sv_comp(y[i1], I) - pI;
-  const bool s0 = sv_same_sign(neg, C0), s1 = sv_same_sign(neg, C1);
-  if (s0 && s1) {
-    lam[i1] = C0 / neg;
-    lam[i2] = C1 / neg;
-  } else if (s0) {
-    bits &= ~(1u << i2);
-    lam[i1] = 1.;
-  } else {
-    bits &= ~(1u << i1);
-    lam[i2] = 1.;
-  }
+GG_HD double sv_triple(V3<double> a, V3<double> b, V3<double> c) { return dot(a, cross(b, c)); }
+
+GG_HD void sv_finish(const V3<double>* y, SvPick& r) {
+  V3<double> pt = v3<double>(0., 0., 0.);
+  for (int k = 0; k < 4; ++k)
+    if (r.keep & (1u << k)) pt = pt + sc(y[k], r.lam[k]);
+  r.d2 = dot(pt, pt);
 }
 
-GG_HD void sv_face(const V3<double> y[4], unsigned& bits, double lam[4]) {  // s2d
-  unsigned cnt = 0, i0 = 0, i1 = 0, i2 = 0;
-  for (unsigned i = 0; i < 4; ++i)
-    if (bits & (1u << i)) {
-      if (cnt == 0) i0 = i;
-      else if (cnt == 1) i1 = i;
-      else i2 = i;
-      ++cnt;
-    }
-  const V3<double> n = cross(y[i1] - y[i0], y[i2] - y[i0]);
-  const V3<double> p0 = sc(n, dot(y[i0], n) / dot(n, n));
-  const V3<double>&a = y[i0], &b = y[i1], &c = y[i2];
-  unsigned ix = 1, iy = 2;
-  double mu_max = b.y * c.z + a.y * b.z + c.y * a.z - b.y * a.z - c.y * b.z - a.y * c.z;
-  double mu = b.z * a.x + c.z * b.x + a.z * c.x - b.z * c.x - a.z * b.x - c.z * a.x;
-  if (fabs(mu) > fabs(mu_max)) {
-    mu_max = mu;
-    ix = 0;
-  }
-  mu = b.x * c.y + a.x * b.y + c.x * a.y - b.x * a.y - c.x * b.y - a.x * c.y;
-  if (fabs(mu) > fabs(mu_max)) {
-    mu_max = mu;
-    ix = 0;
-    iy = 1;
-  }
-  const double px = sv_comp(p0, ix), py = sv_comp(p0, iy);
-  const double ax = sv_comp(a, ix), ay = sv_comp(a, iy), bx = sv_comp(b, ix), by = sv_comp(b, iy);
-  const double cx = sv_comp(c, ix), cy = sv_comp(c, iy);
-  double C[3];
-  C[0] = px * by + py * cx + bx * cy - px * cy - py * bx - cx * by;
-  C[1] = px * cy + py * ax + cx * ay - px * ay - py * cx - ax * cy;
-  C[2] = px * ay + py * bx + ax * by - px * by - py * ax - bx * ay;
-  const bool sg[3] = {sv_same_sign(mu_max, C[0]), sv_same_sign(mu_max, C[1]), sv_same_sign(mu_max, C[2])};
-  if (sg[0] && sg[1] && sg[2]) {
-    lam[i0] = C[0] / mu_max;
-    lam[i1] = C[1] / mu_max;
-    lam[i2] = C[2] / mu_max;
-    return;
-  }
-  double d = 1.e9;
-  unsigned nb = 0;
-  const unsigned idx[3] = {i0, i1, i2};
-  for (unsigned j = 0; j < 3; ++j) {
-    if (sg[j]) continue;
-    unsigned used = bits & ~(1u << idx[j]);
-    double nl[4] = {0., 0., 0., 0.};
-    sv_edge(y, used, nl);
-    V3<double> pt = v3<double>(0., 0., 0.);
-    for (unsigned i = 0; i < 4; ++i)
-      if (used & (1u << i)) pt = pt + sc(y[i], nl[i]);
-    const double ds = dot(pt, pt);
-    if (ds < d) {
-      nb = used;
-      d = ds;
-      for (int i = 0; i < 4; ++i) lam[i] = nl[i];
-    }
-  }
-  bits = nb;
+GG_HD SvPick sv_pick_vertex(const V3<double>* y, int a) {
+  SvPick r{1u << a, {0., 0., 0., 0.}, 0.};
+  r.lam[a] = 1.;
+  r.d2 = dot(y[a], y[a]);
+  return r;
 }
 
-GG_HD void sv_tetra(const V3<double> y[4], unsigned& bits, double lam[4]) {  // s3d
-  double C[4];
-  C[0] = y[3].x * y[2].y * y[1].z + y[2].x * y[1].y * y[3].z + y[1].x * y[3].y * y[2].z -
-         y[1].x * y[2].y * y[3].z - y[2].x * y[3].y * y[1].z - y[3].x * y[1].y * y[2].z;
-  C[1] = y[0].x * y[2].y * y[3].z + y[2].x * y[3].y * y[0].z + y[3].x * y[0].y * y[2].z -
-         y[3].x * y[2].y * y[0].z - y[2].x * y[0].y * y[3].z - y[0].x * y[3].y * y[2].z;
-  C[2] = y[3].x * y[1].y * y[0].z + y[1].x * y[0].y * y[3].z + y[0].x * y[3].y * y[1].z -
-         y[0].x * y[1].y * y[3].z - y[1].x * y[3].y * y[0].z - y[3].x * y[0].y * y[1].z;
-  C[3] = y[0].x * y[1].y * y[2].z + y[1].x * y[2].y * y[0].z + y[2].x * y[0].y * y[1].z -
-         y[2].x * y[1].y * y[0].z - y[1].x * y[0].y * y[2].z - y[0].x * y[2].y * y[1].z;
-  const double dM = C[0] + C[1] + C[2] + C[3];
-  bool sg[4];
-  int nsame = 0;
-  for (int i = 0; i < 4; ++i) {
-    sg[i] = sv_same_sign(dM, C[i]);
-    nsame += sg[i] ? 1 : 0;
-  }
-  if (nsame == 4) {
-    for (int i = 0; i < 4; ++i) lam[i] = C[i] / dM;
-    return;
-  }
-  double d = 1.e9;
-  unsigned nb = 0;
-  for (unsigned j = 0; j < 4; ++j) {
-    if (sg[j]) continue;
-    unsigned used = bits & ~(1u << j);
-    double nl[4] = {0., 0., 0., 0.};
-    sv_face(y, used, nl);
-    V3<double> pt = v3<double>(0., 0., 0.);
-    for (unsigned i = 0; i < 4; ++i)
-      if (used & (1u << i)) pt = pt + sc(y[i], nl[i]);
-    const double ds = dot(pt, pt);
-    if (ds < d) {
-      nb = used;
-      d = ds;
-      for (int i = 0; i < 4; ++i) lam[i] = nl[i];
-    }
-  }
-  bits = nb;
+GG_HD SvPick sv_pick_segment(const V3<double>* y, int a, int b) {
+  const V3<double> t = y[b] - y[a];
+  const double tt = dot(t, t);
+  const double u = -dot(y[a], t);
+  if (!(u > 0.)) return sv_pick_vertex(y, a);        // the origin projects before a
+  if (!(u < tt)) return sv_pick_vertex(y, b);        // ... past b (or a, b coincide)
+  SvPick r{(1u << a) | (1u << b), {0., 0., 0., 0.}, 0.};
+  r.lam[b] = u / tt;
+  r.lam[a] = (tt - u) / tt;
+  sv_finish(y, r);
+  return r;
 }
 
+GG_HD SvPick sv_pick_triangle(const V3<double>* y, int a, int b, int c) {
+  const V3<double> n = cross(y[b] - y[a], y[c] - y[a]);
+  const double nn = dot(n, n);
+  const int vx[3] = {a, b, c};
+  double area[3] = {0., 0., 0.};
+  if (nn > 0.) {
+    const V3<double> p = sc(n, dot(n, y[a]) / nn);
+    area[0] = dot(n, cross(y[b] - p, y[c] - p));
+    area[1] = dot(n, cross(y[c] - p, y[a] - p));
+    area[2] = dot(n, cross(y[a] - p, y[b] - p));
+  }
+  if (area[0] > 0. && area[1] > 0. && area[2] > 0.) {
+    const double total = area[0] + area[1] + area[2];
+    SvPick r{(1u << a) | (1u << b) | (1u << c), {0., 0., 0., 0.}, 0.};
+    for (int k = 0; k < 3; ++k) r.lam[vx[k]] = area[k] / total;
+    sv_finish(y, r);
+    return r;
+  }
+  SvPick best{0u, {0., 0., 0., 0.}, INFINITY};
+  for (int k = 0; k < 3; ++k) {
+    if (area[k] > 0.) continue;  // the projection is on y_k's side of the opposite edge
+    const SvPick e = sv_pick_segment(y, vx[(k + 1) % 3], vx[(k + 2) % 3]);
+    if (e.d2 < best.d2) best = e;
+  }
+  return best;
+}
+
+GG_HD SvPick sv_pick_tetrahedron(const V3<double>* y) {
+  const double vol[4] = {sv_triple(y[1], y[2] - y[1], y[3] - y[1]), -sv_triple(y[0], y[2] - y[0], y[3] - y[0]),
+                         sv_triple(y[0], y[1] - y[0], y[3] - y[0]), -sv_triple(y[0], y[1] - y[0], y[2] - y[0])};
+  const double total = sv_triple(y[1] - y[0], y[2] - y[0], y[3] - y[0]);
+  bool same[4];
+  for (int k = 0; k < 4; ++k) same[k] = vol[k] != 0. && ((vol[k] > 0.) == (total > 0.));
+  if (total != 0. && same[0] && same[1] && same[2] && same[3]) {
+    const double sum = (vol[0] + vol[1]) + (vol[2] + vol[3]);
+    SvPick r{15u, {vol[0] / sum, vol[1] / sum, vol[2] / sum, vol[3] / sum}, 0.};
+    return r;  // the origin is inside: distance zero
+  }
+  SvPick best{0u, {0., 0., 0., 0.}, INFINITY};
+  for (int k = 0; k < 4; ++k) {
+    if (same[k] && total != 0.) continue;
+    const SvPick f = sv_pick_triangle(y, (k + 1) & 3, (k + 2) & 3, (k + 3) & 3);
+    if (f.d2 < best.d2) best = f;
+  }
+  return best;
+}
+
+// GJK iteration with the signed-volume sub-algorithm.  The outer loop is the
+// reference's closest_points_GJK_SV (GJK_SV.cpp:428-517, Nesterov acceleration
+// off, its default): start at A(0) - B(0), stop on the optimality gap
+// (relative rel_error or absolute 1e-4 rel_error), on a support point already
+// in the simplex, on a full simplex, at distance <= EPSILON2 or after 1000
+// iterations.
 GG_HD GjkResult<double> gjk_sv_distance(const LocalBody<double>& A, const LocalBody<double>& B, double rel_error) {
-  unsigned bits = 0, last = 0;
-  V3<double> p[4], q[4], y[4];
-  double lam[4] = {0., 0., 0., 0.};
   const V3<double> zero = v3<double>(0., 0., 0.);
-  for (int i = 0; i < 4; ++i) p[i] = q[i] = y[i] = zero;
+  V3<double> y[4], p[4], q[4];
+  double lam[4] = {0., 0., 0., 0.};
+  for (int i = 0; i < 4; ++i) y[i] = p[i] = q[i] = zero;
+  int n = 0;  // vertices in the simplex
   const double abs_error = 1.e-4 * rel_error;
   V3<double> v = lb_apply(A, support_local(A, zero)) - lb_apply(B, support_local(B, zero));
-  V3<double> w = v;
   double dist = norm(v);
-  int num = 0, exit_reason = 3;
+  int iters = 0, exit_reason = 3;
   double lower = -dist;
-  while (bits < 15 && dist > kEpsilon2 && num < 1000) {
-    ++num;
-    for (unsigned k = 0; k < 4; ++k)
-      if (!(bits & (1u << k))) {
-        last = k;
-        break;
-      }
-    p[last] = support_local(A, lb_vecmat(-v, A));
-    q[last] = support_local(B, lb_vecmat(v, B));
-    w = lb_apply(A, p[last]) - lb_apply(B, q[last]);
+  while (n < 4 && dist > kEpsilon2 && iters < 1000) {
+    ++iters;
+    const V3<double> pa = support_local(A, lb_vecmat(-v, A));
+    const V3<double> qb = support_local(B, lb_vecmat(v, B));
+    const V3<double> w = lb_apply(A, pa) - lb_apply(B, qb);
     const double sep = dot(v, w) / dist;
     if (sep > lower) lower = sep;
-    const double mu = dist - sep;
-    if (mu < dist * rel_error || mu < abs_error) {
+    const double gap = dist - sep;
+    if (gap < dist * rel_error || gap < abs_error) {
       exit_reason = 0;
       break;
     }
-    bool degen = false;
-    for (unsigned i = 0; i < 4; ++i)
-      if ((bits & (1u << i)) && y[i].x == w.x && y[i].y == w.y && y[i].z == w.z) degen = true;
-    if (degen) {
+    bool repeated = false;
+    for (int k = 0; k < n; ++k) repeated = repeated || (y[k].x == w.x && y[k].y == w.y && y[k].z == w.z);
+    if (repeated) {
       exit_reason = 1;
       break;
     }
-    y[last] = w;
-    bits |= 1u << last;
-    const int used = (int)((bits & 1u) + ((bits >> 1) & 1u) + ((bits >> 2) & 1u) + ((bits >> 3) & 1u));
-    if (used == 1) {
-      for (unsigned i = 0; i < 4; ++i)
-        if (bits & (1u << i)) lam[i] = 1.;
-    } else if (used == 2) {
-      sv_edge(y, bits, lam);
-    } else if (used == 3) {
-      sv_face(y, bits, lam);
-    } else {
-      sv_tetra(y, bits, lam);
-    }
+    y[n] = w;
+    p[n] = pa;
+    q[n] = qb;
+    ++n;
+    SvPick pick;
+    if (n == 1) pick = sv_pick_vertex(y, 0);
+    else if (n == 2) pick = sv_pick_segment(y, 0, 1);
+    else if (n == 3) pick = sv_pick_triangle(y, 0, 1, 2);
+    else pick = sv_pick_tetrahedron(y);
+    // In exact arithmetic the new support point is part of the answer whenever
+    // the optimality gap is still open; when rounding drops it, the next
+    // iteration would find the same point again and cycle: stop here, with the
+    // answer of the current simplex (like a support point already in it).
+    const bool dropped = !(pick.keep & (1u << (n - 1)));
+    // pack the kept vertices to the front, in their order
+    int m = 0;
     v = zero;
-    for (unsigned i = 0; i < 4; ++i)
-      if (bits & (1u << i)) v = v + sc(y[i], lam[i]);
-    dist = norm(v);
-  }
-  V3<double> pa = zero, pb = zero;
-  for (unsigned i = 0; i < 4; ++i)
-    if (bits & (1u << i)) {
-      pa = pa + sc(p[i], lam[i]);
-      pb = pb + sc(q[i], lam[i]);
+    for (int k = 0; k < n; ++k) {
+      if (!(pick.keep & (1u << k))) continue;
+      y[m] = y[k];
+      p[m] = p[k];
+      q[m] = q[k];
+      lam[m] = pick.lam[k];
+      v = v + sc(y[m], lam[m]);
+      ++m;
     }
+    n = m;
+    dist = norm(v);
+    if (dropped) {
+      exit_reason = 1;
+      break;
+    }
+  }
+  V3<double> wa = zero, wb = zero;
+  for (int k = 0; k < n; ++k) {
+    wa = wa + sc(p[k], lam[k]);
+    wb = wb + sc(q[k], lam[k]);
+  }
   GjkResult<double> r;
-  r.pa = lb_apply(A, pa);
-  r.pb = lb_apply(B, pb);
+  r.pa = lb_apply(A, wa);
+  r.pb = lb_apply(B, wb);
   r.dist = dist;
-  r.iters = num;
+  r.iters = iters;
   r.exit = exit_reason;
   r.lower = lower;
   return r;

@@ -342,22 +342,29 @@ __global__ void __launch_bounds__(256) gather_kernel(StepArgs<R> a, int gather_f
 }
 
 // ---------------------------------------------------------------------------
-// contact memory lookup in the owner's row of the previous step
+// contact memory lookup in the owner's row of the previous step.  The keys of
+// the first 8 entries are loaded together (no load waits on a comparison);
+// longer rows continue one entry at a time.
 template <typename R>
 __device__ __forceinline__ bool find_memory(const StepArgs<R>& a, int row, int other, int flags,
                                             PairMemory<R>& m) {
   const HistEntry<R>* h = a.hist_prev + (size_t)row * a.hist_cap;
-  int n = a.hist_n_prev[row];
-  for (int k = 0; k < n; ++k) {
-    HistEntry<R> e = h[k];
-    if (e.other == other && e.flags == flags) {
-      m.kdelta = v3<R>(e.kd[0], e.kd[1], e.kd[2]);
-      m.prev_normal = v3<R>(e.n[0], e.n[1], e.n[2]);
-      m.spring = v3<R>(e.sp[0], e.sp[1], e.sp[2]);
-      return true;
-    }
-  }
-  return false;
+  const int n = a.hist_n_prev[row];
+  int found = -1;
+  int2 key[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) key[k] = k < n ? make_int2(h[k].other, h[k].flags) : make_int2(-1, -1);
+#pragma unroll
+  for (int k = 7; k >= 0; --k)
+    if (key[k].x == other && key[k].y == flags) found = k;
+  for (int k = 8; found < 0 && k < n; ++k)
+    if (h[k].other == other && h[k].flags == flags) found = k;
+  if (found < 0) return false;
+  const HistEntry<R>& e = h[found];
+  m.kdelta = v3<R>(e.kd[0], e.kd[1], e.kd[2]);
+  m.prev_normal = v3<R>(e.n[0], e.n[1], e.n[2]);
+  m.spring = v3<R>(e.sp[0], e.sp[1], e.sp[2]);
+  return true;
 }
 
 template <typename R>
@@ -382,13 +389,41 @@ __device__ __forceinline__ void atomic_max_pos_double(unsigned long long* addr, 
 }
 
 // Applies the contact law for the pair (p0, p1) seen from p0 and returns the
-// force on p0 and the rolling torque on p0.
+// force on p0, its rolling torque, and the torques of the contact force about
+// both centres (lever0 x f, lever1 x (-f); Torsor::addForce, Torsor.cpp:184-189).
+// The mixed path (R = float) forms the normal part of the law in double from
+// `pd` (normal_part_fp64), and takes the normal force's share of the torques in
+// double: for spheres the lever is parallel to the normal, so lever x f_normal
+// vanishes, but the FP32 product of the two rounded vectors leaves a residue of
+// 1e-7 |lever| |f|, which can exceed the true torque of the tangential force.
+// The FP64 path runs the reference's expressions throughout.
 template <typename R>
-__device__ __forceinline__ LawResult<R> pair_law(const StepArgs<R>& a, const LawParams<R>& L, R dt,
-                                                 const ContactGeom& g, const BodyAtContact<R>& b0,
-                                                 const BodyAtContact<R>& b1, bool existed, PairMemory<R>& mem) {
-  return apply_contact_law(L, dt, from_d3<R>(g.overlap_vector), R(-g.overlap), b0, b1, existed, mem);
+__device__ __forceinline__ LawResult<R> pair_law(const LawParams<R>& L, R dt, const ContactGeom& g,
+                                                 const BodyAtContact<R>& b0, const BodyAtContact<R>& b1,
+                                                 const PairFp64& pd, bool existed, PairMemory<R>& mem, V3<R>& t0,
+                                                 V3<R>& t1) {
+  if constexpr (sizeof(R) == 4) {
+    const V3<double> pen = v3<double>(g.overlap_vector.x, g.overlap_vector.y, g.overlap_vector.z);
+    const NormalFp64<R> nd = normal_part_fp64(L, pen, -g.overlap, pd);
+    const V3<double> tn0 = cross(pd.lev0, nd.delFN64), tn1 = cross(pd.lev1, -nd.delFN64);
+    const LawResult<R> res = apply_contact_law_fp64_normal(L, dt, nd, b0, b1, existed, mem);
+    t0 = v3<R>(R(tn0.x), R(tn0.y), R(tn0.z)) + cross(b0.lever, res.tangential);
+    t1 = v3<R>(R(tn1.x), R(tn1.y), R(tn1.z)) + cross(b1.lever, -res.tangential);
+    return res;
+  } else {
+    const LawResult<R> res =
+        apply_contact_law(L, dt, from_d3<R>(g.overlap_vector), R(-g.overlap), b0, b1, existed, mem);
+    t0 = cross(b0.lever, res.force);
+    t1 = cross(b1.lever, -res.force);
+    return res;
+  }
 }
+
+template <typename R>
+__device__ __forceinline__ V3<double> widen(V3<R> a) {
+  return v3<double>(double(a.x), double(a.y), double(a.z));
+}
+__device__ __forceinline__ V3<double> dvec(D3 a) { return v3<double>(a.x, a.y, a.z); }
 
 // Contact with a pair error: RigidBodyWithCrust::ClosestPoint_ErreurHandling
 // (RigidBodyWithCrust.cpp:532-588) for two spheres, whose crust-x10 shrunk
@@ -480,19 +515,47 @@ __device__ ContactGeom convex_closest_point(const StepArgs<R>& a, const BodyRef&
 }
 
 // ---------------------------------------------------------------------------
-// contacts: the broadphase and the exact bounding-sphere test, one thread per
-// particle (cell-sorted order).  For every neighbour j != i of the 27
-// surrounding cells (LinkedCell::ComputeForces as a set, LinkedCell.cpp:
-// 1019-1103) it tests |x_j - x_i| - (r_i + r_j) < 0 in double with the
-// reference's rounding (for spheres this is the contact decision of
-// ClosestPointSPHERESPHERE, RigidBodyWithCrust.cpp:611-613; for other convex
-// bodies the circumscribed-sphere prefilter of ClosestPoint, :279-282) and
-// appends j's slot to the particle's contact list.  Few live registers: the
-// contact law runs in forces_kernel over the lists only.
+// The force evaluation runs in three phases.
+//
+// A. contacts (one thread per particle, cell-sorted order): the broadphase over
+//    the 27 surrounding cells with the exact double overlap test, then the
+//    obstacles linked to the particle's cell.  Each particle gets a list of
+//    entries: a contacting particle's slot, with kOwnBit set when this particle
+//    owns the pair (the lower id), or -1 - k for a candidate obstacle k.  Every
+//    owned entry (owned pairs and obstacles) becomes a work item.
+// B. pairs (one thread per work item): the narrowphase, the contact memory of
+//    the owner and the contact law, ONCE per pair.  The owner writes the
+//    results of both sides: its own entry's slot gets (f, lever_p0 x f + M) and
+//    the partner's entry for the pair (found in the partner's list) gets (-f,
+//    lever_p1 x (-f) - M), the exact values the partner would compute with the
+//    law from its side; and the updated memory goes to the owner's row at the
+//    entry's rank among its owned entries.
+// C. sums (one thread per particle): weight + every entry's result in list
+//    order (deterministic: no float atomics), coordination, and the owner's
+//    memory row packed (entries without a contact or without a memory law
+//    leave a hole that is squeezed out here).
+
+constexpr int kOwnBit = 1 << 30;  // list entry: this particle owns the pair
+__device__ __forceinline__ int entry_slot(int e) { return e & (kOwnBit - 1); }
+__device__ __forceinline__ bool entry_owned(int e) { return e < 0 || (e & kOwnBit); }
+
+// contacts: the broadphase and the exact bounding-sphere test.  For every
+// neighbour j != i of the 27 surrounding cells (LinkedCell::ComputeForces as a
+// set, LinkedCell.cpp:1019-1103) it tests |x_j - x_i| - (r_i + r_j) < 0 in
+// double with the reference's rounding (for spheres this is the contact
+// decision of ClosestPointSPHERESPHERE, RigidBodyWithCrust.cpp:611-613; for
+// other convex bodies the circumscribed-sphere prefilter of ClosestPoint,
+// :279-282) and appends j's slot.  Then the obstacles of the cell
+// (SimpleObstacle::InterAction's candidates, SimpleObstacle.cpp:222-270):
+// static ones linked at set-up, moving ones whose box meets the twice-expanded
+// cell (LinkedCell.cpp:1568-1585), each kept when its box meets the particle's
+// circumscribed sphere box (BBox::InZone).
 template <typename R>
-__device__ __forceinline__ void contacts_one(const StepArgs<R>& a, int s, unsigned long long& ncand) {
+__device__ __forceinline__ void contacts_one(const StepArgs<R>& a, int s, unsigned long long& ncand,
+                                             unsigned long long& nobs_cand, int& n_work) {
   const ParticleArrays<R>& P = a.cur;
   const double4 xi = P.xr[s];
+  const int idi = P.meta[s].x;
   const SysDev& S = a.sys[P.meta[s].w];
   const D3 Xi = d3(xi.x, xi.y, xi.z);
   // the particle's cell from the key of the current positions (the cell lists
@@ -510,7 +573,7 @@ __device__ __forceinline__ void contacts_one(const StepArgs<R>& a, int s, unsign
     r1[r] = ok ? a.cell_start[cell_index(S, i1, j, k) + 1] : 0;
   }
   int* list = a.clist + (size_t)s * a.clist_cap;
-  int cnt = 0;
+  int cnt = 0, owned = 0;
   auto test = [&](int p, const double4& xj) {
     // cheap rejection of far candidates: the squared distance against the
     // squared radius sum with a 1e-12 relative margin (rounding of either
@@ -521,11 +584,13 @@ __device__ __forceinline__ void contacts_one(const StepArgs<R>& a, int s, unsign
     D3 ab;
     double nab;
     // |AB| and r_A + r_B are symmetric in IEEE arithmetic, so the test
-    // gives the same bits whichever body is A
+    // gives the same bits whichever body is A: both particles list the pair
     const double dist = sphere_sphere_overlap(Xi, xi.w, d3(xj.x, xj.y, xj.z), xj.w, &ab, &nab);
     if (dist < 0. && p != s) {
-      if (cnt < a.clist_cap) list[cnt] = p;
+      const bool own = idi < P.meta[p].x;
+      if (cnt < a.clist_cap) list[cnt] = p | (own ? kOwnBit : 0);
       ++cnt;
+      owned += own ? 1 : 0;
     }
   };
 #pragma unroll
@@ -545,193 +610,7 @@ __device__ __forceinline__ void contacts_one(const StepArgs<R>& a, int s, unsign
       test(pa, P.xr[pa]);
     }
   }
-  if (cnt > a.clist_cap) {
-    set_status(a.stats, GRAINS_GPU_PAIR_OVERFLOW);
-    cnt = a.clist_cap;
-  }
-  a.ccount[s] = cnt;
-  ncand -= 1;  // the particle itself
-}
-
-// warp sum of a per-thread count into a statistics counter (every lane of the
-// warp calls it)
-__device__ __forceinline__ void warp_add(unsigned long long* dst, unsigned long long v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
-}
-
-template <typename R>
-__global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  unsigned long long ncand = 0;
-  if (s < a.n) contacts_one(a, s, ncand);
-  warp_add(&a.stats->n_cand, ncand);
-}
-
-// ---------------------------------------------------------------------------
-// forces: one thread per particle over its contact list.  Every pair is met
-// by both of its particles; both evaluate the same contact law with the lower
-// id as p0 (same inputs, same instructions -> bit-identical forces of
-// opposite sign) and the lower id owns the pair's contact memory.
-// statistics of the force evaluation, summed per thread then per warp
-struct ForceStats {
-  unsigned long long nobs_cand, ncont_own, nobs_cont, ngjk, ngjk_it;
-  double ov_sum, ov_max;
-};
-
-__device__ __forceinline__ void flush_force_stats(StatsDev* st, ForceStats& f) {
-  const unsigned full = 0xffffffffu;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    f.nobs_cand += __shfl_down_sync(full, f.nobs_cand, o);
-    f.ncont_own += __shfl_down_sync(full, f.ncont_own, o);
-    f.nobs_cont += __shfl_down_sync(full, f.nobs_cont, o);
-    f.ngjk += __shfl_down_sync(full, f.ngjk, o);
-    f.ngjk_it += __shfl_down_sync(full, f.ngjk_it, o);
-    f.ov_sum += __shfl_down_sync(full, f.ov_sum, o);
-    f.ov_max = fmax(f.ov_max, __shfl_down_sync(full, f.ov_max, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    if (f.nobs_cand) atomicAdd(&st->n_obs_cand, f.nobs_cand);
-    if (f.ncont_own) atomicAdd(&st->n_contacts, f.ncont_own);
-    if (f.nobs_cont) atomicAdd(&st->n_obs_contacts, f.nobs_cont);
-    if (f.ngjk) atomicAdd(&st->n_gjk_calls, f.ngjk);
-    if (f.ngjk_it) atomicAdd(&st->n_gjk_iters, f.ngjk_it);
-    if (f.ov_sum > 0.) atomicAdd(&st->overlap_sum, f.ov_sum);
-    if (f.ov_max > 0.) atomic_max_pos_double(&st->overlap_max_bits, f.ov_max);
-  }
-}
-
-template <typename R, bool DIAG, bool CONVEX, bool SV = false>
-__device__ __forceinline__ void forces_one(const StepArgs<R>& a, int s, R dt, ForceStats& fs) {
-  const ParticleArrays<R>& P = a.cur;
-  const double4 xi = P.xr[s];
-  const int4 mi = P.meta[s];
-  const double4 mdi = P.md[s];
-  const V3<R> vi = ld3<R>(P.v[s]);
-  const V3<R> wi = ld3<R>(P.w[s]);
-  const int oi = P.orig[s];
-  const SysDev& S = a.sys[mi.w];
-  const D3 Xi = d3(xi.x, xi.y, xi.z);
-  const ShapeDev shi = a.shapes[mi.z];
-
-  // InitializeForces(withWeight): torsor = weight (Particle.cpp:1409-1416)
-  V3<R> F = v3<R>(R(S.gx * mdi.x), R(S.gy * mdi.x), R(S.gz * mdi.x));
-  V3<R> T = v3<R>(R(0), R(0), R(0));
-  int ncontact = 0, nnext = 0;
-  unsigned long long &nobs_cand = fs.nobs_cand, &ncont_own = fs.ncont_own, &nobs_cont = fs.nobs_cont,
-                     &ngjk = fs.ngjk, &ngjk_it = fs.ngjk_it;
-  double &ov_max = fs.ov_max, &ov_sum = fs.ov_sum;
-
-  // the particle's cell from the key of the current positions (the kick
-  // computed it with cell_of): no divisions here
-  const int local = (int)P.key[s] - S.cell_offset;
-  const int ci = local % S.nbi, ck = (local / S.nbi) % S.nbk, cj = local / (S.nbi * S.nbk);
-
-  {
-    const int nlist = a.ccount[s];
-    const int* list = a.clist + (size_t)s * a.clist_cap;
-    for (int q = 0; q < nlist; ++q) {
-      {
-        const int t = list[q];
-        const double4 xj = P.xr[t];
-        const int idj = P.meta[t].x;
-        const bool own = mi.x < idj;
-        const D3 Xj = d3(xj.x, xj.y, xj.z);
-        const D3 A = own ? Xi : Xj, B = own ? Xj : Xi;
-        const double ra = own ? xi.w : xj.w, rb = own ? xj.w : xi.w;
-        const int4 mj = P.meta[t];
-        const ShapeDev shj = a.shapes[mj.z];
-        ContactGeom g;
-        if (!CONVEX || (shi.type == GRAINS_GPU_SPHERE && shj.type == GRAINS_GPU_SPHERE)) {
-          D3 ab;
-          double nab;
-          const double dist = sphere_sphere_overlap(A, ra, B, rb, &ab, &nab);
-          if (!(dist < 0.)) continue;
-          const double4 mdj = P.md[t];
-          const double crust_sum = xadd(own ? mdi.y : mdj.y, own ? mdj.y : mdi.y);
-          g = sphere_sphere_features(A, ra, ab, nab, dist, crust_sum);
-          if (g.status) {
-            bool fatal;
-            g = sphere_sphere_error_handling(A, ra, own ? mdi.y : mdj.y, B, rb, own ? mdj.y : mdi.y, fatal);
-            set_status(a.stats, fatal ? GRAINS_GPU_CONTACT_ERROR : GRAINS_GPU_CONTACT_HANDLED);
-            if (fatal) continue;
-          }
-        } else {
-          // general convex pair: circumscribed-sphere test then GJK on crust-shrunk bodies
-          const double4 mdj = P.md[t];
-          BodyRef ba, bb;
-          const int sa = own ? s : t, sbx = own ? t : s;
-          make_body_ref(a, own ? mi.z : mj.z, sa, own ? mdi.y : mdj.y, ba);
-          make_body_ref(a, own ? mj.z : mi.z, sbx, own ? mdj.y : mdi.y, bb);
-          int it = 0, handled = 0;
-          g = convex_closest_point<R, SV>(a, ba, bb, it, handled);
-          if (own && g.status != 2) {
-            ++ngjk;
-            ngjk_it += it;
-          }
-          if (g.status == 2) continue;  // bounding spheres apart
-          if (handled) set_status(a.stats, g.status == 1 ? GRAINS_GPU_CONTACT_ERROR : GRAINS_GPU_CONTACT_HANDLED);
-          if (g.status == 1) continue;
-          if (!(g.overlap < 0.)) continue;
-          (void)mdj;
-        }
-        // contact: p0 = owner (lower id)
-        const double4 mdj = P.md[t];
-        const V3<R> vj = ld3<R>(P.v[t]), wj = ld3<R>(P.w[t]);
-        BodyAtContact<R> b0, b1;
-        const D3 lev0 = xsub3(g.point, A), lev1 = xsub3(g.point, B);
-        b0.v = own ? vi : vj;
-        b0.w = own ? wi : wj;
-        b0.lever = from_d3<R>(lev0);
-        b0.pos_minus_contact = from_d3<R>(xsub3(A, g.point));
-        b0.mass = R(own ? mdi.x : mdj.x);
-        b0.req = R(own ? mdi.z : mdj.z);
-        b1.v = own ? vj : vi;
-        b1.w = own ? wj : wi;
-        b1.lever = from_d3<R>(lev1);
-        b1.pos_minus_contact = from_d3<R>(xsub3(B, g.point));
-        b1.mass = R(own ? mdj.x : mdi.x);
-        b1.req = R(own ? mdj.z : mdi.z);
-        const int mat0 = own ? mi.y : mj.y, mat1 = own ? mj.y : mi.y;
-        const LawParams<R> L = a.laws[S.law_offset + mat0 * S.n_mat + mat1];
-        PairMemory<R> mem;
-        const int row0 = own ? oi : P.orig[t];
-        const int other = own ? idj : mi.x;
-        bool existed = false;
-        if (law_has_memory(L.type)) existed = find_memory(a, row0, other, 0, mem);
-        LawResult<R> res = pair_law(a, L, dt, g, b0, b1, existed, mem);
-        if (own && law_has_memory(L.type)) store_memory(a, oi, nnext, other, 0, mem);
-        // Torsor::addForce (Torsor.cpp:184-189); p1 gets -delFN - delFT
-        const V3<R> f = own ? res.force : -res.force;
-        F = F + f;
-        T = T + cross(own ? b0.lever : b1.lever, f);
-        if (law_has_torque(L)) T = T + (own ? res.torque : -res.torque);
-        ++ncontact;
-        if (own) {
-          ++ncont_own;
-          const double o = fabs(g.overlap);
-          ov_sum += o;
-          ov_max = fmax(ov_max, o);
-          if (DIAG && a.pairs) {
-            unsigned long long slot = atomicAdd(a.pairs_n, 1ull);
-            if (slot < (unsigned long long)a.pairs_cap) {
-              a.pairs[2 * slot] = mi.x;
-              a.pairs[2 * slot + 1] = idj;
-              if (a.pair_force) {
-                a.pair_force[3 * slot] = double(res.force.x);
-                a.pair_force[3 * slot + 1] = double(res.force.y);
-                a.pair_force[3 * slot + 2] = double(res.force.z);
-              }
-            }
-          }
-        }
-      }
-    }
-  }
-
-  // obstacles linked to the particle's cell (SimpleObstacle::InterAction, SimpleObstacle.cpp:222-270)
+  // obstacles linked to the particle's cell
   {
     const int cell = cell_index(S, ci, cj, ck);
     const int ob0 = a.cell_obs_start[cell], ob1 = a.cell_obs_start[cell + 1];
@@ -747,7 +626,6 @@ __device__ __forceinline__ void forces_one(const StepArgs<R>& a, int s, R dt, Fo
       } else {
         oidx = a.moving_idx[S.moving_offset + (u - nstat)];
         const ObstacleDev& O = a.obs[oidx];
-        // cell link of a moving obstacle: AABB vs twice-expanded cell (LinkedCell.cpp:1568-1585)
         if (!in_zone(d3(O.bbc[0], O.bbc[1], O.bbc[2]), d3(O.bbe[0], O.bbe[1], O.bbe[2]), cg, S.ex, S.ey, S.ez))
           continue;
       }
@@ -755,79 +633,456 @@ __device__ __forceinline__ void forces_one(const StepArgs<R>& a, int s, R dt, Fo
       if (!in_zone(d3(O.bbc[0], O.bbc[1], O.bbc[2]), d3(O.bbe[0], O.bbe[1], O.bbe[2]), Xi, xi.w, xi.w, xi.w))
         continue;
       ++nobs_cand;
-      M3 ob;
-      for (int q = 0; q < 9; ++q) ob.m[q] = O.b[q];
-      const D3 oo = d3(O.o[0], O.o[1], O.o[2]);
-      const double crust_sum = xadd(mdi.y, O.crust);
-      ContactGeom g;
-      const ShapeDev& sho = a.shapes[O.shape];
-      if (!CONVEX || (shi.type == GRAINS_GPU_SPHERE && sho.type == GRAINS_GPU_BOX)) {
-        g = sphere_box(Xi, xi.w, crust_sum, ob, oo, d3(sho.ext[0], sho.ext[1], sho.ext[2]));
-        if (g.status) {
-          set_status(a.stats, GRAINS_GPU_CONTACT_ERROR);
-          continue;
-        }
-      } else {
-        BodyRef ba, bb;
-        make_body_ref(a, mi.z, s, mdi.y, ba);
-        make_obstacle_ref(a, oidx, bb);
-        int it = 0, handled = 0;
-        g = convex_closest_point<R, SV>(a, ba, bb, it, handled);
-        if (g.status != 2) {
-          ++ngjk;
-          ngjk_it += it;
-        }
-        if (g.status == 2) continue;
-        if (handled) set_status(a.stats, g.status == 1 ? GRAINS_GPU_CONTACT_ERROR : GRAINS_GPU_CONTACT_HANDLED);
-        if (g.status == 1) continue;
-      }
-      if (!(g.overlap < 0.)) continue;
-      // contact: p0 = particle, p1 = obstacle (mass 1e20, velocity at point, Obstacle.cpp:128-133)
-      BodyAtContact<R> b0, b1;
-      b0.v = vi;
-      b0.w = wi;
-      b0.lever = from_d3<R>(xsub3(g.point, Xi));
-      b0.pos_minus_contact = from_d3<R>(xsub3(Xi, g.point));
-      b0.mass = R(mdi.x);
-      b0.req = R(mdi.z);
-      // the law adds w x lever to the centre velocity (velocity_at)
-      const D3 olev = xsub3(g.point, oo);
-      b1.v = v3<R>(R(O.vel[0]), R(O.vel[1]), R(O.vel[2]));
-      b1.w = v3<R>(R(O.omega[0]), R(O.omega[1]), R(O.omega[2]));
-      b1.lever = from_d3<R>(olev);
-      b1.pos_minus_contact = from_d3<R>(xsub3(oo, g.point));
-      b1.mass = R(kObstacleMass);
-      b1.req = R(pow((0.75 / kPi) * sho.volume, 1. / 3.));
-      const LawParams<R> L = a.laws[S.law_offset + mi.y * S.n_mat + O.material];
-      PairMemory<R> mem;
-      const int oloc = oidx - S.obs_offset;
-      bool existed = false;
-      if (law_has_memory(L.type)) existed = find_memory(a, oi, oloc, 1, mem);
-      LawResult<R> res = pair_law(a, L, dt, g, b0, b1, existed, mem);
-      if (law_has_memory(L.type)) store_memory(a, oi, nnext, oloc, 1, mem);
-      F = F + res.force;
-      T = T + cross(b0.lever, res.force);
-      if (law_has_torque(L)) T = T + res.torque;
-      ++ncontact;
-      ++nobs_cont;
-      const double o = fabs(g.overlap);
-      ov_sum += o;
-      ov_max = fmax(ov_max, o);
+      if (cnt < a.clist_cap) list[cnt] = -1 - oidx;
+      ++cnt;
+      ++owned;
     }
   }
-
-  P.F[s] = st3<R>(F);
-  P.T[s] = st3<R>(T);
-  a.coord[s] = ncontact;
-  a.hist_n_next[oi] = nnext;
+  if (cnt > a.clist_cap) {
+    set_status(a.stats, GRAINS_GPU_PAIR_OVERFLOW);
+    cnt = a.clist_cap;
+  }
+  a.ccount[s] = cnt;
+  ncand -= 1;  // the particle itself
+  n_work = owned;  // recounted by the caller when the list overflowed
 }
 
+// work items of the owned entries of particle s, at `base` onward; the rank
+// of an owned entry among the particle's owned entries is its contact-memory
+// position
+template <typename R>
+__device__ __forceinline__ void emit_work(const StepArgs<R>& a, int s, int base) {
+  const int* list = a.clist + (size_t)s * a.clist_cap;
+  const int cnt = a.ccount[s];
+  const long long limit = (long long)a.n * a.clist_cap;  // the work array's size
+  int rank = 0;
+  for (int q = 0; q < cnt; ++q) {
+    if (!entry_owned(list[q])) continue;
+    if ((long long)base + rank >= limit) {  // a counter left over from an unfinished evaluation
+      set_status(a.stats, GRAINS_GPU_CUDA_ERROR);
+      return;
+    }
+    a.work[base + rank] = make_int2(s, q | (rank << 9));
+    ++rank;
+  }
+}
+
+// warp sum of a per-thread count into a statistics counter (every lane of the
+// warp calls it)
+__device__ __forceinline__ void warp_add(unsigned long long* dst, unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v) atomicAdd(dst, v);
+}
+
+// one warp-aggregated reservation of work-item slots for every lane's count
+// (every lane of the warp calls it); returns the lane's first slot
+__device__ __forceinline__ int warp_reserve(int* counter, int count) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  int incl = count;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(full, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const int total = __shfl_sync(full, incl, 31);
+  int base = 0;
+  if (lane == 31 && total > 0) base = atomicAdd(counter, total);
+  base = __shfl_sync(full, base, 31);
+  return base + incl - count;
+}
+
+// contacts of particles first, first + stride, ... (all particles when the
+// threads of the grid start at 0 .. stride - 1); the trip count is uniform
+// across a warp for the warp-wide reservation and reductions
+template <typename R>
+__device__ __forceinline__ void contacts_range(const StepArgs<R>& a, int first, int stride) {
+  const int padded = (a.n + stride - 1) / stride * stride;
+  unsigned long long ncand = 0, nobs = 0;
+  for (int s = first; s < padded; s += stride) {
+    int nw = 0;
+    if (s < a.n) {
+      contacts_one(a, s, ncand, nobs, nw);
+      if (nw > 0 && a.ccount[s] == a.clist_cap) {  // the list may have overflowed: count what it holds
+        const int* list = a.clist + (size_t)s * a.clist_cap;
+        nw = 0;
+        for (int q = 0; q < a.clist_cap; ++q) nw += entry_owned(list[q]) ? 1 : 0;
+      }
+    }
+    const int base = warp_reserve(a.work_n, nw);
+    if (nw > 0) emit_work(a, s, base);
+  }
+  warp_add(&a.stats->n_cand, ncand);
+  warp_add(&a.stats->n_obs_cand, nobs);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) contacts_kernel(StepArgs<R> a) {
+  contacts_range(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+// ---------------------------------------------------------------------------
+// statistics of the force evaluation, summed per thread then per warp
+struct ForceStats {
+  unsigned long long ncont_own, nobs_cont, ngjk, ngjk_it;
+  double ov_sum, ov_max;
+};
+
+__device__ __forceinline__ void flush_force_stats(StatsDev* st, ForceStats& f) {
+  const unsigned full = 0xffffffffu;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    f.ncont_own += __shfl_down_sync(full, f.ncont_own, o);
+    f.nobs_cont += __shfl_down_sync(full, f.nobs_cont, o);
+    f.ngjk += __shfl_down_sync(full, f.ngjk, o);
+    f.ngjk_it += __shfl_down_sync(full, f.ngjk_it, o);
+    f.ov_sum += __shfl_down_sync(full, f.ov_sum, o);
+    f.ov_max = fmax(f.ov_max, __shfl_down_sync(full, f.ov_max, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (f.ncont_own) atomicAdd(&st->n_contacts, f.ncont_own);
+    if (f.nobs_cont) atomicAdd(&st->n_obs_contacts, f.nobs_cont);
+    if (f.ngjk) atomicAdd(&st->n_gjk_calls, f.ngjk);
+    if (f.ngjk_it) atomicAdd(&st->n_gjk_iters, f.ngjk_it);
+    if (f.ov_sum > 0.) atomicAdd(&st->overlap_sum, f.ov_sum);
+    if (f.ov_max > 0.) atomic_max_pos_double(&st->overlap_max_bits, f.ov_max);
+  }
+}
+
+// result of one list entry: (force, flag) and torque; flag 0 = no contact,
+// 1 = contact, 3 = contact whose owner stored a memory entry
+template <typename R>
+__device__ __forceinline__ void put_result(const StepArgs<R>& a, size_t slot, V3<R> f, V3<R> t, int flag) {
+  a.res_f[slot] = st3<R>(f, R(flag));
+  a.res_t[slot] = st3<R>(t);
+}
+template <typename R>
+__device__ __forceinline__ void put_no_contact(const StepArgs<R>& a, size_t slot) {
+  R4<R> z;
+  z.x = z.y = z.z = z.w = R(0);
+  a.res_f[slot] = z;
+}
+// a hole in the owner's next memory row (no contact, or a law without memory)
+template <typename R>
+__device__ __forceinline__ void put_memory_hole(const StepArgs<R>& a, int row, int rank) {
+  if (rank < a.hist_cap) a.hist_next[(size_t)row * a.hist_cap + rank].flags = -1;
+}
+template <typename R>
+__device__ __forceinline__ void put_memory(const StepArgs<R>& a, int row, int rank, int other, int flags,
+                                           const PairMemory<R>& m) {
+  if (rank >= a.hist_cap) {
+    set_status(a.stats, GRAINS_GPU_HISTORY_FULL);
+    return;
+  }
+  HistEntry<R> e;
+  e.other = other;
+  e.flags = flags;
+  e.kd[0] = m.kdelta.x; e.kd[1] = m.kdelta.y; e.kd[2] = m.kdelta.z;
+  e.n[0] = m.prev_normal.x; e.n[1] = m.prev_normal.y; e.n[2] = m.prev_normal.z;
+  e.sp[0] = m.spring.x; e.sp[1] = m.spring.y; e.sp[2] = m.spring.z;
+  a.hist_next[(size_t)row * a.hist_cap + rank] = e;
+}
+
+// B. one owned list entry: particle pair (p0 = this particle, the lower id)
+// or particle-obstacle candidate (p0 = the particle, p1 = the obstacle)
 template <typename R, bool DIAG, bool CONVEX, bool SV = false>
-__global__ void __launch_bounds__(128) forces_kernel(StepArgs<R> a, R dt) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  ForceStats fs{0, 0, 0, 0, 0, 0., 0.};
-  if (s < a.n) forces_one<R, DIAG, CONVEX, SV>(a, s, dt, fs);
+__device__ __forceinline__ void pair_one(const StepArgs<R>& a, int2 item, R dt, ForceStats& fs) {
+  const ParticleArrays<R>& P = a.cur;
+  const int s = item.x, q = item.y & 511, rank = item.y >> 9;
+  const size_t my_slot = (size_t)s * a.clist_cap + q;
+  const int e = a.clist[my_slot];
+  const double4 xi = P.xr[s];
+  const int4 mi = P.meta[s];
+  const double4 mdi = P.md[s];
+  const V3<R> vi = ld3<R>(P.v[s]);
+  const V3<R> wi = ld3<R>(P.w[s]);
+  const int oi = P.orig[s];
+  const SysDev& S = a.sys[mi.w];
+  const D3 Xi = d3(xi.x, xi.y, xi.z);
+
+  if (e >= 0) {
+    // ---- particle pair: this particle (s) is p0, the partner (t) p1
+    const int t = entry_slot(e);
+    const double4 xj = P.xr[t];
+    const int4 mj = P.meta[t];
+    // the partner's entry for this pair: its first 16 entries are loaded
+    // together (no load waits on a comparison), longer lists continue singly
+    const int* tl = a.clist + (size_t)t * a.clist_cap;
+    const int tn = a.ccount[t];
+    int qp = -1;
+    {
+      int4 ch[4];
+#pragma unroll
+      for (int c = 0; c < 4; ++c)
+        ch[c] = 4 * c < tn ? reinterpret_cast<const int4*>(tl)[c] : make_int4(-1, -1, -1, -1);
+#pragma unroll
+      for (int c = 3; c >= 0; --c) {
+        const int v[4] = {ch[c].w, ch[c].z, ch[c].y, ch[c].x};
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+          if (v[u] == s && 4 * c + 3 - u < tn) qp = 4 * c + 3 - u;  // a partner's entry for s never has kOwnBit
+      }
+      for (int k = 16; qp < 0 && k < tn; ++k)
+        if (tl[k] == s) qp = k;
+    }
+    const size_t other_slot = (size_t)t * a.clist_cap + (qp < 0 ? 0 : qp);
+    const D3 Xj = d3(xj.x, xj.y, xj.z);
+    ContactGeom g;
+    bool contact = true;
+    const double4 mdj = P.md[t];
+    if (!CONVEX || (a.shapes[mi.z].type == GRAINS_GPU_SPHERE && a.shapes[mj.z].type == GRAINS_GPU_SPHERE)) {
+      D3 ab;
+      double nab;
+      const double dist = sphere_sphere_overlap(Xi, xi.w, Xj, xj.w, &ab, &nab);
+      contact = dist < 0.;
+      if (contact) {
+        g = sphere_sphere_features(Xi, xi.w, ab, nab, dist, xadd(mdi.y, mdj.y));
+        if (g.status) {
+          bool fatal;
+          g = sphere_sphere_error_handling(Xi, xi.w, mdi.y, Xj, xj.w, mdj.y, fatal);
+          set_status(a.stats, fatal ? GRAINS_GPU_CONTACT_ERROR : GRAINS_GPU_CONTACT_HANDLED);
+          contact = !fatal;
+        }
+      }
+    } else {
+      // general convex pair: circumscribed-sphere test then GJK on crust-shrunk bodies
+      BodyRef ba, bb;
+      make_body_ref(a, mi.z, s, mdi.y, ba);
+      make_body_ref(a, mj.z, t, mdj.y, bb);
+      int it = 0, handled = 0;
+      g = convex_closest_point<R, SV>(a, ba, bb, it, handled);
+      if (g.status != 2) {
+        ++fs.ngjk;
+        fs.ngjk_it += it;
+      }
+      if (handled) set_status(a.stats, g.status == 1 ? GRAINS_GPU_CONTACT_ERROR : GRAINS_GPU_CONTACT_HANDLED);
+      contact = g.status == 0 && g.overlap < 0.;
+    }
+    if (!contact) {
+      put_no_contact(a, my_slot);
+      if (qp >= 0) put_no_contact(a, other_slot);
+      put_memory_hole(a, oi, rank);
+      return;
+    }
+    if (qp < 0) set_status(a.stats, GRAINS_GPU_PAIR_OVERFLOW);  // the partner's list overflowed
+    const V3<R> vj = ld3<R>(P.v[t]), wj = ld3<R>(P.w[t]);
+    const D3 lev0 = xsub3(g.point, Xi), lev1 = xsub3(g.point, Xj);
+    BodyAtContact<R> b0, b1;
+    b0.v = vi;
+    b0.w = wi;
+    b0.lever = from_d3<R>(lev0);
+    b0.pos_minus_contact = from_d3<R>(xsub3(Xi, g.point));
+    b0.mass = R(mdi.x);
+    b0.req = R(mdi.z);
+    b1.v = vj;
+    b1.w = wj;
+    b1.lever = from_d3<R>(lev1);
+    b1.pos_minus_contact = from_d3<R>(xsub3(Xj, g.point));
+    b1.mass = R(mdj.x);
+    b1.req = R(mdj.z);
+    const LawParams<R> L = a.laws[S.law_offset + mi.y * S.n_mat + mj.y];
+    PairMemory<R> mem;
+    bool existed = false;
+    if (law_has_memory(L.type)) existed = find_memory(a, oi, mj.x, 0, mem);
+    PairFp64 pd;
+    if constexpr (sizeof(R) == 4) {
+      pd.v0 = widen(vi);
+      pd.w0 = widen(wi);
+      pd.lev0 = dvec(lev0);
+      pd.v1 = widen(vj);
+      pd.w1 = widen(wj);
+      pd.lev1 = dvec(lev1);
+      pd.m0 = mdi.x;
+      pd.m1 = mdj.x;
+      pd.req0 = mdi.z;
+      pd.req1 = mdj.z;
+    }
+    V3<R> t0, t1;
+    LawResult<R> res = pair_law(L, dt, g, b0, b1, pd, existed, mem, t0, t1);
+    int flag = 1;
+    if (law_has_memory(L.type)) {
+      put_memory(a, oi, rank, mj.x, 0, mem);
+      flag = 3;
+    } else {
+      put_memory_hole(a, oi, rank);
+    }
+    // p0 gets f at the contact point, p1 gets -f (and the rolling torques +M / -M)
+    if (law_has_torque(L)) {
+      t0 = t0 + res.torque;
+      t1 = t1 + (-res.torque);
+    }
+    put_result(a, my_slot, res.force, t0, flag);
+    if (qp >= 0) put_result(a, other_slot, -res.force, t1, 1);
+    ++fs.ncont_own;
+    const double o = fabs(g.overlap);
+    fs.ov_sum += o;
+    fs.ov_max = fmax(fs.ov_max, o);
+    if (DIAG && a.pairs) {
+      unsigned long long slot = atomicAdd(a.pairs_n, 1ull);
+      if (slot < (unsigned long long)a.pairs_cap) {
+        a.pairs[2 * slot] = mi.x;
+        a.pairs[2 * slot + 1] = mj.x;
+        a.pair_sys[slot] = mi.w;
+        if (a.pair_force) {
+          a.pair_force[3 * slot] = double(res.force.x);
+          a.pair_force[3 * slot + 1] = double(res.force.y);
+          a.pair_force[3 * slot + 2] = double(res.force.z);
+        }
+      }
+    }
+    return;
+  }
+
+  // ---- obstacle candidate (SimpleObstacle::InterAction, SimpleObstacle.cpp:222-270)
+  const int oidx = -1 - e;
+  const ObstacleDev& O = a.obs[oidx];
+  const D3 oo = d3(O.o[0], O.o[1], O.o[2]);
+  const ShapeDev& sho = a.shapes[O.shape];
+  ContactGeom g;
+  if (!CONVEX || (a.shapes[mi.z].type == GRAINS_GPU_SPHERE && sho.type == GRAINS_GPU_BOX)) {
+    M3 ob;
+    for (int k = 0; k < 9; ++k) ob.m[k] = O.b[k];
+    g = sphere_box(Xi, xi.w, xadd(mdi.y, O.crust), ob, oo, d3(sho.ext[0], sho.ext[1], sho.ext[2]));
+    if (g.status) {
+      set_status(a.stats, GRAINS_GPU_CONTACT_ERROR);
+      g.overlap = 1.;
+    }
+  } else {
+    BodyRef ba, bb;
+    make_body_ref(a, mi.z, s, mdi.y, ba);
+    make_obstacle_ref(a, oidx, bb);
+    int it = 0, handled = 0;
+    g = convex_closest_point<R, SV>(a, ba, bb, it, handled);
+    if (g.status != 2) {
+      ++fs.ngjk;
+      fs.ngjk_it += it;
+    }
+    if (handled) set_status(a.stats, g.status == 1 ? GRAINS_GPU_CONTACT_ERROR : GRAINS_GPU_CONTACT_HANDLED);
+    if (g.status != 0) g.overlap = 1.;
+  }
+  if (!(g.overlap < 0.)) {
+    put_no_contact(a, my_slot);
+    put_memory_hole(a, oi, rank);
+    return;
+  }
+  // p0 = particle, p1 = obstacle (mass 1e20, velocity at the point, Obstacle.cpp:128-133)
+  BodyAtContact<R> b0, b1;
+  b0.v = vi;
+  b0.w = wi;
+  b0.lever = from_d3<R>(xsub3(g.point, Xi));
+  b0.pos_minus_contact = from_d3<R>(xsub3(Xi, g.point));
+  b0.mass = R(mdi.x);
+  b0.req = R(mdi.z);
+  // the law adds w x lever to the centre velocity (velocity_at)
+  const D3 olev = xsub3(g.point, oo);
+  b1.v = v3<R>(R(O.vel[0]), R(O.vel[1]), R(O.vel[2]));
+  b1.w = v3<R>(R(O.omega[0]), R(O.omega[1]), R(O.omega[2]));
+  b1.lever = from_d3<R>(olev);
+  b1.pos_minus_contact = from_d3<R>(xsub3(oo, g.point));
+  b1.mass = R(kObstacleMass);
+  b1.req = R(pow((0.75 / kPi) * sho.volume, 1. / 3.));
+  const LawParams<R> L = a.laws[S.law_offset + mi.y * S.n_mat + O.material];
+  PairMemory<R> mem;
+  const int oloc = oidx - S.obs_offset;
+  bool existed = false;
+  if (law_has_memory(L.type)) existed = find_memory(a, oi, oloc, 1, mem);
+  PairFp64 pd;
+  if constexpr (sizeof(R) == 4) {
+    pd.v0 = widen(vi);
+    pd.w0 = widen(wi);
+    pd.lev0 = dvec(xsub3(g.point, Xi));
+    pd.v1 = v3<double>(O.vel[0], O.vel[1], O.vel[2]);
+    pd.w1 = v3<double>(O.omega[0], O.omega[1], O.omega[2]);
+    pd.lev1 = dvec(olev);
+    pd.m0 = mdi.x;
+    pd.m1 = kObstacleMass;
+    pd.req0 = mdi.z;
+    pd.req1 = pow((0.75 / kPi) * sho.volume, 1. / 3.);
+  }
+  V3<R> t0, t1;
+  LawResult<R> res = pair_law(L, dt, g, b0, b1, pd, existed, mem, t0, t1);
+  int flag = 1;
+  if (law_has_memory(L.type)) {
+    put_memory(a, oi, rank, oloc, 1, mem);
+    flag = 3;
+  } else {
+    put_memory_hole(a, oi, rank);
+  }
+  if (law_has_torque(L)) t0 = t0 + res.torque;
+  put_result(a, my_slot, res.force, t0, flag);
+  ++fs.nobs_cont;
+  const double o = fabs(g.overlap);
+  fs.ov_sum += o;
+  fs.ov_max = fmax(fs.ov_max, o);
+}
+
+// work items [first, n_items) with the given stride; `padded`: a bound with a
+// uniform trip count for the warp reductions of the statistics
+template <typename R, bool DIAG, bool CONVEX, bool SV = false>
+__device__ __forceinline__ void pairs_range(const StepArgs<R>& a, int first, int stride, R dt) {
+  const int n_items = (int)min((long long)*(volatile int*)a.work_n, (long long)a.n * a.clist_cap);
+  const int padded = (n_items + stride - 1) / stride * stride;
+  ForceStats fs{0, 0, 0, 0, 0., 0.};
+  for (int k = first; k < padded; k += stride)
+    if (k < n_items) pair_one<R, DIAG, CONVEX, SV>(a, a.work[k], dt, fs);
   flush_force_stats(a.stats, fs);
+}
+
+// blocks per SM the register allocation of the sphere kernels must allow
+#ifndef GG_PAIRS_MIN_BLOCKS
+#define GG_PAIRS_MIN_BLOCKS 1
+#endif
+template <typename R, bool DIAG, bool CONVEX, bool SV = false>
+__global__ void __launch_bounds__(128, CONVEX ? 1 : GG_PAIRS_MIN_BLOCKS) pairs_kernel(StepArgs<R> a, R dt) {
+  pairs_range<R, DIAG, CONVEX, SV>(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, dt);
+}
+
+// C. the torsor of particle s: InitializeForces(withWeight) (torsor = weight,
+// Particle.cpp:1409-1416) then every contact in list order; the coordination
+// number; the owner's next memory row packed.  Clears the work counter for the
+// next evaluation (thread 0; every pair item was read before this kernel).
+template <typename R>
+__device__ __forceinline__ void sum_one(const StepArgs<R>& a, int s) {
+  const ParticleArrays<R>& P = a.cur;
+  const int sysi = P.meta[s].w;
+  const double mass = P.md[s].x;
+  const SysDev& S = a.sys[sysi];
+  V3<R> F = v3<R>(R(S.gx * mass), R(S.gy * mass), R(S.gz * mass));
+  V3<R> T = v3<R>(R(0), R(0), R(0));
+  const int cnt = a.ccount[s];
+  const size_t base = (size_t)s * a.clist_cap;
+  const int* list = a.clist + base;
+  int ncontact = 0, owned = 0;
+  for (int q = 0; q < cnt; ++q) {
+    const R4<R> rf = a.res_f[base + q];
+    owned += entry_owned(list[q]) ? 1 : 0;
+    if (rf.w == R(0)) continue;
+    F = F + ld3<R>(rf);
+    T = T + ld3<R>(a.res_t[base + q]);
+    ++ncontact;
+  }
+  a.coord[s] = ncontact;
+  // pack the memory row: holes (flags -1) are squeezed out, order kept
+  const int row = P.orig[s];
+  HistEntry<R>* h = a.hist_next + (size_t)row * a.hist_cap;
+  const int m = min(owned, a.hist_cap);
+  int kept = 0;
+  for (int r = 0; r < m; ++r) {
+    if (h[r].flags < 0) continue;
+    if (kept != r) h[kept] = h[r];
+    ++kept;
+  }
+  a.hist_n_next[row] = kept;
+  P.F[s] = st3<R>(F);
+  P.T[s] = st3<R>(T);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) sums_kernel(StepArgs<R> a) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s == 0) *a.work_n = 0;
+  if (s < a.n) sum_one(a, s);
 }
 
 template <typename R>
@@ -1156,23 +1411,26 @@ int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int
   const int fb = (a.forces_block >= 32 && a.forces_block <= 128) ? a.forces_block : 128;
   if (phases & 1) contacts_kernel<R><<<grid_for(a.n, cb), cb, 0, s>>>(a);
   if (!(phases & 2)) return check_launch();
-  const int g = grid_for(a.n, fb);
+  // about two work items per thread in a settled packing; the grid-stride
+  // loop takes any count
+  const int g = (int)std::min<long long>(grid_for(2ll * a.n, fb), 1ll << 20);
   if (a.has_convex && a.gjk_sv) {  // the signed-volume GJK: a kernel of its own
     if (diag)
-      forces_kernel<R, true, true, true><<<g, fb, 0, s>>>(a, R(dt));
+      pairs_kernel<R, true, true, true><<<g, fb, 0, s>>>(a, R(dt));
     else
-      forces_kernel<R, false, true, true><<<g, fb, 0, s>>>(a, R(dt));
+      pairs_kernel<R, false, true, true><<<g, fb, 0, s>>>(a, R(dt));
   } else if (a.has_convex) {
     if (diag)
-      forces_kernel<R, true, true><<<g, fb, 0, s>>>(a, R(dt));
+      pairs_kernel<R, true, true><<<g, fb, 0, s>>>(a, R(dt));
     else
-      forces_kernel<R, false, true><<<g, fb, 0, s>>>(a, R(dt));
+      pairs_kernel<R, false, true><<<g, fb, 0, s>>>(a, R(dt));
   } else {
     if (diag)
-      forces_kernel<R, true, false><<<g, fb, 0, s>>>(a, R(dt));
+      pairs_kernel<R, true, false><<<g, fb, 0, s>>>(a, R(dt));
     else
-      forces_kernel<R, false, false><<<g, fb, 0, s>>>(a, R(dt));
+      pairs_kernel<R, false, false><<<g, fb, 0, s>>>(a, R(dt));
   }
+  sums_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
   return check_launch();
 }
 
@@ -1264,7 +1522,6 @@ __global__ void __launch_bounds__(kPersistentThreads) persistent_steps_kernel(
   const int nthreads = gridDim.x * blockDim.x;
   const int tid = blockIdx.x * blockDim.x + threadIdx.x;
   const int n = a.n, C = a.n_cells;
-  const int n_pad = (n + nthreads - 1) / nthreads * nthreads;  // uniform trip counts for warp reductions
   int* status = &a.stats->status;
   __shared__ int offset_s;
   for (int step = 0; step < n_steps; ++step) {
@@ -1311,19 +1568,12 @@ __global__ void __launch_bounds__(kPersistentThreads) persistent_steps_kernel(
     } else {
       ++since_gather;
     }
-    {
-      unsigned long long ncand = 0;
-      for (int s = tid; s < n_pad; s += nthreads)
-        if (s < n) contacts_one(a, s, ncand);
-      warp_add(&a.stats->n_cand, ncand);
-    }
+    contacts_range(a, tid, nthreads);
     if (!grid_barrier(bar, status)) return;
-    {
-      ForceStats fs{0, 0, 0, 0, 0, 0., 0.};
-      for (int s = tid; s < n_pad; s += nthreads)
-        if (s < n) forces_one<R, false, CONVEX>(a, s, dt_r, fs);
-      flush_force_stats(a.stats, fs);
-    }
+    pairs_range<R, false, CONVEX>(a, tid, nthreads, dt_r);
+    if (!grid_barrier(bar, status)) return;
+    if (tid == 0) *a.work_n = 0;  // every block has read the count
+    for (int s = tid; s < n; s += nthreads) sum_one(a, s);
     {
       HistEntry<R>* h = a.hist_prev;
       a.hist_prev = a.hist_next;

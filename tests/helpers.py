@@ -42,16 +42,15 @@ def rel_err_quantile(a, b, floor, q):
 
 
 def check_contact_forces(fg, fo, floor, precision):
-    """Per-contact forces: FP64 at rounding level.  Mixed: 1e-5 for 99 % of the
-    contacts and 1e-4 for all.  The FP32 law rounds each term to ~6e-8 of
-    itself, but where the elastic and viscous normal terms nearly cancel (a
-    contact about to open) the relative error of their sum grows by the
-    cancellation ratio."""
+    """Per-contact forces: FP64 at rounding level; mixed precision within
+    1e-5 for every contact (the north star's bar).  The mixed law forms its
+    normal part (the elastic and viscous terms, which nearly cancel on a
+    contact about to open) in double, so FP32 rounding enters only the
+    tangential part and the final force, about 1e-7 of the force."""
     if precision == FP64:
         assert rel_err(fg, fo, floor) < 1e-12
     else:
-        assert rel_err_quantile(fg, fo, floor, 0.99) < 1e-5
-        assert rel_err(fg, fo, floor) < 1e-4
+        assert rel_err(fg, fo, floor) < 1e-5
 
 
 TANGENT_SO = None

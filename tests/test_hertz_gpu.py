@@ -5,7 +5,8 @@ which the reference fixtures hertz_dense125 and hertz_memory216_rolling pin.
 Dense clusters, advanced by the oracle under the Hertz law until most lattice
 neighbours touch, then one force evaluation and a short trajectory from the
 same state on both sides.  Bars as for the Hooke laws: plain FP64 forces within
-1e-12 relative (floor: the particle weight), mixed precision within 1e-5."""
+1e-12 relative (floor: the particle weight), mixed precision within 1e-5;
+mixed torques within 3e-5 of the 1e-7 N m floor."""
 import numpy as np
 import pytest
 
@@ -54,7 +55,11 @@ def test_one_force_evaluation(oracle_lib, gpu_lib, law, precision):
     assert np.array_equal(do["coordination"], dg["coordination"])
     weight = sc.particles["mass"][0] * 9.81
     assert rel_err(dg["force"], do["force"], weight) < (1e-12 if precision == FP64 else 1e-5)
-    assert rel_err(dg["torque"], do["torque"], weight * 1e-3) < (1e-10 if precision == FP64 else 1e-5)
+    # mixed torques: a particle's torque is the sum of its contacts' tangential
+    # torques (|lever| |F_t| ~ 1e-5 N m here), which nearly cancel, each
+    # carrying FP32 rounding of 1e-7 of itself; against the 1e-7 N m floor that
+    # is up to a few 1e-5
+    assert rel_err(dg["torque"], do["torque"], weight * 1e-3) < (1e-10 if precision == FP64 else 3e-5)
     pg, fg = g.contact_forces()
     po, fo = o.contact_forces()
     assert np.array_equal(pg, po)
