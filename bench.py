@@ -10,7 +10,14 @@ workload, replayed from CUDA graphs on resident device state; the default
 (after W warm-up chunks and a reset).  L2 is flushed (a 256 MiB write)
 between timed chunks.  `value` is particle-steps/s of the
 whole job (all ranks); `e2e` is the same metric through the C ABI with host
-buffers: upload of the state, the chunk, download of the state.
+buffers in pinned memory: update of the kinematic state, the chunk, download
+of the state.
+
+Config 1 starts from a sparse lattice (mean coordination ~0.1 over its 20,000
+steps), so the line also carries a `settled` leg: the bed settled on the
+device (70,000 steps), saved as a reference reload file and read back, then
+10 x 1,000 steps timed in mixed precision and in FP64 from that state (mean
+coordination ~5), with its per-phase times, roofline and contact-force error.
 
 With --gpus N (launched by torchrun) every rank runs an independent replica
 (the single system is not partitioned across GPUs): weak scaling.
@@ -32,16 +39,21 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-# Algorithmic HBM bytes per particle of the per-step kernels (z = mean
-# coordination number, contacts per particle incl. walls; R4 = 16 B in mixed
-# precision, 32 B in FP64; a contact-memory entry is 44 B / 80 B):
-#  contacts_kernel: own position+radius (32) and meta (16) in, the 9 cell-row
-#   ranges (72), list length (4) and z list entries (4 z) out; the neighbours'
-#   positions are re-read from L1/L2 and not counted.
-#  forces_kernel: own xr, meta, md (32 + 16 + 32), v, w (2 R4), upload index,
-#   list length, cell obstacle range (4 + 4 + 8) and z list entries in, the z
-#   memory entries looked up; F, T (2 R4), coordination and memory count (8)
-#   and the z/2 owned memory entries out.
+# Algorithmic HBM bytes per particle of one launch of each step kernel: every
+# array the kernel must touch, once (z = contacts per particle incl. walls,
+# the list entries of the force evaluation; R4 = 16 B in mixed precision, 32 B
+# in FP64; a contact-memory entry is 44 B / 80 B; a pair's two list entries and
+# its work item count once per particle on average):
+#  contacts_kernel: own position+radius (32), meta (16) and cell key (4), the
+#   9 cell-row ranges (72), list length (4) in/out; z list entries (4 z) and
+#   z/2 work items (8 z/2) out.  Neighbour positions are re-read from L1/L2
+#   and not counted.
+#  pairs_kernel: own xr, meta, md, upload index (32 + 16 + 32 + 4), v, w
+#   (2 R4), the list (4 z) and the work items (8 z/2) in; the owner's z/2
+#   memory entries in and out; the results of the z entries (2 R4 each) out.
+#  sums_kernel: md, meta, upload index, list length (32 + 16 + 4 + 4), the list
+#   (4 z) and the z results (2 R4 each) in; F, T (2 R4), coordination and
+#   memory count (8) out, the memory row packed (z/2 entries in place).
 #  kick_move_kernel: xr, q, meta, md (32 + 32 + 16 + 32), v, w, wbf, inertia,
 #   F, T (6 R4) in; xr, q (64), v, w, wbf (3 R4), cell key and count (8) out.
 #   Bodies that are not spheres also carry their rotation matrix (72 B in and out).
@@ -49,9 +61,11 @@ def kernel_bytes(kernel, precision, z, basis=False):
     r4 = 16 if precision == "mixed" else 32
     entry = 44 if precision == "mixed" else 80
     if kernel == "contacts":
-        return 32 + 16 + 72 + 4 + 4 * z
-    if kernel == "forces":
-        return (32 + 16 + 32 + 2 * r4 + 16 + 4 * z + z * entry) + (2 * r4 + 8 + (z / 2.0) * entry)
+        return 32 + 16 + 4 + 72 + 4 + 4 * z + 8 * z / 2.0
+    if kernel == "pairs":
+        return 84 + 2 * r4 + 4 * z + 8 * z / 2.0 + 2 * (z / 2.0) * entry + 2 * r4 * z
+    if kernel == "sums":
+        return 56 + 4 * z + 2 * r4 * z + 2 * r4 + 8 + (z / 2.0) * entry
     return (32 + 32 + 16 + 32 + 6 * r4) + (64 + 3 * r4 + 8) + (144 if basis else 0)
 
 
@@ -64,13 +78,16 @@ def parse():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--workload", default="polydisperse_200k")
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-steps", type=int, default=10)
     ap.add_argument("--ref-dem-steps", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison run")
     ap.add_argument("--adjoint", action="store_true", help="time the adjoint workload (4,096 spheres)")
     ap.add_argument("--no-io", action="store_true", help="skip the reload / RawData file writers")
+    ap.add_argument("--settle-steps", type=int, default=None,
+                    help="DEM steps that settle the bed before the settled leg (0: no settled leg; default "
+                         "70,000 for polydisperse_200k, 100,000 for drum_100k, none otherwise)")
+    ap.add_argument("--settled-chunks", type=int, default=10, help="timed chunks of the settled leg")
     return ap.parse_args()
 
 
@@ -277,11 +294,11 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def contact_force_error(lib, sc, state, mem, device):
+def contact_force_error(lib, sc, state, mem, device, where):
     """Per-contact relative error of the mixed-precision contact forces against
     the plain FP64 path on identical states and contact memories: max and 99th
     percentile of |f_mixed - f_fp64| / max(|f_fp64|, weight) over the
-    particle-particle contacts."""
+    particle-particle contacts of every system."""
     from pacific_b200 import scenarios as S
     from pacific_b200.abi import FP64, MIXED, Simulation
     p = dict(sc.particles)
@@ -289,14 +306,15 @@ def contact_force_error(lib, sc, state, mem, device):
         p[k] = state[k]
     if sc.particles.get("basis") is not None:
         p["basis"] = state["basis"]
-    sc2 = S.Scenario(sc.name, sc.shapes, sc.domains, sc.laws, sc.obstacles, p, sc.dt, sc.n_steps)
+    sc2 = S.Scenario(sc.name, sc.shapes, sc.domains, sc.laws, sc.obstacles, p, sc.dt, sc.n_steps, meta=sc.meta)
     res = {}
     for name, prec in [("fp64", FP64), ("mixed", MIXED)]:
         s = Simulation(lib, prec, max_particles=sc.n, n_systems=len(sc.domains), device=device)
         S.apply(s, sc2)
         s.upload_contact_memory(mem)
         s.compute_forces(0.0, sc.dt)
-        res[name] = s.contact_forces()
+        per = [s.contact_forces(k) for k in range(len(sc.domains))]
+        res[name] = (np.concatenate([q[0] for q in per]), np.concatenate([q[1] for q in per]))
         s.close()
     (p64, f64_), (pm, fm) = res["fp64"], res["mixed"]
     if len(p64) == 0 or not np.array_equal(p64, pm):
@@ -304,8 +322,117 @@ def contact_force_error(lib, sc, state, mem, device):
     w = float(np.min(sc.particles["mass"])) * 9.81
     rel = np.linalg.norm(fm - f64_, axis=1) / np.maximum(np.linalg.norm(f64_, axis=1), w)
     return {"max": float(rel.max()), "p99": float(np.quantile(rel, 0.99)), "median": float(np.median(rel)),
-            "n_contacts": int(len(rel)), "pairs_equal": True, "floor": "particle weight",
-            "state": "end of the timed run, same state and contact memory in both precisions"}
+            "n_contacts": int(len(rel)), "systems": len(sc.domains), "pairs_equal": True, "floor": "particle weight",
+            "state": where + ", same state and contact memory in both precisions"}
+
+
+def profile_run(sim, sc, n_steps, t):
+    """Per-phase device times (ms per DEM step) of n_steps uncaptured steps and
+    the dominant kernel of the step with its algorithmic bytes."""
+    tp, prof = sim.profile_kernels(n_steps, t, sc.dt)
+    return tp, {k: v[0] / n_steps for k, v in prof.items()}, {k: v for k, v in prof.items()}
+
+
+def roofline(prof_tot, sc, precision, z, peak, peak_kind, traffic_of):
+    from pacific_b200 import scenarios as S
+    dom = max(["contacts", "pairs", "sums", "kick_move"], key=lambda k: prof_tot[k][0])
+    k_ms, k_n = prof_tot[dom]
+    basis = any(sc.shapes[k][0] != S.SPHERE for k in set(np.asarray(sc.particles["shape"]).tolist()))
+    alg = sc.n * kernel_bytes(dom, precision, z, basis)
+    achieved = alg / (k_ms / k_n / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic_of(dom), "kernel": dom + "_kernel", "peak_source": peak_kind,
+            "algorithmic_bytes_per_launch": alg, "mean_coordination": z, "launch_ms": k_ms / k_n}
+
+
+def mean_coordination(sim, sc, t):
+    sim.reset_stats()
+    sim.compute_forces(t, sc.dt)
+    st = sim.stats()
+    return (2.0 * st["n_contacts"] + st["n_obstacle_contacts"]) / sc.n
+
+
+def settled_leg(args, lib, sc, local, flush, peak, peak_kind):
+    """The 200k bed settled on the device: `settle_steps` DEM steps from the
+    initial state, saved as a reference reload file (hybrid binary) and read
+    back; then `settled_chunks` x chunk steps timed in mixed precision and in
+    FP64 from that same state (after the same warm-up), the per-phase times,
+    the roofline of the dominant kernel and the contact-force error there."""
+    import tempfile
+    import torch
+    from pacific_b200 import scenarios as S
+    from pacific_b200.abi import FP64, MIXED, Simulation, read_reload_particles
+    sim = Simulation(lib, MIXED, max_particles=sc.n, device=local)
+    S.apply(sim, sc)
+    sim.initialize_leapfrog(0.0, sc.dt)
+    t, done = 0.0, 0
+    while done < args.settle_steps:
+        k = min(5000, args.settle_steps - done)
+        t = sim.step(k, t, sc.dt)
+        done += k
+    sim.synchronize()
+    z_settled = mean_coordination(sim, sc, t)
+    with tempfile.TemporaryDirectory(prefix="gg_settled") as d:
+        path = os.path.join(d, "settled_Particles.bin")
+        t0 = time.perf_counter()
+        nbytes = sim.write_reload_particles(path, binary=True)
+        w_s = time.perf_counter() - t0
+        r = read_reload_particles(lib, path, True)
+    sim.close()
+    p = dict(sc.particles)
+    order = np.argsort(r["id"])
+    for k in ["position", "quaternion", "velocity", "omega"]:
+        p[k] = np.ascontiguousarray(r[k][order])
+    sc2 = S.Scenario(sc.name, sc.shapes, sc.domains, sc.laws, sc.obstacles, p, sc.dt, sc.n_steps, meta=sc.meta)
+    mem = r["memory"]
+    out = {"settle_steps": args.settle_steps, "mean_coordination_after_settling": z_settled,
+           "reload_file": {"bytes": int(nbytes), "write_ms": w_s * 1e3, "format": "hybrid binary"}}
+
+    def run(prec):
+        s = Simulation(lib, prec, max_particles=sc.n, device=local)
+        S.apply(s, sc2)
+        s.upload_contact_memory(mem)
+        s.initialize_leapfrog(t, sc.dt)
+        stream = torch.cuda.ExternalStream(s.stream_handle(), device=local)
+        tt = t
+        for _ in range(args.warmup):
+            tt = s.step(args.chunk, tt, sc.dt)
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+              for _ in range(args.settled_chunks)]
+        torch.cuda.synchronize()
+        for k in range(args.settled_chunks):
+            with torch.cuda.stream(stream):
+                flush.fill_(k & 0xFF)
+                ev[k][0].record(stream)
+            tt = s.step(args.chunk, tt, sc.dt)
+            ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in ev)
+        return s, tt, ms
+    sm, tm, ms_m = run(MIXED)
+    z = mean_coordination(sm, sc, tm)
+    gst = sm.stats()  # of that one force evaluation
+    _, per_step, tot = profile_run(sm, sc, 500, tm)
+    sm.close()
+    s64, _, ms_64 = run(FP64)
+    s64.close()
+    steps = args.settled_chunks * args.chunk
+    v_m, v_64 = sc.n * steps / (ms_m / 1e3), sc.n * steps / (ms_64 / 1e3)
+    out.update({"value": v_m, "unit": "particle-steps/s", "ms_per_dem_step": ms_m / steps,
+                "timed_dem_steps": steps, "mean_coordination": z,
+                "fp64": {"value": v_64, "ms_per_dem_step": ms_64 / steps, "mixed_over_fp64": v_m / v_64},
+                "kernels_ms_per_dem_step": per_step,
+                "roofline": roofline(tot, sc, "mixed", z, peak, peak_kind,
+                                     lambda k: profiled_traffic(k, sc.name + "_settled", "mixed")),
+                "contact_force_error": contact_force_error(lib, sc, sc2.particles, mem, local,
+                                                           "the settled bed read back from its reload file")})
+    if gst["n_gjk_calls"]:
+        # GJK calls and iterations of one force evaluation (the running
+        # statistics of AppCollision::addToContactsFeatures, AppCollision.cpp:160-187)
+        out["gjk"] = {"calls_per_dem_step": gst["n_gjk_calls"],
+                      "mean_iterations": gst["n_gjk_iterations"] / gst["n_gjk_calls"],
+                      "pairs_per_s": gst["n_gjk_calls"] / (ms_m / 1e3 / steps)}
+    return out
 
 
 def run_adjoint(args, rank, world, local):
@@ -447,42 +574,40 @@ def main():
     prof_tot = {}
     zs = []
     for k in range(args.steps):
-        tp, prof = sim.profile_kernels(args.chunk, tp, sc.dt)
+        tp, _, prof = profile_run(sim, sc, args.chunk, tp)
         for name, (ms_k, n_k) in prof.items():
             a0, b0 = prof_tot.get(name, (0.0, 0))
             prof_tot[name] = (a0 + ms_k, b0 + n_k)
-        sim.reset_stats()
-        sim.compute_forces(tp, sc.dt)
-        st3 = sim.stats()
-        zs.append((2.0 * st3["n_contacts"] + st3["n_obstacle_contacts"]) / sc.n)
+        zs.append(mean_coordination(sim, sc, tp))
     z = float(np.mean(zs))
-    dom = max(["contacts", "forces", "kick_move"], key=lambda k: prof_tot[k][0])
-    fk_ms, fk_n = prof_tot[dom]
-    basis = any(sc.shapes[k][0] != S.SPHERE for k in set(np.asarray(sc.particles["shape"]).tolist()))
-    alg_bytes = sc.n * kernel_bytes(dom, args.precision, z, basis)
-    achieved = alg_bytes / (fk_ms / fk_n / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
-    traffic = profiled_traffic(dom, sc.name, args.precision)
     n_prof = args.chunk * args.steps
-    prof = prof_tot
 
-    # end to end through the C ABI with host buffers: state up, one chunk, state down
-    host = sim.download()
-    e2e_times = []
-    h2d = d2h = 0
-    for k in range(args.e2e_steps + 1):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
+    # end to end through the C ABI with host buffers in pinned memory, over
+    # the same window of K chunks from the initial state: every chunk updates
+    # the kinematic state from the host, steps, and downloads the state and
+    # the coordination numbers
+    def pinned(shape, dtype):
+        return torch.empty(shape, dtype=dtype, pin_memory=True).numpy()
+    host = {"position": pinned((sc.n, 3), torch.float64), "quaternion": pinned((sc.n, 4), torch.float64),
+            "velocity": pinned((sc.n, 3), torch.float64), "omega": pinned((sc.n, 3), torch.float64),
+            "coordination": pinned((sc.n,), torch.int32)}
+    sim.update(sc.particles)
+    sim.initialize_leapfrog(0.0, sc.dt)
+    t = 0.0
+    sim.download(out=host)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for k in range(args.steps):
         sim.update(host)
         t = sim.step(args.chunk, t, sc.dt)
-        host = sim.download()
-        el = time.perf_counter() - t0
-        h2d = sum(host[kk].nbytes for kk in ["position", "quaternion", "velocity", "omega"])
-        d2h = sum(v.nbytes for v in host.values())
-        if k > 0:
-            e2e_times.append(el)
-    e2e_s = float(np.median(e2e_times))
+        sim.download(out=host)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    h2d = sum(host[kk].nbytes for kk in ["position", "quaternion", "velocity", "omega"])
+    d2h = sum(v.nbytes for v in host.values())
     e2e_value = total_particles * args.chunk / e2e_s
+    gather_every = sim.tuning()["gather_every"]
+    launches = sim.launches_per_step() * args.chunk * args.steps + (args.chunk * args.steps) // gather_every
 
     line = {
         "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
@@ -494,14 +619,12 @@ def main():
                    "dem_steps_per_step": args.chunk, "dt": sc.dt,
                    "parallelism": "replicas" if world > 1 else "1gpu",
                    "l2": "flushed (256 MiB write) between timed steps"},
-        "gpu_launches": int(sim.launches_per_step() * args.chunk * args.steps),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "kernel": dom + "_kernel", "peak_source": peak_kind,
-                     "algorithmic_bytes_per_launch": alg_bytes, "mean_coordination": z,
-                     "launch_ms": fk_ms / fk_n},
+        "gpu_launches": int(launches),
+        "roofline": roofline(prof_tot, sc, args.precision, z, peak, peak_kind,
+                             lambda k: profiled_traffic(k, sc.name, args.precision)),
         "e2e": {"value": e2e_value, "unit": "particle-steps/s", "h2d_bytes_per_step": int(h2d),
-                "d2h_bytes_per_step": int(d2h)},
-        "kernels_ms_per_dem_step": {k: v[0] / n_prof for k, v in prof.items()},
+                "d2h_bytes_per_step": int(d2h), "host_buffers": "pinned", "over_device": e2e_value / value},
+        "kernels_ms_per_dem_step": {k: v[0] / n_prof for k, v in prof_tot.items()},
         "kernel_timing": "uncaptured re-run of the timed window with CUDA events around each phase",
         "status": st["status"],
         "clocks": clk.summary(),
@@ -518,10 +641,11 @@ def main():
         v64 = total_particles * args.chunk * args.steps / (ms64 / 1e3)
         line["fp64"] = {"value": v64, "unit": "particle-steps/s", "ms_per_step": ms64 / args.steps,
                         "mixed_over_fp64": value / v64}
-        if len(sc.domains) == 1:
-            line["contact_force_error"] = contact_force_error(lib, sc, st_end, mem_end, local)
-        else:  # contact-memory ids are per system; the comparison is run on single systems
-            line["contact_force_error"] = None
+        line["contact_force_error"] = contact_force_error(lib, sc, st_end, mem_end, local, "end of the timed run")
+    if args.settle_steps is None:
+        args.settle_steps = {"polydisperse_200k": 70000, "drum_100k": 100000}.get(sc.name, 0)
+    if world == 1 and prec == MIXED and args.settle_steps > 0 and not args.no_fp64:
+        line["settled"] = settled_leg(args, lib, sc, local, flush, peak, peak_kind)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"], cpu_sim = cpu_baseline(scenario(args.workload), args.cpu_steps, keep=True)

@@ -354,13 +354,24 @@ int grains_gpu_autotune(grains_gpu_ctx* ctx, double time, double dt, int32_t tri
                         grains_gpu_tuning* best, double* best_ms);
 
 /* ---- timing helpers for benchmarks ---------------------------------------- */
-/* Times each kernel of n_steps uncaptured steps with CUDA events on the
- * context stream.  names: '\n'-separated kernel names (cap bytes); ms[k]:
- * total milliseconds of kernel k; launches[k]: its launch count. */
+/* Times each phase of n_steps uncaptured steps with CUDA events on the
+ * context stream: first_move, sort_gather, contacts, pairs, sums, kick_move.
+ * names: '\n'-separated phase names (cap bytes); ms[k]: total milliseconds of
+ * phase k; launches[k]: its kernel launches. */
 int grains_gpu_profile_kernels(grains_gpu_ctx* ctx, int32_t n_steps, double* time, double dt,
                                char* names, size_t cap, double* ms, int64_t* launches,
                                int32_t max_kernels, int32_t* n_kernels);
-/* Number of kernel launches one call of grains_gpu_step(n_steps) issues. */
+/* No counterpart in the reference: a test hook of the persistent launch's
+ * failure path.  polls = how many times a grid-barrier wait polls before it
+ * gives up (default 2^24, about a second), skip_block = a block that leaves the
+ * kernel before its first barrier (-1 = none), so that the other blocks' waits
+ * run out: they set GRAINS_GPU_TIMEOUT and return, and the context stays
+ * usable (upload the state again before stepping on). */
+int grains_gpu_set_barrier_test(grains_gpu_ctx* ctx, int64_t polls, int32_t skip_block);
+/* Kernel launches of one middle step of grains_gpu_step: the cell sort (4),
+ * contacts, pairs, sums, kick_move, and the obstacle move when obstacles
+ * move.  The permutation of the arrays into cell order adds one launch every
+ * gather_every steps (grains_gpu_tuning). */
 int grains_gpu_launches_per_step(grains_gpu_ctx* ctx, int64_t* launches);
 
 /* ---- allocation-free contact detection ------------------------------------- */

@@ -159,6 +159,7 @@ _GPU_ONLY = {
     "get_stream": [_VP, C.POINTER(_VP)],
     "synchronize": [_VP],
     "launches_per_step": [_VP, C.POINTER(C.c_int64)],
+    "set_barrier_test": [_VP, C.c_int64, C.c_int32],
     "profile_kernels": [_VP, C.c_int32, _P_F64, C.c_double, C.c_char_p, C.c_size_t, _P_F64,
                         C.POINTER(C.c_int64), C.c_int32, _P_I32],
     "shape_properties": [C.c_int32, _P_F64, C.c_int32, _P_F64, _P_F64, _P_F64],
@@ -458,19 +459,25 @@ class Simulation:
         self._keep_update = list(arrs.values())
         self._check(self.lib.fn["update_particles"](self.ctx, C.byref(s)))
 
-    def download(self):
+    def download(self, out=None):
+        """The state in upload order.  `out`: preallocated arrays to fill (for
+        example views of pinned host memory), keyed like the result; fields
+        left out of it are not downloaded."""
         n = self.n
-        out = {
-            "id": np.zeros(n, np.int32),
-            "position": np.zeros((n, 3)),
-            "quaternion": np.zeros((n, 4)),
-            "basis": np.zeros((n, 9)),
-            "velocity": np.zeros((n, 3)),
-            "omega": np.zeros((n, 3)),
-            "force": np.zeros((n, 3)),
-            "torque": np.zeros((n, 3)),
-            "coordination": np.zeros(n, np.int32),
-        }
+        if out is None:
+            out = {
+                "id": np.zeros(n, np.int32),
+                "position": np.zeros((n, 3)),
+                "quaternion": np.zeros((n, 4)),
+                "basis": np.zeros((n, 9)),
+                "velocity": np.zeros((n, 3)),
+                "omega": np.zeros((n, 3)),
+                "force": np.zeros((n, 3)),
+                "torque": np.zeros((n, 3)),
+                "coordination": np.zeros(n, np.int32),
+            }
+        for k, a in out.items():
+            assert a.flags["C_CONTIGUOUS"] and a.dtype == (np.int32 if k in ("id", "coordination") else np.float64)
         s = Particles()
         s.n = n
         for k, a in out.items():
@@ -626,6 +633,10 @@ class Simulation:
         h = _VP()
         self._check(self.lib.fn["get_stream"](self.ctx, C.byref(h)))
         return h.value
+
+    def set_barrier_test(self, polls=1 << 24, skip_block=-1):
+        """Test hook of the persistent launch's bounded grid-barrier wait."""
+        self._check(self.lib.fn["set_barrier_test"](self.ctx, polls, skip_block))
 
     def launches_per_step(self):
         n = C.c_int64()

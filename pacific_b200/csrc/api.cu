@@ -80,8 +80,7 @@ struct grains_gpu_ctx {
   int n_cells = 0;
   bool uploaded = false;
   bool tables_dirty = true;
-  double* stage = nullptr;        // host-ordered staging of the kinematic state (13 doubles / particle)
-  double* stage_basis = nullptr;  // 9 doubles / particle
+  char* stage = nullptr;  // device staging of update / download in upload order (30 x 8 B per particle)
   bool sorted = false;      // cur arrays are in cell order for the current positions
   bool keys_valid = false;  // key and cell counts hold the cells of the current positions
   bool pending_kick2 = false;
@@ -152,6 +151,8 @@ struct grains_gpu_ctx {
   int gather_every = 16;  // steps between two gathers of the arrays into cell order
   int since_gather = 0;   // sorts without a gather since the last one
   int persistent = 0;     // middle steps in one cooperative launch instead of graphs
+  long long barrier_polls = 1ll << 24;  // its grid-barrier wait bound (grains_gpu_set_barrier_test)
+  int barrier_skip_block = -1;
   unsigned* pbar = nullptr;  // grid-barrier state of the persistent launch
   int* psums = nullptr;      // its scan scratch (one int per block)
   int pblocks = 0;
@@ -551,6 +552,8 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   a.pair_sys = c->pair_sys;
   a.gjk_tol = c->gjk_tol;
   a.gjk_sv = c->gjk_sv;
+  a.barrier_polls = c->barrier_polls;
+  a.barrier_skip_block = c->barrier_skip_block;
   a.contacts_block = c->contacts_block;
   a.forces_block = c->forces_block;
   return a;
@@ -627,13 +630,13 @@ int flush_kick(grains_gpu_ctx* c) {
   return rc ? fail(c, rc, "advance-velocity launch failed") : 0;
 }
 
-int forces_now(grains_gpu_ctx* c, double dt, int diag, int phases = 3) {
+int forces_now(grains_gpu_ctx* c, double dt, int diag, int phases = 7) {
   if (!c->sorted) {
     if (int rc = sort_now(c, 1)) return rc;
   }
   int rc = with_args(c, [&](auto& a) { return launch_forces(a, c->stream, dt, diag, phases); });
   if (rc) return fail(c, rc, "force kernel launch failed");
-  if (phases & 2) c->hcur = 1 - c->hcur;
+  if (phases & 4) c->hcur = 1 - c->hcur;
   return 0;
 }
 
@@ -869,7 +872,6 @@ int grains_gpu_destroy(grains_gpu_ctx* c) {
   if (c->stage) cudaFree(c->stage);
   for (void* p : {(void*)c->clist, (void*)c->ccount, c->res_f, c->res_t, (void*)c->work})
     if (p) cudaFree(p);
-  if (c->stage_basis) cudaFree(c->stage_basis);
   if (c->pbar) cudaFree(c->pbar);
   if (c->psums) cudaFree(c->psums);
   for (void* p : {(void*)c->d_row_id, (void*)c->d_row_sys, (void*)c->d_row_keys, (void*)c->d_key_rows,
@@ -1380,99 +1382,80 @@ int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
   return finish_call(c);
 }
 
+namespace {
+// the device staging buffer of update / download: 30 doubles per particle
+int ensure_stage(grains_gpu_ctx* c) {
+  if (c->stage) return 0;
+  void* q = nullptr;
+  CK(cudaMalloc(&q, (size_t)c->cap * 30 * sizeof(double)));
+  c->stage = (char*)q;
+  return 0;
+}
+}  // namespace
+
+// The state is permuted into upload order and widened to double on the device
+// (pack_download_kernel); each requested field then goes to the caller's array
+// in one copy (from pinned caller memory the copies run at the link's rate).
 int grains_gpu_download_particles(grains_gpu_ctx* c, grains_gpu_particles* p) {
   if (!c || !p) return GRAINS_GPU_INVALID_ARGUMENT;
   if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "no particles uploaded");
   if (int rc = flush_kick(c)) return rc;
-  const int64_t n = c->n;
-  auto& b = c->buf[c->cur];
-  std::vector<double4> xr(n), q(n);
-  std::vector<int4> meta(n);
-  std::vector<int> orig(n), coord(n);
-  std::vector<double> basis(c->has_basis ? 9 * n : 0);
-  const size_t r4 = 4 * c->rsize;
-  std::vector<char> v(n * r4), w(n * r4), F(n * r4), T(n * r4);
-  CK(cudaMemcpyAsync(xr.data(), b.xr, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(q.data(), b.q, n * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(meta.data(), b.meta, n * sizeof(int4), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(orig.data(), b.orig, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(coord.data(), c->coord, n * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-  if (c->has_basis) CK(cudaMemcpyAsync(basis.data(), b.basis, 9 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(v.data(), b.v, n * r4, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(w.data(), b.w, n * r4, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(F.data(), b.F, n * r4, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaMemcpyAsync(T.data(), b.T, n * r4, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  const bool dbl = c->precision == GRAINS_GPU_FP64;
-  auto get = [&](const std::vector<char>& src, int64_t s, int k) -> double {
-    return dbl ? ((const double*)src.data())[4 * s + k] : (double)((const float*)src.data())[4 * s + k];
+  if (int rc = ensure_stage(c)) return rc;
+  const int64_t n = c->n, m = std::min<int64_t>(p->n, n);
+  double* d = (double*)c->stage;
+  DownloadStage st{};
+  st.position = p->position ? d : nullptr;
+  st.quaternion = p->quaternion ? d + 3 * n : nullptr;
+  st.basis = p->basis ? d + 7 * n : nullptr;
+  st.velocity = p->velocity ? d + 16 * n : nullptr;
+  st.omega = p->omega ? d + 19 * n : nullptr;
+  st.force = p->force ? d + 22 * n : nullptr;
+  st.torque = p->torque ? d + 25 * n : nullptr;
+  st.coordination = p->coordination ? (int*)(d + 28 * n) : nullptr;
+  st.id = p->id ? (int*)(d + 29 * n) : nullptr;
+  int rc = with_args(c, [&](auto& a) { return launch_pack_download(a, c->stream, st); });
+  if (rc) return fail(c, rc, "download launch failed");
+  auto get = [&](void* dst, const void* src, size_t bytes) -> int {
+    if (dst && bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return 0;
   };
-  const int64_t m = std::min<int64_t>(p->n, n);
-  for (int64_t s = 0; s < n; ++s) {
-    int64_t i = orig[s];
-    if (i >= m) continue;
-    if (p->id) p->id[i] = meta[s].x;
-    if (p->position) { p->position[3 * i] = xr[s].x; p->position[3 * i + 1] = xr[s].y; p->position[3 * i + 2] = xr[s].z; }
-    if (p->quaternion) {
-      p->quaternion[4 * i] = q[s].x; p->quaternion[4 * i + 1] = q[s].y;
-      p->quaternion[4 * i + 2] = q[s].z; p->quaternion[4 * i + 3] = q[s].w;
-    }
-    if (p->basis) {
-      if (c->has_basis) {
-        for (int k = 0; k < 9; ++k) p->basis[9 * i + k] = basis[9 * s + k];
-      } else {  // spheres: the rotation matrix of the quaternion
-        double x = q[s].x, y = q[s].y, z = q[s].z, w0 = q[s].w;
-        double mm[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - w0 * z), 2 * (x * z + w0 * y),
-                        2 * (x * y + w0 * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w0 * x),
-                        2 * (x * z - w0 * y), 2 * (y * z + w0 * x), 1 - 2 * (x * x + y * y)};
-        for (int k = 0; k < 9; ++k) p->basis[9 * i + k] = mm[k];
-      }
-    }
-    for (int k = 0; k < 3; ++k) {
-      if (p->velocity) p->velocity[3 * i + k] = get(v, s, k);
-      if (p->omega) p->omega[3 * i + k] = get(w, s, k);
-      if (p->force) p->force[3 * i + k] = get(F, s, k);
-      if (p->torque) p->torque[3 * i + k] = get(T, s, k);
-    }
-    if (p->coordination) p->coordination[i] = coord[s];
-  }
+  rc = get(p->position, st.position, 3 * m * sizeof(double));
+  rc = rc ? rc : get(p->quaternion, st.quaternion, 4 * m * sizeof(double));
+  rc = rc ? rc : get(p->basis, st.basis, 9 * m * sizeof(double));
+  rc = rc ? rc : get(p->velocity, st.velocity, 3 * m * sizeof(double));
+  rc = rc ? rc : get(p->omega, st.omega, 3 * m * sizeof(double));
+  rc = rc ? rc : get(p->force, st.force, 3 * m * sizeof(double));
+  rc = rc ? rc : get(p->torque, st.torque, 3 * m * sizeof(double));
+  rc = rc ? rc : get(p->coordination, st.coordination, m * sizeof(int));
+  rc = rc ? rc : get(p->id, st.id, m * sizeof(int));
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
   p->n = m;
   return 0;
 }
 
+// The caller's arrays go to the device staging in one copy each; the update
+// kernel scatters them into the cell-ordered state.
 int grains_gpu_update_particles(grains_gpu_ctx* c, const grains_gpu_particles* p) {
   if (!c || !p) return GRAINS_GPU_INVALID_ARGUMENT;
   if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "upload particles first");
   if (p->n != c->n) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "update must cover every uploaded particle");
   if (!p->position || !p->quaternion || !p->velocity || !p->omega)
     return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "missing kinematic array");
+  if (int rc = ensure_stage(c)) return rc;
   const int64_t n = c->n;
-  if (!c->stage) {
-    void* q = nullptr;
-    CK(cudaMalloc(&q, (size_t)c->cap * 13 * sizeof(double)));
-    c->stage = (double*)q;
-  }
-  if (c->has_basis && p->basis && !c->stage_basis) {
-    void* q = nullptr;
-    CK(cudaMalloc(&q, (size_t)c->cap * 9 * sizeof(double)));
-    c->stage_basis = (double*)q;
-  }
-  std::vector<double> h((size_t)n * 13);
-  for (int64_t i = 0; i < n; ++i) {
-    double* e = &h[13 * i];
-    for (int k = 0; k < 3; ++k) e[k] = p->position[3 * i + k];
-    for (int k = 0; k < 4; ++k) e[3 + k] = p->quaternion[4 * i + k];
-    for (int k = 0; k < 3; ++k) e[7 + k] = p->velocity[3 * i + k];
-    for (int k = 0; k < 3; ++k) e[10 + k] = p->omega[3 * i + k];
-  }
   if (int rc = flush_kick(c)) return rc;
-  CK(cudaMemcpyAsync(c->stage, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  double* d = (double*)c->stage;
   const bool with_basis = c->has_basis && p->basis;
+  KinematicStage st{d, d + 3 * n, d + 7 * n, d + 10 * n, with_basis ? d + 13 * n : nullptr};
+  CK(cudaMemcpyAsync((void*)st.position, p->position, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync((void*)st.quaternion, p->quaternion, 4 * n * sizeof(double), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaMemcpyAsync((void*)st.velocity, p->velocity, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync((void*)st.omega, p->omega, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   if (with_basis)
-    CK(cudaMemcpyAsync(c->stage_basis, p->basis, (size_t)n * 9 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-  int rc = with_args(c, [&](auto& a) {
-    return launch_update_dynamic(a, c->stream, c->stage, with_basis ? c->stage_basis : nullptr);
-  });
+    CK(cudaMemcpyAsync((void*)st.basis, p->basis, 9 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int rc = with_args(c, [&](auto& a) { return launch_update_dynamic(a, c->stream, st); });
   if (rc) return fail(c, rc, "update launch failed");
   c->keys_valid = false;
   c->sorted = false;
@@ -1897,11 +1880,19 @@ int grains_gpu_reset_stats(grains_gpu_ctx* c) {
   return 0;
 }
 
+int grains_gpu_set_barrier_test(grains_gpu_ctx* c, int64_t polls, int32_t skip_block) {
+  if (!c || polls < 1) return GRAINS_GPU_INVALID_ARGUMENT;
+  c->barrier_polls = polls;
+  c->barrier_skip_block = skip_block < 0 ? -1 : skip_block;
+  return 0;
+}
+
 int grains_gpu_launches_per_step(grains_gpu_ctx* c, int64_t* launches) {
   if (!c || !launches) return GRAINS_GPU_INVALID_ARGUMENT;
-  // middle steps: scan (2: scan_tiles, scan_finish), scatter, cell_sort,
-  // gather, contacts, forces, kick_move
-  *launches = launches_per_middle_step();
+  // a middle step: scan_tiles, scan_finish, scatter, cell_sort, contacts,
+  // pairs, sums, kick_move, and the obstacle move when obstacles move; the
+  // gather runs one step in gather_every on top
+  *launches = launches_per_middle_step() + (c->n_moving > 0 ? 1 : 0);
   return 0;
 }
 
@@ -1914,10 +1905,10 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time,
   if (!c->sorted)
     if (int rc = sort_now(c, 1)) return rc;
   // same schedule as grains_gpu_step, uncaptured, with events around each phase
-  cudaEvent_t ev[6];
+  cudaEvent_t ev[7];
   for (auto& e : ev) CK(cudaEventCreate(&e));
-  double acc[5] = {0, 0, 0, 0, 0};  // first move, sort+gather, contact lists, contact law, kick/move
-  int64_t cnt[5] = {0, 0, 0, 0, 0};
+  double acc[6] = {0, 0, 0, 0, 0, 0};  // first move, sort+gather, contact lists, pair law, sums, kick/move
+  int64_t cnt[6] = {0, 0, 0, 0, 0, 0};
   CK(cudaEventRecord(ev[0], c->stream));
   if (int rc = first_move(c, dt, *time)) return rc;
   CK(cudaEventRecord(ev[1], c->stream));
@@ -1935,6 +1926,8 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time,
     CK(cudaEventRecord(ev[3], c->stream));
     if (int rc = forces_now(c, dt, 0, 2)) return rc;
     CK(cudaEventRecord(ev[4], c->stream));
+    if (int rc = forces_now(c, dt, 0, 4)) return rc;
+    CK(cudaEventRecord(ev[5], c->stream));
     if (!last) {
       int rc = with_args(c, [&](auto& a) { return launch_kick_move(a, c->stream, 1, 0.5 * dt, 1, 0.5 * dt, dt); });
       if (rc) return fail(c, rc, "kick/move launch failed");
@@ -1942,23 +1935,24 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time,
       c->sorted = false;
       if (int rc2 = move_obstacles(c, dt)) return rc2;
     }
-    CK(cudaEventRecord(ev[5], c->stream));
-    CK(cudaEventSynchronize(ev[5]));
-    float t[4] = {0, 0, 0, 0};
-    for (int q = 0; q < 4; ++q) cudaEventElapsedTime(&t[q], ev[1 + q], ev[2 + q]);
-    for (int q = 0; q < 4; ++q) acc[1 + q] += t[q];
-    cnt[1] += 6;
+    CK(cudaEventRecord(ev[6], c->stream));
+    CK(cudaEventSynchronize(ev[6]));
+    float t[5] = {0, 0, 0, 0, 0};
+    for (int q = 0; q < 5; ++q) cudaEventElapsedTime(&t[q], ev[1 + q], ev[2 + q]);
+    for (int q = 0; q < 5; ++q) acc[1 + q] += t[q];
+    cnt[1] += 4;  // scan_tiles, scan_finish, scatter, cell_sort (+ a gather one step in gather_every)
     cnt[2] += 1;
     cnt[3] += 1;
-    if (!last) cnt[4] += 1;
+    cnt[4] += 1;
+    if (!last) cnt[5] += 1;
   }
   c->pending_kick2 = true;
   c->pending_dt = 0.5 * dt;
   for (auto& e : ev) cudaEventDestroy(e);
   for (int k = 0; k < n_steps; ++k) *time += dt;
   c->steps_done += n_steps;
-  std::snprintf(names, cap, "first_move\nsort_gather\ncontacts\nforces\nkick_move");
-  const int nk = max_kernels < 5 ? max_kernels : 5;
+  std::snprintf(names, cap, "first_move\nsort_gather\ncontacts\npairs\nsums\nkick_move");
+  const int nk = max_kernels < 6 ? max_kernels : 6;
   for (int k = 0; k < nk; ++k) {
     ms[k] = acc[k];
     launches[k] = cnt[k];

@@ -183,6 +183,8 @@ struct StepArgs {
   int* pair_sys;         // diagnostic: system of each contact pair
   double gjk_tol;
   int gjk_sv;            // the signed-volume GJK for non-spherical pairs
+  long long barrier_polls;  // persistent kernel: polls before a grid-barrier wait gives up
+  int barrier_skip_block;   // persistent kernel: a block that leaves at once (a test of the bounded wait), or -1
   int contacts_block;    // threads per block of contacts_kernel (<= 256)
   int forces_block;      // threads per block of forces_kernel (<= 128)
 };
@@ -198,15 +200,24 @@ int launch_bin(const StepArgs<R>& a, cudaStream_t s);
 // other buffer; the permutation becomes the identity)
 template <typename R>
 int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather, int gather_forces);
-// phases: 1 = contact lists, 2 = contact law, 3 = both
+// phases (bits): 1 = contact lists, 2 = pair narrowphase and law, 4 = per-particle sums
 template <typename R>
-int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int phases = 3);
+int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int phases = 7);
 template <typename R>
 int launch_zero_kdelta(const StepArgs<R>& a, cudaStream_t s);
-// stage: 13 doubles per particle in upload order (position 3, quaternion 4,
-// velocity 3, omega 3) and optionally 9 basis doubles per particle
+// device arrays in upload order of grains_gpu_update_particles (basis may be null)
+struct KinematicStage {
+  const double *position, *quaternion, *velocity, *omega, *basis;
+};
+// device arrays in upload order of grains_gpu_download_particles (any may be null)
+struct DownloadStage {
+  double *position, *quaternion, *basis, *velocity, *omega, *force, *torque;
+  int *coordination, *id;
+};
 template <typename R>
-int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const double* stage, const double* stage_basis);
+int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const KinematicStage& st);
+template <typename R>
+int launch_pack_download(const StepArgs<R>& a, cudaStream_t s, const DownloadStage& d);
 template <typename R>
 int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int include_obstacles, int* out,
                            int cap, unsigned long long* count);

@@ -1098,28 +1098,86 @@ __global__ void zero_kdelta_kernel(StepArgs<R> a) {
   }
 }
 
-// overwrite the kinematic state from a host-ordered staging area
+// overwrite the kinematic state from upload-order arrays on the device
+// (ParticleKinematics::setAngularVelocity gives the body-frame rate)
 template <typename R>
-__global__ void update_dynamic_kernel(StepArgs<R> a, const double* st, const double* sb) {
+__global__ void update_dynamic_kernel(StepArgs<R> a, KinematicStage st) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   const ParticleArrays<R>& P = a.cur;
   const size_t i = (size_t)P.orig[s];
-  const double* e = st + 13 * i;
   double4 xr = P.xr[s];
-  xr.x = e[0];
-  xr.y = e[1];
-  xr.z = e[2];
+  xr.x = st.position[3 * i];
+  xr.y = st.position[3 * i + 1];
+  xr.z = st.position[3 * i + 2];
   P.xr[s] = xr;
-  P.q[s] = make_double4(e[3], e[4], e[5], e[6]);
-  P.v[s] = st3<R>(v3<R>(R(e[7]), R(e[8]), R(e[9])));
-  Qt<double> q{v3<double>(e[3], e[4], e[5]), e[6]};
-  V3<double> w = v3<double>(e[10], e[11], e[12]);
+  const double* qi = st.quaternion + 4 * i;
+  P.q[s] = make_double4(qi[0], qi[1], qi[2], qi[3]);
+  P.v[s] = st3<R>(v3<R>(R(st.velocity[3 * i]), R(st.velocity[3 * i + 1]), R(st.velocity[3 * i + 2])));
+  Qt<double> q{v3<double>(qi[0], qi[1], qi[2]), qi[3]};
+  V3<double> w = v3<double>(st.omega[3 * i], st.omega[3 * i + 1], st.omega[3 * i + 2]);
   P.w[s] = st3<R>(v3<R>(R(w.x), R(w.y), R(w.z)));
-  V3<double> wbf = q_to_body(q, w);  // ParticleKinematics::setAngularVelocity
+  V3<double> wbf = q_to_body(q, w);
   P.wbf[s] = st3<R>(v3<R>(R(wbf.x), R(wbf.y), R(wbf.z)));
-  if (a.has_basis && sb)
-    for (int k = 0; k < 9; ++k) P.basis[9 * (size_t)s + k] = sb[9 * i + k];
+  if (a.has_basis && st.basis)
+    for (int k = 0; k < 9; ++k) P.basis[9 * (size_t)s + k] = st.basis[9 * i + k];
+}
+
+// the state in upload order, one array per field (any may be null): the
+// device side of grains_gpu_download_particles.  Spheres without a stored
+// basis get the rotation matrix of their quaternion.
+template <typename R>
+__global__ void pack_download_kernel(StepArgs<R> a, DownloadStage d) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const ParticleArrays<R>& P = a.cur;
+  const size_t i = (size_t)P.orig[s];
+  const double4 xr = P.xr[s], q = P.q[s];
+  if (d.position) {
+    d.position[3 * i] = xr.x;
+    d.position[3 * i + 1] = xr.y;
+    d.position[3 * i + 2] = xr.z;
+  }
+  if (d.quaternion) {
+    d.quaternion[4 * i] = q.x;
+    d.quaternion[4 * i + 1] = q.y;
+    d.quaternion[4 * i + 2] = q.z;
+    d.quaternion[4 * i + 3] = q.w;
+  }
+  if (d.basis) {
+    if (a.has_basis) {
+      for (int k = 0; k < 9; ++k) d.basis[9 * i + k] = P.basis[9 * (size_t)s + k];
+    } else {
+      const double x = q.x, y = q.y, z = q.z, w0 = q.w;
+      const double m[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - w0 * z), 2 * (x * z + w0 * y),
+                           2 * (x * y + w0 * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w0 * x),
+                           2 * (x * z - w0 * y), 2 * (y * z + w0 * x), 1 - 2 * (x * x + y * y)};
+      for (int k = 0; k < 9; ++k) d.basis[9 * i + k] = m[k];
+    }
+  }
+  const R4<R> v = P.v[s], w = P.w[s], F = P.F[s], T = P.T[s];
+  if (d.velocity) {
+    d.velocity[3 * i] = double(v.x);
+    d.velocity[3 * i + 1] = double(v.y);
+    d.velocity[3 * i + 2] = double(v.z);
+  }
+  if (d.omega) {
+    d.omega[3 * i] = double(w.x);
+    d.omega[3 * i + 1] = double(w.y);
+    d.omega[3 * i + 2] = double(w.z);
+  }
+  if (d.force) {
+    d.force[3 * i] = double(F.x);
+    d.force[3 * i + 1] = double(F.y);
+    d.force[3 * i + 2] = double(F.z);
+  }
+  if (d.torque) {
+    d.torque[3 * i] = double(T.x);
+    d.torque[3 * i + 1] = double(T.y);
+    d.torque[3 * i + 2] = double(T.z);
+  }
+  if (d.coordination) d.coordination[i] = a.coord[s];
+  if (d.id) d.id[i] = P.meta[s].x;
 }
 
 // Imposed motion of one obstacle over the step ending at T
@@ -1410,7 +1468,11 @@ int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int
   const int cb = (a.contacts_block >= 32 && a.contacts_block <= 256) ? a.contacts_block : 256;
   const int fb = (a.forces_block >= 32 && a.forces_block <= 128) ? a.forces_block : 128;
   if (phases & 1) contacts_kernel<R><<<grid_for(a.n, cb), cb, 0, s>>>(a);
-  if (!(phases & 2)) return check_launch();
+  if (!(phases & 6)) return check_launch();
+  if (!(phases & 2)) {
+    sums_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
+    return check_launch();
+  }
   // about two work items per thread in a settled packing; the grid-stride
   // loop takes any count
   const int g = (int)std::min<long long>(grid_for(2ll * a.n, fb), 1ll << 20);
@@ -1430,7 +1492,7 @@ int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int
     else
       pairs_kernel<R, false, false><<<g, fb, 0, s>>>(a, R(dt));
   }
-  sums_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
+  if (phases & 4) sums_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
   return check_launch();
 }
 
@@ -1453,9 +1515,16 @@ int launch_obstacle_move(ObstacleDev* obs, const int* moving_idx, int n_moving, 
 #endif
 
 template <typename R>
-int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const double* stage, const double* stage_basis) {
+int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const KinematicStage& st) {
   if (a.n == 0) return 0;
-  update_dynamic_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, stage, stage_basis);
+  update_dynamic_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, st);
+  return check_launch();
+}
+
+template <typename R>
+int launch_pack_download(const StepArgs<R>& a, cudaStream_t s, const DownloadStage& d) {
+  if (a.n == 0) return 0;
+  pack_download_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, d);
   return check_launch();
 }
 
@@ -1479,12 +1548,13 @@ int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int in
 // occupancy of the heaviest (the contact law).  Kept as a tuning choice.
 
 constexpr int kPersistentThreads = 128;
-constexpr long long kBarrierSpinLimit = 1ll << 24;  // x 64 ns sleep: about a second
+// default bound of a barrier wait: 2^24 polls x 64 ns sleep, about a second
+// (StepArgs::barrier_polls; a test lowers it to make the wait run out)
 
 // Grid barrier with a bounded wait: bar[0] counts arrivals, bar[1] is the
 // generation.  A wait that runs out sets GRAINS_GPU_TIMEOUT and returns false;
 // the kernel then returns, and the others run out at their next barrier.
-__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status) {
+__device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status, long long polls) {
   __shared__ int ok_s;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -1499,7 +1569,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned* bar, int* status) {
     } else {
       long long it = 0;
       while (*gen == g) {
-        if (++it > kBarrierSpinLimit || (*((volatile int*)status) & GRAINS_GPU_TIMEOUT)) {
+        if (++it > polls || (*((volatile int*)status) & GRAINS_GPU_TIMEOUT)) {
           ok = 0;
           atomicOr(status, GRAINS_GPU_TIMEOUT);
           break;
@@ -1524,6 +1594,9 @@ __global__ void __launch_bounds__(kPersistentThreads) persistent_steps_kernel(
   const int n = a.n, C = a.n_cells;
   int* status = &a.stats->status;
   __shared__ int offset_s;
+  // a test of the bounded wait: this block leaves before the first barrier,
+  // so that the others' waits run out
+  if ((int)blockIdx.x == a.barrier_skip_block) return;
   for (int step = 0; step < n_steps; ++step) {
     // exclusive scan of the cell counts: a chunk per block, then the offsets
     {
@@ -1539,7 +1612,7 @@ __global__ void __launch_bounds__(kPersistentThreads) persistent_steps_kernel(
         run += total;
       }
       if (threadIdx.x == 0) sums[blockIdx.x] = run;
-      if (!grid_barrier(bar, status)) return;
+      if (!grid_barrier(bar, status, a.barrier_polls)) return;
       if (threadIdx.x == 0) {
         int o = 0;
         for (int b = 0; b < (int)blockIdx.x; ++b) o += sums[b];
@@ -1552,26 +1625,26 @@ __global__ void __launch_bounds__(kPersistentThreads) persistent_steps_kernel(
         a.cell_start[i] = v;
         a.cell_cursor[i] = v;
       }
-      if (!grid_barrier(bar, status)) return;
+      if (!grid_barrier(bar, status, a.barrier_polls)) return;
     }
     for (int s = tid; s < n; s += nthreads) scatter_one(a, s);
-    if (!grid_barrier(bar, status)) return;
+    if (!grid_barrier(bar, status, a.barrier_polls)) return;
     for (int c = tid; c < C; c += nthreads) cell_sort_one(a, c);
-    if (!grid_barrier(bar, status)) return;
+    if (!grid_barrier(bar, status, a.barrier_polls)) return;
     if (since_gather + 1 >= gather_every) {
       for (int t = tid; t < n; t += nthreads) gather_one(a, t, 0);
       const ParticleArrays<R> tmp = a.cur;
       a.cur = a.alt;
       a.alt = tmp;
       since_gather = 0;
-      if (!grid_barrier(bar, status)) return;
+      if (!grid_barrier(bar, status, a.barrier_polls)) return;
     } else {
       ++since_gather;
     }
     contacts_range(a, tid, nthreads);
-    if (!grid_barrier(bar, status)) return;
+    if (!grid_barrier(bar, status, a.barrier_polls)) return;
     pairs_range<R, false, CONVEX>(a, tid, nthreads, dt_r);
-    if (!grid_barrier(bar, status)) return;
+    if (!grid_barrier(bar, status, a.barrier_polls)) return;
     if (tid == 0) *a.work_n = 0;  // every block has read the count
     for (int s = tid; s < n; s += nthreads) sum_one(a, s);
     {
@@ -1582,13 +1655,13 @@ __global__ void __launch_bounds__(kPersistentThreads) persistent_steps_kernel(
       a.hist_n_prev = a.hist_n_next;
       a.hist_n_next = hn;
     }
-    if (!grid_barrier(bar, status)) return;
+    if (!grid_barrier(bar, status, a.barrier_polls)) return;
     for (int s = tid; s < n; s += nthreads)
       integrate(a, a.cur, a.cur, s, ld3<R>(a.cur.F[s]), ld3<R>(a.cur.T[s]), 1, R(0.5) * dt_r, 1, R(0.5) * dt_r, dt);
     if (blockIdx.x == 0 && n_moving > 0)
       obstacle_move_block(const_cast<ObstacleDev*>(a.obs), a.moving_idx, n_moving, a.loads, a.load_flags, a.n_sys,
                           a.shapes, a.verts, dt, clock, 0., 0);
-    if (!grid_barrier(bar, status)) return;
+    if (!grid_barrier(bar, status, a.barrier_polls)) return;
   }
 }
 
@@ -1630,7 +1703,8 @@ int launch_persistent_steps(const StepArgs<R>& a, cudaStream_t s, int n_steps, d
   template int launch_sort_and_gather<R>(const StepArgs<R>&, cudaStream_t, int, int);                      \
   template int launch_forces<R>(const StepArgs<R>&, cudaStream_t, double, int, int);                       \
   template int launch_zero_kdelta<R>(const StepArgs<R>&, cudaStream_t);                                    \
-  template int launch_update_dynamic<R>(const StepArgs<R>&, cudaStream_t, const double*, const double*);     \
+  template int launch_update_dynamic<R>(const StepArgs<R>&, cudaStream_t, const KinematicStage&);             \
+  template int launch_pack_download<R>(const StepArgs<R>&, cudaStream_t, const DownloadStage&);              \
   template int launch_candidate_pairs<R>(const StepArgs<R>&, cudaStream_t, int, int, int*, int,           \
                                          unsigned long long*);                                            \
   template int persistent_blocks<R>(const StepArgs<R>&);                                                   \

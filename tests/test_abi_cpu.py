@@ -13,7 +13,7 @@ from pacific_b200.abi import BOX, CYLINDER, POLYHEDRON, SPHERE
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "grains_gpu.h")
-GPU_ONLY = {"get_stream", "synchronize", "launches_per_step", "profile_kernels", "shape_properties",
+GPU_ONLY = {"get_stream", "synchronize", "launches_per_step", "set_barrier_test", "profile_kernels", "shape_properties",
             "sphere_contacts_noalloc", "adjoint_create", "adjoint_destroy", "adjoint_last_error",
             "adjoint_law_slots", "adjoint_forward", "adjoint_contact_signature", "adjoint_backward",
             "get_tuning", "set_tuning", "autotune", "reload_open", "reload_last_error", "reload_get",

@@ -99,3 +99,39 @@ def test_persistent_steps_give_identical_runs(gpu_lib, case):
         s.close()
     for k in ["position", "velocity", "omega", "force", "obstacles"]:
         assert np.array_equal(runs[0][k], runs[1][k]), k
+
+
+def test_persistent_barrier_wait_runs_out_and_the_context_recovers(gpu_lib):
+    """The persistent launch's grid barrier waits a bounded number of polls.
+    With the test hook one block leaves before the first barrier and the wait
+    bound is 1,000 polls: the other blocks' waits run out, GRAINS_GPU_TIMEOUT
+    comes back through the status word (no fault, no hang), and the same
+    context then runs the steps again to the bits of a fresh context."""
+    from pacific_b200.abi import TIMEOUT, GrainsError
+    sc = evolved_box()
+    s = make(gpu_lib, sc, FP64)
+    s.set_tuning(persistent=1)
+    s.set_barrier_test(polls=1000, skip_block=0)
+    s.initialize_leapfrog(0.0, sc.dt)
+    with pytest.raises(GrainsError) as err:
+        s.step(20, 0.0, sc.dt)
+        s.synchronize()
+    assert err.value.code & TIMEOUT
+    # recovery: default bound, status cleared, state uploaded again
+    s.set_barrier_test()
+    s.reset_stats()
+    s.update(sc.particles)
+    s.upload_contact_memory({k: np.zeros((0, 3)) if k in ("kdelta", "prev_normal", "spring_torque")
+                             else np.zeros(0, np.int32) for k in ("owner", "other", "kdelta", "prev_normal",
+                                                                  "spring_torque")})
+    s.initialize_leapfrog(0.0, sc.dt)
+    s.step(20, 0.0, sc.dt)
+    s.synchronize()
+    assert s.stats()["status"] == 0
+    fresh = make(gpu_lib, sc, FP64)
+    fresh.set_tuning(persistent=1)
+    fresh.initialize_leapfrog(0.0, sc.dt)
+    fresh.step(20, 0.0, sc.dt)
+    a, b = s.download(), fresh.download()
+    for k in ["position", "velocity", "omega"]:
+        assert np.array_equal(a[k], b[k]), k
