@@ -279,3 +279,42 @@ def test_drum_contacts_match_oracle(oracle_lib, gpu_lib, precision):
     po, fo = o2.contact_forces()
     assert np.array_equal(pg, po)
     check_contact_forces(fg, fo, weight, precision)
+
+
+def test_grid_spanning_many_scan_tiles(oracle_lib, gpu_lib):
+    """A dense cluster of 512 spheres in a corner of a 60 mm box: a grid of
+    30 x 30 x 30 = 27,000 cells, over six 4,096-cell tiles of the cell-count
+    scan (scan_tiles / scan_finish), so the finishing blocks add the totals of
+    earlier tiles.  Against the oracle after 30 steps (FP64): candidate and
+    contact pairs equal, states at rounding level, status clear; and the
+    persistent launch (its own scan) gives the same bits."""
+    sc = S.dense_cluster(512, seed=12, velocity_sigma=0.1)
+    lo, hi = np.zeros(3), np.array([60.0, 60.0, 60.0]) * S.MM
+    shapes = [sc.shapes[0]]
+    wshapes, obs = S.box_walls(lo, hi, "xXyYzZ", 0.5 * S.MM, 0.05 * S.MM, len(shapes), -1)
+    sc.shapes = shapes + wshapes
+    sc.obstacles = [obs]
+    sc.domains = [dict(sc.domains[0], origin=lo, size=hi - lo)]
+    o, g = both(oracle_lib, gpu_lib, sc)
+    assert np.array_equal(o.candidate_pairs(include_obstacles=True), g.candidate_pairs(include_obstacles=True))
+    for s in (o, g):
+        s.compute_forces(0.0, sc.dt)
+    assert pair_set(g.contact_pairs()) == pair_set(o.contact_pairs())
+    assert len(o.contact_pairs()) > 500
+    runs = []
+    for s in (o, g):
+        s.initialize_leapfrog(0.0, sc.dt)
+        t = s.step(30, 0.0, sc.dt)
+        s.compute_forces(t, sc.dt)
+        runs.append(s.download())
+    assert pair_set(g.contact_pairs()) == pair_set(o.contact_pairs())
+    assert np.max(np.abs(runs[1]["position"] - runs[0]["position"])) < 1e-13
+    weight = sc.particles["mass"][0] * 9.81
+    assert rel_err(runs[1]["force"], runs[0]["force"], weight) < 1e-12
+    assert g.stats()["status"] == 0
+    p = make(gpu_lib, sc, FP64)
+    p.set_tuning(persistent=1)
+    p.initialize_leapfrog(0.0, sc.dt)
+    t = p.step(30, 0.0, sc.dt)
+    p.compute_forces(t, sc.dt)
+    assert np.array_equal(p.download()["position"], runs[1]["position"])
