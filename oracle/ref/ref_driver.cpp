@@ -16,6 +16,7 @@
 // The reference keeps process-wide static state (factories, counters), so one
 // context per process is supported.
 #include "../../include/grains_gpu.h"
+#include "LinkedCellGPU.hh"
 
 #include <unistd.h>
 
@@ -79,6 +80,17 @@ class OracleGrains : public Grains {
   }
   double& time() { return m_time; }
   double& dt() { return m_dt; }
+  // The collision App of this simulation replaced by `app`, as Grains::
+  // Construction would register it in place of its LinkedCell (Grains.cpp:
+  // 777-780): the first App of m_allApp and m_collision.  The stock LinkedCell
+  // stays alive (its cells hold the particles' links) and is returned.
+  LinkedCell* use_app(LinkedCell* app) {
+    LinkedCell* old = m_collision;
+    for (App*& a : m_allApp)
+      if (a == old) a = app;
+    m_collision = app;
+    return old;
+  }
   AllInsertionWindows const& windows() const { return m_insertion_windows; }
 };
 
@@ -105,6 +117,7 @@ struct grains_gpu_ctx {
   std::vector<grains_gpu_obstacle_loading> loads;  // explicit imposed motions
   int collision = GRAINS_GPU_GJK;                   // <CollisionDetection Type=...>
   OracleGrains* g = nullptr;
+  LinkedCell* stock_lc = nullptr;  // the reference's LinkedCell after grains_ref_use_gpu_app
   std::string dir;
   std::string err;
   int status = 0;
@@ -217,7 +230,14 @@ int grains_ref_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
 
 int grains_ref_destroy(grains_gpu_ctx* c) {
   if (!c) return 0;
-  delete c->g;
+  // The reference's Grains object is left alive on purpose: its destructor
+  // deletes the contact-force models of ContactBuilderFactory's static table
+  // without erasing them (ContactBuilderFactory.cpp:362-367, Grains.cpp:74),
+  // and the next simulation built in this process would delete them again
+  // when it defines its own (ContactBuilderFactory.cpp:107-108).  The next
+  // simulation replaces the models; the old objects are never used again.
+  c->g = nullptr;
+  c->stock_lc = nullptr;
   std::string cmd = "rm -rf '" + c->dir + "'";
   if (c->dir.rfind("/tmp/grains_ref_", 0) == 0) (void)!system(cmd.c_str());
   delete c;
@@ -636,6 +656,24 @@ static int guarded(grains_gpu_ctx* c, void (*fn)(grains_gpu_ctx*, double, double
   }
   std::cout.rdbuf(old);
   return rc;
+}
+
+// The reference's own time loop with the B200 collision App: LinkedCellGPU
+// takes the place of the reference's LinkedCell in this simulation (as
+// Grains::Construction registers its LinkedCell, Grains.cpp:777-780).  gpu_ctx:
+// a grains_gpu context holding the same particles in the same upload order,
+// with the same shapes, laws and walls.
+int grains_ref_use_gpu_app(grains_gpu_ctx* c, void* gpu_ctx) {
+  if (!c || !c->g || !gpu_ctx || c->stock_lc) return GRAINS_GPU_INVALID_ARGUMENT;
+  LinkedCellGPU* app = new LinkedCellGPU(static_cast<grains_gpu_ctx*>(gpu_ctx));
+  std::map<int, int> row_of_my, rows;
+  for (size_t i = 0; i < c->my_id.size(); ++i) row_of_my[c->my_id[i]] = (int)i;
+  for (auto& kv : c->my_of_ref)
+    if (row_of_my.count(kv.second)) rows[kv.first] = row_of_my[kv.second];
+  app->setRows(rows);
+  app->setName("LinkedCell");
+  c->stock_lc = c->g->use_app(app);
+  return 0;
 }
 
 int grains_ref_compute_forces(grains_gpu_ctx* c, double time, double dt) {
