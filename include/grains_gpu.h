@@ -195,6 +195,11 @@ typedef struct grains_gpu_stats {
   int64_t n_steps_done;
   int32_t status;                 /* accumulated status bits */
   int32_t reserved;
+  /* running means since the last reset, as AppCollision::getOverlapMean /
+   * getNbIterGJKMean report them (AppCollision.cpp:160-187): the overlap of
+   * every contact met, the GJK iterations of every GJK call */
+  double  overlap_mean;
+  double  gjk_iterations_mean;
 } grains_gpu_stats;
 
 typedef struct grains_gpu_ctx grains_gpu_ctx;

@@ -769,6 +769,11 @@ int grains_ref_get_stats(grains_gpu_ctx* c, grains_gpu_stats* st) {
   st->n_obstacle_contacts = no;
   st->n_steps_done = c->steps;
   st->status = c->status;
+  // the reference's own running statistics (AppCollision.cpp:160-187); they
+  // run over the whole simulation (reset_stats does not clear them)
+  st->overlap_max = c->g->lc()->getOverlapMax();
+  st->overlap_mean = c->g->lc()->getOverlapMean();
+  st->gjk_iterations_mean = c->g->lc()->getNbIterGJKMean();
   return 0;
 }
 

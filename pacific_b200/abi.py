@@ -117,7 +117,8 @@ class Stats(C.Structure):
                 ("n_obstacle_candidates", C.c_int64), ("n_contacts", C.c_int64),
                 ("n_obstacle_contacts", C.c_int64), ("n_gjk_calls", C.c_int64), ("n_gjk_iterations", C.c_int64),
                 ("overlap_max", C.c_double), ("overlap_sum", C.c_double), ("n_steps_done", C.c_int64),
-                ("status", C.c_int32), ("reserved", C.c_int32)]
+                ("status", C.c_int32), ("reserved", C.c_int32), ("overlap_mean", C.c_double),
+                ("gjk_iterations_mean", C.c_double)]
 
 
 _VP = C.c_void_p

@@ -113,7 +113,7 @@ struct grains_gpu_ctx {
   int* ccount = nullptr;
   void* res_f = nullptr;  // per list entry: force and contact flag, torque (R4 each)
   void* res_t = nullptr;
-  int2* work = nullptr;   // owned list entries of an evaluation
+  int4* work = nullptr;   // owned list entries of an evaluation
   int* work_n = nullptr;
   int clist_cap = 0;
   int64_t clist_alloc = 0;
@@ -744,8 +744,8 @@ int ensure_lists(grains_gpu_ctx* c, int cap_per) {
     c->res_f = q;
     CK(cudaMalloc(&q, (size_t)need * r4));
     c->res_t = q;
-    CK(cudaMalloc(&q, (size_t)need * sizeof(int2)));
-    c->work = (int2*)q;
+    CK(cudaMalloc(&q, (size_t)need * sizeof(int4)));
+    c->work = (int4*)q;
     c->clist_alloc = need;
     for (int k = 0; k < 4; ++k)  // graphs hold the old pointers
       if (c->graph[k]) {
@@ -1870,6 +1870,9 @@ int grains_gpu_get_stats(grains_gpu_ctx* c, grains_gpu_stats* st) {
   st->overlap_sum = d.overlap_sum;
   st->n_steps_done = c->steps_done;
   st->status = d.status;
+  const double met = double(d.n_contacts + d.n_obs_contacts);
+  st->overlap_mean = met > 0. ? d.overlap_sum / met : 0.;
+  st->gjk_iterations_mean = d.n_gjk_calls ? double(d.n_gjk_iters) / double(d.n_gjk_calls) : 0.;
   return 0;
 }
 

@@ -19,7 +19,7 @@
 //     index, double buffered (prev -> next each force evaluation).
 //   contact lists (scratch of a force evaluation): L entries per particle
 //     (clist), the result of each entry (res_f, res_t: R4 each) and the work
-//     items of the owned entries (work: int2 per entry at most).
+//     items of the owned entries (work: int4 per entry at most).
 #pragma once
 
 #include <cstdint>
@@ -174,7 +174,8 @@ struct StepArgs {
   int clist_cap;
   typename Vec4<R>::type* res_f;  // per list entry: force on this particle, w = contact flag
   typename Vec4<R>::type* res_t;  // per list entry: torque on this particle
-  int2* work;            // owned list entries of this evaluation: (particle, entry | memory rank << 9)
+  int4* work;            // owned list entries of this evaluation: (particle, entry, index | memory rank << 9,
+                         // memory row)
   int* work_n;           // their count (cleared by the sums kernel)
   int* pairs;            // diagnostic contact pair output (2 ints per pair) or null
   int pairs_cap;

@@ -342,23 +342,36 @@ __global__ void __launch_bounds__(256) gather_kernel(StepArgs<R> a, int gather_f
 }
 
 // ---------------------------------------------------------------------------
-// contact memory lookup in the owner's row of the previous step.  The keys of
-// the first 8 entries are loaded together (no load waits on a comparison);
-// longer rows continue one entry at a time.
+// Contact memory lookup in the owner's row of the previous step, in two
+// parts so that the loads of the row start with the pair's other loads: the
+// entry count and the keys of the first 4 entries (MemoryKeys), then the match
+// and the payload of the matched entry; longer rows continue one entry at a
+// time.
+struct MemoryKeys {
+  int n;
+  int2 key[4];
+};
+
 template <typename R>
-__device__ __forceinline__ bool find_memory(const StepArgs<R>& a, int row, int other, int flags,
+__device__ __forceinline__ MemoryKeys memory_keys(const StepArgs<R>& a, int row) {
+  const HistEntry<R>* h = a.hist_prev + (size_t)row * a.hist_cap;
+  MemoryKeys k;
+  k.n = a.hist_n_prev[row];
+#pragma unroll
+  for (int j = 0; j < 4; ++j) k.key[j] = j < a.hist_cap ? make_int2(h[j].other, h[j].flags) : make_int2(-1, -1);
+  return k;
+}
+
+template <typename R>
+__device__ __forceinline__ bool find_memory(const StepArgs<R>& a, int row, const MemoryKeys& k, int other, int flags,
                                             PairMemory<R>& m) {
   const HistEntry<R>* h = a.hist_prev + (size_t)row * a.hist_cap;
-  const int n = a.hist_n_prev[row];
   int found = -1;
-  int2 key[8];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) key[k] = k < n ? make_int2(h[k].other, h[k].flags) : make_int2(-1, -1);
-#pragma unroll
-  for (int k = 7; k >= 0; --k)
-    if (key[k].x == other && key[k].y == flags) found = k;
-  for (int k = 8; found < 0 && k < n; ++k)
-    if (h[k].other == other && h[k].flags == flags) found = k;
+  for (int j = 3; j >= 0; --j)
+    if (j < k.n && k.key[j].x == other && k.key[j].y == flags) found = j;
+  for (int j = 4; found < 0 && j < k.n; ++j)
+    if (h[j].other == other && h[j].flags == flags) found = j;
   if (found < 0) return false;
   const HistEntry<R>& e = h[found];
   m.kdelta = v3<R>(e.kd[0], e.kd[1], e.kd[2]);
@@ -647,22 +660,26 @@ __device__ __forceinline__ void contacts_one(const StepArgs<R>& a, int s, unsign
   n_work = owned;  // recounted by the caller when the list overflowed
 }
 
-// work items of the owned entries of particle s, at `base` onward; the rank
-// of an owned entry among the particle's owned entries is its contact-memory
-// position
+// work items of the owned entries of particle s, at `base` onward: (particle,
+// the entry itself, entry index | memory rank << 9, the particle's memory
+// row).  The rank of an owned entry among the particle's owned entries is its
+// contact-memory position.  Carrying the entry and the row lets the pair
+// kernel issue every load of its second level at once.
 template <typename R>
 __device__ __forceinline__ void emit_work(const StepArgs<R>& a, int s, int base) {
   const int* list = a.clist + (size_t)s * a.clist_cap;
   const int cnt = a.ccount[s];
+  const int row = a.cur.orig[s];
   const long long limit = (long long)a.n * a.clist_cap;  // the work array's size
   int rank = 0;
   for (int q = 0; q < cnt; ++q) {
-    if (!entry_owned(list[q])) continue;
+    const int e = list[q];
+    if (!entry_owned(e)) continue;
     if ((long long)base + rank >= limit) {  // a counter left over from an unfinished evaluation
       set_status(a.stats, GRAINS_GPU_CUDA_ERROR);
       return;
     }
-    a.work[base + rank] = make_int2(s, q | (rank << 9));
+    a.work[base + rank] = make_int4(s, e, q | (rank << 9), row);
     ++rank;
   }
 }
@@ -763,11 +780,6 @@ __device__ __forceinline__ void put_no_contact(const StepArgs<R>& a, size_t slot
   z.x = z.y = z.z = z.w = R(0);
   a.res_f[slot] = z;
 }
-// a hole in the owner's next memory row (no contact, or a law without memory)
-template <typename R>
-__device__ __forceinline__ void put_memory_hole(const StepArgs<R>& a, int row, int rank) {
-  if (rank < a.hist_cap) a.hist_next[(size_t)row * a.hist_cap + rank].flags = -1;
-}
 template <typename R>
 __device__ __forceinline__ void put_memory(const StepArgs<R>& a, int row, int rank, int other, int flags,
                                            const PairMemory<R>& m) {
@@ -787,17 +799,16 @@ __device__ __forceinline__ void put_memory(const StepArgs<R>& a, int row, int ra
 // B. one owned list entry: particle pair (p0 = this particle, the lower id)
 // or particle-obstacle candidate (p0 = the particle, p1 = the obstacle)
 template <typename R, bool DIAG, bool CONVEX, bool SV = false>
-__device__ __forceinline__ void pair_one(const StepArgs<R>& a, int2 item, R dt, ForceStats& fs) {
+__device__ __forceinline__ void pair_one(const StepArgs<R>& a, int4 item, R dt, ForceStats& fs) {
   const ParticleArrays<R>& P = a.cur;
-  const int s = item.x, q = item.y & 511, rank = item.y >> 9;
+  const int s = item.x, e = item.y, q = item.z & 511, rank = item.z >> 9, oi = item.w;
   const size_t my_slot = (size_t)s * a.clist_cap + q;
-  const int e = a.clist[my_slot];
   const double4 xi = P.xr[s];
   const int4 mi = P.meta[s];
   const double4 mdi = P.md[s];
   const V3<R> vi = ld3<R>(P.v[s]);
   const V3<R> wi = ld3<R>(P.w[s]);
-  const int oi = P.orig[s];
+  const MemoryKeys keys = memory_keys(a, oi);
   const SysDev& S = a.sys[mi.w];
   const D3 Xi = d3(xi.x, xi.y, xi.z);
 
@@ -862,7 +873,6 @@ __device__ __forceinline__ void pair_one(const StepArgs<R>& a, int2 item, R dt, 
     if (!contact) {
       put_no_contact(a, my_slot);
       if (qp >= 0) put_no_contact(a, other_slot);
-      put_memory_hole(a, oi, rank);
       return;
     }
     if (qp < 0) set_status(a.stats, GRAINS_GPU_PAIR_OVERFLOW);  // the partner's list overflowed
@@ -884,7 +894,7 @@ __device__ __forceinline__ void pair_one(const StepArgs<R>& a, int2 item, R dt, 
     const LawParams<R> L = a.laws[S.law_offset + mi.y * S.n_mat + mj.y];
     PairMemory<R> mem;
     bool existed = false;
-    if (law_has_memory(L.type)) existed = find_memory(a, oi, mj.x, 0, mem);
+    if (law_has_memory(L.type)) existed = find_memory(a, oi, keys, mj.x, 0, mem);
     PairFp64 pd;
     if constexpr (sizeof(R) == 4) {
       pd.v0 = widen(vi);
@@ -904,8 +914,6 @@ __device__ __forceinline__ void pair_one(const StepArgs<R>& a, int2 item, R dt, 
     if (law_has_memory(L.type)) {
       put_memory(a, oi, rank, mj.x, 0, mem);
       flag = 3;
-    } else {
-      put_memory_hole(a, oi, rank);
     }
     // p0 gets f at the contact point, p1 gets -f (and the rolling torques +M / -M)
     if (law_has_torque(L)) {
@@ -963,7 +971,6 @@ __device__ __forceinline__ void pair_one(const StepArgs<R>& a, int2 item, R dt, 
   }
   if (!(g.overlap < 0.)) {
     put_no_contact(a, my_slot);
-    put_memory_hole(a, oi, rank);
     return;
   }
   // p0 = particle, p1 = obstacle (mass 1e20, velocity at the point, Obstacle.cpp:128-133)
@@ -986,7 +993,7 @@ __device__ __forceinline__ void pair_one(const StepArgs<R>& a, int2 item, R dt, 
   PairMemory<R> mem;
   const int oloc = oidx - S.obs_offset;
   bool existed = false;
-  if (law_has_memory(L.type)) existed = find_memory(a, oi, oloc, 1, mem);
+  if (law_has_memory(L.type)) existed = find_memory(a, oi, keys, oloc, 1, mem);
   PairFp64 pd;
   if constexpr (sizeof(R) == 4) {
     pd.v0 = widen(vi);
@@ -1006,8 +1013,6 @@ __device__ __forceinline__ void pair_one(const StepArgs<R>& a, int2 item, R dt, 
   if (law_has_memory(L.type)) {
     put_memory(a, oi, rank, oloc, 1, mem);
     flag = 3;
-  } else {
-    put_memory_hole(a, oi, rank);
   }
   if (law_has_torque(L)) t0 = t0 + res.torque;
   put_result(a, my_slot, res.force, t0, flag);
@@ -1040,39 +1045,53 @@ __global__ void __launch_bounds__(128, CONVEX ? 1 : GG_PAIRS_MIN_BLOCKS) pairs_k
 
 // C. the torsor of particle s: InitializeForces(withWeight) (torsor = weight,
 // Particle.cpp:1409-1416) then every contact in list order; the coordination
-// number; the owner's next memory row packed.  Clears the work counter for the
-// next evaluation (thread 0; every pair item was read before this kernel).
+// number; the owner's next memory row packed: an owned entry whose result flag
+// is 3 stored its memory at its rank, the others left a hole, and the kept
+// entries move down over the holes (rows without holes are not touched).  The
+// results of four entries are loaded at a time.
 template <typename R>
 __device__ __forceinline__ void sum_one(const StepArgs<R>& a, int s) {
   const ParticleArrays<R>& P = a.cur;
   const int sysi = P.meta[s].w;
   const double mass = P.md[s].x;
+  const int row = P.orig[s];
   const SysDev& S = a.sys[sysi];
   V3<R> F = v3<R>(R(S.gx * mass), R(S.gy * mass), R(S.gz * mass));
   V3<R> T = v3<R>(R(0), R(0), R(0));
   const int cnt = a.ccount[s];
   const size_t base = (size_t)s * a.clist_cap;
   const int* list = a.clist + base;
-  int ncontact = 0, owned = 0;
-  for (int q = 0; q < cnt; ++q) {
-    const R4<R> rf = a.res_f[base + q];
-    owned += entry_owned(list[q]) ? 1 : 0;
-    if (rf.w == R(0)) continue;
-    F = F + ld3<R>(rf);
-    T = T + ld3<R>(a.res_t[base + q]);
-    ++ncontact;
+  HistEntry<R>* h = a.hist_next + (size_t)row * a.hist_cap;
+  int ncontact = 0, owned = 0, kept = 0;
+  for (int q0 = 0; q0 < cnt; q0 += 4) {
+    R4<R> rf[4], rt[4];
+    int e[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const bool in = q0 + u < cnt;
+      if (in) {
+        rf[u] = a.res_f[base + q0 + u];
+        rt[u] = a.res_t[base + q0 + u];
+        e[u] = list[q0 + u];
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      if (q0 + u >= cnt) break;
+      if (entry_owned(e[u])) {
+        const int rank = owned++;
+        if (rank < a.hist_cap && rf[u].w == R(3)) {
+          if (kept != rank) h[kept] = h[rank];
+          ++kept;
+        }
+      }
+      if (rf[u].w == R(0)) continue;
+      F = F + ld3<R>(rf[u]);
+      T = T + ld3<R>(rt[u]);
+      ++ncontact;
+    }
   }
   a.coord[s] = ncontact;
-  // pack the memory row: holes (flags -1) are squeezed out, order kept
-  const int row = P.orig[s];
-  HistEntry<R>* h = a.hist_next + (size_t)row * a.hist_cap;
-  const int m = min(owned, a.hist_cap);
-  int kept = 0;
-  for (int r = 0; r < m; ++r) {
-    if (h[r].flags < 0) continue;
-    if (kept != r) h[kept] = h[r];
-    ++kept;
-  }
   a.hist_n_next[row] = kept;
   P.F[s] = st3<R>(F);
   P.T[s] = st3<R>(T);
