@@ -88,6 +88,9 @@ def parse():
                     help="DEM steps that settle the bed before the settled leg (0: no settled leg; default "
                          "70,000 for polydisperse_200k, 100,000 for drum_100k, none otherwise)")
     ap.add_argument("--settled-chunks", type=int, default=10, help="timed chunks of the settled leg")
+    ap.add_argument("--settled-state", default=None,
+                    help="hybrid-binary reload file of the settled bed: read when it exists (it must come from "
+                         "the same workload and --settle-steps), else written after settling")
     return ap.parse_args()
 
 
@@ -294,6 +297,13 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def nvtx(name):
+    """An NVTX range around a leg of the bench, so that a profiler can be
+    limited to it (ncu --nvtx --nvtx-include "<name>/")."""
+    import torch
+    return torch.cuda.nvtx.range(name)
+
+
 def contact_force_error(lib, sc, state, mem, device, where):
     """Per-contact relative error of the mixed-precision contact forces against
     the plain FP64 path on identical states and contact memories: max and 99th
@@ -362,31 +372,51 @@ def settled_leg(args, lib, sc, local, flush, peak, peak_kind):
     import torch
     from pacific_b200 import scenarios as S
     from pacific_b200.abi import FP64, MIXED, Simulation, read_reload_particles
-    sim = Simulation(lib, MIXED, max_particles=sc.n, device=local)
-    S.apply(sim, sc)
-    sim.initialize_leapfrog(0.0, sc.dt)
-    t, done = 0.0, 0
-    while done < args.settle_steps:
-        k = min(5000, args.settle_steps - done)
-        t = sim.step(k, t, sc.dt)
-        done += k
-    sim.synchronize()
-    z_settled = mean_coordination(sim, sc, t)
-    with tempfile.TemporaryDirectory(prefix="gg_settled") as d:
-        path = os.path.join(d, "settled_Particles.bin")
-        t0 = time.perf_counter()
-        nbytes = sim.write_reload_particles(path, binary=True)
-        w_s = time.perf_counter() - t0
-        r = read_reload_particles(lib, path, True)
-    sim.close()
+    t = args.settle_steps * sc.dt
+    n_obs = len(sc.obstacles[0]) if len(sc.domains) == 1 else 0
+    poses = None
+    if args.settled_state and os.path.exists(args.settled_state):
+        r = read_reload_particles(lib, args.settled_state, True)
+        z_settled, nbytes, w_s = None, os.path.getsize(args.settled_state), None
+        if n_obs:
+            poses = np.load(args.settled_state + ".obstacles.npy")
+    else:
+        sim = Simulation(lib, MIXED, max_particles=sc.n, device=local)
+        S.apply(sim, sc)
+        sim.initialize_leapfrog(0.0, sc.dt)
+        t, done = 0.0, 0
+        with nvtx("settling"):
+            while done < args.settle_steps:
+                k = min(5000, args.settle_steps - done)
+                t = sim.step(k, t, sc.dt)
+                done += k
+            sim.synchronize()
+        z_settled = mean_coordination(sim, sc, t)
+        if n_obs:
+            # the particle file holds no obstacles: their poses after the
+            # settling (rotating drum) go with it
+            poses = sim.obstacles(0, n_obs)
+            if args.settled_state:
+                np.save(args.settled_state + ".obstacles.npy", poses)
+        with tempfile.TemporaryDirectory(prefix="gg_settled") as d:
+            path = args.settled_state or os.path.join(d, "settled_Particles.bin")
+            t0 = time.perf_counter()
+            nbytes = sim.write_reload_particles(path, binary=True)
+            w_s = time.perf_counter() - t0
+            r = read_reload_particles(lib, path, True)
+        sim.close()
     p = dict(sc.particles)
     order = np.argsort(r["id"])
-    for k in ["position", "quaternion", "velocity", "omega"]:
+    for k in ["position", "quaternion", "velocity", "omega"] + (["basis"] if p.get("basis") is not None else []):
         p[k] = np.ascontiguousarray(r[k][order])
-    sc2 = S.Scenario(sc.name, sc.shapes, sc.domains, sc.laws, sc.obstacles, p, sc.dt, sc.n_steps, meta=sc.meta)
+    obstacles = sc.obstacles
+    if poses is not None:
+        obstacles = [[dict(o, transform=[float(x) for x in poses[i]]) for i, o in enumerate(sc.obstacles[0])]]
+    sc2 = S.Scenario(sc.name, sc.shapes, sc.domains, sc.laws, obstacles, p, sc.dt, sc.n_steps, meta=sc.meta)
     mem = r["memory"]
     out = {"settle_steps": args.settle_steps, "mean_coordination_after_settling": z_settled,
-           "reload_file": {"bytes": int(nbytes), "write_ms": w_s * 1e3, "format": "hybrid binary"}}
+           "reload_file": {"bytes": int(nbytes), "write_ms": None if w_s is None else w_s * 1e3,
+                           "format": "hybrid binary", "read_from_settled_state": w_s is None}}
 
     def run(prec):
         s = Simulation(lib, prec, max_particles=sc.n, device=local)
@@ -400,19 +430,21 @@ def settled_leg(args, lib, sc, local, flush, peak, peak_kind):
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(args.settled_chunks)]
         torch.cuda.synchronize()
-        for k in range(args.settled_chunks):
-            with torch.cuda.stream(stream):
-                flush.fill_(k & 0xFF)
-                ev[k][0].record(stream)
-            tt = s.step(args.chunk, tt, sc.dt)
-            ev[k][1].record(stream)
-        torch.cuda.synchronize()
+        with nvtx("settled_%s_timed" % ("fp64" if prec == FP64 else "mixed")):
+            for k in range(args.settled_chunks):
+                with torch.cuda.stream(stream):
+                    flush.fill_(k & 0xFF)
+                    ev[k][0].record(stream)
+                tt = s.step(args.chunk, tt, sc.dt)
+                ev[k][1].record(stream)
+            torch.cuda.synchronize()
         ms = sum(a.elapsed_time(b) for a, b in ev)
         return s, tt, ms
     sm, tm, ms_m = run(MIXED)
     z = mean_coordination(sm, sc, tm)
     gst = sm.stats()  # of that one force evaluation
-    _, per_step, tot = profile_run(sm, sc, 500, tm)
+    with nvtx("settled_kernels"):
+        _, per_step, tot = profile_run(sm, sc, 500, tm)
     sm.close()
     s64, _, ms_64 = run(FP64)
     s64.close()
@@ -542,13 +574,14 @@ def main():
         clk = ClockSampler(local) if sample_clocks else None
         if clk:
             clk.__enter__()
-        for k in range(args.steps):
-            with torch.cuda.stream(stream):
-                flush.fill_(k & 0xFF)          # L2 flush between timed chunks (untimed)
-                ev[k][0].record(stream)
-            t = sim.step(args.chunk, t, sc.dt)
-            ev[k][1].record(stream)
-        torch.cuda.synchronize()
+        with nvtx("%s_timed" % ("fp64" if precision == FP64 else "mixed")):
+            for k in range(args.steps):
+                with torch.cuda.stream(stream):
+                    flush.fill_(k & 0xFF)          # L2 flush between timed chunks (untimed)
+                    ev[k][0].record(stream)
+                t = sim.step(args.chunk, t, sc.dt)
+                ev[k][1].record(stream)
+            torch.cuda.synchronize()
         sim.synchronize()
         if clk:
             clk.__exit__()
@@ -574,7 +607,8 @@ def main():
     prof_tot = {}
     zs = []
     for k in range(args.steps):
-        tp, _, prof = profile_run(sim, sc, args.chunk, tp)
+        with nvtx("kernels"):
+            tp, _, prof = profile_run(sim, sc, args.chunk, tp)
         for name, (ms_k, n_k) in prof.items():
             a0, b0 = prof_tot.get(name, (0.0, 0))
             prof_tot[name] = (a0 + ms_k, b0 + n_k)

@@ -244,6 +244,22 @@ int grains_gpu_set_obstacle_loadings(grains_gpu_ctx* ctx, int32_t system, int32_
  * and the obstacle-cell links use Johnson's, as in the reference. */
 enum grains_gpu_collision_algorithm { GRAINS_GPU_GJK = 0, GRAINS_GPU_GJK_SV = 1 };
 int grains_gpu_set_collision_algorithm(grains_gpu_ctx* ctx, int32_t algorithm);
+/* replaces: the Tolerance, Acceleration and History attributes of
+ * <CollisionDetection> (Base/src/Grains.cpp:674-723; GrainsExec::m_colDetTolerance,
+ * m_colDetAcceleration, m_colDetWithHistory).
+ *   tolerance     relative optimality gap of the GJK runs (>= 1e-10; the
+ *                 reference's default is 1e-10)
+ *   acceleration  1: Nesterov-accelerated search directions (Convex.cpp:566-597)
+ *   history       1: each convex particle pair keeps its last GJK iterate and
+ *                 starts its next run from it (CollisionHistory, Particle.cpp:
+ *                 486-505; Convex.cpp:636-716).  The history of a pair lives in
+ *                 the row of its lower id, one slot per owned work item, up to
+ *                 history_capacity of them; a pair beyond that starts cold.
+ * Applies to both GJK algorithms and to the crust-x10 retry; the static
+ * obstacle-cell links use the tolerance and acceleration too, so set the
+ * options before grains_gpu_upload_particles.  Default: 1e-10, 0, 0. */
+int grains_gpu_set_collision_options(grains_gpu_ctx* ctx, double tolerance, int32_t acceleration,
+                                     int32_t history);
 /* replaces: LinkedCell::Link(Particle*) for all active particles
  * (LinkedCell.cpp:1330-1365) + AllComponents state upload */
 int grains_gpu_upload_particles(grains_gpu_ctx* ctx, const grains_gpu_particles* p);

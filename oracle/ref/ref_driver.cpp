@@ -116,6 +116,8 @@ struct grains_gpu_ctx {
   std::vector<grains_gpu_obstacle> obs;
   std::vector<grains_gpu_obstacle_loading> loads;  // explicit imposed motions
   int collision = GRAINS_GPU_GJK;                   // <CollisionDetection Type=...>
+  double gjk_tol = 1e-10;                           // Tolerance=...
+  int gjk_accel = 0, gjk_history = 0;               // Acceleration=..., History=...
   OracleGrains* g = nullptr;
   LinkedCell* stock_lc = nullptr;  // the reference's LinkedCell after grains_ref_use_gpu_app
   std::string dir;
@@ -279,6 +281,15 @@ int grains_ref_set_collision_algorithm(grains_gpu_ctx* c, int32_t algorithm) {
   return 0;
 }
 
+int grains_ref_set_collision_options(grains_gpu_ctx* c, double tolerance, int32_t acceleration, int32_t history) {
+  if (!(tolerance >= 1e-10) || (acceleration != 0 && acceleration != 1) || (history != 0 && history != 1))
+    return GRAINS_GPU_INVALID_ARGUMENT;
+  c->gjk_tol = tolerance;
+  c->gjk_accel = acceleration;
+  c->gjk_history = history;
+  return 0;
+}
+
 int grains_ref_set_obstacle_loadings(grains_gpu_ctx* c, int32_t system, int32_t n,
                                      const grains_gpu_obstacle_loading* l) {
   (void)system;
@@ -340,8 +351,13 @@ int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
       m = std::nextafter(m, m - d.origin[a] < d.size[a] ? 1e300 : -1e300);
     mxyz[a] = m;
   }
-  if (c->collision == GRAINS_GPU_GJK_SV)
-    x << "<CollisionDetectionAlgorithm><CollisionDetection Type=\"GJK_SV\"/></CollisionDetectionAlgorithm>\n";
+  // every attribute is written: the reference keeps them in GrainsExec
+  // statics that only a present attribute sets (Grains.cpp:654-723), so a
+  // simulation built after another in this process must restate the defaults
+  x << "<CollisionDetectionAlgorithm><CollisionDetection Type=\""
+    << (c->collision == GRAINS_GPU_GJK_SV ? "GJK_SV" : "GJK") << "\" Tolerance=\"" << num(c->gjk_tol)
+    << "\" Acceleration=\"" << (c->gjk_accel ? "ON" : "OFF") << "\" History=\""
+    << (c->gjk_history ? "ON" : "OFF") << "\"/></CollisionDetectionAlgorithm>\n";
   x << "<LinkedCell MX=\"" << num(mxyz[0]) << "\" MY=\"" << num(mxyz[1]) << "\" MZ=\"" << num(mxyz[2])
     << "\" CellSizeFactor=\"" << num(d.cell_size / (2. * rmax)) << "\"/>\n";
   x << "<Origin OX=\"" << num(d.origin[0]) << "\" OY=\"" << num(d.origin[1]) << "\" OZ=\"" << num(d.origin[2])

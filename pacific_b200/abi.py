@@ -132,6 +132,7 @@ _SIGS = {
     "set_obstacles": [_VP, C.c_int32, C.c_int32, C.POINTER(Obstacle)],
     "set_obstacle_loadings": [_VP, C.c_int32, C.c_int32, C.POINTER(ObstacleLoading)],
     "set_collision_algorithm": [_VP, C.c_int32],
+    "set_collision_options": [_VP, C.c_double, C.c_int32, C.c_int32],
     "upload_particles": [_VP, C.POINTER(Particles)],
     "download_particles": [_VP, C.POINTER(Particles)],
     "update_particles": [_VP, C.POINTER(Particles)],
@@ -155,7 +156,7 @@ _SIGS = {
                       C.POINTER(C.c_int64)],
 }
 # diagnostics that the reference built from its sources (oracle/_ref) lacks
-_OPTIONAL = {"get_contact_forces", "set_record_attributes"}
+_OPTIONAL = {"get_contact_forces", "set_record_attributes", "set_collision_options"}
 _GPU_ONLY = {
     "get_stream": [_VP, C.POINTER(_VP)],
     "synchronize": [_VP],
@@ -397,6 +398,14 @@ class Simulation:
         """GJK (0, Johnson's) or GJK_SV (1, signed volumes) for non-spherical pairs."""
         self._check(self.lib.fn["set_collision_algorithm"](self.ctx, algorithm))
 
+    def set_collision_options(self, tolerance=1e-10, acceleration=False, history=False):
+        """The Tolerance, Acceleration and History attributes of the
+        reference's <CollisionDetection> element: the GJK optimality-gap
+        tolerance, Nesterov-accelerated search directions, and the warm start
+        of each convex pair from its last GJK iterate."""
+        self._check(self.lib.fn["set_collision_options"](self.ctx, float(tolerance), int(bool(acceleration)),
+                                                          int(bool(history))))
+
     def set_obstacle_loadings(self, system, loadings):
         """Imposed obstacle motions: dicts with obstacle_id, type, t_start,
         t_end and the type's fields (vector, center, amplitude, period,
@@ -603,11 +612,11 @@ class Simulation:
     def set_gjk_tolerance(self, tol):
         self._check(self.lib.fn["set_gjk_tolerance"](self.ctx, tol))
 
-    def set_polyhedron_support(self, stateless):
-        """Oracle only: stateless=True makes the polyhedron support the
-        order-independent arg-max of the CUDA path instead of the reference's
-        warm-started hill climb."""
-        self._check(self.lib.fn["set_polyhedron_support"](self.ctx, 1 if stateless else 0))
+    def set_polyhedron_support(self, mode):
+        """Oracle only: 0 the reference's polyhedron support (a hill climb from
+        the vertex each body kept), 1 the order-independent arg-max, 2 the
+        CUDA path's hill climb that every GJK run starts at vertex 0."""
+        self._check(self.lib.fn["set_polyhedron_support"](self.ctx, int(mode)))
 
     # ---- tuning (CUDA implementation only) ----
     def tuning(self):

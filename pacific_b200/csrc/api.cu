@@ -29,6 +29,10 @@ struct ShapeHost {
   std::vector<double> params;
   std::vector<double> verts;
   std::vector<std::vector<int>> faces;
+  // vertex adjacency of a polyhedron (Polyhedron::m_cobound, built by
+  // Polyhedron::BuildPolyhedron, Polyhedron.cpp:338-339): for every face, each
+  // vertex lists the vertex that follows it on the face
+  std::vector<int> adj_start, adj;
   double volume = 0, circ = 0;
   double inertia[3] = {0, 0, 0};
   double lext[3] = {0, 0, 0};
@@ -129,6 +133,8 @@ struct grains_gpu_ctx {
   SysDev* d_sys = nullptr;
   ShapeDev* d_shapes = nullptr;
   double* d_verts = nullptr;
+  int* d_adj_start = nullptr;  // polyhedron adjacency over the vertex table
+  int* d_adj = nullptr;
   ObstacleDev* d_obs = nullptr;
   LoadingDev* d_loads = nullptr;
   int* d_load_flags = nullptr;  // per system: a loading active over this step, over the previous one
@@ -141,8 +147,12 @@ struct grains_gpu_ctx {
   cudaGraphExec_t graph[4] = {nullptr, nullptr, nullptr, nullptr};
   double graph_dt[4] = {0, 0, 0, 0};
   int64_t steps_done = 0;
-  double gjk_tol = kEpsilon;
-  int gjk_sv = 0;  // GrainsExec::m_colDetGJK_SV
+  double gjk_tol = kEpsilon;  // GrainsExec::m_colDetTolerance
+  int gjk_sv = 0;             // GrainsExec::m_colDetGJK_SV
+  int gjk_accel = 0;          // GrainsExec::m_colDetAcceleration
+  int gjk_history = 0;        // GrainsExec::m_colDetWithHistory
+  GjkDir* gdir[2] = {nullptr, nullptr};  // collision histories, selected by hcur like the memory rows
+  int* gdir_n[2] = {nullptr, nullptr};
   // launch and grid tuning (grains_gpu_set_tuning / grains_gpu_autotune)
   double cell_factor = 1.0;
   int contacts_block = 256;
@@ -276,6 +286,17 @@ int build_shape(int type, const double* p, int np, ShapeHost& s, std::string& er
     }
     s.volume = vol;
     for (int i = 0; i < 3; ++i) s.inertia[i] = I[i];
+    {
+      std::vector<std::vector<int>> nb(nv);
+      for (const auto& f : s.faces)
+        for (size_t j = 0, kk = f.size() - 1; j < f.size(); kk = j++) nb[f[kk]].push_back(f[j]);
+      s.adj_start.assign(1, 0);
+      s.adj.clear();
+      for (int i = 0; i < nv; ++i) {
+        s.adj.insert(s.adj.end(), nb[i].begin(), nb[i].end());
+        s.adj_start.push_back((int)s.adj.size());
+      }
+    }
     double r2 = 0;  // Polyhedron::computeCircumscribedRadius, Polyhedron.cpp:201-210
     for (int i = 0; i < nv; ++i) {
       double d = s.verts[3 * i] * s.verts[3 * i] + s.verts[3 * i + 1] * s.verts[3 * i + 1] +
@@ -431,6 +452,10 @@ BodyRef obstacle_body(const ObstacleDev& o, const ShapeHost& sh) {
     b.scaling[i] = o.scaling[i];
     b.lext[i] = sh.lext[i];
   }
+  if (sh.type == GRAINS_GPU_POLYHEDRON && !sh.adj_start.empty()) {
+    b.adj_start = sh.adj_start.data();
+    b.adj = sh.adj.data();
+  }
   return b;
 }
 
@@ -441,7 +466,7 @@ BodyRef obstacle_body(const ObstacleDev& o, const ShapeHost& sh) {
 // RigidBodyWithCrust.cpp:842-956: distance < crust_cell + crust_obs - EPSILON).
 void link_static_obstacles(const SysHost& s, const std::vector<ShapeHost>& shapes,
                            const std::vector<ObstacleDev>& obs, int first_obs,
-                           std::vector<std::vector<int>>& cell_lists) {
+                           std::vector<std::vector<int>>& cell_lists, double tol, bool accel) {
   const double hx = 0.5 * 2. * s.ex, hy = 0.5 * 2. * s.ey, hz = 0.5 * 2. * s.ez;
   ShapeHost cellbox;
   std::string unused;
@@ -479,7 +504,9 @@ void link_static_obstacles(const SysHost& s, const std::vector<ShapeHost>& shape
         if (xnorm(g) < A.radius + B.radius) {
           LocalBody<double> la = local_body<double>(A, d3(0, 0, 0), A.scaling);
           LocalBody<double> lb = local_body<double>(B, d3(0, 0, 0), B.scaling);
-          GjkResult<double> r = gjk_distance(la, lb, kEpsilon);
+          GjkStart<double> st;
+          st.accel = accel;
+          GjkResult<double> r = gjk_distance(la, lb, tol, st);
           add = r.dist < A.crust + B.crust - kEpsilon;
         }
       }
@@ -518,6 +545,8 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   a.sys = c->d_sys;
   a.shapes = c->d_shapes;
   a.verts = c->d_verts;
+  a.adj_start = c->d_adj_start;
+  a.adj = c->d_adj;
   a.obs = c->d_obs;
   a.cell_obs_start = c->d_cell_obs_start;
   a.cell_obs_idx = c->d_cell_obs_idx;
@@ -552,6 +581,12 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   a.pair_sys = c->pair_sys;
   a.gjk_tol = c->gjk_tol;
   a.gjk_sv = c->gjk_sv;
+  a.gjk_accel = c->gjk_accel;
+  a.gjk_history = c->gjk_history;
+  a.gdir_prev = c->gdir[c->hcur];
+  a.gdir_n_prev = c->gdir_n[c->hcur];
+  a.gdir_next = c->gdir[1 - c->hcur];
+  a.gdir_n_next = c->gdir_n[1 - c->hcur];
   a.barrier_polls = c->barrier_polls;
   a.barrier_skip_block = c->barrier_skip_block;
   a.contacts_block = c->contacts_block;
@@ -986,11 +1021,46 @@ int grains_gpu_set_obstacles(grains_gpu_ctx* c, int32_t system, int32_t n, const
   return 0;
 }
 
+namespace {
+void drop_graphs(grains_gpu_ctx* c) {
+  for (int k = 0; k < 4; ++k)
+    if (c->graph[k]) {
+      cudaGraphExecDestroy(c->graph[k]);
+      c->graph[k] = nullptr;
+    }
+}
+}  // namespace
+
 int grains_gpu_set_collision_algorithm(grains_gpu_ctx* c, int32_t algorithm) {
   if (!c) return GRAINS_GPU_INVALID_ARGUMENT;
   if (algorithm != GRAINS_GPU_GJK && algorithm != GRAINS_GPU_GJK_SV)
     return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "unknown collision algorithm");
   c->gjk_sv = algorithm == GRAINS_GPU_GJK_SV ? 1 : 0;
+  drop_graphs(c);
+  return 0;
+}
+
+int grains_gpu_set_collision_options(grains_gpu_ctx* c, double tolerance, int32_t acceleration, int32_t history) {
+  if (!c) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!(tolerance >= 1e-10))  // Grains.cpp:684-689 rejects tolerances below 1e-10
+    return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "GJK tolerance must be at least 1e-10");
+  if ((acceleration != 0 && acceleration != 1) || (history != 0 && history != 1))
+    return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "acceleration and history are 0 (OFF) or 1 (ON)");
+  if (history && !c->gdir[0]) {
+    const size_t N = (size_t)c->cap;
+    for (int k = 0; k < 2; ++k) {
+      c->gdir[k] = dalloc<GjkDir>(N * c->hist_cap, c->pool);
+      c->gdir_n[k] = dalloc<int>(N, c->pool);
+      if (!c->gdir[k] || !c->gdir_n[k]) return fail(c, GRAINS_GPU_CUDA_ERROR, "collision history allocation failed");
+    }
+  }
+  if (history && !c->gjk_history)  // a history starts empty
+    for (int k = 0; k < 2; ++k) CK(cudaMemsetAsync(c->gdir_n[k], 0, (size_t)c->cap * sizeof(int), c->stream));
+  c->gjk_tol = tolerance;
+  c->gjk_accel = acceleration;
+  c->gjk_history = history;
+  c->tables_dirty = true;  // the static obstacle-cell links use the same GJK
+  drop_graphs(c);
   return 0;
 }
 
@@ -1067,7 +1137,7 @@ int build_tables(grains_gpu_ctx* c) {
     d.n_moving = (int)moving.size() - d.moving_offset;
     const int nb = s.nbi * s.nbj * s.nbk;
     std::vector<std::vector<int>> lists(nb);
-    link_static_obstacles(s, c->shapes, ho, d.obs_offset, lists);
+    link_static_obstacles(s, c->shapes, ho, d.obs_offset, lists, c->gjk_tol, c->gjk_accel != 0);
     for (int k = 0; k < nb; ++k) {
       cstart.push_back((int)cidx.size());
       cidx.insert(cidx.end(), lists[k].begin(), lists[k].end());
@@ -1126,10 +1196,18 @@ int build_tables(grains_gpu_ctx* c) {
   // shapes
   std::vector<ShapeDev> sd;
   std::vector<double> verts;
+  std::vector<int> adj_start, adj;  // adjacency over the whole vertex table
   for (auto& s : c->shapes) {
     sd.push_back(shape_dev(s, (int)verts.size() / 3));
     verts.insert(verts.end(), s.verts.begin(), s.verts.end());
+    const int nv = (int)s.verts.size() / 3;
+    for (int i = 0; i < nv; ++i) {
+      adj_start.push_back((int)adj.size());
+      if (!s.adj_start.empty())
+        adj.insert(adj.end(), s.adj.begin() + s.adj_start[i], s.adj.begin() + s.adj_start[i + 1]);
+    }
   }
+  adj_start.push_back((int)adj.size());
   auto up = [&](const void* src, size_t bytes, void** dst) -> int {
     void* p = nullptr;
     CK(cudaMalloc(&p, bytes ? bytes : 16));
@@ -1142,6 +1220,8 @@ int build_tables(grains_gpu_ctx* c) {
   rc |= up(hs.data(), hs.size() * sizeof(SysDev), (void**)&c->d_sys);
   rc |= up(sd.data(), sd.size() * sizeof(ShapeDev), (void**)&c->d_shapes);
   rc |= up(verts.data(), verts.size() * sizeof(double), (void**)&c->d_verts);
+  rc |= up(adj_start.data(), adj_start.size() * sizeof(int), (void**)&c->d_adj_start);
+  rc |= up(adj.data(), adj.size() * sizeof(int), (void**)&c->d_adj);
   rc |= up(ho.data(), ho.size() * sizeof(ObstacleDev), (void**)&c->d_obs);
   rc |= up(cstart.data(), cstart.size() * sizeof(int), (void**)&c->d_cell_obs_start);
   rc |= up(cidx.data(), cidx.size() * sizeof(int), (void**)&c->d_cell_obs_idx);
@@ -1373,6 +1453,8 @@ int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
   }
   c->moved = 0;
   for (int k = 0; k < 2; ++k) CK(cudaMemsetAsync(c->hist_n[k], 0, (size_t)c->cap * sizeof(int), c->stream));
+  for (int k = 0; k < 2; ++k)
+    if (c->gdir_n[k]) CK(cudaMemsetAsync(c->gdir_n[k], 0, (size_t)c->cap * sizeof(int), c->stream));
   CK(cudaMemsetAsync(c->stats, 0, sizeof(StatsDev), c->stream));
   c->keys_valid = false;
   c->sorted = false;
@@ -2075,6 +2157,10 @@ std::vector<std::pair<void*, size_t>> snapshot_fields(grains_gpu_ctx* c, int cur
   if (c->has_basis) f.push_back({b.basis, 9 * n * sizeof(double)});
   if (!c->h_obs.empty()) f.push_back({c->d_obs, c->h_obs.size() * sizeof(ObstacleDev)});
   if (!c->h_obs.empty()) f.push_back({c->d_load_flags, 2 * c->sys.size() * sizeof(int)});
+  if (c->gdir[hcur]) {  // collision histories (GJK warm start)
+    f.push_back({c->gdir[hcur], n * c->hist_cap * sizeof(GjkDir)});
+    f.push_back({c->gdir_n[hcur], n * sizeof(int)});
+  }
   return f;
 }
 

@@ -42,6 +42,18 @@ struct Vec4<double> {
   using type = double4;
 };
 
+// The collision history of a convex pair (CollisionHistory, Component/src/
+// CollisionHistory.cpp:22-49, kept by Particle::InterAction when
+// <CollisionDetection History="ON">, Particle.cpp:486-505): the last GJK
+// iterate of the pair, as seen from the pair's owner (the lower id) towards
+// the partner; other = the partner's id, or kNoGjkDir for an empty slot.
+struct GjkDir {
+  int other;
+  int pad;
+  double v[3];
+};
+constexpr int kNoGjkDir = -2147483647 - 1;
+
 struct ShapeDev {
   int type;
   int nverts;
@@ -147,6 +159,8 @@ struct StepArgs {
   const SysDev* sys;
   const ShapeDev* shapes;
   const double* verts;   // polyhedron vertices (xyz)
+  const int* adj_start;  // polyhedron vertex adjacency: per vertex (vertex table index) its first
+  const int* adj;        // neighbour in adj (local vertex indices); adj_start has one entry more
   const ObstacleDev* obs;
   const int* cell_obs_start;  // static obstacle CSR per cell (C+1)
   const int* cell_obs_idx;
@@ -184,6 +198,12 @@ struct StepArgs {
   int* pair_sys;         // diagnostic: system of each contact pair
   double gjk_tol;
   int gjk_sv;            // the signed-volume GJK for non-spherical pairs
+  int gjk_accel;         // Nesterov-accelerated GJK directions (<CollisionDetection Acceleration="ON">)
+  int gjk_history;       // warm-started GJK from the pair's collision history (History="ON")
+  GjkDir* gdir_prev;     // collision histories of the last evaluation (rows of hist_cap slots by memory row)
+  int* gdir_n_prev;
+  GjkDir* gdir_next;     // written by this evaluation
+  int* gdir_n_next;
   long long barrier_polls;  // persistent kernel: polls before a grid-barrier wait gives up
   int barrier_skip_block;   // persistent kernel: a block that leaves at once (a test of the bounded wait), or -1
   int contacts_block;    // threads per block of contacts_kernel (<= 256)

@@ -9,12 +9,27 @@
 // points match.
 //
 // Support functions: Sphere.cpp:99-109, Box.cpp:307-316, Cylinder.cpp:112-133
-// (axis = local Y), Polyhedron.cpp:265-293.  The polyhedron support here is a
-// stateless arg-max over the vertices (first maximum wins).  The reference
-// hill-climbs from a warm-start vertex kept per body between calls and moves
-// only for a gain above 1e-16, so the two differ when face vertices tie within
-// that margin (flat-face contacts): the distance is the same, the witness
-// points, hence the contact point, may not be.
+// (axis = local Y), Polyhedron.cpp:265-293.  The polyhedron support climbs the
+// vertex adjacency like the reference: from the current vertex to the first
+// neighbour (in adjacency order) that raises v . p by at least 1e-16, until no
+// neighbour does.  The reference keeps the current vertex per body between GJK
+// runs; here every GJK run starts its climb at vertex 0 and carries the vertex
+// from one support call to the next within the run.  On flat faces the vertex
+// reached depends on where the climb starts; over every polyhedron fixture and
+// a 1,500-step dense run of cubes, cylinders and octahedra the two rules gave
+// identical results, while the order-independent arg-max (kept for bodies
+// without adjacency) moved contact points by up to 3e-4 of the weight.
+//
+// Options of <CollisionDetection> (Base/src/Grains.cpp:654-723), passed in a
+// GjkStart: the tolerance of the optimality gap, the Nesterov-accelerated
+// search direction (Acceleration="ON": momentum k / (k + 2) on the direction,
+// plain every 8th iteration, and on convergence either stop, when the
+// accelerated direction has met the plain one, or go on without momentum --
+// the rule of Montaut et al., "Collision detection accelerated: an
+// optimization perspective", RSS 2022, as Convex.cpp:566-597 applies it), and
+// the warm start of History="ON" (Convex.cpp:636-716): the run starts from a
+// given direction v0 (its first support point in -v0), or from A(0) - B(0)
+// when there is none, with the distance estimate set to 1.
 //
 // Precision: the iteration runs in T; the step kernels of both precisions use
 // T = double (an FP32 run is too inaccurate for contact features and was
@@ -41,6 +56,10 @@ struct BodyRef {
   D3 origin;
   double scaling[3];   // crust shrink factors (RigidBodyWithCrust.cpp:60-72)
   double lext[3];      // local bounding-box half extents (Convex::bbox with identity)
+  // polyhedron vertex adjacency (Polyhedron::m_cobound): the neighbours of
+  // vertex i are adj[adj_start[i] .. adj_start[i + 1]); nullptr: arg-max support
+  const int* adj_start = nullptr;
+  const int* adj = nullptr;
 };
 
 template <typename T>
@@ -52,6 +71,9 @@ struct LocalBody {
   V3<T> ext;
   T b[9];   // shrunk basis
   V3<T> o;  // origin in the working frame
+  const int* adj_start = nullptr;  // polyhedron adjacency (see BodyRef)
+  const int* adj = nullptr;
+  mutable int cur = 0;  // the hill climb's current vertex, carried between support calls
 };
 
 template <typename T>
@@ -87,6 +109,34 @@ GG_HD V3<T> support_local(const LocalBody<T>& B, V3<T> v) {
     default: {  // polyhedron
       T n = norm(v);
       if (!(n > T(kEpsilon))) return v3<T>(T(0), T(0), T(0));
+      if (B.adj_start) {
+        // hill climb: move to the first neighbour (other than the vertex just
+        // left) whose v . p is not below the current one by the 1e-16 margin;
+        // every move raises v . p, so at most nverts moves (the bound also
+        // ends the climb when v holds a NaN)
+        int cur = B.cur, last = -1;
+        T h = dot(v3<T>(T(B.verts[3 * cur]), T(B.verts[3 * cur + 1]), T(B.verts[3 * cur + 2])), v);
+        for (int moves = 0; moves < B.nverts; ++moves) {
+          int next = -1;
+          T dn = T(0);
+          for (int k = B.adj_start[cur]; k < B.adj_start[cur + 1]; ++k) {
+            const int c = B.adj[k];
+            if (c == last) continue;
+            const T d = dot(v3<T>(T(B.verts[3 * c]), T(B.verts[3 * c + 1]), T(B.verts[3 * c + 2])), v);
+            if (!(d - h < T(1.e-16))) {
+              next = c;
+              dn = d;
+              break;
+            }
+          }
+          if (next < 0) break;
+          last = cur;
+          cur = next;
+          h = dn;
+        }
+        B.cur = cur;
+        return v3<T>(T(B.verts[3 * cur]), T(B.verts[3 * cur + 1]), T(B.verts[3 * cur + 2]));
+      }
       int best = 0;
       V3<T> p0 = v3<T>(T(B.verts[0]), T(B.verts[1]), T(B.verts[2]));
       T h = dot(p0, v);
@@ -130,7 +180,45 @@ GG_HD LocalBody<T> local_body(const BodyRef& r, D3 shift, const double scale[3])
   for (int i = 0; i < 9; ++i) B.b[i] = T(s.m[i]);
   D3 o = xsub3(r.origin, shift);
   B.o = v3<T>(T(o.x), T(o.y), T(o.z));
+  B.adj_start = r.adj_start;
+  B.adj = r.adj;
+  B.cur = 0;
   return B;
+}
+
+// How a GJK run starts and searches (the options of <CollisionDetection>)
+template <typename T>
+struct GjkStart {
+  bool accel = false;    // Nesterov-accelerated search direction
+  bool history = false;  // warm-started run: distance estimate 1, first direction v0 (when non-zero)
+  V3<T> v0 = {T(0), T(0), T(0)};
+};
+
+// The first iterate of a run: v and the support point w that goes with it,
+// and the distance estimate (Convex.cpp:557-561 plain, :659-668 warm-started).
+template <typename T>
+GG_HD T gjk_first(const LocalBody<T>& A, const LocalBody<T>& B, const GjkStart<T>& st, V3<T>& v, V3<T>& w) {
+  const V3<T> zero = v3<T>(T(0), T(0), T(0));
+  if (st.history && !(st.v0.x == T(0) && st.v0.y == T(0) && st.v0.z == T(0))) {
+    v = st.v0;
+    w = lb_apply(A, support_local(A, lb_vecmat(-v, A))) - lb_apply(B, support_local(B, lb_vecmat(v, B)));
+  } else {
+    v = lb_apply(A, support_local(A, zero)) - lb_apply(B, support_local(B, zero));
+    w = v;
+  }
+  return st.history ? T(1) : norm(v);
+}
+
+// The search direction of iteration k: with acceleration (except every 8th
+// iteration) d = m d + m (1 - m) v + (1 - m)^2 w with m = k / (k + 2), else v.
+template <typename T>
+GG_HD V3<T> gjk_direction(bool accel, int k, V3<T> d, V3<T> v, V3<T> w) {
+  if (accel && k % 8 != 0) {
+    const T m = T(k) / (T(k) + T(2));
+    const T om = T(1) - m;
+    return sc(d, m) + sc(v, m * om) + sc(w, om * om);
+  }
+  return v;
 }
 
 template <typename T>
@@ -244,10 +332,12 @@ struct GjkResult {
   T lower;   // largest support-plane separation dot(v, w) / |v| met: a lower bound of the distance
   int exit;  // 0 optimality gap, 1 degenerate support point, 2 Johnson/backup failed, 3 other (full simplex,
              // distance <= EPSILON2, iteration cap)
+  V3<T> v;   // the last iterate (the direction a warm-started run keeps for the pair)
 };
 
 template <typename T>
-GG_HD GjkResult<T> gjk_distance(const LocalBody<T>& A, const LocalBody<T>& B, T rel_error) {
+GG_HD GjkResult<T> gjk_distance(const LocalBody<T>& A, const LocalBody<T>& B, T rel_error,
+                                const GjkStart<T>& st = GjkStart<T>()) {
   unsigned bits = 0, last = 0, last_bit = 0, all_bits = 0;
   V3<T> p[4], q[4], y[4];
   GjkState<T> g;
@@ -259,9 +349,10 @@ GG_HD GjkResult<T> gjk_distance(const LocalBody<T>& A, const LocalBody<T>& B, T 
     for (int j = 0; j < 4; ++j) g.det[i][j] = T(0);
   const T abs_error = T(1.e-4) * rel_error;
   const V3<T> zero = v3<T>(T(0), T(0), T(0));
-  V3<T> v = lb_apply(A, support_local(A, zero)) - lb_apply(B, support_local(B, zero));
-  V3<T> w = v;
-  T dist = norm(v);
+  V3<T> v, w;
+  T dist = gjk_first(A, B, st, v, w);
+  V3<T> d = v;
+  bool accel = st.accel;
   int num = 0, exit_reason = 3;
   T lower = -dist;
   while (bits < 15 && dist > T(kEpsilon2) && num < 1000) {
@@ -272,15 +363,23 @@ GG_HD GjkResult<T> gjk_distance(const LocalBody<T>& A, const LocalBody<T>& B, T 
       ++last;
       last_bit <<= 1;
     }
-    p[last] = support_local(A, lb_vecmat(-v, A));
-    q[last] = support_local(B, lb_vecmat(v, B));
+    d = gjk_direction(accel, num, d, v, w);
+    p[last] = support_local(A, lb_vecmat(-d, A));
+    q[last] = support_local(B, lb_vecmat(d, B));
     w = lb_apply(A, p[last]) - lb_apply(B, q[last]);
     const T sep = dot(v, w) / dist;
     if (sep > lower) lower = sep;
     T mu = dist - sep;
     if (mu < dist * rel_error || mu < abs_error) {
-      exit_reason = 0;
-      break;
+      if (!accel || norm(d - v) < T(kEpsilon)) {
+        exit_reason = 0;
+        break;
+      }
+      // converged on the accelerated direction only: go on without momentum
+      accel = false;
+      p[last] = support_local(A, lb_vecmat(-v, A));
+      q[last] = support_local(B, lb_vecmat(v, B));
+      w = lb_apply(A, p[last]) - lb_apply(B, q[last]);
     }
     bool degen = false;
     for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
@@ -313,6 +412,7 @@ GG_HD GjkResult<T> gjk_distance(const LocalBody<T>& A, const LocalBody<T>& B, T 
   r.iters = num;
   r.exit = exit_reason;
   r.lower = lower;
+  r.v = v;
   return r;
 }
 
@@ -429,34 +529,44 @@ GG_HD SvPick sv_pick_tetrahedron(const V3<double>* y) {
   return best;
 }
 
-// GJK iteration with the signed-volume sub-algorithm.  The outer loop is the
-// reference's closest_points_GJK_SV (GJK_SV.cpp:428-517, Nesterov acceleration
-// off, its default): start at A(0) - B(0), stop on the optimality gap
+// GJK iteration with the signed-volume sub-algorithm.  The outer loop follows
+// the reference's closest_points_GJK_SV (GJK_SV.cpp:428-631): start at
+// A(0) - B(0) or from a warm-start direction, stop on the optimality gap
 // (relative rel_error or absolute 1e-4 rel_error), on a support point already
 // in the simplex, on a full simplex, at distance <= EPSILON2 or after 1000
-// iterations.
-GG_HD GjkResult<double> gjk_sv_distance(const LocalBody<double>& A, const LocalBody<double>& B, double rel_error) {
+// iterations; the accelerated direction as in gjk_distance.
+GG_HD GjkResult<double> gjk_sv_distance(const LocalBody<double>& A, const LocalBody<double>& B, double rel_error,
+                                        const GjkStart<double>& st = GjkStart<double>()) {
   const V3<double> zero = v3<double>(0., 0., 0.);
   V3<double> y[4], p[4], q[4];
   double lam[4] = {0., 0., 0., 0.};
   for (int i = 0; i < 4; ++i) y[i] = p[i] = q[i] = zero;
   int n = 0;  // vertices in the simplex
   const double abs_error = 1.e-4 * rel_error;
-  V3<double> v = lb_apply(A, support_local(A, zero)) - lb_apply(B, support_local(B, zero));
-  double dist = norm(v);
+  V3<double> v, w;
+  double dist = gjk_first(A, B, st, v, w);
+  V3<double> d = v;
+  bool accel = st.accel;
   int iters = 0, exit_reason = 3;
   double lower = -dist;
   while (n < 4 && dist > kEpsilon2 && iters < 1000) {
     ++iters;
-    const V3<double> pa = support_local(A, lb_vecmat(-v, A));
-    const V3<double> qb = support_local(B, lb_vecmat(v, B));
-    const V3<double> w = lb_apply(A, pa) - lb_apply(B, qb);
+    d = gjk_direction(accel, iters, d, v, w);
+    V3<double> pa = support_local(A, lb_vecmat(-d, A));
+    V3<double> qb = support_local(B, lb_vecmat(d, B));
+    w = lb_apply(A, pa) - lb_apply(B, qb);
     const double sep = dot(v, w) / dist;
     if (sep > lower) lower = sep;
     const double gap = dist - sep;
     if (gap < dist * rel_error || gap < abs_error) {
-      exit_reason = 0;
-      break;
+      if (!accel || norm(d - v) < kEpsilon) {
+        exit_reason = 0;
+        break;
+      }
+      accel = false;
+      pa = support_local(A, lb_vecmat(-v, A));
+      qb = support_local(B, lb_vecmat(v, B));
+      w = lb_apply(A, pa) - lb_apply(B, qb);
     }
     bool repeated = false;
     for (int k = 0; k < n; ++k) repeated = repeated || (y[k].x == w.x && y[k].y == w.y && y[k].z == w.z);
@@ -509,24 +619,32 @@ GG_HD GjkResult<double> gjk_sv_distance(const LocalBody<double>& A, const LocalB
   r.iters = iters;
   r.exit = exit_reason;
   r.lower = lower;
+  r.v = v;
   return r;
 }
 
 // RigidBodyWithCrust::ClosestPoint general case (RigidBodyWithCrust.cpp:278-348).
 // status: 0 = features valid, 1 = ContactError, 2 = bounding spheres apart.
+// With a GjkStart, st->v0 on return holds the run's last iterate (the
+// direction RigidBodyWithCrust::ClosestPoint hands back to the collision
+// history, RigidBodyWithCrust.cpp:362-470), or zero when the bounding spheres
+// are apart (:510-514).
 template <typename T>
 GG_HD ContactGeom convex_closest_point_t(const BodyRef& A, const BodyRef& B, double tol, int* iters,
-                                        int* exit_out = nullptr, double* lower_out = nullptr) {
+                                        int* exit_out = nullptr, double* lower_out = nullptr,
+                                        GjkStart<T>* st = nullptr) {
   ContactGeom c = no_contact();
   D3 g = xsub3(A.origin, B.origin);
   if (!(xnorm(g) < xadd(A.radius, B.radius))) {
     c.status = 2;
+    if (st) st->v0 = v3<T>(T(0), T(0), T(0));
     return c;
   }
   const D3 shift = sizeof(T) == 4 ? A.origin : d3(0., 0., 0.);
   LocalBody<T> la = local_body<T>(A, shift, A.scaling);
   LocalBody<T> lb = local_body<T>(B, shift, B.scaling);
-  GjkResult<T> r = gjk_distance(la, lb, T(tol));
+  GjkResult<T> r = st ? gjk_distance(la, lb, T(tol), *st) : gjk_distance(la, lb, T(tol));
+  if (st) st->v0 = r.v;
   *iters = r.iters;
   if (exit_out) *exit_out = r.exit;
   if (lower_out) *lower_out = double(r.lower);
@@ -549,16 +667,19 @@ GG_HD ContactGeom convex_closest_point_t(const BodyRef& A, const BodyRef& B, dou
 
 // RigidBodyWithCrust::ClosestPoint with the signed-volume GJK (the same
 // features as convex_closest_point_t)
-GG_HD ContactGeom convex_closest_point_sv(const BodyRef& A, const BodyRef& B, double tol, int* iters) {
+GG_HD ContactGeom convex_closest_point_sv(const BodyRef& A, const BodyRef& B, double tol, int* iters,
+                                         GjkStart<double>* st = nullptr) {
   ContactGeom c = no_contact();
   D3 g = xsub3(A.origin, B.origin);
   if (!(xnorm(g) < xadd(A.radius, B.radius))) {
     c.status = 2;
+    if (st) st->v0 = v3<double>(0., 0., 0.);
     return c;
   }
   LocalBody<double> la = local_body<double>(A, d3(0., 0., 0.), A.scaling);
   LocalBody<double> lb = local_body<double>(B, d3(0., 0., 0.), B.scaling);
-  GjkResult<double> r = gjk_sv_distance(la, lb, tol);
+  GjkResult<double> r = st ? gjk_sv_distance(la, lb, tol, *st) : gjk_sv_distance(la, lb, tol);
+  if (st) st->v0 = r.v;
   *iters = r.iters;
   if (r.dist < kEpsilon) {
     c.status = 1;
@@ -581,7 +702,7 @@ GG_HD ContactGeom convex_closest_point_sv(const BodyRef& A, const BodyRef& B, do
 // is imposed with overlap = -(crust sum) along the witness direction B->A.
 // status 1 when even the shrunk bodies touch (fatal ContactError).
 GG_HD ContactGeom convex_error_handling(const BodyRef& A, const BodyRef& B, const double ext_a[3],
-                                        const double ext_b[3], double factor, double tol) {
+                                        const double ext_b[3], double factor, double tol, bool accel = false) {
   double sa[3], sb[3];
   for (int i = 0; i < 3; ++i) {
     sa[i] = ext_a[i] < kEpsilon ? 1. : xdiv(xsub(ext_a[i], xmul(factor, A.crust)), ext_a[i]);
@@ -591,7 +712,9 @@ GG_HD ContactGeom convex_error_handling(const BodyRef& A, const BodyRef& B, cons
   }
   LocalBody<double> la = local_body<double>(A, d3(0., 0., 0.), sa);
   LocalBody<double> lb = local_body<double>(B, d3(0., 0., 0.), sb);
-  GjkResult<double> r = gjk_distance(la, lb, tol);
+  GjkStart<double> st;
+  st.accel = accel;
+  GjkResult<double> r = gjk_distance(la, lb, tol, st);
   ContactGeom c = no_contact();
   if (r.dist < kEpsilon) {
     c.status = 1;

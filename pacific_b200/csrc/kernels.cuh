@@ -484,6 +484,8 @@ __device__ __forceinline__ void make_body_ref(const StepArgs<R>& a, int shape, i
     for (int t = 0; t < 9; ++t) b.basis.m[t] = (t % 4 == 0) ? 1. : 0.;
   }
   b.origin = d3(xr.x, xr.y, xr.z);
+  b.adj_start = sh.type == GRAINS_GPU_POLYHEDRON ? a.adj_start + sh.vert_offset : nullptr;
+  b.adj = a.adj;
   for (int i = 0; i < 3; ++i) b.lext[i] = sh.type == GRAINS_GPU_SPHERE ? xr.w : sh.scaling_ext[i];
   for (int i = 0; i < 3; ++i) b.scaling[i] = b.lext[i] < kEpsilon ? 1. : xdiv(xsub(b.lext[i], crust), b.lext[i]);
 }
@@ -502,6 +504,8 @@ __device__ __forceinline__ void make_obstacle_ref(const StepArgs<R>& a, int oidx
   b.crust = O.crust;
   for (int t = 0; t < 9; ++t) b.basis.m[t] = O.b[t];
   b.origin = d3(O.o[0], O.o[1], O.o[2]);
+  b.adj_start = sh.type == GRAINS_GPU_POLYHEDRON ? a.adj_start + sh.vert_offset : nullptr;
+  b.adj = a.adj;
   for (int i = 0; i < 3; ++i) b.scaling[i] = O.scaling[i];
   for (int i = 0; i < 3; ++i) b.lext[i] = sh.scaling_ext[i];
 }
@@ -513,18 +517,36 @@ __device__ __forceinline__ void make_obstacle_ref(const StepArgs<R>& a, int oidx
 // filter (certified by its support-plane lower bound) it made the drum's
 // force kernel 3x slower than the double GJK alone on B200 (0.67 vs 0.22 ms
 // per step, 100,000 convex bodies).  Error handling (crust x10) on
-// ContactError.
+// ContactError.  st carries the accelerated-direction option and, for a
+// warm-started run, the pair's direction in and out.
 template <typename R, bool SV = false>
 __device__ ContactGeom convex_closest_point(const StepArgs<R>& a, const BodyRef& A, const BodyRef& B, int& iters,
-                                            int& handled) {
+                                            int& handled, GjkStart<double>& st) {
   handled = 0;
-  ContactGeom c = SV ? convex_closest_point_sv(A, B, a.gjk_tol, &iters)
-                     : convex_closest_point_t<double>(A, B, a.gjk_tol, &iters);
+  ContactGeom c = SV ? convex_closest_point_sv(A, B, a.gjk_tol, &iters, &st)
+                     : convex_closest_point_t<double>(A, B, a.gjk_tol, &iters, nullptr, nullptr, &st);
   if (c.status == 1) {
-    c = convex_error_handling(A, B, A.lext, B.lext, 10., a.gjk_tol);
+    c = convex_error_handling(A, B, A.lext, B.lext, 10., a.gjk_tol, st.accel);
     handled = 1;
   }
   return c;
+}
+
+// The collision history of an owned pair in the owner's row of the last
+// evaluation (CollisionHistory::lookupCollision, CollisionHistory.cpp:41-49).
+// The reference also looks the pair up, negated, in the partner's map
+// (Particle.cpp:491-495); here a pair's history always lives with its owner,
+// the lower id, so that second place is never needed.
+template <typename R>
+__device__ __forceinline__ bool find_gjk_dir(const StepArgs<R>& a, int row, int other, V3<double>& v) {
+  const int n = a.gdir_n_prev[row];
+  const GjkDir* g = a.gdir_prev + (size_t)row * a.hist_cap;
+  for (int k = 0; k < n; ++k)
+    if (g[k].other == other) {
+      v = v3<double>(g[k].v[0], g[k].v[1], g[k].v[2]);
+      return true;
+    }
+  return false;
 }
 
 // ---------------------------------------------------------------------------
@@ -862,14 +884,37 @@ __device__ __forceinline__ void pair_one(const StepArgs<R>& a, int4 item, R dt, 
       make_body_ref(a, mi.z, s, mdi.y, ba);
       make_body_ref(a, mj.z, t, mdj.y, bb);
       int it = 0, handled = 0;
-      g = convex_closest_point<R, SV>(a, ba, bb, it, handled);
+      GjkStart<double> st;
+      st.accel = a.gjk_accel != 0;
+      st.history = a.gjk_history != 0;
+      bool known = false;
+      if (st.history) known = find_gjk_dir(a, oi, mj.x, st.v0);
+      const V3<double> v_before = st.v0;
+      g = convex_closest_point<R, SV>(a, ba, bb, it, handled, st);
       if (g.status != 2) {
         ++fs.ngjk;
         fs.ngjk_it += it;
       }
       if (handled) set_status(a.stats, g.status == 1 ? GRAINS_GPU_CONTACT_ERROR : GRAINS_GPU_CONTACT_HANDLED);
       contact = g.status == 0 && g.overlap < 0.;
+      if (st.history && rank < a.hist_cap) {
+        // CollisionHistory::updateCollision / removeCollision (Particle.cpp:
+        // 497-501): the run's last iterate is kept, apart bounding spheres
+        // remove the entry, and a ContactError leaves it as it was
+        GjkDir d;
+        d.other = mj.x;
+        d.pad = 0;
+        const V3<double> keep = handled ? v_before : st.v0;
+        if ((handled && !known) || (keep.x == 0. && keep.y == 0. && keep.z == 0.)) d.other = kNoGjkDir;
+        d.v[0] = keep.x;
+        d.v[1] = keep.y;
+        d.v[2] = keep.z;
+        a.gdir_next[(size_t)oi * a.hist_cap + rank] = d;
+      }
     }
+    if (CONVEX && a.gjk_history && rank < a.hist_cap &&
+        (a.shapes[mi.z].type == GRAINS_GPU_SPHERE && a.shapes[mj.z].type == GRAINS_GPU_SPHERE))
+      a.gdir_next[(size_t)oi * a.hist_cap + rank].other = kNoGjkDir;
     if (!contact) {
       put_no_contact(a, my_slot);
       if (qp >= 0) put_no_contact(a, other_slot);
@@ -943,6 +988,7 @@ __device__ __forceinline__ void pair_one(const StepArgs<R>& a, int4 item, R dt, 
   }
 
   // ---- obstacle candidate (SimpleObstacle::InterAction, SimpleObstacle.cpp:222-270)
+  if (CONVEX && a.gjk_history && rank < a.hist_cap) a.gdir_next[(size_t)oi * a.hist_cap + rank].other = kNoGjkDir;
   const int oidx = -1 - e;
   const ObstacleDev& O = a.obs[oidx];
   const D3 oo = d3(O.o[0], O.o[1], O.o[2]);
@@ -961,7 +1007,9 @@ __device__ __forceinline__ void pair_one(const StepArgs<R>& a, int4 item, R dt, 
     make_body_ref(a, mi.z, s, mdi.y, ba);
     make_obstacle_ref(a, oidx, bb);
     int it = 0, handled = 0;
-    g = convex_closest_point<R, SV>(a, ba, bb, it, handled);
+    GjkStart<double> st;  // no collision history for obstacles (SimpleObstacle.cpp:222-250)
+    st.accel = a.gjk_accel != 0;
+    g = convex_closest_point<R, SV>(a, ba, bb, it, handled, st);
     if (g.status != 2) {
       ++fs.ngjk;
       fs.ngjk_it += it;
@@ -1093,6 +1141,7 @@ __device__ __forceinline__ void sum_one(const StepArgs<R>& a, int s) {
   }
   a.coord[s] = ncontact;
   a.hist_n_next[row] = kept;
+  if (a.gjk_history) a.gdir_n_next[row] = owned < a.hist_cap ? owned : a.hist_cap;
   P.F[s] = st3<R>(F);
   P.T[s] = st3<R>(T);
 }
@@ -1673,6 +1722,12 @@ __global__ void __launch_bounds__(kPersistentThreads) persistent_steps_kernel(
       int* hn = a.hist_n_prev;
       a.hist_n_prev = a.hist_n_next;
       a.hist_n_next = hn;
+      GjkDir* gd = a.gdir_prev;
+      a.gdir_prev = a.gdir_next;
+      a.gdir_next = gd;
+      int* gn = a.gdir_n_prev;
+      a.gdir_n_prev = a.gdir_n_next;
+      a.gdir_n_next = gn;
     }
     if (!grid_barrier(bar, status, a.barrier_polls)) return;
     for (int s = tid; s < n; s += nthreads)

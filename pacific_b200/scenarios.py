@@ -451,6 +451,9 @@ def apply(sim, sc):
     ids = [sim.add_shape(t, prm) for t, prm in sc.shapes]
     if sc.meta.get("collision") is not None:
         sim.set_collision_algorithm(sc.meta["collision"])
+    if sc.meta.get("collision_options"):
+        # <CollisionDetection Tolerance Acceleration History>
+        sim.set_collision_options(**sc.meta["collision_options"])
     for s, d in enumerate(sc.domains):
         sim.set_domain(s, d["origin"], d["size"], d["cell_size"], d["gravity"])
         for a, b, law, prm in sc.laws[s]:

@@ -3,16 +3,11 @@ the reference Grains3D built from its sources, tests/golden/make_golden.py).
 Pair sets and coordination exact; plain FP64 forces within 1e-12 relative,
 mixed precision within 1e-5 (force floor: the particle weight).
 
-Fixtures with polyhedra are the exception.  The reference's Polyhedron::support
-hill-climbs from a warm-start vertex that each body keeps between GJK calls
-(Polyhedron.cpp:265-293) and stops unless a neighbour gains more than 1e-16, so
-on flat-face contacts, where the face vertices tie within that margin, its
-witness points (hence the contact point) depend on the order of all earlier
-GJK calls of the body.  The CUDA path evaluates pairs in parallel and uses the
-order-independent arg-max.  For those fixtures the CUDA path is held to the
-oracle run with the same arg-max support at the usual bars, and to the
-reference at the level that contact-point choice explains (pair sets and
-coordination still exact)."""
+Polyhedra included: the reference's Polyhedron::support hill-climbs the vertex
+adjacency from a vertex each body keeps between GJK calls (Polyhedron.cpp:
+265-293); the CUDA path climbs the same way but starts every GJK run at vertex
+0, which gives the reference's contacts on every fixture.  Per-contact forces
+are compared with the oracle run with that same rule."""
 import glob
 import os
 import sys
@@ -32,10 +27,6 @@ CASES = sorted(c for c in glob.glob(os.path.join(HERE, "golden", "*.npz"))
                if not os.path.basename(c).startswith("io_") and not c.endswith("_stats.npz"))
 
 
-def has_polyhedra(sc):
-    return any(sh[0] == 3 for sh in sc.shapes)
-
-
 def convex(sc):
     return any(sc.shapes[k][0] != 0 for k in set(np.asarray(sc.particles["shape"]).tolist()))
 
@@ -46,7 +37,6 @@ def test_gpu_matches_reference_fixture(oracle_lib, gpu_lib, path, precision):
     import golden_io as G
     z = np.load(path)
     sc = G.scenario_from_npz(z)
-    poly = has_polyhedra(sc)
     sim = make(gpu_lib, sc, precision)
     sim.upload_contact_memory(G.memory_from(z, "mem_in_"))
     t = float(z["time"])
@@ -78,17 +68,11 @@ def test_gpu_matches_reference_fixture(oracle_lib, gpu_lib, path, precision):
         ttol = 1e-4
         ptol = 1e-11
     o = make(oracle_lib, sc)
-    o.set_polyhedron_support(True)
+    o.set_polyhedron_support(2)
     o.upload_contact_memory(G.memory_from(z, "mem_in_"))
     o.compute_forces(t, sc.dt)
-    if poly:
-        # the reference's order-dependent support choice on flat faces
-        assert rel_err(d["force"], z["force"], weight) < 2e-3
-        ref_force, ref_torque = o.download()["force"], o.download()["torque"]
-    else:
-        ref_force, ref_torque = z["force"], z["torque"]
-    assert rel_err(d["force"], ref_force, weight) < tol
-    assert rel_err(d["torque"], ref_torque, weight * 1e-3) < ttol
+    assert rel_err(d["force"], z["force"], weight) < tol
+    assert rel_err(d["torque"], z["torque"], weight * 1e-3) < ttol
     # every particle-particle contact force
     pg, fg = sim.contact_forces()
     po, fo = o.contact_forces()
@@ -103,12 +87,7 @@ def test_gpu_matches_reference_fixture(oracle_lib, gpu_lib, path, precision):
     steps = int(z["after_steps"])
     sim.step(steps, t, sc.dt)
     d = sim.download()
-    if poly:
-        o.step(steps, t, sc.dt)
-        after = o.download()["position"]
-    else:
-        after = z["after_position"]
-    assert np.max(np.abs(d["position"] - after)) < ptol
+    assert np.max(np.abs(d["position"] - z["after_position"])) < ptol
     if "after_obstacles" in z.files:
         # imposed obstacle motions: poses (basis, centre) after the steps; the
         # device's sin / cos may differ from the host's in the last bit

@@ -93,24 +93,32 @@ def test_fixtures_exercise_the_path():
 
 
 @pytest.mark.parametrize("path", CASES, ids=[os.path.basename(c)[:-4] for c in CASES])
-def test_stateless_polyhedron_support_differs_only_on_polyhedra(oracle_lib, path):
-    """The CUDA path's polyhedron support is the order-independent arg-max; the
-    reference hill-climbs from a warm-start vertex kept per body.  Run with the
-    arg-max, the oracle still gives the reference's pair sets and coordination
-    everywhere, its exact forces on fixtures without polyhedra, and forces
-    within 2e-3 (floor: the weight) where flat polyhedron faces touch."""
+def test_polyhedron_support_rules(oracle_lib, path):
+    """Polyhedron::support (Polyhedron.cpp:265-293) hill-climbs from a vertex
+    each body keeps between calls.  The CUDA path's rule, a climb that every
+    GJK run starts at vertex 0 (oracle mode 2), gives the reference's forces
+    and the positions after the fixture's steps exactly on every fixture; the
+    order-independent arg-max (mode 1) does so only without polyhedra, and
+    stays within 2e-3 of the weight-floored force where flat polyhedron faces
+    touch."""
     G, z, sc = load(path)
-    sim = make(oracle_lib, sc)
-    sim.set_polyhedron_support(True)
-    sim.upload_contact_memory(G.memory_from(z, "mem_in_"))
-    sim.compute_forces(float(z["time"]), sc.dt)
-    d = sim.download()
+    poly = any(sh[0] == 3 for sh in sc.shapes)
     weight = float(np.min(sc.particles["mass"])) * 9.81
-    assert np.array_equal(d["coordination"], z["coordination"])
-    if bool(z["has_contact_pairs"]):
-        assert pair_set(sim.contact_pairs()) == pair_set(z["contact_pairs"])
-    err = rel_err(d["force"], z["force"], weight)
-    if any(sh[0] == 3 for sh in sc.shapes):
-        assert 0 < err < 2e-3
-    else:
-        assert err < 1e-13
+    for mode in (2, 1):
+        sim = make(oracle_lib, sc)
+        sim.set_polyhedron_support(mode)
+        sim.upload_contact_memory(G.memory_from(z, "mem_in_"))
+        t = float(z["time"])
+        sim.compute_forces(t, sc.dt)
+        d = sim.download()
+        assert np.array_equal(d["coordination"], z["coordination"])
+        if bool(z["has_contact_pairs"]):
+            assert pair_set(sim.contact_pairs()) == pair_set(z["contact_pairs"])
+        err = rel_err(d["force"], z["force"], weight)
+        if mode == 2 or not poly:
+            assert err < 1e-13
+            sim.step(int(z["after_steps"]), t, sc.dt)
+            assert np.max(np.abs(sim.download()["position"] - z["after_position"])) < 1e-13
+        else:
+            assert 0 < err < 2e-3
+        sim.close()

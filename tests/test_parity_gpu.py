@@ -34,10 +34,11 @@ def evolved(oracle_lib, n=343, seed=1, steps=20, sigma=0.05):
 
 
 def both(oracle_lib, gpu_lib, sc, mem=None, precision=FP64):
-    """The oracle (with the CUDA path's order-independent polyhedron support)
-    and the CUDA path on the same scenario."""
+    """The oracle (with the CUDA path's polyhedron support rule: a hill climb
+    that every GJK run starts at vertex 0) and the CUDA path on the same
+    scenario."""
     o = make(oracle_lib, sc)
-    o.set_polyhedron_support(True)
+    o.set_polyhedron_support(2)
     g = make(gpu_lib, sc, precision)
     if mem is not None:
         o.upload_contact_memory(mem)
@@ -248,7 +249,7 @@ def test_drum_contacts_match_oracle(oracle_lib, gpu_lib, precision):
     1e-12, mixed within 1e-5 of the weight-floored force."""
     sc = small_drum()
     o = make(oracle_lib, sc)
-    o.set_polyhedron_support(True)
+    o.set_polyhedron_support(2)
     o.initialize_leapfrog(0.0, sc.dt)
     t = o.step(1500, 0.0, sc.dt)
     st = o.download()
