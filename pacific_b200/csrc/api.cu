@@ -119,6 +119,8 @@ struct grains_gpu_ctx {
   void* res_t = nullptr;
   int4* work = nullptr;   // owned list entries of an evaluation
   int* work_n = nullptr;
+  GjkOut* gjk_out = nullptr;  // per work item: the GJK kernel's narrowphase result (convex scenarios)
+  int* gjk_next = nullptr;    // the GJK kernel's work-item counter
   int clist_cap = 0;
   int64_t clist_alloc = 0;
   int* pairs = nullptr;  // contact pairs of the last compute_forces (diagnostic)
@@ -574,6 +576,9 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   a.res_t = (typename Vec4<R>::type*)c->res_t;
   a.work = c->work;
   a.work_n = c->work_n;
+  // the signed-volume GJK keeps its runs in the pair kernel
+  a.gjk_out = c->gjk_sv ? nullptr : c->gjk_out;
+  a.gjk_next = c->gjk_next;
   a.pairs = c->pairs;
   a.pairs_cap = c->pairs_cap;
   a.pairs_n = c->pairs_n;
@@ -764,8 +769,8 @@ int last_step(grains_gpu_ctx* c, double dt) {
 // result of each entry (two R4) and the work items; grown, never shrunk.
 int ensure_lists(grains_gpu_ctx* c, int cap_per) {
   const int64_t need = (int64_t)c->cap * cap_per;
-  if (need > c->clist_alloc) {
-    for (void** p : {(void**)&c->clist, &c->res_f, &c->res_t, (void**)&c->work})
+  if (need > c->clist_alloc || (c->has_convex && !c->gjk_out)) {
+    for (void** p : {(void**)&c->clist, &c->res_f, &c->res_t, (void**)&c->work, (void**)&c->gjk_out})
       if (*p) {
         cudaFree(*p);
         *p = nullptr;
@@ -781,6 +786,10 @@ int ensure_lists(grains_gpu_ctx* c, int cap_per) {
     c->res_t = q;
     CK(cudaMalloc(&q, (size_t)need * sizeof(int4)));
     c->work = (int4*)q;
+    if (c->has_convex) {  // one narrowphase result per possible work item
+      CK(cudaMalloc(&q, (size_t)need * sizeof(GjkOut)));
+      c->gjk_out = (GjkOut*)q;
+    }
     c->clist_alloc = need;
     for (int k = 0; k < 4; ++k)  // graphs hold the old pointers
       if (c->graph[k]) {
@@ -878,8 +887,9 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
     c->pair_sys = dalloc<int>((size_t)c->pairs_cap, c->pool);
     c->clock = dalloc<double>(1, c->pool);
     c->work_n = dalloc<int>(1, c->pool);
+    c->gjk_next = dalloc<int>(1, c->pool);
     ok = c->coord && c->perm && c->stats && c->pairs && c->pairs_n && c->pair_force && c->pair_sys && c->clock &&
-         c->work_n;
+         c->work_n && c->gjk_next;
   }
   if (!ok) {
     c->err = "cudaMalloc failed for the requested capacity";
@@ -890,6 +900,7 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
   cudaMemsetAsync(c->perm, 0, N * sizeof(int), c->stream);
   cudaMemsetAsync(c->stats, 0, sizeof(StatsDev), c->stream);
   cudaMemsetAsync(c->work_n, 0, sizeof(int), c->stream);
+  cudaMemsetAsync(c->gjk_next, 0, sizeof(int), c->stream);
   cudaStreamSynchronize(c->stream);
   *out = c;
   return 0;
@@ -905,7 +916,7 @@ int grains_gpu_destroy(grains_gpu_ctx* c) {
   for (int k = 0; k < 2; ++k)
     if (c->buf[k].basis) cudaFree(c->buf[k].basis);
   if (c->stage) cudaFree(c->stage);
-  for (void* p : {(void*)c->clist, (void*)c->ccount, c->res_f, c->res_t, (void*)c->work})
+  for (void* p : {(void*)c->clist, (void*)c->ccount, c->res_f, c->res_t, (void*)c->work, (void*)c->gjk_out})
     if (p) cudaFree(p);
   if (c->pbar) cudaFree(c->pbar);
   if (c->psums) cudaFree(c->psums);

@@ -54,6 +54,18 @@ struct GjkDir {
 };
 constexpr int kNoGjkDir = -2147483647 - 1;
 
+// The narrowphase result of one work item from the GJK kernel (the features of
+// RigidBodyWithCrust::ClosestPoint): contact point, overlap vector, overlap
+// distance; status 0 features, 1 ContactError even after the crust-x10 retry,
+// 2 bounding spheres apart; handled = the retry was used.
+struct GjkOut {
+  double point[3];
+  double ov[3];
+  double overlap;
+  int status;
+  int handled;
+};
+
 struct ShapeDev {
   int type;
   int nverts;
@@ -200,6 +212,8 @@ struct StepArgs {
   int gjk_sv;            // the signed-volume GJK for non-spherical pairs
   int gjk_accel;         // Nesterov-accelerated GJK directions (<CollisionDetection Acceleration="ON">)
   int gjk_history;       // warm-started GJK from the pair's collision history (History="ON")
+  GjkOut* gjk_out;       // per work item: the GJK kernel's narrowphase result (null: GJK inline in the pair kernel)
+  int* gjk_next;         // the GJK kernel's work-item counter (cleared by the sums kernel)
   GjkDir* gdir_prev;     // collision histories of the last evaluation (rows of hist_cap slots by memory row)
   int* gdir_n_prev;
   GjkDir* gdir_next;     // written by this evaluation

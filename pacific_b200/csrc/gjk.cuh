@@ -221,43 +221,78 @@ GG_HD V3<T> gjk_direction(bool accel, int k, V3<T> d, V3<T> v, V3<T> w) {
   return v;
 }
 
+// The arrays of a Johnson GJK run, as a view of kGjkWords numbers `stride`
+// apart: the sub-determinants of every subset s of the 4-point simplex for
+// each of its points i (32 values, packed by subset: the entries of s start at
+// the number of point slots of the subsets below it), the dot products of the
+// simplex points (16), the points of A - B, and the support points of A and B
+// in their local frames (3 x 4 x 3).  A run on its own keeps them in a local
+// array (stride 1); the GJK kernel keeps those of its 64 threads interleaved
+// in shared memory (stride 64), so that a warp's accesses fall in distinct
+// banks.
+constexpr int kGjkWords = 32 + 16 + 36;
 template <typename T>
 struct GjkState {
-  T det[16][4];
-  T dp[4][4];
+  T* base;
+  int stride;
+  GG_HD static int at(unsigned s, unsigned i) {
+    // sum of the sizes of the subsets 0 .. s-1, bytes of two constants
+    const unsigned long long lo = 0x0907050402010000ull, hi = 0x1C191614110F0D0Cull;
+    const unsigned start = unsigned((s < 8 ? lo >> (8 * s) : hi >> (8 * (s - 8))) & 0xffu);
+#if defined(__CUDA_ARCH__)
+    return int(start + __popc(s & ((1u << i) - 1u)));
+#else
+    return int(start + __builtin_popcount(s & ((1u << i) - 1u)));
+#endif
+  }
+  GG_HD T& det(unsigned s, unsigned i) const { return base[at(s, i) * stride]; }
+  GG_HD T& dp(unsigned i, unsigned j) const { return base[(32 + 4 * i + j) * stride]; }
+  GG_HD V3<T> vec(int k) const {  // k: 0-3 y, 4-7 p, 8-11 q
+    const T* b = base + (48 + 3 * k) * stride;
+    return v3<T>(b[0], b[stride], b[2 * stride]);
+  }
+  GG_HD void set_vec(int k, V3<T> v) const {
+    T* b = base + (48 + 3 * k) * stride;
+    b[0] = v.x;
+    b[stride] = v.y;
+    b[2 * stride] = v.z;
+  }
+  GG_HD V3<T> y(unsigned i) const { return vec(int(i)); }
+  GG_HD V3<T> p(unsigned i) const { return vec(4 + int(i)); }
+  GG_HD V3<T> q(unsigned i) const { return vec(8 + int(i)); }
 };
 
 template <typename T>
-GG_HD void gjk_det(unsigned bits, unsigned last, unsigned last_bit, unsigned all_bits, const V3<T> y[4],
-                   GjkState<T>& g) {
+GG_HD void gjk_det(unsigned bits, unsigned last, unsigned last_bit, unsigned all_bits, const GjkState<T>& g) {
+  const V3<T> yl = g.y(last);
   for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
-    if (bits & bit) g.dp[i][last] = g.dp[last][i] = dot(y[i], y[last]);
-  g.dp[last][last] = dot(y[last], y[last]);
-  g.det[last_bit][last] = T(1);
+    if (bits & bit) g.dp(i, last) = g.dp(last, i) = dot(g.y(i), yl);
+  g.dp(last, last) = dot(yl, yl);
+  g.det(last_bit, last) = T(1);
   for (unsigned j = 0, sj = 1; j < 4; ++j, sj <<= 1) {
     if (!(bits & sj)) continue;
     unsigned s2 = sj | last_bit;
-    g.det[s2][j] = g.dp[last][last] - g.dp[last][j];
-    g.det[s2][last] = g.dp[j][j] - g.dp[j][last];
+    g.det(s2, j) = g.dp(last, last) - g.dp(last, j);
+    g.det(s2, last) = g.dp(j, j) - g.dp(j, last);
     for (unsigned k = 0, sk = 1; k < j; ++k, sk <<= 1) {
       if (!(bits & sk)) continue;
       unsigned s3 = sk | s2;
-      g.det[s3][k] = g.det[s2][j] * (g.dp[j][j] - g.dp[j][k]) + g.det[s2][last] * (g.dp[last][j] - g.dp[last][k]);
-      g.det[s3][j] = g.det[sk | last_bit][k] * (g.dp[k][k] - g.dp[k][j]) +
-                     g.det[sk | last_bit][last] * (g.dp[last][k] - g.dp[last][j]);
-      g.det[s3][last] = g.det[sk | sj][k] * (g.dp[k][k] - g.dp[k][last]) +
-                        g.det[sk | sj][j] * (g.dp[j][k] - g.dp[j][last]);
+      g.det(s3, k) = g.det(s2, j) * (g.dp(j, j) - g.dp(j, k)) + g.det(s2, last) * (g.dp(last, j) - g.dp(last, k));
+      g.det(s3, j) = g.det(sk | last_bit, k) * (g.dp(k, k) - g.dp(k, j)) +
+                     g.det(sk | last_bit, last) * (g.dp(last, k) - g.dp(last, j));
+      g.det(s3, last) = g.det(sk | sj, k) * (g.dp(k, k) - g.dp(k, last)) +
+                        g.det(sk | sj, j) * (g.dp(j, k) - g.dp(j, last));
     }
   }
   if (all_bits == 15) {
-    g.det[15][0] = g.det[14][1] * (g.dp[1][1] - g.dp[1][0]) + g.det[14][2] * (g.dp[2][1] - g.dp[2][0]) +
-                   g.det[14][3] * (g.dp[3][1] - g.dp[3][0]);
-    g.det[15][1] = g.det[13][0] * (g.dp[0][0] - g.dp[0][1]) + g.det[13][2] * (g.dp[2][0] - g.dp[2][1]) +
-                   g.det[13][3] * (g.dp[3][0] - g.dp[3][1]);
-    g.det[15][2] = g.det[11][0] * (g.dp[0][0] - g.dp[0][2]) + g.det[11][1] * (g.dp[1][0] - g.dp[1][2]) +
-                   g.det[11][3] * (g.dp[3][0] - g.dp[3][2]);
-    g.det[15][3] = g.det[7][0] * (g.dp[0][0] - g.dp[0][3]) + g.det[7][1] * (g.dp[1][0] - g.dp[1][3]) +
-                   g.det[7][2] * (g.dp[2][0] - g.dp[2][3]);
+    g.det(15, 0) = g.det(14, 1) * (g.dp(1, 1) - g.dp(1, 0)) + g.det(14, 2) * (g.dp(2, 1) - g.dp(2, 0)) +
+                   g.det(14, 3) * (g.dp(3, 1) - g.dp(3, 0));
+    g.det(15, 1) = g.det(13, 0) * (g.dp(0, 0) - g.dp(0, 1)) + g.det(13, 2) * (g.dp(2, 0) - g.dp(2, 1)) +
+                   g.det(13, 3) * (g.dp(3, 0) - g.dp(3, 1));
+    g.det(15, 2) = g.det(11, 0) * (g.dp(0, 0) - g.dp(0, 2)) + g.det(11, 1) * (g.dp(1, 0) - g.dp(1, 2)) +
+                   g.det(11, 3) * (g.dp(3, 0) - g.dp(3, 2));
+    g.det(15, 3) = g.det(7, 0) * (g.dp(0, 0) - g.dp(0, 3)) + g.det(7, 1) * (g.dp(1, 0) - g.dp(1, 3)) +
+                   g.det(7, 2) * (g.dp(2, 0) - g.dp(2, 3));
   }
 }
 
@@ -266,8 +301,8 @@ GG_HD bool gjk_valid(unsigned s, unsigned all_bits, const GjkState<T>& g) {
   for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1) {
     if (!(all_bits & bit)) continue;
     if (s & bit) {
-      if (g.det[s][i] <= T(kEpsilon3)) return false;
-    } else if (g.det[s | bit][i] > T(0)) {
+      if (g.det(s, i) <= T(kEpsilon3)) return false;
+    } else if (g.det(s | bit, i) > T(0)) {
       return false;
     }
   }
@@ -275,13 +310,13 @@ GG_HD bool gjk_valid(unsigned s, unsigned all_bits, const GjkState<T>& g) {
 }
 
 template <typename T>
-GG_HD V3<T> gjk_vector(unsigned bits, const V3<T> y[4], const GjkState<T>& g) {
+GG_HD V3<T> gjk_vector(unsigned bits, const GjkState<T>& g) {
   T sum = T(0);
   V3<T> v = v3<T>(T(0), T(0), T(0));
   for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
     if (bits & bit) {
-      sum += g.det[bits][i];
-      v = v + sc(y[i], g.det[bits][i]);
+      sum += g.det(bits, i);
+      v = v + sc(g.y(i), g.det(bits, i));
     }
   return sc(v, T(1) / sum);
 }
@@ -289,30 +324,30 @@ GG_HD V3<T> gjk_vector(unsigned bits, const V3<T> y[4], const GjkState<T>& g) {
 template <typename T>
 GG_HD bool gjk_proper(unsigned s, const GjkState<T>& g) {
   for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
-    if ((s & bit) && g.det[s][i] <= T(kEpsilon3)) return false;
+    if ((s & bit) && g.det(s, i) <= T(kEpsilon3)) return false;
   return true;
 }
 
 template <typename T>
-GG_HD bool gjk_closest(unsigned& bits, unsigned last, unsigned last_bit, unsigned all_bits, const V3<T> y[4],
-                       GjkState<T>& g, V3<T>& v) {
-  gjk_det(bits, last, last_bit, all_bits, y, g);
+GG_HD bool gjk_closest(unsigned& bits, unsigned last, unsigned last_bit, unsigned all_bits, const GjkState<T>& g,
+                       V3<T>& v) {
+  gjk_det(bits, last, last_bit, all_bits, g);
   for (unsigned s = bits; s; --s) {
     if ((s & bits) == s && gjk_valid(s | last_bit, all_bits, g)) {
       bits = s | last_bit;
-      v = gjk_vector(bits, y, g);
+      v = gjk_vector(bits, g);
       return true;
     }
   }
   if (gjk_valid(last_bit, all_bits, g)) {
     bits = last_bit;
-    v = y[last];
+    v = g.y(last);
     return true;
   }
   T best = T(INFINITY);
   for (unsigned s = all_bits; s; --s) {  // backup procedure
     if ((s & all_bits) == s && gjk_proper(s, g)) {
-      V3<T> u = gjk_vector(s, y, g);
+      V3<T> u = gjk_vector(s, g);
       T d2 = norm2(u);
       if (d2 < best) {
         best = d2;
@@ -335,85 +370,125 @@ struct GjkResult {
   V3<T> v;   // the last iterate (the direction a warm-started run keeps for the pair)
 };
 
+// The Johnson GJK run as a resumable state: gjk_begin sets up the first
+// iterate, gjk_iterate performs one pass of the loop of closest_points
+// (Convex.cpp:563-618) and says whether the run has ended, gjk_end forms the
+// witness points.  gjk_distance strings them together; the lane-persistent GJK
+// kernel interleaves the passes of different pairs on one thread.
+template <typename T>
+struct GjkRun {
+  unsigned bits, last, last_bit, all_bits;
+  GjkState<T> g;  // the run's arrays (the caller's storage)
+  V3<T> v, w, d;
+  T dist, lower, rel_error, abs_error;
+  int num, exit_reason;
+  bool accel;
+};
+
+template <typename T>
+GG_HD void gjk_begin(GjkRun<T>& r, const LocalBody<T>& A, const LocalBody<T>& B, T rel_error,
+                     const GjkStart<T>& st) {
+  r.bits = r.last = r.last_bit = r.all_bits = 0;
+  for (int i = 0; i < kGjkWords; ++i) r.g.base[i * r.g.stride] = T(0);
+  r.rel_error = rel_error;
+  r.abs_error = T(1.e-4) * rel_error;
+  r.dist = gjk_first(A, B, st, r.v, r.w);
+  r.d = r.v;
+  r.accel = st.accel;
+  r.num = 0;
+  r.exit_reason = 3;
+  r.lower = -r.dist;
+}
+
+// one pass of the loop; true when the run has ended
+template <typename T>
+GG_HD bool gjk_iterate(GjkRun<T>& r, const LocalBody<T>& A, const LocalBody<T>& B) {
+  if (!(r.bits < 15 && r.dist > T(kEpsilon2) && r.num < 1000)) return true;
+  ++r.num;
+  r.last = 0;
+  r.last_bit = 1;
+  while (r.bits & r.last_bit) {
+    ++r.last;
+    r.last_bit <<= 1;
+  }
+  const unsigned last = r.last;
+  r.d = gjk_direction(r.accel, r.num, r.d, r.v, r.w);
+  V3<T> pl = support_local(A, lb_vecmat(-r.d, A));
+  V3<T> ql = support_local(B, lb_vecmat(r.d, B));
+  r.w = lb_apply(A, pl) - lb_apply(B, ql);
+  const T sep = dot(r.v, r.w) / r.dist;
+  if (sep > r.lower) r.lower = sep;
+  T mu = r.dist - sep;
+  if (mu < r.dist * r.rel_error || mu < r.abs_error) {
+    if (!r.accel || norm(r.d - r.v) < T(kEpsilon)) {
+      r.g.set_vec(4 + int(last), pl);
+      r.g.set_vec(8 + int(last), ql);
+      r.exit_reason = 0;
+      return true;
+    }
+    // converged on the accelerated direction only: go on without momentum
+    r.accel = false;
+    pl = support_local(A, lb_vecmat(-r.v, A));
+    ql = support_local(B, lb_vecmat(r.v, B));
+    r.w = lb_apply(A, pl) - lb_apply(B, ql);
+  }
+  r.g.set_vec(4 + int(last), pl);
+  r.g.set_vec(8 + int(last), ql);
+  bool degen = false;
+  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+    if (r.all_bits & bit) {
+      const V3<T> yi = r.g.y(i);
+      if (yi.x == r.w.x && yi.y == r.w.y && yi.z == r.w.z) degen = true;
+    }
+  if (degen) {
+    r.exit_reason = 1;
+    return true;
+  }
+  r.g.set_vec(int(last), r.w);
+  r.all_bits = r.bits | r.last_bit;
+  if (!gjk_closest(r.bits, last, r.last_bit, r.all_bits, r.g, r.v)) {
+    r.exit_reason = 2;
+    return true;
+  }
+  r.dist = norm(r.v);
+  return false;
+}
+
+template <typename T>
+GG_HD GjkResult<T> gjk_end(const GjkRun<T>& r, const LocalBody<T>& A, const LocalBody<T>& B) {
+  GjkResult<T> out;
+  T sum = T(0);
+  const V3<T> zero = v3<T>(T(0), T(0), T(0));
+  V3<T> pa = zero, pb = zero;
+  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
+    if (r.bits & bit) {
+      const T di = r.g.det(r.bits, i);
+      sum += di;
+      pa = pa + sc(r.g.p(i), di);
+      pb = pb + sc(r.g.q(i), di);
+    }
+  T s = T(1) / sum;
+  out.pa = lb_apply(A, sc(pa, s));
+  out.pb = lb_apply(B, sc(pb, s));
+  out.dist = r.dist;
+  out.iters = r.num;
+  out.exit = r.exit_reason;
+  out.lower = r.lower;
+  out.v = r.v;
+  return out;
+}
+
 template <typename T>
 GG_HD GjkResult<T> gjk_distance(const LocalBody<T>& A, const LocalBody<T>& B, T rel_error,
                                 const GjkStart<T>& st = GjkStart<T>()) {
-  unsigned bits = 0, last = 0, last_bit = 0, all_bits = 0;
-  V3<T> p[4], q[4], y[4];
-  GjkState<T> g;
-  for (int i = 0; i < 4; ++i) {
-    p[i] = q[i] = y[i] = v3<T>(T(0), T(0), T(0));
-    for (int j = 0; j < 4; ++j) g.dp[i][j] = T(0);
+  T words[kGjkWords];
+  GjkRun<T> r;
+  r.g.base = words;
+  r.g.stride = 1;
+  gjk_begin(r, A, B, rel_error, st);
+  while (!gjk_iterate(r, A, B)) {
   }
-  for (int i = 0; i < 16; ++i)
-    for (int j = 0; j < 4; ++j) g.det[i][j] = T(0);
-  const T abs_error = T(1.e-4) * rel_error;
-  const V3<T> zero = v3<T>(T(0), T(0), T(0));
-  V3<T> v, w;
-  T dist = gjk_first(A, B, st, v, w);
-  V3<T> d = v;
-  bool accel = st.accel;
-  int num = 0, exit_reason = 3;
-  T lower = -dist;
-  while (bits < 15 && dist > T(kEpsilon2) && num < 1000) {
-    ++num;
-    last = 0;
-    last_bit = 1;
-    while (bits & last_bit) {
-      ++last;
-      last_bit <<= 1;
-    }
-    d = gjk_direction(accel, num, d, v, w);
-    p[last] = support_local(A, lb_vecmat(-d, A));
-    q[last] = support_local(B, lb_vecmat(d, B));
-    w = lb_apply(A, p[last]) - lb_apply(B, q[last]);
-    const T sep = dot(v, w) / dist;
-    if (sep > lower) lower = sep;
-    T mu = dist - sep;
-    if (mu < dist * rel_error || mu < abs_error) {
-      if (!accel || norm(d - v) < T(kEpsilon)) {
-        exit_reason = 0;
-        break;
-      }
-      // converged on the accelerated direction only: go on without momentum
-      accel = false;
-      p[last] = support_local(A, lb_vecmat(-v, A));
-      q[last] = support_local(B, lb_vecmat(v, B));
-      w = lb_apply(A, p[last]) - lb_apply(B, q[last]);
-    }
-    bool degen = false;
-    for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
-      if ((all_bits & bit) && y[i].x == w.x && y[i].y == w.y && y[i].z == w.z) degen = true;
-    if (degen) {
-      exit_reason = 1;
-      break;
-    }
-    y[last] = w;
-    all_bits = bits | last_bit;
-    if (!gjk_closest(bits, last, last_bit, all_bits, y, g, v)) {
-      exit_reason = 2;
-      break;
-    }
-    dist = norm(v);
-  }
-  GjkResult<T> r;
-  T sum = T(0);
-  V3<T> pa = zero, pb = zero;
-  for (unsigned i = 0, bit = 1; i < 4; ++i, bit <<= 1)
-    if (bits & bit) {
-      sum += g.det[bits][i];
-      pa = pa + sc(p[i], g.det[bits][i]);
-      pb = pb + sc(q[i], g.det[bits][i]);
-    }
-  T s = T(1) / sum;
-  r.pa = lb_apply(A, sc(pa, s));
-  r.pb = lb_apply(B, sc(pb, s));
-  r.dist = dist;
-  r.iters = num;
-  r.exit = exit_reason;
-  r.lower = lower;
-  r.v = v;
-  return r;
+  return gjk_end(r, A, B);
 }
 
 // ---- the signed-volume GJK ------------------------------------------------------
@@ -623,6 +698,29 @@ GG_HD GjkResult<double> gjk_sv_distance(const LocalBody<double>& A, const LocalB
   return r;
 }
 
+// The contact features of a finished distance run (RigidBodyWithCrust.cpp:
+// 314-348): status 1 (ContactError) when the crust-shrunk bodies touch, else
+// the contact point midway between the witness points, the overlap vector
+// along B -> A, and the overlap distance - crust_a - crust_b.
+template <typename T>
+GG_HD ContactGeom gjk_features(const GjkResult<T>& r, double crust_sum, D3 shift) {
+  ContactGeom c = no_contact();
+  double distance = double(r.dist);
+  if (distance < kEpsilon) {
+    c.status = 1;
+    return c;
+  }
+  V3<T> ba = r.pa - r.pb;
+  V3<T> pc = dv(r.pa, T(2)) + dv(r.pb, T(2));
+  V3<T> ov = round3(dv(ba, r.dist));
+  ov = sc(ov, T(crust_sum) - r.dist);
+  c.point = xadd3(d3(double(pc.x), double(pc.y), double(pc.z)), shift);
+  c.overlap_vector = d3(double(ov.x), double(ov.y), double(ov.z));
+  c.overlap = distance - crust_sum;
+  c.status = 0;
+  return c;
+}
+
 // RigidBodyWithCrust::ClosestPoint general case (RigidBodyWithCrust.cpp:278-348).
 // status: 0 = features valid, 1 = ContactError, 2 = bounding spheres apart.
 // With a GjkStart, st->v0 on return holds the run's last iterate (the
@@ -648,21 +746,7 @@ GG_HD ContactGeom convex_closest_point_t(const BodyRef& A, const BodyRef& B, dou
   *iters = r.iters;
   if (exit_out) *exit_out = r.exit;
   if (lower_out) *lower_out = double(r.lower);
-  double distance = double(r.dist);
-  if (distance < kEpsilon) {
-    c.status = 1;
-    return c;
-  }
-  V3<T> ba = r.pa - r.pb;
-  V3<T> pc = dv(r.pa, T(2)) + dv(r.pb, T(2));
-  double crust_sum = xadd(A.crust, B.crust);
-  V3<T> ov = round3(dv(ba, r.dist));
-  ov = sc(ov, T(crust_sum) - r.dist);
-  c.point = xadd3(d3(double(pc.x), double(pc.y), double(pc.z)), shift);
-  c.overlap_vector = d3(double(ov.x), double(ov.y), double(ov.z));
-  c.overlap = distance - crust_sum;
-  c.status = 0;
-  return c;
+  return gjk_features(r, xadd(A.crust, B.crust), shift);
 }
 
 // RigidBodyWithCrust::ClosestPoint with the signed-volume GJK (the same

@@ -22,6 +22,8 @@
 
 #include <algorithm>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 #include "contact_law.cuh"
 #include "device_state.h"
@@ -29,6 +31,8 @@
 #include "gjk.cuh"
 
 namespace gg {
+
+namespace cg = cooperative_groups;
 
 template <typename R>
 using R4 = typename Vec4<R>::type;
@@ -820,8 +824,10 @@ __device__ __forceinline__ void put_memory(const StepArgs<R>& a, int row, int ra
 
 // B. one owned list entry: particle pair (p0 = this particle, the lower id)
 // or particle-obstacle candidate (p0 = the particle, p1 = the obstacle)
-template <typename R, bool DIAG, bool CONVEX, bool SV = false>
-__device__ __forceinline__ void pair_one(const StepArgs<R>& a, int4 item, R dt, ForceStats& fs) {
+// GEOM: the narrowphase of general convex pairs comes from the GJK kernel
+// (gjk_out) instead of running here
+template <typename R, bool DIAG, bool CONVEX, bool SV = false, bool GEOM = false>
+__device__ __forceinline__ void pair_one(const StepArgs<R>& a, int idx, int4 item, R dt, ForceStats& fs) {
   const ParticleArrays<R>& P = a.cur;
   const int s = item.x, e = item.y, q = item.z & 511, rank = item.z >> 9, oi = item.w;
   const size_t my_slot = (size_t)s * a.clist_cap + q;
@@ -878,6 +884,10 @@ __device__ __forceinline__ void pair_one(const StepArgs<R>& a, int4 item, R dt, 
           contact = !fatal;
         }
       }
+    } else if constexpr (GEOM) {
+      // the GJK kernel's result for this work item
+      g = gjk_result(a.gjk_out[idx]);
+      contact = g.status == 0 && g.overlap < 0.;
     } else {
       // general convex pair: circumscribed-sphere test then GJK on crust-shrunk bodies
       BodyRef ba, bb;
@@ -1002,6 +1012,9 @@ __device__ __forceinline__ void pair_one(const StepArgs<R>& a, int4 item, R dt, 
       set_status(a.stats, GRAINS_GPU_CONTACT_ERROR);
       g.overlap = 1.;
     }
+  } else if constexpr (GEOM) {
+    g = gjk_result(a.gjk_out[idx]);
+    if (g.status != 0) g.overlap = 1.;
   } else {
     BodyRef ba, bb;
     make_body_ref(a, mi.z, s, mdi.y, ba);
@@ -1070,15 +1083,204 @@ __device__ __forceinline__ void pair_one(const StepArgs<R>& a, int4 item, R dt, 
   fs.ov_max = fmax(fs.ov_max, o);
 }
 
+// ---------------------------------------------------------------------------
+// B0. The GJK phase of convex scenarios (Johnson's GJK): every work item whose
+// pair needs the general narrowphase gets RigidBodyWithCrust::ClosestPoint's
+// features written to gjk_out[item]; the pair kernel then applies the law.
+//
+// The runs take 1 to 30+ iterations, so one run per thread leaves most lanes
+// of a warp idle while the longest run of the warp finishes (5 of 32 lanes
+// active on the settled drum).  Here each thread keeps a run in flight and
+// takes the next work item as soon as its run ends: every pass of the loop is
+// one GJK iteration on every busy lane.  The arithmetic of a run is that of
+// gjk_distance (same state, same passes), so results do not depend on the
+// schedule.
+
+__device__ __forceinline__ ContactGeom gjk_result(const GjkOut& o) {
+  ContactGeom g;
+  g.point = d3(o.point[0], o.point[1], o.point[2]);
+  g.overlap_vector = d3(o.ov[0], o.ov[1], o.ov[2]);
+  g.overlap = o.overlap;
+  g.status = o.status;
+  return g;
+}
+
+// whether a work item's pair needs the general narrowphase (the sphere-sphere
+// and sphere-box cases of ClosestPoint are analytic, RigidBodyWithCrust.cpp:
+// 218-258)
+template <typename R>
+__device__ __forceinline__ bool needs_gjk(const StepArgs<R>& a, int4 item) {
+  const int ts = a.shapes[a.cur.meta[item.x].z].type;
+  if (item.y >= 0) return !(ts == GRAINS_GPU_SPHERE && a.shapes[a.cur.meta[entry_slot(item.y)].z].type == GRAINS_GPU_SPHERE);
+  return !(ts == GRAINS_GPU_SPHERE && a.shapes[a.obs[-1 - item.y].shape].type == GRAINS_GPU_BOX);
+}
+
+// the bodies of a work item: p0 = the particle, p1 = the partner or obstacle
+template <typename R>
+__device__ __forceinline__ void item_bodies(const StepArgs<R>& a, int4 item, BodyRef& ba, BodyRef& bb) {
+  const int s = item.x;
+  make_body_ref(a, a.cur.meta[s].z, s, a.cur.md[s].y, ba);
+  if (item.y >= 0) {
+    const int t = entry_slot(item.y);
+    make_body_ref(a, a.cur.meta[t].z, t, a.cur.md[t].y, bb);
+  } else {
+    make_obstacle_ref(a, -1 - item.y, bb);
+  }
+}
+
+// one work-item index per calling lane, from a warp-aggregated atomic
+__device__ __forceinline__ int take_item(int* counter) {
+  cg::coalesced_group g = cg::coalesced_threads();
+  int base = 0;
+  if (g.thread_rank() == 0) base = atomicAdd(counter, (int)g.size());
+  return g.shfl(base, 0) + (int)g.thread_rank();
+}
+
+template <typename R>
+struct GjkLane {
+  int idx;        // work item in flight
+  int4 item;
+  double crust_sum;
+  bool known;     // the pair's history was found
+  V3<double> v_before;
+  LocalBody<double> la, lb;
+  GjkRun<double> run;
+};
+
+// the collision history of a particle pair (Particle.cpp:497-504): the run's
+// last iterate, or the entry as it was when a ContactError was handled, or a
+// hole (bounding spheres apart, zero direction)
+template <typename R>
+__device__ __forceinline__ void store_gjk_dir(const StepArgs<R>& a, int4 item, int partner_id, int status,
+                                              int handled, bool known, V3<double> before, V3<double> after) {
+  const int rank = item.z >> 9;
+  if (rank >= a.hist_cap) return;
+  GjkDir d;
+  d.other = partner_id;
+  d.pad = 0;
+  const V3<double> keep = handled ? before : after;
+  if (status == 2 || (handled && !known) || (keep.x == 0. && keep.y == 0. && keep.z == 0.)) d.other = kNoGjkDir;
+  d.v[0] = keep.x;
+  d.v[1] = keep.y;
+  d.v[2] = keep.z;
+  a.gdir_next[(size_t)item.w * a.hist_cap + rank] = d;
+}
+
+// takes work items until one needs a GJK run and starts it; items whose
+// bounding spheres are apart are finished on the way.  False when none is left.
+template <typename R>
+__device__ bool gjk_lane_start(const StepArgs<R>& a, int n_items, GjkLane<R>& L) {
+  for (;;) {
+    const int k = take_item(a.gjk_next);
+    if (k >= n_items) return false;
+    const int4 item = a.work[k];
+    if (!needs_gjk(a, item)) continue;
+    BodyRef ba, bb;
+    item_bodies(a, item, ba, bb);
+    const bool pair = item.y >= 0;
+    const int partner = pair ? a.cur.meta[entry_slot(item.y)].x : 0;
+    GjkStart<double> st;
+    st.accel = a.gjk_accel != 0;
+    st.history = pair && a.gjk_history != 0;
+    L.known = st.history && find_gjk_dir(a, item.w, partner, st.v0);
+    const D3 g = xsub3(ba.origin, bb.origin);
+    if (!(xnorm(g) < xadd(ba.radius, bb.radius))) {  // RigidBodyWithCrust.cpp:278-282
+      GjkOut& o = a.gjk_out[k];
+      o.status = 2;
+      o.handled = 0;
+      o.overlap = 1.;
+      if (st.history) store_gjk_dir(a, item, partner, 2, 0, L.known, st.v0, st.v0);
+      continue;
+    }
+    L.idx = k;
+    L.item = item;
+    L.crust_sum = xadd(ba.crust, bb.crust);
+    L.v_before = st.v0;
+    L.la = local_body<double>(ba, d3(0., 0., 0.), ba.scaling);
+    L.lb = local_body<double>(bb, d3(0., 0., 0.), bb.scaling);
+    gjk_begin(L.run, L.la, L.lb, a.gjk_tol, st);  // L.run.g: the lane's shared-memory arrays
+    return true;
+  }
+}
+
+// the features of a finished run, the crust-x10 retry on ContactError, the
+// history and the statistics
+template <typename R>
+__device__ void gjk_lane_finish(const StepArgs<R>& a, GjkLane<R>& L, unsigned long long& ngjk,
+                                unsigned long long& nit) {
+  const GjkResult<double> r = gjk_end(L.run, L.la, L.lb);
+  ContactGeom c = gjk_features(r, L.crust_sum, d3(0., 0., 0.));
+  ++ngjk;
+  nit += r.iters;
+  int handled = 0;
+  if (c.status == 1) {
+    BodyRef ba, bb;
+    item_bodies(a, L.item, ba, bb);
+    c = convex_error_handling(ba, bb, ba.lext, bb.lext, 10., a.gjk_tol, a.gjk_accel != 0);
+    handled = 1;
+    set_status(a.stats, c.status == 1 ? GRAINS_GPU_CONTACT_ERROR : GRAINS_GPU_CONTACT_HANDLED);
+  }
+  GjkOut& o = a.gjk_out[L.idx];
+  o.point[0] = c.point.x;
+  o.point[1] = c.point.y;
+  o.point[2] = c.point.z;
+  o.ov[0] = c.overlap_vector.x;
+  o.ov[1] = c.overlap_vector.y;
+  o.ov[2] = c.overlap_vector.z;
+  o.overlap = c.overlap;
+  o.status = c.status;
+  o.handled = handled;
+  if (L.item.y >= 0 && a.gjk_history)
+    store_gjk_dir(a, L.item, a.cur.meta[entry_slot(L.item.y)].x, c.status, handled, L.known, L.v_before, r.v);
+}
+
+// Starting a run (the bodies, the history, the first iterate) costs about as
+// much as two GJK iterations, so lanes whose run has ended wait until half the
+// warp is idle (or nothing else runs) and start their next runs together.
+// The arrays of each thread's run (sub-determinants, dot products, simplex and
+// support points: 672 bytes) live in shared memory, interleaved across the
+// block's 64 threads; in local memory they overflowed L1 and were written back
+// to DRAM (1.9 GB per launch on the settled drum).
+constexpr int kGjkBlock = 64;
+template <typename R>
+__global__ void __launch_bounds__(kGjkBlock) gjk_kernel(StepArgs<R> a) {
+  __shared__ double words[kGjkWords * kGjkBlock];
+  const unsigned full = 0xffffffffu;
+  const int n_items = (int)min((long long)*(volatile int*)a.work_n, (long long)a.n * a.clist_cap);
+  unsigned long long ngjk = 0, nit = 0;
+  GjkLane<R> L;
+  L.run.g.base = words + threadIdx.x;
+  L.run.g.stride = kGjkBlock;
+  bool busy = gjk_lane_start(a, n_items, L);
+  bool drained = !busy;  // no work item is left for this lane
+  for (;;) {
+    if (busy && gjk_iterate(L.run, L.la, L.lb)) {
+      gjk_lane_finish(a, L, ngjk, nit);
+      busy = false;
+    }
+    const unsigned waiting = __ballot_sync(full, !busy && !drained);
+    const unsigned running = __ballot_sync(full, busy);
+    if (!waiting && !running) break;
+    if (__popc(waiting) >= 16 || !running) {
+      if (!busy && !drained) {
+        busy = gjk_lane_start(a, n_items, L);
+        drained = !busy;
+      }
+    }
+  }
+  warp_add(&a.stats->n_gjk_calls, ngjk);
+  warp_add(&a.stats->n_gjk_iters, nit);
+}
+
 // work items [first, n_items) with the given stride; `padded`: a bound with a
 // uniform trip count for the warp reductions of the statistics
-template <typename R, bool DIAG, bool CONVEX, bool SV = false>
+template <typename R, bool DIAG, bool CONVEX, bool SV = false, bool GEOM = false>
 __device__ __forceinline__ void pairs_range(const StepArgs<R>& a, int first, int stride, R dt) {
   const int n_items = (int)min((long long)*(volatile int*)a.work_n, (long long)a.n * a.clist_cap);
   const int padded = (n_items + stride - 1) / stride * stride;
   ForceStats fs{0, 0, 0, 0, 0., 0.};
   for (int k = first; k < padded; k += stride)
-    if (k < n_items) pair_one<R, DIAG, CONVEX, SV>(a, a.work[k], dt, fs);
+    if (k < n_items) pair_one<R, DIAG, CONVEX, SV, GEOM>(a, k, a.work[k], dt, fs);
   flush_force_stats(a.stats, fs);
 }
 
@@ -1086,9 +1288,9 @@ __device__ __forceinline__ void pairs_range(const StepArgs<R>& a, int first, int
 #ifndef GG_PAIRS_MIN_BLOCKS
 #define GG_PAIRS_MIN_BLOCKS 1
 #endif
-template <typename R, bool DIAG, bool CONVEX, bool SV = false>
+template <typename R, bool DIAG, bool CONVEX, bool SV = false, bool GEOM = false>
 __global__ void __launch_bounds__(128, CONVEX ? 1 : GG_PAIRS_MIN_BLOCKS) pairs_kernel(StepArgs<R> a, R dt) {
-  pairs_range<R, DIAG, CONVEX, SV>(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, dt);
+  pairs_range<R, DIAG, CONVEX, SV, GEOM>(a, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, dt);
 }
 
 // C. the torsor of particle s: InitializeForces(withWeight) (torsor = weight,
@@ -1149,7 +1351,10 @@ __device__ __forceinline__ void sum_one(const StepArgs<R>& a, int s) {
 template <typename R>
 __global__ void __launch_bounds__(256) sums_kernel(StepArgs<R> a) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s == 0) *a.work_n = 0;
+  if (s == 0) {
+    *a.work_n = 0;
+    if (a.gjk_next) *a.gjk_next = 0;
+  }
   if (s < a.n) sum_one(a, s);
 }
 
@@ -1530,6 +1735,22 @@ int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather, int
   return check_launch();
 }
 
+// the GJK kernel keeps every SM full: its resident blocks per SM x the SMs
+template <typename R>
+int gjk_grid() {
+  static int grid = 0;
+  if (!grid) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // as much shared memory as the SM has, for the runs' arrays
+    cudaFuncSetAttribute(gjk_kernel<R>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gjk_kernel<R>, kGjkBlock, 0);
+    grid = (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  }
+  return grid;
+}
+
 template <typename R>
 int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int phases) {
   if (a.n == 0) return 0;
@@ -1549,6 +1770,12 @@ int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int
       pairs_kernel<R, true, true, true><<<g, fb, 0, s>>>(a, R(dt));
     else
       pairs_kernel<R, false, true, true><<<g, fb, 0, s>>>(a, R(dt));
+  } else if (a.has_convex && a.gjk_out) {  // the GJK kernel, then the law
+    gjk_kernel<R><<<gjk_grid<R>(), kGjkBlock, 0, s>>>(a);
+    if (diag)
+      pairs_kernel<R, true, true, false, true><<<g, fb, 0, s>>>(a, R(dt));
+    else
+      pairs_kernel<R, false, true, false, true><<<g, fb, 0, s>>>(a, R(dt));
   } else if (a.has_convex) {
     if (diag)
       pairs_kernel<R, true, true><<<g, fb, 0, s>>>(a, R(dt));
