@@ -271,6 +271,15 @@ int grains_gpu_download_particles(grains_gpu_ctx* ctx, grains_gpu_particles* p);
  * of an adaptor whose host copy of the state stays authoritative, like
  * AllComponents in the reference (AllComponents.cpp:151-233). */
 int grains_gpu_update_particles(grains_gpu_ctx* ctx, const grains_gpu_particles* p);
+/* The kinematic state of some of the uploaded particles: rows[k] (distinct
+ * upload indices) gets entry k of p's position, quaternion, basis (when given),
+ * velocity and omega arrays (n_rows entries each; p->n is ignored); the other
+ * particles keep theirs untouched.  The ghost refresh of a domain-decomposed
+ * run overwrites only its ghosts this way, as the reference's
+ * GrainsMPIWrapper::UpdateClones updates only the clones
+ * (GrainsMPIWrapper.cpp:1556-1684). */
+int grains_gpu_update_particle_rows(grains_gpu_ctx* ctx, int64_t n_rows, const int64_t* rows,
+                                    const grains_gpu_particles* p);
 int grains_gpu_upload_contact_memory(grains_gpu_ctx* ctx, const grains_gpu_contact_memory* m);
 /* n on input = capacity; on output = number of entries written (owner-side
  * and mirrored entries both listed, like the reference's two maps) */

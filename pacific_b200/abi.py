@@ -133,6 +133,7 @@ _SIGS = {
     "set_obstacle_loadings": [_VP, C.c_int32, C.c_int32, C.POINTER(ObstacleLoading)],
     "set_collision_algorithm": [_VP, C.c_int32],
     "set_collision_options": [_VP, C.c_double, C.c_int32, C.c_int32],
+    "update_particle_rows": [_VP, C.c_int64, C.POINTER(C.c_int64), C.c_void_p],
     "upload_particles": [_VP, C.POINTER(Particles)],
     "download_particles": [_VP, C.POINTER(Particles)],
     "update_particles": [_VP, C.POINTER(Particles)],
@@ -156,7 +157,7 @@ _SIGS = {
                       C.POINTER(C.c_int64)],
 }
 # diagnostics that the reference built from its sources (oracle/_ref) lacks
-_OPTIONAL = {"get_contact_forces", "set_record_attributes", "set_collision_options"}
+_OPTIONAL = {"get_contact_forces", "set_record_attributes", "set_collision_options", "update_particle_rows"}
 _GPU_ONLY = {
     "get_stream": [_VP, C.POINTER(_VP)],
     "synchronize": [_VP],
@@ -468,6 +469,22 @@ class Simulation:
             setattr(s, k, _ptr(a, C.c_double))
         self._keep_update = list(arrs.values())
         self._check(self.lib.fn["update_particles"](self.ctx, C.byref(s)))
+
+    def update_rows(self, rows, p):
+        """Overwrites the kinematic state of the particles at upload indices
+        `rows` (distinct) with the arrays of `p` (one entry per row: position,
+        quaternion, velocity, omega, and basis when given); the other
+        particles are untouched."""
+        rows = np.ascontiguousarray(rows, dtype=np.int64)
+        arrs = {k: f64(p[k]) for k in ["position", "quaternion", "velocity", "omega"]}
+        arrs["basis"] = f64(p["basis"]) if p.get("basis") is not None else None
+        s = Particles()
+        s.n = len(rows)
+        for k, a in arrs.items():
+            setattr(s, k, _ptr(a, C.c_double))
+        self._keep_update = list(arrs.values()) + [rows]
+        self._check(self.lib.fn["update_particle_rows"](self.ctx, len(rows), rows.ctypes.data_as(C.POINTER(C.c_int64)),
+                                                        C.byref(s)))
 
     def download(self, out=None):
         """The state in upload order.  `out`: preallocated arrays to fill (for

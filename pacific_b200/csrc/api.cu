@@ -85,6 +85,7 @@ struct grains_gpu_ctx {
   bool uploaded = false;
   bool tables_dirty = true;
   char* stage = nullptr;  // device staging of update / download in upload order (30 x 8 B per particle)
+  char* row_scratch = nullptr;  // grains_gpu_update_particle_rows: rows, slot of every upload index
   bool sorted = false;      // cur arrays are in cell order for the current positions
   bool keys_valid = false;  // key and cell counts hold the cells of the current positions
   bool pending_kick2 = false;
@@ -916,6 +917,7 @@ int grains_gpu_destroy(grains_gpu_ctx* c) {
   for (int k = 0; k < 2; ++k)
     if (c->buf[k].basis) cudaFree(c->buf[k].basis);
   if (c->stage) cudaFree(c->stage);
+  if (c->row_scratch) cudaFree(c->row_scratch);
   for (void* p : {(void*)c->clist, (void*)c->ccount, c->res_f, c->res_t, (void*)c->work, (void*)c->gjk_out})
     if (p) cudaFree(p);
   if (c->pbar) cudaFree(c->pbar);
@@ -1549,6 +1551,48 @@ int grains_gpu_update_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
   if (with_basis)
     CK(cudaMemcpyAsync((void*)st.basis, p->basis, 9 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   int rc = with_args(c, [&](auto& a) { return launch_update_dynamic(a, c->stream, st); });
+  if (rc) return fail(c, rc, "update launch failed");
+  c->keys_valid = false;
+  c->sorted = false;
+  if ((rc = sort_now(c, 1))) return rc;
+  return finish_call(c);
+}
+
+int grains_gpu_update_particle_rows(grains_gpu_ctx* c, int64_t n_rows, const int64_t* rows,
+                                    const grains_gpu_particles* p) {
+  if (!c || !p || n_rows < 0 || (n_rows && !rows)) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "upload particles first");
+  if (n_rows > c->n) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "more rows than particles");
+  if (n_rows == 0) return 0;
+  if (!p->position || !p->quaternion || !p->velocity || !p->omega)
+    return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "missing kinematic array");
+  std::vector<char> seen((size_t)c->n, 0);
+  for (int64_t k = 0; k < n_rows; ++k) {
+    if (rows[k] < 0 || rows[k] >= c->n) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "row out of range");
+    if (seen[(size_t)rows[k]]++) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "a row appears twice");
+  }
+  if (int rc = ensure_stage(c)) return rc;
+  if (!c->row_scratch) {  // the rows and the slot of every upload index
+    void* q = nullptr;
+    CK(cudaMalloc(&q, (size_t)c->cap * (sizeof(long long) + sizeof(int))));
+    c->row_scratch = (char*)q;
+  }
+  if (int rc = flush_kick(c)) return rc;
+  const int64_t m = n_rows;
+  double* d = (double*)c->stage;
+  const bool with_basis = c->has_basis && p->basis;
+  KinematicStage st{d, d + 3 * m, d + 7 * m, d + 10 * m, with_basis ? d + 13 * m : nullptr};
+  long long* drows = (long long*)c->row_scratch;
+  int* slot_of = (int*)(c->row_scratch + (size_t)c->cap * sizeof(long long));
+  CK(cudaMemcpyAsync(drows, rows, m * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync((void*)st.position, p->position, 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync((void*)st.quaternion, p->quaternion, 4 * m * sizeof(double), cudaMemcpyHostToDevice,
+                     c->stream));
+  CK(cudaMemcpyAsync((void*)st.velocity, p->velocity, 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync((void*)st.omega, p->omega, 3 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (with_basis)
+    CK(cudaMemcpyAsync((void*)st.basis, p->basis, 9 * m * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int rc = with_args(c, [&](auto& a) { return launch_update_rows(a, c->stream, st, drows, m, slot_of); });
   if (rc) return fail(c, rc, "update launch failed");
   c->keys_valid = false;
   c->sorted = false;

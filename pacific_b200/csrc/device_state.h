@@ -251,6 +251,11 @@ struct DownloadStage {
 };
 template <typename R>
 int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const KinematicStage& st);
+// the kinematic state of the upload indices rows[0 .. n_rows) from stage
+// entries 0 .. n_rows (slot_of: n ints of scratch)
+template <typename R>
+int launch_update_rows(const StepArgs<R>& a, cudaStream_t s, const KinematicStage& st, const long long* rows,
+                       long long n_rows, int* slot_of);
 template <typename R>
 int launch_pack_download(const StepArgs<R>& a, cudaStream_t s, const DownloadStage& d);
 template <typename R>

@@ -1374,11 +1374,8 @@ __global__ void zero_kdelta_kernel(StepArgs<R> a) {
 // overwrite the kinematic state from upload-order arrays on the device
 // (ParticleKinematics::setAngularVelocity gives the body-frame rate)
 template <typename R>
-__global__ void update_dynamic_kernel(StepArgs<R> a, KinematicStage st) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= a.n) return;
+__device__ __forceinline__ void set_kinematics(const StepArgs<R>& a, int s, const KinematicStage& st, size_t i) {
   const ParticleArrays<R>& P = a.cur;
-  const size_t i = (size_t)P.orig[s];
   double4 xr = P.xr[s];
   xr.x = st.position[3 * i];
   xr.y = st.position[3 * i + 1];
@@ -1394,6 +1391,28 @@ __global__ void update_dynamic_kernel(StepArgs<R> a, KinematicStage st) {
   P.wbf[s] = st3<R>(v3<R>(R(wbf.x), R(wbf.y), R(wbf.z)));
   if (a.has_basis && st.basis)
     for (int k = 0; k < 9; ++k) P.basis[9 * (size_t)s + k] = st.basis[9 * i + k];
+}
+
+template <typename R>
+__global__ void update_dynamic_kernel(StepArgs<R> a, KinematicStage st) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  set_kinematics(a, s, st, (size_t)a.cur.orig[s]);
+}
+
+// slot of every upload index (the inverse of orig)
+template <typename R>
+__global__ void slot_of_row_kernel(StepArgs<R> a, int* slot_of) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < a.n) slot_of[a.cur.orig[s]] = s;
+}
+
+// the kinematic state of the listed upload indices (stage entry k for rows[k])
+template <typename R>
+__global__ void update_rows_kernel(StepArgs<R> a, KinematicStage st, const long long* rows, long long n_rows,
+                                   const int* slot_of) {
+  long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n_rows) set_kinematics(a, slot_of[rows[k]], st, (size_t)k);
 }
 
 // the state in upload order, one array per field (any may be null): the
@@ -1817,6 +1836,15 @@ int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const KinematicS
 }
 
 template <typename R>
+int launch_update_rows(const StepArgs<R>& a, cudaStream_t s, const KinematicStage& st, const long long* rows,
+                       long long n_rows, int* slot_of) {
+  if (a.n == 0 || n_rows == 0) return 0;
+  slot_of_row_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, slot_of);
+  update_rows_kernel<R><<<(int)((n_rows + 255) / 256), 256, 0, s>>>(a, st, rows, n_rows, slot_of);
+  return check_launch();
+}
+
+template <typename R>
 int launch_pack_download(const StepArgs<R>& a, cudaStream_t s, const DownloadStage& d) {
   if (a.n == 0) return 0;
   pack_download_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, d);
@@ -2005,6 +2033,8 @@ int launch_persistent_steps(const StepArgs<R>& a, cudaStream_t s, int n_steps, d
   template int launch_forces<R>(const StepArgs<R>&, cudaStream_t, double, int, int);                       \
   template int launch_zero_kdelta<R>(const StepArgs<R>&, cudaStream_t);                                    \
   template int launch_update_dynamic<R>(const StepArgs<R>&, cudaStream_t, const KinematicStage&);             \
+  template int launch_update_rows<R>(const StepArgs<R>&, cudaStream_t, const KinematicStage&, const long long*,  \
+                                     long long, int*);                                                      \
   template int launch_pack_download<R>(const StepArgs<R>&, cudaStream_t, const DownloadStage&);              \
   template int launch_candidate_pairs<R>(const StepArgs<R>&, cudaStream_t, int, int, int*, int,           \
                                          unsigned long long*);                                            \

@@ -448,6 +448,17 @@ def drum(n=100_000, seed=3, radius=110.0 * MM, length=147.0 * MM, n_boxes=64, rp
 def apply(sim, sc):
     """Registers shapes, domains, laws and obstacles of `sc` on `sim` and
     uploads the particles.  Returns the shape-id map."""
+    ids = setup(sim, sc)
+    p = dict(sc.particles)
+    p["shape"] = np.asarray(ids, np.int32)[np.asarray(p["shape"])]
+    sim.upload(p)
+    return ids
+
+
+def setup(sim, sc):
+    """Everything of `apply` but the particle upload: shapes, collision
+    options, domains, laws, obstacles and their loadings.  Returns the
+    shape-id map (scenario shape index -> registered shape id)."""
     ids = [sim.add_shape(t, prm) for t, prm in sc.shapes]
     if sc.meta.get("collision") is not None:
         sim.set_collision_algorithm(sc.meta["collision"])
@@ -467,7 +478,4 @@ def apply(sim, sc):
         loads = sc.meta.get("loadings")
         if loads and loads[s]:
             sim.set_obstacle_loadings(s, loads[s])
-    p = dict(sc.particles)
-    p["shape"] = np.asarray(ids, np.int32)[np.asarray(p["shape"])]
-    sim.upload(p)
     return ids
