@@ -25,6 +25,9 @@
 
 #include <stddef.h>
 #include <stdint.h>
+#ifndef __cplusplus
+#include <stdbool.h>
+#endif
 
 #ifdef __cplusplus
 extern "C" {
@@ -280,6 +283,74 @@ int grains_gpu_update_particles(grains_gpu_ctx* ctx, const grains_gpu_particles*
  * (GrainsMPIWrapper.cpp:1556-1684). */
 int grains_gpu_update_particle_rows(grains_gpu_ctx* ctx, int64_t n_rows, const int64_t* rows,
                                     const grains_gpu_particles* p);
+/* replaces: Particle::setFluidDensity / setFluidCorrectedAcceleration with
+ * AllComponents::computeWeight and setParticlesCouplingFactor (Particle.cpp:
+ * 414-419, 820-825, 1284-1288; ParticleKinematics.cpp:483-488), the fluid
+ * set-up of GrainsCoupledWithFluid (Fluid/src/GrainsCoupledWithFluid.cpp:
+ * 1200-1207).  Immersed particles: the weight becomes m (1 - rho_f / rho_p) g
+ * and, when corrected != 0, the translational and angular accelerations are
+ * divided by 1 - rho_f / rho_p (SecondOrderLeapFrog.cpp:50-52,
+ * ParticleKinematics3D.cpp:64-69).  particle_density: rho_p in upload order
+ * (n values; may be null when fluid_density is 0, which switches the fluid
+ * off).  Set after grains_gpu_upload_particles; an upload clears it. */
+int grains_gpu_set_fluid(grains_gpu_ctx* ctx, double fluid_density, int32_t corrected,
+                         const double* particle_density);
+/* replaces: AppPRSHydroFT::setHydroFT + ComputeForces (Fluid/src/
+ * AppPRSHydroFT.cpp:29-73): a force (at the centre) and a torque per particle,
+ * 3 doubles each in upload order, added to every force evaluation after the
+ * contact forces until set again; both null removes them.  An upload clears
+ * them. */
+int grains_gpu_set_hydro_forces(grains_gpu_ctx* ctx, const double* force, const double* torque);
+/* replaces: GrainsCoupledWithFluid::updateParticlesVelocity (Fluid/src/
+ * GrainsCoupledWithFluid.cpp:1126-1185): translational and angular velocity
+ * (world frame) of every particle, 3 doubles each in upload order. */
+int grains_gpu_set_velocities(grains_gpu_ctx* ctx, const double* velocity, const double* omega);
+/* replaces: GrainsCoupledWithFluid::Simulation(dt_fluid) (Fluid/src/
+ * GrainsCoupledWithFluid.cpp:123-229): the DEM steps of one fluid step.
+ * dteff = max(min(max_dt, dt_fluid / *ndt), min_dt); *ndt becomes
+ * (size_t)(dt_fluid / dteff) (the count carries over to the next call, as
+ * m_ndt does) and *ndt kick-drift-kick steps of dt_fluid / *ndt run
+ * (grains_gpu_step); *time advances by dt_fluid. */
+int grains_gpu_fluid_step(grains_gpu_ctx* ctx, double dt_fluid, double min_dt, double max_dt, int64_t* ndt,
+                          double* time);
+/* replaces: GrainsCoupledWithFluid::GrainsToFluid (Fluid/src/
+ * GrainsCoupledWithFluid.cpp:912-1120) as GrainsToBasilisk passes it on
+ * (InterfaceCBasilisk/src/InterfaceGrains3DBasilisk.cpp:64-87): the rigid
+ * bodies for the fluid solver as one line of space-separated tokens (each
+ * followed by one space).  Per particle, by increasing id: index, corner code
+ * (Convex::getNbCorners: 1 sphere, 666 box, 777 cylinder, vertex count
+ * polyhedron), "P", velocity, angular velocity, density, mass, the
+ * space-fixed inertia tensor (xx xy xz yy yz zz), the rotation matrix, the
+ * centre, the circumscribed radius, then the envelope points in world
+ * coordinates and the faces (RigidBody::writePositionInFluid).  *len = the
+ * size with the terminating 0; buf may be null to query it. */
+int grains_gpu_fluid_features(grains_gpu_ctx* ctx, char* buf, int64_t cap, int64_t* len);
+/* No counterpart in the reference: attaches a context set up through this
+ * interface to the fluid solvers' C interface below, with the time-step
+ * bounds of <Simulation><TimeStep mindt maxdt ndt> (GrainsCoupledWithFluid.cpp:
+ * 509-531).  The reference builds its coupled simulation from its XML and
+ * reload files in Init_Grains; that input layer is the host's here. */
+int grains_gpu_basilisk_attach(grains_gpu_ctx* ctx, double min_dt, double max_dt, int64_t ndt);
+/* The fluid solvers' C interface, same names and signatures as
+ * InterfaceCBasilisk/include/InterfaceGrains3DBasilisk.h:12-30, driving the
+ * attached context.  Init_Grains applies the fluid density and the
+ * acceleration correction (its input file name and restart flag are not
+ * read) and starts the leapfrog; Simu_Grains = grains_gpu_fluid_step;
+ * GrainsToBasilisk = grains_gpu_fluid_features in a malloc'ed string (free
+ * it); UpdateVelocityGrains sets the velocities from an m x 6 array ordered by
+ * id; NumberOfRigidBodiesInBasilisk reports the particles and no obstacle.
+ * SaveResults_Grains and checkParaviewPostProcessing_Grains write nothing
+ * (the Paraview writers are out of scope).  Like the reference, errors end
+ * the process with a message. */
+void Init_Grains(char const* inputfile, double fluid_rho, const bool b_restart, const bool b_fluidcorrectedacc);
+void Simu_Grains(const double dt_fluid);
+char* GrainsToBasilisk(int* pstrsize);
+void SetInitialTime(double tinit);
+void SaveResults_Grains(void);
+void checkParaviewPostProcessing_Grains(char* solid_resDir);
+void UpdateVelocityGrains(double** arrayv, const int m);
+void SetInitialCycleNumber(int cycle0);
+void NumberOfRigidBodiesInBasilisk(size_t* nparticles, size_t* nobstacles);
 int grains_gpu_upload_contact_memory(grains_gpu_ctx* ctx, const grains_gpu_contact_memory* m);
 /* n on input = capacity; on output = number of entries written (owner-side
  * and mirrored entries both listed, like the reference's two maps) */

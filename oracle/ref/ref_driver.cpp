@@ -44,6 +44,7 @@
 #include "Polyhedron.hh"
 #include "Quaternion.hh"
 #include "ReaderXML.hh"
+#include "AppPRSHydroFT.hh"
 #include "RigidBodyWithCrust.hh"
 #include "RawDataPostProcessingWriter.hh"
 #include "SimpleObstacle.hh"
@@ -92,6 +93,19 @@ class OracleGrains : public Grains {
     return old;
   }
   AllInsertionWindows const& windows() const { return m_insertion_windows; }
+  // the fluid's hydrodynamic force App of GrainsCoupledWithFluid::Forces
+  // (Fluid/src/GrainsCoupledWithFluid.cpp:455-462): registered after the
+  // collision App, with arrays for the active particles
+  AppPRSHydroFT* hydro_app() {
+    if (!m_hydro) {
+      m_hydro = new AppPRSHydroFT();
+      m_hydro->setName("PRSHydroFT");
+      m_allApp.push_back(m_hydro);
+      m_hydro->allocateHydroFT(m_allcomponents.getActiveParticles()->size());
+    }
+    return m_hydro;
+  }
+  AppPRSHydroFT* m_hydro = nullptr;
 };
 
 struct ShapeSpec {
@@ -223,6 +237,10 @@ int grains_ref_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
   if (!cfg || !out || cfg->n_systems != 1) return GRAINS_GPU_INVALID_ARGUMENT;
   grains_gpu_ctx* c = new grains_gpu_ctx();
   c->cfg = *cfg;
+  // the fluid settings are statics of Particle: back to the defaults
+  // (Particle.cpp:21-23) for every new simulation
+  Particle::setFluidDensity(0.);
+  Particle::setFluidCorrectedAcceleration(true);
   char tmpl[] = "/tmp/grains_ref_XXXXXX";
   char* d = mkdtemp(tmpl);
   c->dir = d ? d : "/tmp";
@@ -287,6 +305,85 @@ int grains_ref_set_collision_options(grains_gpu_ctx* c, double tolerance, int32_
   c->gjk_tol = tolerance;
   c->gjk_accel = acceleration;
   c->gjk_history = history;
+  return 0;
+}
+
+// Particle::setFluidDensity / setFluidCorrectedAcceleration, then the
+// weights and coupling factors of every particle (the reference's own
+// computeWeight / setCouplingFactor; rho_p is each particle's class density)
+int grains_ref_set_fluid(grains_gpu_ctx* c, double rho_f, int32_t corrected, const double* density) {
+  (void)density;
+  if (!c->g) return GRAINS_GPU_NOT_READY;
+  Particle::setFluidDensity(rho_f);
+  Particle::setFluidCorrectedAcceleration(corrected != 0);
+  for (auto& kv : c->part_of_my) {
+    kv.second->computeWeight();
+    kv.second->setCouplingFactor();
+  }
+  return 0;
+}
+
+// AppPRSHydroFT::setHydroFT: its arrays follow the active particle list
+int grains_ref_set_hydro_forces(grains_gpu_ctx* c, const double* force, const double* torque) {
+  if (!c->g) return GRAINS_GPU_NOT_READY;
+  std::map<Particle*, size_t> row;
+  for (size_t i = 0; i < c->my_id.size(); ++i) row[c->part_of_my[c->my_id[i]]] = i;
+  std::vector<std::vector<double>> h;
+  for (Particle* P : *c->g->comps().getActiveParticles()) {
+    if (P->getTag() >= 2) continue;
+    std::vector<double> e(6, 0.);
+    const size_t i = row[P];
+    for (int k = 0; k < 3; ++k) {
+      if (force) e[k] = force[3 * i + k];
+      if (torque) e[3 + k] = torque[3 * i + k];
+    }
+    h.push_back(e);
+  }
+  c->g->hydro_app()->setHydroFT(&h);
+  return 0;
+}
+
+// GrainsCoupledWithFluid::GrainsToFluid (Fluid/src/GrainsCoupledWithFluid.cpp:
+// 912-1120) for the particles of this simulation, with the reference's own
+// objects and number formatting, tokenised as GrainsToBasilisk does
+// (InterfaceGrains3DBasilisk.cpp:64-87); particles by increasing id of the
+// caller, indexed from 0
+int grains_ref_fluid_features(grains_gpu_ctx* c, char* buf, int64_t cap, int64_t* len) {
+  if (!c->g) return GRAINS_GPU_NOT_READY;
+  auto D = [](double x) { return GrainsExec::doubleToString(ios::scientific, FORMAT16DIGITS, x); };
+  ostringstream pf;
+  pf << c->part_of_my.size() << endl;
+  int k = 0;
+  for (auto& kv : c->part_of_my) {
+    Particle* P = kv.second;
+    vector<double> inertia(6, 0.);
+    P->computeInertiaTensorSpaceFixed(inertia);
+    Matrix mr = P->getRigidBody()->getTransform()->getBasis();
+    Vector3 const* vt = P->getTranslationalVelocity();
+    Vector3 const* vr = P->getAngularVelocity();
+    Point3 const* ce = P->getPosition();
+    pf << k << " " << P->getNbCorners() << endl;
+    pf << "P " << D((*vt)[X]) << " " << D((*vt)[Y]) << " " << D((*vt)[Z]) << " " << D((*vr)[X]) << " "
+       << D((*vr)[Y]) << " " << D((*vr)[Z]) << " " << D(P->getDensity()) << " " << D(P->getMass());
+    for (int t = 0; t < 6; ++t) pf << " " << D(inertia[t]);
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < 3; ++q) pf << " " << D(mr[r][q]);
+    pf << " " << D((*ce)[X]) << " " << D((*ce)[Y]) << " " << D((*ce)[Z]) << endl;
+    pf << P->getCircumscribedRadius();
+    P->writePositionInFluid(pf);
+    ++k;
+  }
+  istringstream iss(pf.str());
+  std::string out, tok;
+  while (iss >> tok) {
+    out += tok;
+    out += ' ';
+  }
+  *len = (int64_t)out.size() + 1;
+  if (buf) {
+    if (cap < *len) return GRAINS_GPU_INVALID_ARGUMENT;
+    std::memcpy(buf, out.c_str(), out.size() + 1);
+  }
   return 0;
 }
 

@@ -134,6 +134,11 @@ _SIGS = {
     "set_collision_algorithm": [_VP, C.c_int32],
     "set_collision_options": [_VP, C.c_double, C.c_int32, C.c_int32],
     "update_particle_rows": [_VP, C.c_int64, C.POINTER(C.c_int64), C.c_void_p],
+    "set_fluid": [_VP, C.c_double, C.c_int32, _P_F64],
+    "set_hydro_forces": [_VP, _P_F64, _P_F64],
+    "set_velocities": [_VP, _P_F64, _P_F64],
+    "fluid_step": [_VP, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_int64), C.POINTER(C.c_double)],
+    "fluid_features": [_VP, C.c_char_p, C.c_int64, C.POINTER(C.c_int64)],
     "upload_particles": [_VP, C.POINTER(Particles)],
     "download_particles": [_VP, C.POINTER(Particles)],
     "update_particles": [_VP, C.POINTER(Particles)],
@@ -157,7 +162,8 @@ _SIGS = {
                       C.POINTER(C.c_int64)],
 }
 # diagnostics that the reference built from its sources (oracle/_ref) lacks
-_OPTIONAL = {"get_contact_forces", "set_record_attributes", "set_collision_options", "update_particle_rows"}
+_OPTIONAL = {"get_contact_forces", "set_record_attributes", "set_collision_options", "update_particle_rows",
+             "set_fluid", "set_hydro_forces", "set_velocities", "fluid_step", "fluid_features"}
 _GPU_ONLY = {
     "get_stream": [_VP, C.POINTER(_VP)],
     "synchronize": [_VP],
@@ -469,6 +475,49 @@ class Simulation:
             setattr(s, k, _ptr(a, C.c_double))
         self._keep_update = list(arrs.values())
         self._check(self.lib.fn["update_particles"](self.ctx, C.byref(s)))
+
+    def set_fluid(self, fluid_density, corrected=True, particle_density=None):
+        """Immersed particles (the fluid set-up of GrainsCoupledWithFluid):
+        buoyant weights m (1 - rho_f / rho_p) g and, when `corrected`,
+        accelerations divided by 1 - rho_f / rho_p.  particle_density: rho_p
+        per particle in upload order."""
+        d = f64(particle_density) if particle_density is not None else None
+        self._keep_fluid = d
+        self._check(self.lib.fn["set_fluid"](self.ctx, float(fluid_density), int(bool(corrected)),
+                                             _ptr(d, C.c_double) if d is not None else None))
+
+    def set_hydro_forces(self, force=None, torque=None):
+        """The fluid's force and torque on every particle (upload order, 3
+        each), added to every force evaluation; None removes them."""
+        f = f64(force) if force is not None else None
+        t = f64(torque) if torque is not None else None
+        self._keep_hydro = (f, t)
+        self._check(self.lib.fn["set_hydro_forces"](self.ctx, _ptr(f, C.c_double) if f is not None else None,
+                                                    _ptr(t, C.c_double) if t is not None else None))
+
+    def set_velocities(self, velocity, omega):
+        """Translational and angular (world) velocities of every particle,
+        upload order."""
+        v, w = f64(velocity), f64(omega)
+        self._check(self.lib.fn["set_velocities"](self.ctx, _ptr(v, C.c_double), _ptr(w, C.c_double)))
+
+    def fluid_step(self, dt_fluid, min_dt, max_dt, ndt, time):
+        """The DEM steps of one fluid step (GrainsCoupledWithFluid::
+        Simulation): returns (the new step count, the new time)."""
+        n = C.c_int64(int(ndt))
+        t = C.c_double(float(time))
+        self._check(self.lib.fn["fluid_step"](self.ctx, float(dt_fluid), float(min_dt), float(max_dt), C.byref(n),
+                                              C.byref(t)))
+        return n.value, t.value
+
+    def fluid_features(self):
+        """The rigid bodies for the fluid solver (GrainsToFluid, tokenised as
+        GrainsToBasilisk passes it on), as a str."""
+        n = C.c_int64(0)
+        self._check(self.lib.fn["fluid_features"](self.ctx, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        self._check(self.lib.fn["fluid_features"](self.ctx, buf, n.value, C.byref(n)))
+        return buf.value.decode()
 
     def update_rows(self, rows, p):
         """Overwrites the kinematic state of the particles at upload indices

@@ -86,6 +86,16 @@ struct grains_gpu_ctx {
   bool tables_dirty = true;
   char* stage = nullptr;  // device staging of update / download in upload order (30 x 8 B per particle)
   char* row_scratch = nullptr;  // grains_gpu_update_particle_rows: rows, slot of every upload index
+  int fluid_corrected = 0;      // grains_gpu_set_fluid
+  // host copies of the uploaded particles for the fluid coupling's export
+  // (upload order): id, shape, mass, principal inertia, circumscribed radius,
+  // density (grains_gpu_set_fluid; else mass / volume)
+  struct {
+    std::vector<int> id, shape;
+    std::vector<double> mass, inertia, radius, density;
+  } fh;
+  double* d_hydro = nullptr;    // grains_gpu_set_hydro_forces: 6 doubles per upload index
+  bool hydro_on = false;
   bool sorted = false;      // cur arrays are in cell order for the current positions
   bool keys_valid = false;  // key and cell counts hold the cells of the current positions
   bool pending_kick2 = false;
@@ -586,6 +596,8 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   a.pair_force = c->pair_force;
   a.pair_sys = c->pair_sys;
   a.gjk_tol = c->gjk_tol;
+  a.fluid_corrected = c->fluid_corrected;
+  a.hydro = c->hydro_on ? c->d_hydro : nullptr;
   a.gjk_sv = c->gjk_sv;
   a.gjk_accel = c->gjk_accel;
   a.gjk_history = c->gjk_history;
@@ -918,6 +930,7 @@ int grains_gpu_destroy(grains_gpu_ctx* c) {
     if (c->buf[k].basis) cudaFree(c->buf[k].basis);
   if (c->stage) cudaFree(c->stage);
   if (c->row_scratch) cudaFree(c->row_scratch);
+  if (c->d_hydro) cudaFree(c->d_hydro);
   for (void* p : {(void*)c->clist, (void*)c->ccount, c->res_f, c->res_t, (void*)c->work, (void*)c->gjk_out})
     if (p) cudaFree(p);
   if (c->pbar) cudaFree(c->pbar);
@@ -1364,6 +1377,12 @@ int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
   };
   if (dbl) { vd.resize(4 * n); wd.resize(4 * n); wbfd.resize(4 * n); Id.resize(4 * n); zd.assign(4 * n, 0.); }
   else { vf.resize(4 * n); wf.resize(4 * n); wbff.resize(4 * n); If.resize(4 * n); zf.assign(4 * n, 0.f); }
+  c->fh.id.assign(n, 0);
+  c->fh.shape.assign(n, 0);
+  c->fh.mass.assign(n, 0.);
+  c->fh.inertia.assign(3 * n, 0.);
+  c->fh.radius.assign(n, 0.);
+  c->fh.density.assign(n, 0.);
   for (int64_t i = 0; i < n; ++i) {
     const ShapeHost& sh = c->shapes[p->shape[i]];
     xr[i] = make_double4(p->position[3 * i], p->position[3 * i + 1], p->position[3 * i + 2], p->radius[i]);
@@ -1375,6 +1394,12 @@ int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
     md[i] = make_double4(p->mass[i], p->crust[i], req, 0.);
     meta[i] = make_int4(p->id[i], p->material[i], p->shape[i], p->system ? p->system[i] : 0);
     orig[i] = (int)i;
+    c->fh.id[i] = p->id[i];
+    c->fh.shape[i] = p->shape[i];
+    c->fh.mass[i] = p->mass[i];
+    for (int k = 0; k < 3; ++k) c->fh.inertia[3 * i + k] = p->inertia[3 * i + k];
+    c->fh.radius[i] = p->radius[i];
+    c->fh.density[i] = p->mass[i] / vol;
     put(vd, vf, i, p->velocity[3 * i], p->velocity[3 * i + 1], p->velocity[3 * i + 2]);
     V3<double> w = v3<double>(p->omega[3 * i], p->omega[3 * i + 1], p->omega[3 * i + 2]);
     put(wd, wf, i, w.x, w.y, w.z);
@@ -1465,6 +1490,8 @@ int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
     CK(cudaStreamSynchronize(c->stream));  // the host vectors above are pageable
   }
   c->moved = 0;
+  c->fluid_corrected = 0;  // md.w (rho_f / rho_p) was uploaded as 0
+  c->hydro_on = false;
   for (int k = 0; k < 2; ++k) CK(cudaMemsetAsync(c->hist_n[k], 0, (size_t)c->cap * sizeof(int), c->stream));
   for (int k = 0; k < 2; ++k)
     if (c->gdir_n[k]) CK(cudaMemsetAsync(c->gdir_n[k], 0, (size_t)c->cap * sizeof(int), c->stream));
@@ -1598,6 +1625,321 @@ int grains_gpu_update_particle_rows(grains_gpu_ctx* c, int64_t n_rows, const int
   c->sorted = false;
   if ((rc = sort_now(c, 1))) return rc;
   return finish_call(c);
+}
+
+int grains_gpu_set_fluid(grains_gpu_ctx* c, double fluid_density, int32_t corrected,
+                         const double* particle_density) {
+  if (!c) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "upload particles first");
+  if (!(fluid_density >= 0.) || (corrected != 0 && corrected != 1))
+    return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "bad fluid density or correction flag");
+  if (fluid_density > 0. && !particle_density)
+    return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "particle densities are needed with a fluid");
+  const int64_t n = c->n;
+  std::vector<double> ratio((size_t)n, 0.);
+  for (int64_t i = 0; fluid_density > 0. && i < n; ++i) {
+    if (!(particle_density[i] > 0.)) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "particle density <= 0");
+    ratio[(size_t)i] = fluid_density / particle_density[i];  // Particle::m_fluidDensity / m_density
+  }
+  if (int rc = ensure_stage(c)) return rc;
+  CK(cudaMemcpyAsync(c->stage, ratio.data(), (size_t)n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int rc = with_args(c, [&](auto& a) { return launch_set_fluid_ratio(a, c->stream, (const double*)c->stage); });
+  if (rc) return fail(c, rc, "fluid set-up launch failed");
+  c->fluid_corrected = fluid_density > 0. ? corrected : 0;
+  if (particle_density)
+    for (int64_t i = 0; i < n; ++i) c->fh.density[(size_t)i] = particle_density[i];
+  drop_graphs(c);
+  return finish_call(c);
+}
+
+int grains_gpu_set_velocities(grains_gpu_ctx* c, const double* velocity, const double* omega) {
+  if (!c || !velocity || !omega) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "upload particles first");
+  if (int rc = ensure_stage(c)) return rc;
+  if (int rc = flush_kick(c)) return rc;
+  const int64_t n = c->n;
+  double* d = (double*)c->stage;
+  CK(cudaMemcpyAsync(d, velocity, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(d + 3 * n, omega, 3 * n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  int rc = with_args(c, [&](auto& a) { return launch_set_velocities(a, c->stream, d, d + 3 * n); });
+  if (rc) return fail(c, rc, "velocity launch failed");
+  return finish_call(c);
+}
+
+int grains_gpu_fluid_step(grains_gpu_ctx* c, double dt_fluid, double min_dt, double max_dt, int64_t* ndt,
+                          double* time) {
+  if (!c || !ndt || !time || !(dt_fluid > 0.) || !(min_dt > 0.) || !(max_dt >= min_dt) || *ndt < 1)
+    return GRAINS_GPU_INVALID_ARGUMENT;
+  // GrainsCoupledWithFluid::Simulation (Fluid/src/GrainsCoupledWithFluid.cpp:
+  // 123-135): the DEM steps of one fluid step, from the previous count
+  const double dteff = std::max(std::min(max_dt, dt_fluid / double(*ndt)), min_dt);
+  const int64_t m = (int64_t)(size_t)(dt_fluid / dteff);
+  if (m < 1) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "fluid step shorter than the DEM step");
+  *ndt = m;
+  const double dt = dt_fluid / double(m);
+  int64_t done = 0;
+  while (done < m) {  // grains_gpu_step takes an int32 count
+    const int32_t k = (int32_t)std::min<int64_t>(m - done, 1 << 30);
+    if (int rc = grains_gpu_step(c, k, time, dt)) return rc;
+    done += k;
+  }
+  return 0;
+}
+
+namespace {
+// GrainsExec::doubleToString(ios::scientific, FORMAT16DIGITS, x): scientific
+// with 16 digits, a zero as the stream prints it
+void put_sci(std::string& o, double x) {
+  char b[64];
+  if (x == 0.)
+    std::snprintf(b, sizeof(b), "%s", std::signbit(x) ? "-0" : "0");
+  else
+    std::snprintf(b, sizeof(b), "%.16e", x);
+  o += b;
+  o += ' ';
+}
+void put_int(std::string& o, long long k) {
+  o += std::to_string(k);
+  o += ' ';
+}
+}  // namespace
+
+int grains_gpu_fluid_features(grains_gpu_ctx* c, char* buf, int64_t cap, int64_t* len) {
+  if (!c || !len) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "upload particles first");
+  const int64_t n = c->n;
+  std::vector<double> pos(3 * n), quat(4 * n), basis(9 * n), vel(3 * n), om(3 * n);
+  grains_gpu_particles p{};
+  p.n = n;
+  p.position = pos.data();
+  p.quaternion = quat.data();
+  p.basis = basis.data();
+  p.velocity = vel.data();
+  p.omega = om.data();
+  if (int rc = grains_gpu_download_particles(c, &p)) return rc;
+  std::vector<int64_t> order(n);
+  for (int64_t i = 0; i < n; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return c->fh.id[a] < c->fh.id[b]; });
+  // GrainsCoupledWithFluid::GrainsToFluid (Fluid/src/GrainsCoupledWithFluid.cpp:
+  // 912-1120), as GrainsToBasilisk tokenises it (InterfaceGrains3DBasilisk.cpp:
+  // 64-87): every token followed by one space
+  std::string o;
+  put_int(o, n);
+  for (int64_t k = 0; k < n; ++k) {
+    const int64_t i = order[k];
+    const ShapeHost& sh = c->shapes[c->fh.shape[i]];
+    const double* B = basis.data() + 9 * i;
+    // Particle::computeInertiaTensorSpaceFixed (Particle.cpp:1798-1822):
+    // Mr (I_body Mr^t), matrix products summed in index order
+    double Ib[9] = {c->fh.inertia[3 * i], 0., 0., 0., c->fh.inertia[3 * i + 1], 0., 0., 0., c->fh.inertia[3 * i + 2]};
+    double Bt[9], T1[9], Is[9];
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < 3; ++q) Bt[3 * r + q] = B[3 * q + r];
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < 3; ++q)
+        T1[3 * r + q] = Ib[3 * r] * Bt[q] + Ib[3 * r + 1] * Bt[3 + q] + Ib[3 * r + 2] * Bt[6 + q];
+    for (int r = 0; r < 3; ++r)
+      for (int q = 0; q < 3; ++q)
+        Is[3 * r + q] = B[3 * r] * T1[q] + B[3 * r + 1] * T1[3 + q] + B[3 * r + 2] * T1[6 + q];
+    // corners code and envelope (Convex::getNbCorners / getEnvelope / getFaces)
+    std::vector<double> env;
+    const std::vector<std::vector<int>>* faces = nullptr;
+    static const std::vector<std::vector<int>> box_faces = {{4, 5, 6, 7}, {5, 1, 2, 6}, {1, 0, 3, 2},
+                                                            {0, 4, 7, 3}, {4, 0, 1, 5}, {3, 7, 6, 2}};
+    long long corners = 1;
+    if (sh.type == GRAINS_GPU_SPHERE) {
+      env = {0., 0., 0.};
+    } else if (sh.type == GRAINS_GPU_BOX) {  // Box::setCornersFaces (Box.cpp:92-148)
+      const double ex = sh.ext.x, ey = sh.ext.y, ez = sh.ext.z;
+      env = {-ex, -ey, -ez, ex, -ey, -ez, ex, -ey, ez, -ex, -ey, ez, -ex, ey, -ez, ex, ey, -ez, ex, ey, ez, -ex, ey, ez};
+      faces = &box_faces;
+      corners = 666;
+    } else if (sh.type == GRAINS_GPU_CYLINDER) {  // Cylinder::getEnvelope (Cylinder.cpp:142-152)
+      env = {0., -sh.half_height, 0., sh.radius, -sh.half_height, 0., 0., sh.half_height, 0.};
+      corners = 777;
+    } else {  // Polytope::getEnvelope, the polyhedron's faces
+      env = sh.verts;
+      faces = &sh.faces;
+      corners = (long long)sh.verts.size() / 3;
+    }
+    put_int(o, k);
+    put_int(o, corners);
+    o += "P ";
+    for (int t = 0; t < 3; ++t) put_sci(o, vel[3 * i + t]);
+    for (int t = 0; t < 3; ++t) put_sci(o, om[3 * i + t]);
+    put_sci(o, c->fh.density[i]);
+    put_sci(o, c->fh.mass[i]);
+    put_sci(o, Is[0]);
+    put_sci(o, Is[1]);
+    put_sci(o, Is[2]);
+    put_sci(o, Is[4]);
+    put_sci(o, Is[5]);
+    put_sci(o, Is[8]);
+    for (int t = 0; t < 9; ++t) put_sci(o, B[t]);
+    for (int t = 0; t < 3; ++t) put_sci(o, pos[3 * i + t]);
+    char rb[64];  // the circumscribed radius as the stream prints a double by default
+    std::snprintf(rb, sizeof(rb), "%g", sh.type == GRAINS_GPU_SPHERE ? c->fh.radius[i] : sh.circ);
+    o += rb;
+    o += ' ';
+    // RigidBody::writePositionInFluid (Geometry/src/RigidBody.cpp:445-497)
+    const size_t np = env.size() / 3;
+    put_int(o, (long long)np);
+    for (size_t t = 0; t < np; ++t) {
+      const double x = env[3 * t], y = env[3 * t + 1], z = env[3 * t + 2];
+      put_sci(o, B[0] * x + B[1] * y + B[2] * z + pos[3 * i]);
+      put_sci(o, B[3] * x + B[4] * y + B[5] * z + pos[3 * i + 1]);
+      put_sci(o, B[6] * x + B[7] * y + B[8] * z + pos[3 * i + 2]);
+    }
+    if (faces) {
+      put_int(o, (long long)faces->size());
+      for (const auto& f : *faces) {
+        put_int(o, (long long)f.size());
+        for (int v : f) put_int(o, v);
+      }
+    } else {
+      put_int(o, 0);
+    }
+  }
+  *len = (int64_t)o.size() + 1;
+  if (buf) {
+    if (cap < *len) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "buffer too small for the features");
+    std::memcpy(buf, o.c_str(), o.size() + 1);
+  }
+  return 0;
+}
+
+int grains_gpu_set_hydro_forces(grains_gpu_ctx* c, const double* force, const double* torque) {
+  if (!c) return GRAINS_GPU_INVALID_ARGUMENT;
+  if (!c->uploaded) return fail(c, GRAINS_GPU_NOT_READY, "upload particles first");
+  const bool on = force || torque;
+  if (on) {
+    if (!c->d_hydro) {
+      void* q = nullptr;
+      CK(cudaMalloc(&q, (size_t)c->cap * 6 * sizeof(double)));
+      c->d_hydro = (double*)q;
+    }
+    const int64_t n = c->n;
+    std::vector<double> h((size_t)n * 6, 0.);
+    for (int64_t i = 0; i < n; ++i)
+      for (int k = 0; k < 3; ++k) {
+        if (force) h[6 * i + k] = force[3 * i + k];
+        if (torque) h[6 * i + 3 + k] = torque[3 * i + k];
+      }
+    CK(cudaMemcpyAsync(c->d_hydro, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));  // h is pageable
+  }
+  if (on != c->hydro_on) drop_graphs(c);
+  c->hydro_on = on;
+  return 0;
+}
+
+// ---- the fluid solvers' C interface (InterfaceGrains3DBasilisk.h:12-30) ----
+// The reference keeps one coupled simulation in a static (InterfaceGrains3DBasilisk
+// .cpp:16) built by Init_Grains from its XML and reload files; here the caller
+// sets up a context through the grains_gpu calls and attaches it, and the
+// interface drives that context.
+namespace {
+struct BasiliskState {
+  grains_gpu_ctx* ctx = nullptr;
+  double min_dt = 0., max_dt = 0.;
+  int64_t ndt = 1;
+  double time = 0.;
+  int cycle = 0;
+};
+BasiliskState g_basilisk;
+
+[[noreturn]] void basilisk_abort(const char* where, const std::string& why) {
+  // the reference ends the run on a set-up or simulation error (grainsAbort)
+  std::fprintf(stderr, "%s: %s\n", where, why.c_str());
+  std::exit(1);
+}
+void basilisk_check(const char* where, int rc) {
+  if (rc) {
+    char m[512] = {0};
+    if (g_basilisk.ctx) grains_gpu_last_error(g_basilisk.ctx, m, sizeof(m));
+    basilisk_abort(where, m[0] ? m : "grains_gpu error");
+  }
+}
+grains_gpu_ctx* basilisk_ctx(const char* where) {
+  if (!g_basilisk.ctx) basilisk_abort(where, "no context attached (grains_gpu_basilisk_attach)");
+  return g_basilisk.ctx;
+}
+}  // namespace
+
+int grains_gpu_basilisk_attach(grains_gpu_ctx* c, double min_dt, double max_dt, int64_t ndt) {
+  if (!c || !(min_dt > 0.) || !(max_dt >= min_dt) || ndt < 1) return GRAINS_GPU_INVALID_ARGUMENT;
+  g_basilisk = BasiliskState();
+  g_basilisk.ctx = c;
+  g_basilisk.min_dt = min_dt;
+  g_basilisk.max_dt = max_dt;
+  g_basilisk.ndt = ndt;
+  return 0;
+}
+
+void Init_Grains(char const* inputfile, double fluid_rho, const bool b_restart, const bool b_fluidcorrectedacc) {
+  (void)inputfile;
+  (void)b_restart;
+  grains_gpu_ctx* c = basilisk_ctx("Init_Grains");
+  // GrainsCoupledWithFluid(fluid_density) and setFluidCorrectedAcceleration
+  // (InterfaceGrains3DBasilisk.cpp:28-48), then the leapfrog start
+  basilisk_check("Init_Grains", grains_gpu_set_fluid(c, fluid_rho, b_fluidcorrectedacc ? 1 : 0, c->fh.density.data()));
+  basilisk_check("Init_Grains", grains_gpu_initialize_leapfrog(c, g_basilisk.time, g_basilisk.min_dt));
+}
+
+void Simu_Grains(const double dt_fluid) {
+  grains_gpu_ctx* c = basilisk_ctx("Simu_Grains");
+  basilisk_check("Simu_Grains", grains_gpu_fluid_step(c, dt_fluid, g_basilisk.min_dt, g_basilisk.max_dt,
+                                                      &g_basilisk.ndt, &g_basilisk.time));
+}
+
+char* GrainsToBasilisk(int* pstrsize) {
+  grains_gpu_ctx* c = basilisk_ctx("GrainsToBasilisk");
+  int64_t len = 0;
+  basilisk_check("GrainsToBasilisk", grains_gpu_fluid_features(c, nullptr, 0, &len));
+  char* out = (char*)std::malloc((size_t)len);
+  if (!out) basilisk_abort("GrainsToBasilisk", "out of host memory");
+  basilisk_check("GrainsToBasilisk", grains_gpu_fluid_features(c, out, len, &len));
+  if (pstrsize) *pstrsize = (int)len;
+  return out;
+}
+
+void SetInitialTime(double tinit) { g_basilisk.time = tinit; }
+
+void SetInitialCycleNumber(int cycle0) { g_basilisk.cycle = cycle0; }
+
+void SaveResults_Grains() { ++g_basilisk.cycle; }
+
+void checkParaviewPostProcessing_Grains(char* solid_resDir) { (void)solid_resDir; }
+
+void UpdateVelocityGrains(double** arrayv, const int m) {
+  grains_gpu_ctx* c = basilisk_ctx("UpdateVelocityGrains");
+  const int64_t n = c->n;
+  if (m != n) basilisk_abort("UpdateVelocityGrains", "the fluid holds another number of particles");
+  std::vector<double> pos(3 * n), quat(4 * n), vel(3 * n), om(3 * n);
+  grains_gpu_particles p{};
+  p.n = n;
+  p.position = pos.data();
+  p.quaternion = quat.data();
+  p.velocity = vel.data();
+  p.omega = om.data();
+  basilisk_check("UpdateVelocityGrains", grains_gpu_download_particles(c, &p));
+  // GrainsCoupledWithFluid::updateParticlesVelocity (GrainsCoupledWithFluid.cpp:
+  // 1126-1185): row k of the fluid's array is the particle of the k-th id
+  std::vector<int64_t> order(n);
+  for (int64_t i = 0; i < n; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](int64_t a, int64_t b) { return c->fh.id[a] < c->fh.id[b]; });
+  for (int64_t k = 0; k < n; ++k)
+    for (int t = 0; t < 3; ++t) {
+      vel[3 * order[k] + t] = arrayv[k][t];
+      om[3 * order[k] + t] = arrayv[k][3 + t];
+    }
+  basilisk_check("UpdateVelocityGrains", grains_gpu_set_velocities(c, vel.data(), om.data()));
+}
+
+void NumberOfRigidBodiesInBasilisk(size_t* nparticles, size_t* nobstacles) {
+  grains_gpu_ctx* c = basilisk_ctx("NumberOfRigidBodiesInBasilisk");
+  *nparticles = (size_t)c->n;
+  *nobstacles = 0;
 }
 
 int grains_gpu_upload_contact_memory(grains_gpu_ctx* c, const grains_gpu_contact_memory* m) {

@@ -209,6 +209,8 @@ struct StepArgs {
   double* pair_force;    // diagnostic: force on the lower id of each contact pair (3 doubles) or null
   int* pair_sys;         // diagnostic: system of each contact pair
   double gjk_tol;
+  int fluid_corrected;   // immersed particles: accelerations divided by 1 - rho_f / rho_p (md.w = rho_f / rho_p)
+  const double* hydro;   // per upload index: the fluid's force and torque (6 doubles), or null
   int gjk_sv;            // the signed-volume GJK for non-spherical pairs
   int gjk_accel;         // Nesterov-accelerated GJK directions (<CollisionDetection Acceleration="ON">)
   int gjk_history;       // warm-started GJK from the pair's collision history (History="ON")
@@ -251,6 +253,12 @@ struct DownloadStage {
 };
 template <typename R>
 int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const KinematicStage& st);
+// velocities and angular velocities (world, upload order) of every particle
+template <typename R>
+int launch_set_velocities(const StepArgs<R>& a, cudaStream_t s, const double* vel, const double* omega);
+// md.w = rho_f / rho_p of every particle from ratio (upload order)
+template <typename R>
+int launch_set_fluid_ratio(const StepArgs<R>& a, cudaStream_t s, const double* ratio);
 // the kinematic state of the upload indices rows[0 .. n_rows) from stage
 // entries 0 .. n_rows (slot_of: n ints of scratch)
 template <typename R>

@@ -75,18 +75,18 @@ __device__ __forceinline__ int cell_index(const SysDev& S, int i, int j, int k) 
 // Angular acceleration in the body frame (ParticleKinematicsSphere.cpp:47-54,
 // ParticleKinematics3D.cpp:56-75 with predictor mode on, Grains.cpp:18)
 template <typename R>
-__device__ __forceinline__ V3<R> dwdt(bool sphere, V3<R> I, V3<R> Tbf, V3<R> om) {
-  if (sphere) return v3<R>(Tbf.x / (R(1) * I.x), Tbf.y / (R(1) * I.y), Tbf.z / (R(1) * I.z));
-  return v3<R>(Tbf.x / (R(1) * I.x) + om.y * om.z * (I.y - I.z) / I.x,
-               Tbf.y / (R(1) * I.y) + om.z * om.x * (I.z - I.x) / I.y,
-               Tbf.z / (R(1) * I.z) + om.x * om.y * (I.x - I.y) / I.z);
+__device__ __forceinline__ V3<R> dwdt(bool sphere, V3<R> I, V3<R> Tbf, V3<R> om, R cf) {
+  if (sphere) return v3<R>(Tbf.x / (cf * I.x), Tbf.y / (cf * I.y), Tbf.z / (cf * I.z));
+  return v3<R>(Tbf.x / (cf * I.x) + om.y * om.z * (I.y - I.z) / I.x,
+               Tbf.y / (cf * I.y) + om.z * om.x * (I.z - I.x) / I.y,
+               Tbf.z / (cf * I.z) + om.x * om.y * (I.x - I.y) / I.z);
 }
 // SSP-RK3 of SecondOrderLeapFrog::Move / advanceVelocity (SecondOrderLeapFrog.cpp:55-68)
 template <typename R>
-__device__ __forceinline__ V3<R> rk3(bool sphere, V3<R> I, V3<R> Tbf, V3<R> wbf, R dt) {
-  V3<R> K1 = sc(dwdt(sphere, I, Tbf, wbf), dt);
-  V3<R> K2 = sc(dwdt(sphere, I, Tbf, wbf + K1), dt);
-  V3<R> K3 = sc(dwdt(sphere, I, Tbf, wbf + sc(K1 + K2, R(0.25))), dt);
+__device__ __forceinline__ V3<R> rk3(bool sphere, V3<R> I, V3<R> Tbf, V3<R> wbf, R dt, R cf) {
+  V3<R> K1 = sc(dwdt(sphere, I, Tbf, wbf, cf), dt);
+  V3<R> K2 = sc(dwdt(sphere, I, Tbf, wbf + K1, cf), dt);
+  V3<R> K3 = sc(dwdt(sphere, I, Tbf, wbf + sc(K1 + K2, R(0.25)), cf), dt);
   return wbf + dv((K1 + K2) + sc(K3, R(4)), R(6));
 }
 
@@ -108,19 +108,23 @@ __device__ __forceinline__ void integrate(const StepArgs<R>& a, const ParticleAr
   const V3<R> I = ld3<R>(src.inertia[s]);
   const bool sphere = a.shapes[meta.z].type == 0;
   const R mass = R(md.x);
+  // the coupling factor of an immersed particle (ParticleKinematics::
+  // setCouplingFactor, ParticleKinematics.cpp:483-488): 1 - rho_f / rho_p when
+  // the acceleration is corrected, else 1 (md.w = rho_f / rho_p, 0 in air)
+  const R cf = a.fluid_corrected ? R(1. - md.w) : R(1);
   Qt<double> q{v3<double>(qd.x, qd.y, qd.z), qd.w};
   const Qt<R> qr{v3<R>(R(qd.x), R(qd.y), R(qd.z)), R(qd.w)};
   if (do_kick2) {
     V3<R> Tbf = q_to_body(qr, T);
-    v = v + sc(dv(F, mass * R(1)), dt_kick2);
-    wbf = rk3(sphere, I, Tbf, wbf, dt_kick2);
+    v = v + sc(dv(F, mass * cf), dt_kick2);
+    wbf = rk3(sphere, I, Tbf, wbf, dt_kick2, cf);
     w = q_to_world(qr, wbf);
   }
   if (do_move) {
     V3<R> Tbf = q_to_body(qr, T);
-    v = v + sc(dv(F, mass * R(1)), dt_v);
+    v = v + sc(dv(F, mass * cf), dt_v);
     V3<double> tm = sc(v3<double>(double(v.x), double(v.y), double(v.z)), dt_x);
-    wbf = rk3(sphere, I, Tbf, wbf, dt_v);
+    wbf = rk3(sphere, I, Tbf, wbf, dt_v, cf);
     w = q_to_world(qr, wbf);
     V3<R> meanw = w;
     xr.x = xr.x + tm.x;
@@ -1303,7 +1307,9 @@ template <typename R>
 __device__ __forceinline__ void sum_one(const StepArgs<R>& a, int s) {
   const ParticleArrays<R>& P = a.cur;
   const int sysi = P.meta[s].w;
-  const double mass = P.md[s].x;
+  const double4 md = P.md[s];
+  // Particle::computeWeight (Particle.cpp:414-419): mass * (1 - rho_f / rho_p) * g
+  const double mass = md.x * (1. - md.w);
   const int row = P.orig[s];
   const SysDev& S = a.sys[sysi];
   V3<R> F = v3<R>(R(S.gx * mass), R(S.gy * mass), R(S.gz * mass));
@@ -1340,6 +1346,14 @@ __device__ __forceinline__ void sum_one(const StepArgs<R>& a, int s) {
       T = T + ld3<R>(rt[u]);
       ++ncontact;
     }
+  }
+  if (a.hydro) {
+    // AppPRSHydroFT::ComputeForces (Fluid/src/AppPRSHydroFT.cpp:29-45): the
+    // fluid's force and torque, after the contacts (the collision App comes
+    // first in Grains::m_allApp)
+    const double* h = a.hydro + 6 * (size_t)row;
+    F = F + v3<R>(R(h[0]), R(h[1]), R(h[2]));
+    T = T + v3<R>(R(h[3]), R(h[4]), R(h[5]));
   }
   a.coord[s] = ncontact;
   a.hist_n_next[row] = kept;
@@ -1398,6 +1412,31 @@ __global__ void update_dynamic_kernel(StepArgs<R> a, KinematicStage st) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= a.n) return;
   set_kinematics(a, s, st, (size_t)a.cur.orig[s]);
+}
+
+// translational and angular velocities (world frame, upload order) of every
+// particle; the body-frame angular velocity follows from the quaternion
+// (ParticleKinematics::setAngularVelocity, ParticleKinematics.cpp:197-203)
+template <typename R>
+__global__ void set_velocities_kernel(StepArgs<R> a, const double* vel, const double* omega) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const ParticleArrays<R>& P = a.cur;
+  const size_t i = (size_t)P.orig[s];
+  P.v[s] = st3<R>(v3<R>(R(vel[3 * i]), R(vel[3 * i + 1]), R(vel[3 * i + 2])));
+  const double4 qd = P.q[s];
+  Qt<double> q{v3<double>(qd.x, qd.y, qd.z), qd.w};
+  V3<double> w = v3<double>(omega[3 * i], omega[3 * i + 1], omega[3 * i + 2]);
+  P.w[s] = st3<R>(v3<R>(R(w.x), R(w.y), R(w.z)));
+  V3<double> wbf = q_to_body(q, w);
+  P.wbf[s] = st3<R>(v3<R>(R(wbf.x), R(wbf.y), R(wbf.z)));
+}
+
+// rho_f / rho_p of every particle (upload order) into md.w of the current arrays
+template <typename R>
+__global__ void set_fluid_ratio_kernel(StepArgs<R> a, const double* ratio) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < a.n) a.cur.md[s].w = ratio[a.cur.orig[s]];
 }
 
 // slot of every upload index (the inverse of orig)
@@ -1836,6 +1875,20 @@ int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const KinematicS
 }
 
 template <typename R>
+int launch_set_velocities(const StepArgs<R>& a, cudaStream_t s, const double* vel, const double* omega) {
+  if (a.n == 0) return 0;
+  set_velocities_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, vel, omega);
+  return check_launch();
+}
+
+template <typename R>
+int launch_set_fluid_ratio(const StepArgs<R>& a, cudaStream_t s, const double* ratio) {
+  if (a.n == 0) return 0;
+  set_fluid_ratio_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, ratio);
+  return check_launch();
+}
+
+template <typename R>
 int launch_update_rows(const StepArgs<R>& a, cudaStream_t s, const KinematicStage& st, const long long* rows,
                        long long n_rows, int* slot_of) {
   if (a.n == 0 || n_rows == 0) return 0;
@@ -2033,6 +2086,8 @@ int launch_persistent_steps(const StepArgs<R>& a, cudaStream_t s, int n_steps, d
   template int launch_forces<R>(const StepArgs<R>&, cudaStream_t, double, int, int);                       \
   template int launch_zero_kdelta<R>(const StepArgs<R>&, cudaStream_t);                                    \
   template int launch_update_dynamic<R>(const StepArgs<R>&, cudaStream_t, const KinematicStage&);             \
+  template int launch_set_fluid_ratio<R>(const StepArgs<R>&, cudaStream_t, const double*);                     \
+  template int launch_set_velocities<R>(const StepArgs<R>&, cudaStream_t, const double*, const double*);      \
   template int launch_update_rows<R>(const StepArgs<R>&, cudaStream_t, const KinematicStage&, const long long*,  \
                                      long long, int*);                                                      \
   template int launch_pack_download<R>(const StepArgs<R>&, cudaStream_t, const DownloadStage&);              \

@@ -17,7 +17,12 @@ GPU_ONLY = {"get_stream", "synchronize", "launches_per_step", "set_barrier_test"
             "sphere_contacts_noalloc", "adjoint_create", "adjoint_destroy", "adjoint_last_error",
             "adjoint_law_slots", "adjoint_forward", "adjoint_contact_signature", "adjoint_backward",
             "get_tuning", "set_tuning", "autotune", "reload_open", "reload_last_error", "reload_get",
-            "reload_close", "format_double", "format_doubles"}
+            "reload_close", "format_double", "format_doubles", "basilisk_attach", "fluid_step", "fluid_features"}
+# the fluid solvers' C interface (same names as the reference's
+# InterfaceGrains3DBasilisk.h), exported by the CUDA library
+BASILISK = ["Init_Grains", "Simu_Grains", "GrainsToBasilisk", "SetInitialTime", "SaveResults_Grains",
+            "checkParaviewPostProcessing_Grains", "UpdateVelocityGrains", "SetInitialCycleNumber",
+            "NumberOfRigidBodiesInBasilisk"]
 
 
 def declared():
@@ -61,6 +66,10 @@ def test_cuda_library_exports_every_declared_symbol():
     dll = ctypes.CDLL(pacific_b200.LIB_PATH)
     for n in declared():
         assert hasattr(dll, "grains_gpu_" + n), n
+    txt = open(HEADER).read()
+    for n in BASILISK:
+        assert re.search(r"\b%s\s*\(" % n, txt), n
+        assert hasattr(dll, n), n
 
 
 def test_oracle_exports_the_same_contract(oracle_lib):
