@@ -64,9 +64,13 @@ def kernel_bytes(kernel, precision, z, basis=False):
         return 32 + 16 + 4 + 72 + 4 + 4 * z + 8 * z / 2.0
     if kernel == "pairs":
         return 84 + 2 * r4 + 4 * z + 8 * z / 2.0 + 2 * (z / 2.0) * entry + 2 * r4 * z
+    kick = (32 + 32 + 16 + 32 + 6 * r4) + (64 + 3 * r4 + 8) + (144 if basis else 0)
+    sums = 56 + 4 * z + 2 * r4 * z + 2 * r4 + 8 + (z / 2.0) * entry
     if kernel == "sums":
-        return 56 + 4 * z + 2 * r4 * z + 2 * r4 + 8 + (z / 2.0) * entry
-    return (32 + 32 + 16 + 32 + 6 * r4) + (64 + 3 * r4 + 8) + (144 if basis else 0)
+        return sums
+    if kernel == "sums_kick":  # the sums with the kick: the torsor stays in registers
+        return sums - 2 * r4 + kick - 2 * r4
+    return kick
 
 
 def parse():
@@ -345,7 +349,8 @@ def profile_run(sim, sc, n_steps, t):
 
 def roofline(prof_tot, sc, precision, z, peak, peak_kind, traffic_of):
     from pacific_b200 import scenarios as S
-    dom = max(["contacts", "pairs", "sums", "kick_move"], key=lambda k: prof_tot[k][0])
+    dom = max([k for k in ["contacts", "pairs", "sums", "sums_kick", "kick_move"] if k in prof_tot],
+              key=lambda k: prof_tot[k][0])
     k_ms, k_n = prof_tot[dom]
     basis = any(sc.shapes[k][0] != S.SPHERE for k in set(np.asarray(sc.particles["shape"]).tolist()))
     alg = sc.n * kernel_bytes(dom, precision, z, basis)

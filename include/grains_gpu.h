@@ -456,7 +456,10 @@ int grains_gpu_autotune(grains_gpu_ctx* ctx, double time, double dt, int32_t tri
 
 /* ---- timing helpers for benchmarks ---------------------------------------- */
 /* Times each phase of n_steps uncaptured steps with CUDA events on the
- * context stream: first_move, sort_gather, contacts, pairs, sums, kick_move.
+ * context stream: first_move, sort_gather, contacts, pairs (with the GJK
+ * kernel of convex scenarios), sums_kick (the per-particle sums with the
+ * second half kick and the next step's first half kick, drift and binning),
+ * obstacle_move (the moving obstacles' kernel).
  * names: '\n'-separated phase names (cap bytes); ms[k]: total milliseconds of
  * phase k; launches[k]: its kernel launches. */
 int grains_gpu_profile_kernels(grains_gpu_ctx* ctx, int32_t n_steps, double* time, double dt,
@@ -470,8 +473,8 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* ctx, int32_t n_steps, double* tim
  * usable (upload the state again before stepping on). */
 int grains_gpu_set_barrier_test(grains_gpu_ctx* ctx, int64_t polls, int32_t skip_block);
 /* Kernel launches of one middle step of grains_gpu_step: the cell sort (4),
- * contacts, pairs, sums, kick_move, and the obstacle move when obstacles
- * move.  The permutation of the arrays into cell order adds one launch every
+ * contacts, the GJK kernel (convex scenarios, Johnson's GJK), pairs, the sums
+ * with the kick, and the obstacle move when obstacles move.  The permutation of the arrays into cell order adds one launch every
  * gather_every steps (grains_gpu_tuning). */
 int grains_gpu_launches_per_step(grains_gpu_ctx* ctx, int64_t* launches);
 

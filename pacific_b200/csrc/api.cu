@@ -683,11 +683,11 @@ int flush_kick(grains_gpu_ctx* c) {
   return rc ? fail(c, rc, "advance-velocity launch failed") : 0;
 }
 
-int forces_now(grains_gpu_ctx* c, double dt, int diag, int phases = 7) {
+int forces_now(grains_gpu_ctx* c, double dt, int diag, int phases = 7, int kick = 0) {
   if (!c->sorted) {
     if (int rc = sort_now(c, 1)) return rc;
   }
-  int rc = with_args(c, [&](auto& a) { return launch_forces(a, c->stream, dt, diag, phases); });
+  int rc = with_args(c, [&](auto& a) { return launch_forces(a, c->stream, dt, diag, phases, kick); });
   if (rc) return fail(c, rc, "force kernel launch failed");
   if (phases & 4) c->hcur = 1 - c->hcur;
   return 0;
@@ -718,17 +718,15 @@ int first_move(grains_gpu_ctx* c, double dt, double time) {
   return move_obstacles(c, dt, 1, time + dt);
 }
 
-// A middle step: sort, contact lists, contact law, then the rest of the step
-// (second half kick) with the next step's first half kick and drift in one
-// kernel, which also bins the moved particles.  (Folding that kick into the
-// contact-law kernel was measured 14-15 % slower per step on 200,000 spheres:
-// the combined kernel's registers and serial memory chain cost more than the
-// extra pass over the state.)
+// A middle step: sort, contact lists, contact law, then the per-particle sums
+// with the rest of the step (second half kick) and the next step's first half
+// kick, drift and binning in the same kernel.  (Folding that kick into the
+// contact-law kernel of an earlier design, one thread per particle evaluating
+// every contact, was 14-15 % slower per step on 200,000 spheres; the sums
+// kernel is light, and the fold saves the torsor's round trip and a launch.)
 int middle_step(grains_gpu_ctx* c, double dt) {
   if (int rc = sort_for_step(c)) return rc;
-  if (int rc = forces_now(c, dt, 0)) return rc;
-  int rc = with_args(c, [&](auto& a) { return launch_kick_move(a, c->stream, 1, 0.5 * dt, 1, 0.5 * dt, dt); });
-  if (rc) return fail(c, rc, "kick/move launch failed");
+  if (int rc = forces_now(c, dt, 0, 7, 1)) return rc;
   c->keys_valid = true;
   c->sorted = false;
   return move_obstacles(c, dt);
@@ -2372,9 +2370,10 @@ int grains_gpu_set_barrier_test(grains_gpu_ctx* c, int64_t polls, int32_t skip_b
 int grains_gpu_launches_per_step(grains_gpu_ctx* c, int64_t* launches) {
   if (!c || !launches) return GRAINS_GPU_INVALID_ARGUMENT;
   // a middle step: scan_tiles, scan_finish, scatter, cell_sort, contacts,
-  // pairs, sums, kick_move, and the obstacle move when obstacles move; the
-  // gather runs one step in gather_every on top
-  *launches = launches_per_middle_step() + (c->n_moving > 0 ? 1 : 0);
+  // (the GJK kernel of convex scenarios,) pairs, sums with the kick, and the
+  // obstacle move when obstacles move; the gather runs one step in
+  // gather_every on top
+  *launches = launches_per_middle_step() + (c->has_convex && !c->gjk_sv ? 1 : 0) + (c->n_moving > 0 ? 1 : 0);
   return 0;
 }
 
@@ -2389,7 +2388,7 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time,
   // same schedule as grains_gpu_step, uncaptured, with events around each phase
   cudaEvent_t ev[7];
   for (auto& e : ev) CK(cudaEventCreate(&e));
-  double acc[6] = {0, 0, 0, 0, 0, 0};  // first move, sort+gather, contact lists, pair law, sums, kick/move
+  double acc[6] = {0, 0, 0, 0, 0, 0};  // first move, sort+gather, contact lists, pair law, sums with the kick, obstacle moves
   int64_t cnt[6] = {0, 0, 0, 0, 0, 0};
   CK(cudaEventRecord(ev[0], c->stream));
   if (int rc = first_move(c, dt, *time)) return rc;
@@ -2408,11 +2407,9 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time,
     CK(cudaEventRecord(ev[3], c->stream));
     if (int rc = forces_now(c, dt, 0, 2)) return rc;
     CK(cudaEventRecord(ev[4], c->stream));
-    if (int rc = forces_now(c, dt, 0, 4)) return rc;
+    if (int rc = forces_now(c, dt, 0, 4, last ? 0 : 1)) return rc;  // sums with the kick (a middle step)
     CK(cudaEventRecord(ev[5], c->stream));
     if (!last) {
-      int rc = with_args(c, [&](auto& a) { return launch_kick_move(a, c->stream, 1, 0.5 * dt, 1, 0.5 * dt, dt); });
-      if (rc) return fail(c, rc, "kick/move launch failed");
       c->keys_valid = true;
       c->sorted = false;
       if (int rc2 = move_obstacles(c, dt)) return rc2;
@@ -2426,14 +2423,13 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time,
     cnt[2] += 1;
     cnt[3] += 1;
     cnt[4] += 1;
-    if (!last) cnt[5] += 1;
   }
   c->pending_kick2 = true;
   c->pending_dt = 0.5 * dt;
   for (auto& e : ev) cudaEventDestroy(e);
   for (int k = 0; k < n_steps; ++k) *time += dt;
   c->steps_done += n_steps;
-  std::snprintf(names, cap, "first_move\nsort_gather\ncontacts\npairs\nsums\nkick_move");
+  std::snprintf(names, cap, "first_move\nsort_gather\ncontacts\npairs\nsums_kick\nobstacle_move");
   const int nk = max_kernels < 6 ? max_kernels : 6;
   for (int k = 0; k < nk; ++k) {
     ms[k] = acc[k];
@@ -2698,7 +2694,7 @@ int grains_gpu_autotune(grains_gpu_ctx* c, double time, double dt, int32_t trial
 }  // extern "C"
 
 namespace gg {
-int launches_per_middle_step() { return 8; }
+int launches_per_middle_step() { return 7; }
 
 int context_view(grains_gpu_ctx* c, ContextView* v, std::string& err) {
   if (!c || !v) return GRAINS_GPU_INVALID_ARGUMENT;

@@ -239,7 +239,9 @@ template <typename R>
 int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather, int gather_forces);
 // phases (bits): 1 = contact lists, 2 = pair narrowphase and law, 4 = per-particle sums
 template <typename R>
-int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int phases = 7);
+// kick != 0: the sums kernel also applies the second half kick and the next
+// step's first half kick, drift and binning (a middle step)
+int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int phases = 7, int kick = 0);
 template <typename R>
 int launch_zero_kdelta(const StepArgs<R>& a, cudaStream_t s);
 // device arrays in upload order of grains_gpu_update_particles (basis may be null)

@@ -1304,7 +1304,8 @@ __global__ void __launch_bounds__(128, CONVEX ? 1 : GG_PAIRS_MIN_BLOCKS) pairs_k
 // entries move down over the holes (rows without holes are not touched).  The
 // results of four entries are loaded at a time.
 template <typename R>
-__device__ __forceinline__ void sum_one(const StepArgs<R>& a, int s) {
+__device__ __forceinline__ void sum_one(const StepArgs<R>& a, int s, V3<R>* f_out = nullptr,
+                                        V3<R>* t_out = nullptr) {
   const ParticleArrays<R>& P = a.cur;
   const int sysi = P.meta[s].w;
   const double4 md = P.md[s];
@@ -1360,16 +1361,25 @@ __device__ __forceinline__ void sum_one(const StepArgs<R>& a, int s) {
   if (a.gjk_history) a.gdir_n_next[row] = owned < a.hist_cap ? owned : a.hist_cap;
   P.F[s] = st3<R>(F);
   P.T[s] = st3<R>(T);
+  if (f_out) *f_out = F;
+  if (t_out) *t_out = T;
 }
 
-template <typename R>
-__global__ void __launch_bounds__(256) sums_kernel(StepArgs<R> a) {
+// KICK: the particle's torsor is final here, and the rest of the step needs no
+// other particle: the second half kick of this step and the first half kick,
+// drift and binning of the next (kick_move_kernel's work) follow in the same
+// thread, without the torsor's round trip through memory and a launch.
+template <typename R, bool KICK = false>
+__global__ void __launch_bounds__(256) sums_kernel(StepArgs<R> a, R dt_half, double dt) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s == 0) {
     *a.work_n = 0;
     if (a.gjk_next) *a.gjk_next = 0;
   }
-  if (s < a.n) sum_one(a, s);
+  if (s >= a.n) return;
+  V3<R> F, T;
+  sum_one(a, s, &F, &T);
+  if (KICK) integrate(a, a.cur, a.cur, s, F, T, 1, dt_half, 1, dt_half, dt);
 }
 
 template <typename R>
@@ -1810,14 +1820,20 @@ int gjk_grid() {
 }
 
 template <typename R>
-int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int phases) {
+int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int phases, int kick) {
   if (a.n == 0) return 0;
   const int cb = (a.contacts_block >= 32 && a.contacts_block <= 256) ? a.contacts_block : 256;
   const int fb = (a.forces_block >= 32 && a.forces_block <= 128) ? a.forces_block : 128;
   if (phases & 1) contacts_kernel<R><<<grid_for(a.n, cb), cb, 0, s>>>(a);
   if (!(phases & 6)) return check_launch();
+  auto sums = [&]() {
+    if (kick)
+      sums_kernel<R, true><<<grid_for(a.n, 256), 256, 0, s>>>(a, R(0.5 * dt), dt);
+    else
+      sums_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, R(0), 0.);
+  };
   if (!(phases & 2)) {
-    sums_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
+    sums();
     return check_launch();
   }
   // about two work items per thread in a settled packing; the grid-stride
@@ -1845,7 +1861,7 @@ int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int
     else
       pairs_kernel<R, false, false><<<g, fb, 0, s>>>(a, R(dt));
   }
-  if (phases & 4) sums_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
+  if (phases & 4) sums();
   return check_launch();
 }
 
@@ -2083,7 +2099,7 @@ int launch_persistent_steps(const StepArgs<R>& a, cudaStream_t s, int n_steps, d
   template int launch_kick_move<R>(const StepArgs<R>&, cudaStream_t, int, double, int, double, double);    \
   template int launch_bin<R>(const StepArgs<R>&, cudaStream_t);                                            \
   template int launch_sort_and_gather<R>(const StepArgs<R>&, cudaStream_t, int, int);                      \
-  template int launch_forces<R>(const StepArgs<R>&, cudaStream_t, double, int, int);                       \
+  template int launch_forces<R>(const StepArgs<R>&, cudaStream_t, double, int, int, int);                  \
   template int launch_zero_kdelta<R>(const StepArgs<R>&, cudaStream_t);                                    \
   template int launch_update_dynamic<R>(const StepArgs<R>&, cudaStream_t, const KinematicStage&);             \
   template int launch_set_fluid_ratio<R>(const StepArgs<R>&, cudaStream_t, const double*);                     \
