@@ -132,6 +132,8 @@ struct grains_gpu_ctx {
   int* work_n = nullptr;
   GjkOut* gjk_out = nullptr;  // per work item: the GJK kernel's narrowphase result (convex scenarios)
   int* gjk_next = nullptr;    // the GJK kernel's work-item counter
+  int* gjk_order = nullptr;   // the GJK work items grouped by shape pair
+  int* gjk_bins = nullptr;    // their bin counts and cursors
   int clist_cap = 0;
   int64_t clist_alloc = 0;
   int* pairs = nullptr;  // contact pairs of the last compute_forces (diagnostic)
@@ -590,6 +592,8 @@ StepArgs<R> make_args(grains_gpu_ctx* c) {
   // the signed-volume GJK keeps its runs in the pair kernel
   a.gjk_out = c->gjk_sv ? nullptr : c->gjk_out;
   a.gjk_next = c->gjk_next;
+  a.gjk_order = c->gjk_order;
+  a.gjk_bins = c->gjk_bins;
   a.pairs = c->pairs;
   a.pairs_cap = c->pairs_cap;
   a.pairs_n = c->pairs_n;
@@ -781,7 +785,8 @@ int last_step(grains_gpu_ctx* c, double dt) {
 int ensure_lists(grains_gpu_ctx* c, int cap_per) {
   const int64_t need = (int64_t)c->cap * cap_per;
   if (need > c->clist_alloc || (c->has_convex && !c->gjk_out)) {
-    for (void** p : {(void**)&c->clist, &c->res_f, &c->res_t, (void**)&c->work, (void**)&c->gjk_out})
+    for (void** p : {(void**)&c->clist, &c->res_f, &c->res_t, (void**)&c->work, (void**)&c->gjk_out,
+                     (void**)&c->gjk_order})
       if (*p) {
         cudaFree(*p);
         *p = nullptr;
@@ -797,9 +802,11 @@ int ensure_lists(grains_gpu_ctx* c, int cap_per) {
     c->res_t = q;
     CK(cudaMalloc(&q, (size_t)need * sizeof(int4)));
     c->work = (int4*)q;
-    if (c->has_convex) {  // one narrowphase result per possible work item
+    if (c->has_convex) {  // one narrowphase result per possible work item, their order
       CK(cudaMalloc(&q, (size_t)need * sizeof(GjkOut)));
       c->gjk_out = (GjkOut*)q;
+      CK(cudaMalloc(&q, (size_t)need * sizeof(int)));
+      c->gjk_order = (int*)q;
     }
     c->clist_alloc = need;
     for (int k = 0; k < 4; ++k)  // graphs hold the old pointers
@@ -899,8 +906,9 @@ int grains_gpu_create(const grains_gpu_config* cfg, grains_gpu_ctx** out) {
     c->clock = dalloc<double>(1, c->pool);
     c->work_n = dalloc<int>(1, c->pool);
     c->gjk_next = dalloc<int>(1, c->pool);
+    c->gjk_bins = dalloc<int>(64, c->pool);
     ok = c->coord && c->perm && c->stats && c->pairs && c->pairs_n && c->pair_force && c->pair_sys && c->clock &&
-         c->work_n && c->gjk_next;
+         c->work_n && c->gjk_next && c->gjk_bins;
   }
   if (!ok) {
     c->err = "cudaMalloc failed for the requested capacity";
@@ -929,7 +937,8 @@ int grains_gpu_destroy(grains_gpu_ctx* c) {
   if (c->stage) cudaFree(c->stage);
   if (c->row_scratch) cudaFree(c->row_scratch);
   if (c->d_hydro) cudaFree(c->d_hydro);
-  for (void* p : {(void*)c->clist, (void*)c->ccount, c->res_f, c->res_t, (void*)c->work, (void*)c->gjk_out})
+  for (void* p : {(void*)c->clist, (void*)c->ccount, c->res_f, c->res_t, (void*)c->work, (void*)c->gjk_out,
+                  (void*)c->gjk_order})
     if (p) cudaFree(p);
   if (c->pbar) cudaFree(c->pbar);
   if (c->psums) cudaFree(c->psums);
@@ -2373,7 +2382,7 @@ int grains_gpu_launches_per_step(grains_gpu_ctx* c, int64_t* launches) {
   // (the GJK kernel of convex scenarios,) pairs, sums with the kick, and the
   // obstacle move when obstacles move; the gather runs one step in
   // gather_every on top
-  *launches = launches_per_middle_step() + (c->has_convex && !c->gjk_sv ? 1 : 0) + (c->n_moving > 0 ? 1 : 0);
+  *launches = launches_per_middle_step() + (c->has_convex && !c->gjk_sv ? 3 : 0) + (c->n_moving > 0 ? 1 : 0);
   return 0;
 }
 

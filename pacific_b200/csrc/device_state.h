@@ -216,6 +216,8 @@ struct StepArgs {
   int gjk_history;       // warm-started GJK from the pair's collision history (History="ON")
   GjkOut* gjk_out;       // per work item: the GJK kernel's narrowphase result (null: GJK inline in the pair kernel)
   int* gjk_next;         // the GJK kernel's work-item counter (cleared by the sums kernel)
+  int* gjk_order;        // the GJK work items grouped by shape pair (work-item capacity)
+  int* gjk_bins;         // per shape-pair bin: counts, then placement cursors (2 x 32 ints)
   GjkDir* gdir_prev;     // collision histories of the last evaluation (rows of hist_cap slots by memory row)
   int* gdir_n_prev;
   GjkDir* gdir_next;     // written by this evaluation

@@ -1179,12 +1179,12 @@ __device__ __forceinline__ void store_gjk_dir(const StepArgs<R>& a, int4 item, i
 // takes work items until one needs a GJK run and starts it; items whose
 // bounding spheres are apart are finished on the way.  False when none is left.
 template <typename R>
-__device__ bool gjk_lane_start(const StepArgs<R>& a, int n_items, GjkLane<R>& L) {
+__device__ bool gjk_lane_start(const StepArgs<R>& a, int n_gjk, GjkLane<R>& L) {
   for (;;) {
-    const int k = take_item(a.gjk_next);
-    if (k >= n_items) return false;
+    const int j = take_item(a.gjk_next);
+    if (j >= n_gjk) return false;
+    const int k = a.gjk_order[j];  // the GJK items grouped by shape pair
     const int4 item = a.work[k];
-    if (!needs_gjk(a, item)) continue;
     BodyRef ba, bb;
     item_bodies(a, item, ba, bb);
     const bool pair = item.y >= 0;
@@ -1244,6 +1244,52 @@ __device__ void gjk_lane_finish(const StepArgs<R>& a, GjkLane<R>& L, unsigned lo
     store_gjk_dir(a, L.item, a.cur.meta[entry_slot(L.item.y)].x, c.status, handled, L.known, L.v_before, r.v);
 }
 
+// The GJK items are grouped by the shape types of their pair first (a
+// counting sort into kGjkBins bins), so that the lanes of a warp run the same
+// support functions: counts per bin, then each item placed in its bin.
+constexpr int kGjkBins = 32;
+template <typename R>
+__device__ __forceinline__ int gjk_bin(const StepArgs<R>& a, int4 item) {
+  const int ta = a.shapes[a.cur.meta[item.x].z].type;
+  const int tb = item.y >= 0 ? a.shapes[a.cur.meta[entry_slot(item.y)].z].type
+                             : 4 + a.shapes[a.obs[-1 - item.y].shape].type;
+  return ta * 8 + tb;
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) gjk_count_kernel(StepArgs<R> a) {
+  __shared__ int h[kGjkBins];
+  if (threadIdx.x < kGjkBins) h[threadIdx.x] = 0;
+  __syncthreads();
+  const int n_items = (int)min((long long)*(volatile int*)a.work_n, (long long)a.n * a.clist_cap);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_items; k += gridDim.x * blockDim.x) {
+    const int4 item = a.work[k];
+    if (needs_gjk(a, item)) atomicAdd(&h[gjk_bin(a, item)], 1);
+  }
+  __syncthreads();
+  if (threadIdx.x < kGjkBins && h[threadIdx.x]) atomicAdd(&a.gjk_bins[threadIdx.x], h[threadIdx.x]);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) gjk_place_kernel(StepArgs<R> a) {
+  __shared__ int base[kGjkBins];
+  if (threadIdx.x == 0) {
+    int sum = 0;
+    for (int b = 0; b < kGjkBins; ++b) {
+      base[b] = sum;
+      sum += a.gjk_bins[b];
+    }
+  }
+  __syncthreads();
+  const int n_items = (int)min((long long)*(volatile int*)a.work_n, (long long)a.n * a.clist_cap);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n_items; k += gridDim.x * blockDim.x) {
+    const int4 item = a.work[k];
+    if (!needs_gjk(a, item)) continue;
+    const int b = gjk_bin(a, item);
+    a.gjk_order[base[b] + atomicAdd(&a.gjk_bins[kGjkBins + b], 1)] = k;
+  }
+}
+
 // Starting a run (the bodies, the history, the first iterate) costs about as
 // much as two GJK iterations, so lanes whose run has ended wait until half the
 // warp is idle (or nothing else runs) and start their next runs together.
@@ -1256,7 +1302,8 @@ template <typename R>
 __global__ void __launch_bounds__(kGjkBlock) gjk_kernel(StepArgs<R> a) {
   __shared__ double words[kGjkWords * kGjkBlock];
   const unsigned full = 0xffffffffu;
-  const int n_items = (int)min((long long)*(volatile int*)a.work_n, (long long)a.n * a.clist_cap);
+  int n_items = 0;  // GJK items: the total of the shape-pair bins
+  for (int b = 0; b < kGjkBins; ++b) n_items += a.gjk_bins[b];
   unsigned long long ngjk = 0, nit = 0;
   GjkLane<R> L;
   L.run.g.base = words + threadIdx.x;
@@ -1854,7 +1901,11 @@ int launch_forces(const StepArgs<R>& a, cudaStream_t s, double dt, int diag, int
       pairs_kernel<R, true, true, true><<<g, fb, 0, s>>>(a, R(dt));
     else
       pairs_kernel<R, false, true, true><<<g, fb, 0, s>>>(a, R(dt));
-  } else if (a.has_convex && a.gjk_out) {  // the GJK kernel, then the law
+  } else if (a.has_convex && a.gjk_out) {  // the GJK items grouped by shape pair, the GJK kernel, the law
+    cudaMemsetAsync(a.gjk_bins, 0, 2 * kGjkBins * sizeof(int), s);
+    const int gb = 2 * 148;
+    gjk_count_kernel<R><<<gb, 256, 0, s>>>(a);
+    gjk_place_kernel<R><<<gb, 256, 0, s>>>(a);
     gjk_kernel<R><<<gjk_grid<R>(), kGjkBlock, 0, s>>>(a);
     if (diag)
       pairs_kernel<R, true, true, false, true><<<g, fb, 0, s>>>(a, R(dt));
