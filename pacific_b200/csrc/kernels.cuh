@@ -1298,8 +1298,16 @@ __global__ void __launch_bounds__(256) gjk_place_kernel(StepArgs<R> a) {
 // block's 64 threads; in local memory they overflowed L1 and were written back
 // to DRAM (1.9 GB per launch on the settled drum).
 constexpr int kGjkBlock = 64;
+// idle lanes of a warp that wait before they write their results and start
+// their next runs together
+#ifndef GG_GJK_BATCH
+#define GG_GJK_BATCH 16
+#endif
+#ifndef GG_GJK_MIN_BLOCKS
+#define GG_GJK_MIN_BLOCKS 1
+#endif
 template <typename R>
-__global__ void __launch_bounds__(kGjkBlock) gjk_kernel(StepArgs<R> a) {
+__global__ void __launch_bounds__(kGjkBlock, GG_GJK_MIN_BLOCKS) gjk_kernel(StepArgs<R> a) {
   __shared__ double words[kGjkWords * kGjkBlock];
   const unsigned full = 0xffffffffu;
   int n_items = 0;  // GJK items: the total of the shape-pair bins
@@ -1309,16 +1317,22 @@ __global__ void __launch_bounds__(kGjkBlock) gjk_kernel(StepArgs<R> a) {
   L.run.g.base = words + threadIdx.x;
   L.run.g.stride = kGjkBlock;
   bool busy = gjk_lane_start(a, n_items, L);
+  bool ended = false;    // the lane's run has ended and waits for its results to be written
   bool drained = !busy;  // no work item is left for this lane
   for (;;) {
     if (busy && gjk_iterate(L.run, L.la, L.lb)) {
-      gjk_lane_finish(a, L, ngjk, nit);
       busy = false;
+      ended = true;
     }
     const unsigned waiting = __ballot_sync(full, !busy && !drained);
     const unsigned running = __ballot_sync(full, busy);
     if (!waiting && !running) break;
-    if (__popc(waiting) >= 16 || !running) {
+    if (__popc(waiting) >= GG_GJK_BATCH || !running) {
+      // the ended runs' results and the next runs' starts, together
+      if (ended) {
+        gjk_lane_finish(a, L, ngjk, nit);
+        ended = false;
+      }
       if (!busy && !drained) {
         busy = gjk_lane_start(a, n_items, L);
         drained = !busy;
