@@ -431,7 +431,7 @@ int grains_gpu_reset_stats(grains_gpu_ctx* ctx);
  *   persistent     1: the middle steps of grains_gpu_step run in one
  *                  cooperative launch (every block resident, the phases
  *                  separated by a grid barrier with a bounded wait) instead of
- *                  8 launches per step replayed from graphs; same results.
+ *                  6 launches per step replayed from graphs; same results.
  *                  Pays where launch gaps dominate (small systems). */
 typedef struct grains_gpu_tuning {
   double  cell_factor;

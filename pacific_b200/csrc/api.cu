@@ -2378,7 +2378,7 @@ int grains_gpu_set_barrier_test(grains_gpu_ctx* c, int64_t polls, int32_t skip_b
 
 int grains_gpu_launches_per_step(grains_gpu_ctx* c, int64_t* launches) {
   if (!c || !launches) return GRAINS_GPU_INVALID_ARGUMENT;
-  // a middle step: scan_tiles, scan_finish, scatter, cell_sort, contacts,
+  // a middle step: scan_tiles, scatter, cell_sort, contacts,
   // (the GJK kernel of convex scenarios,) pairs, sums with the kick, and the
   // obstacle move when obstacles move; the gather runs one step in
   // gather_every on top
@@ -2428,7 +2428,7 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* c, int32_t n_steps, double* time,
     float t[5] = {0, 0, 0, 0, 0};
     for (int q = 0; q < 5; ++q) cudaEventElapsedTime(&t[q], ev[1 + q], ev[2 + q]);
     for (int q = 0; q < 5; ++q) acc[1 + q] += t[q];
-    cnt[1] += 4;  // scan_tiles, scan_finish, scatter, cell_sort (+ a gather one step in gather_every)
+    cnt[1] += 3;  // scan_tiles, scatter, cell_sort (+ a gather one step in gather_every)
     cnt[2] += 1;
     cnt[3] += 1;
     cnt[4] += 1;
@@ -2703,7 +2703,7 @@ int grains_gpu_autotune(grains_gpu_ctx* c, double time, double dt, int32_t trial
 }  // extern "C"
 
 namespace gg {
-int launches_per_middle_step() { return 7; }
+int launches_per_middle_step() { return 6; }
 
 int context_view(grains_gpu_ctx* c, ContextView* v, std::string& err) {
   if (!c || !v) return GRAINS_GPU_INVALID_ARGUMENT;

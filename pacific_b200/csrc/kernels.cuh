@@ -221,51 +221,52 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int* total) {
   return base + x - v;
 }
 
-static __global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(const int* in, int* out, int* block_sums, int n) {
+// The launched sort of a step scans the cell counts within tiles of kScanTile
+// cells only: each tile's local exclusive prefix (into the cursor array), its
+// total, and the counts zeroed.  The scatter then counts every cell's
+// particles again, taking each particle's rank in its cell from that atomic,
+// and adds the start of its tile (the sum of the totals before it); the cell
+// sort writes the final cell starts.  No second pass over the cells.
+static __global__ void __launch_bounds__(kScanThreads) scan_tiles_kernel(int* counts, int* local_start, int* tile_sums,
+                                                                         int n) {
   int base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
   int vals[kScanItems];
   int sum = 0;
 #pragma unroll
   for (int t = 0; t < kScanItems; ++t) {
-    vals[t] = (base + t < n) ? in[base + t] : 0;
+    vals[t] = (base + t < n) ? counts[base + t] : 0;
     sum += vals[t];
   }
   int total;
   int pre = block_exclusive_scan(sum, &total);
 #pragma unroll
   for (int t = 0; t < kScanItems; ++t) {
-    if (base + t < n) out[base + t] = pre;
+    if (base + t < n) {
+      local_start[base + t] = pre;
+      counts[base + t] = 0;
+    }
     pre += vals[t];
   }
-  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
 }
 
-// finishes the scan and sets each cell's fill cursor to its start.  A block
-// of 256 cells lies in one tile; it sums the totals of the tiles before its
-// own itself (at most kScanTile of them), so that the tile totals need no
-// scan of their own.  The cell of index n - 1 also writes the grand total.
-constexpr int kScanAddThreads = 256;
-static_assert(kScanTile % kScanAddThreads == 0, "a scan-add block must lie in one tile");
-static __global__ void __launch_bounds__(kScanAddThreads)
-    scan_finish_kernel(int* out, int* cursor, const int* block_sums, const int* counts, int n) {
-  __shared__ int warp_part[kScanAddThreads / 32];
-  const int i = blockIdx.x * kScanAddThreads + threadIdx.x;
-  const int tile = (blockIdx.x * kScanAddThreads) / kScanTile;
-  int part = 0;
-  for (int b = threadIdx.x; b < tile; b += kScanAddThreads) part += block_sums[b];
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
-  if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = part;
+// the start of every tile (exclusive prefix of the tile totals) in shared
+// memory; every thread of the block calls it
+constexpr int kMaxScanTiles = 4096;
+__device__ __forceinline__ void tile_starts(const int* tile_sums, int n_tiles, int* start) {
+  const int per = (n_tiles + blockDim.x - 1) / blockDim.x;
+  const int t0 = threadIdx.x * per;
+  int sum = 0;
+  for (int k = 0; k < per; ++k)
+    if (t0 + k < n_tiles) sum += tile_sums[t0 + k];
+  int total;
+  int pre = block_exclusive_scan(sum, &total);
+  for (int k = 0; k < per; ++k)
+    if (t0 + k < n_tiles) {
+      start[t0 + k] = pre;
+      pre += tile_sums[t0 + k];
+    }
   __syncthreads();
-  int prefix = 0;
-#pragma unroll
-  for (int w = 0; w < kScanAddThreads / 32; ++w) prefix += warp_part[w];
-  if (i < n) {
-    const int v = out[i] + prefix;
-    out[i] = v;
-    cursor[i] = v;
-    if (i == n - 1) out[n] = v + counts[i];
-  }
 }
 
 // slot of each particle in its cell's range; the order inside a cell is
@@ -282,16 +283,30 @@ __device__ __forceinline__ void scatter_one(const StepArgs<R>& a, int s) {
   a.perm[slot] = s;
 }
 
+// the launched scatter: slot = start of the key's tile + the cell's start in
+// the tile + the particle's rank from the cell's count
 template <typename R>
-__global__ void scatter_kernel(StepArgs<R> a) {
-  int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < a.n) scatter_one(a, s);
+__global__ void __launch_bounds__(256) scatter_kernel(StepArgs<R> a) {
+  __shared__ int tile_start[kMaxScanTiles];
+  tile_starts(a.block_sums, (a.n_cells + kScanTile - 1) / kScanTile, tile_start);
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= a.n) return;
+  const unsigned key = a.cur.key[s];
+  const long long slot =
+      (key < (unsigned)a.n_cells)
+          ? (long long)tile_start[key / kScanTile] + a.cell_cursor[key] + atomicAdd(&a.cell_count[key], 1)
+          : -1;
+  if (slot < 0 || slot >= a.n) {
+    set_status(a.stats, GRAINS_GPU_CUDA_ERROR);
+    return;
+  }
+  a.perm[slot] = s;
 }
 
-// order each cell's slots by particle id; resets the count for the next step
+// order the slots [b, e) of cell c by particle id; resets the count for the
+// next step
 template <typename R>
-__device__ __forceinline__ void cell_sort_one(const StepArgs<R>& a, int c) {
-  int b = a.cell_start[c], e = a.cell_start[c + 1];
+__device__ __forceinline__ void cell_sort_range(const StepArgs<R>& a, int c, int b, int e) {
   a.cell_count[c] = 0;
   if (b < 0 || e > a.n || b > e) return;
   for (int i = b + 1; i < e; ++i) {
@@ -306,10 +321,38 @@ __device__ __forceinline__ void cell_sort_one(const StepArgs<R>& a, int c) {
   }
 }
 
+// the cell sort of a fully scanned cell list (the persistent kernel's)
 template <typename R>
-__global__ void cell_sort_kernel(StepArgs<R> a) {
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c < a.n_cells) cell_sort_one(a, c);
+__device__ __forceinline__ void cell_sort_one(const StepArgs<R>& a, int c) {
+  cell_sort_range(a, c, a.cell_start[c], a.cell_start[c + 1]);
+}
+
+// the launched cell sort: the final start of each cell (its tile's start + its
+// start in the tile; its end from the count the scatter rebuilt), then the
+// sort.  The block's 256 cells lie in one tile; the block sums the totals of
+// the tiles before it.
+constexpr int kCellSortThreads = 256;
+static_assert(kScanTile % kCellSortThreads == 0, "a cell-sort block must lie in one scan tile");
+template <typename R>
+__global__ void __launch_bounds__(kCellSortThreads) cell_sort_kernel(StepArgs<R> a) {
+  __shared__ int warp_part[kCellSortThreads / 32];
+  const int c = blockIdx.x * kCellSortThreads + threadIdx.x;
+  const int tile = (blockIdx.x * kCellSortThreads) / kScanTile;
+  int part = 0;
+  for (int t = threadIdx.x; t < tile; t += kCellSortThreads) part += a.block_sums[t];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+  if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = part;
+  __syncthreads();
+  int start = 0;
+#pragma unroll
+  for (int w = 0; w < kCellSortThreads / 32; ++w) start += warp_part[w];
+  if (c < a.n_cells) {
+    const int b = start + a.cell_cursor[c], e = b + a.cell_count[c];
+    a.cell_start[c] = b;
+    if (c == a.n_cells - 1) a.cell_start[c + 1] = e;
+    cell_sort_range(a, c, b, e);
+  }
 }
 
 // permutes every per-particle array into cell order; the permutation then
@@ -1905,11 +1948,10 @@ template <typename R>
 int launch_sort_and_gather(const StepArgs<R>& a, cudaStream_t s, int gather, int gather_forces) {
   const int C = a.n_cells;
   const int nb = grid_for(C, kScanTile);
-  scan_tiles_kernel<<<nb, kScanThreads, 0, s>>>(a.cell_count, a.cell_start, a.block_sums, C);
-  scan_finish_kernel<<<grid_for(C, kScanAddThreads), kScanAddThreads, 0, s>>>(a.cell_start, a.cell_cursor,
-                                                                             a.block_sums, a.cell_count, C);
+  if (nb > kMaxScanTiles) return GRAINS_GPU_INVALID_ARGUMENT;
+  scan_tiles_kernel<<<nb, kScanThreads, 0, s>>>(a.cell_count, a.cell_cursor, a.block_sums, C);
   if (a.n > 0) scatter_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a);
-  cell_sort_kernel<R><<<grid_for(C, 256), 256, 0, s>>>(a);
+  cell_sort_kernel<R><<<grid_for(C, kCellSortThreads), kCellSortThreads, 0, s>>>(a);
   if (a.n > 0 && gather) gather_kernel<R><<<grid_for(a.n, 256), 256, 0, s>>>(a, gather_forces);
   return check_launch();
 }
