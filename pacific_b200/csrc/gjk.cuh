@@ -332,8 +332,10 @@ template <typename T>
 GG_HD bool gjk_closest(unsigned& bits, unsigned last, unsigned last_bit, unsigned all_bits, const GjkState<T>& g,
                        V3<T>& v) {
   gjk_det(bits, last, last_bit, all_bits, g);
-  for (unsigned s = bits; s; --s) {
-    if ((s & bits) == s && gjk_valid(s | last_bit, all_bits, g)) {
+  // the non-empty subsets of bits in decreasing order (s = (s - 1) & bits
+  // steps from one subset to the next smaller one)
+  for (unsigned s = bits; s; s = (s - 1) & bits) {
+    if (gjk_valid(s | last_bit, all_bits, g)) {
       bits = s | last_bit;
       v = gjk_vector(bits, g);
       return true;
@@ -345,8 +347,8 @@ GG_HD bool gjk_closest(unsigned& bits, unsigned last, unsigned last_bit, unsigne
     return true;
   }
   T best = T(INFINITY);
-  for (unsigned s = all_bits; s; --s) {  // backup procedure
-    if ((s & all_bits) == s && gjk_proper(s, g)) {
+  for (unsigned s = all_bits; s; s = (s - 1) & all_bits) {  // backup procedure
+    if (gjk_proper(s, g)) {
       V3<T> u = gjk_vector(s, g);
       T d2 = norm2(u);
       if (d2 < best) {
