@@ -88,14 +88,15 @@ GG_HD V3<T> support_local(const LocalBody<T>& B, V3<T> v) {
       return v3<T>(T(0), T(0), T(0));
     }
     case 1: {  // box
-      T n = norm(v);
-      if (n < T(kEpsilon)) return v3<T>(T(0), T(0), T(0));
+      // |v| < EPSILON tested as |v|^2 < EPSILON^2 here and below: the same
+      // branch except within a rounding of the threshold, without the square
+      // root (two per GJK iteration)
+      if (norm2(v) < T(kEpsilon) * T(kEpsilon)) return v3<T>(T(0), T(0), T(0));
       return v3<T>(v.x < T(0) ? -B.ext.x : B.ext.x, v.y < T(0) ? -B.ext.y : B.ext.y,
                    v.z < T(0) ? -B.ext.z : B.ext.z);
     }
     case 2: {  // cylinder, axis local Y
-      T n = norm(v);
-      if (n > T(kEpsilon)) {
+      if (norm2(v) > T(kEpsilon) * T(kEpsilon)) {
         T s = std::sqrt(v.x * v.x + v.z * v.z);
         if (s > T(kEpsilon)) {
           T d = B.cyl_r / s;
@@ -107,8 +108,7 @@ GG_HD V3<T> support_local(const LocalBody<T>& B, V3<T> v) {
       return v3<T>(T(0), T(0), T(0));
     }
     default: {  // polyhedron
-      T n = norm(v);
-      if (!(n > T(kEpsilon))) return v3<T>(T(0), T(0), T(0));
+      if (!(norm2(v) > T(kEpsilon) * T(kEpsilon))) return v3<T>(T(0), T(0), T(0));
       if (B.adj_start) {
         // hill climb: move to the first neighbour (other than the vertex just
         // left) whose v . p is not below the current one by the 1e-16 margin;
