@@ -130,7 +130,21 @@ enum grains_gpu_motion {
   GRAINS_GPU_CRENEL_TRANSLATION   = 2,  /* vector = direction; amplitude[0] (velocity), period[0] (half cycle) */
   GRAINS_GPU_CONSTANT_ROTATION    = 3,  /* vector = angular velocity; about center when has_center, else
                                            about the obstacle's own centre */
-  GRAINS_GPU_MULTISIN_TRANSLATION = 4   /* vector = direction; per axis amplitude, period, phase_deg */
+  GRAINS_GPU_MULTISIN_TRANSLATION = 4,  /* vector = direction; per axis amplitude, period, phase_deg */
+  /* An imposed force (ObstacleImposedForce "ConstantTranslation", Component/
+   * src/ObstacleImposedForce.cpp:29-80 for the XML, 183-252 for the motion):
+   * vector = the force (AX, AY, AZ), amplitude[0] = the virtual mass (<= 0:
+   * automatic, dt^2 |F| 1e7 / (2 crust)), amplitude[1] = Vmax.  Each move, a
+   * PID controller turns the difference between the contact force on the
+   * obstacle (from the last force evaluation) and the imposed force, along
+   * the force's direction, into the obstacle's translation over the step; until
+   * the contact force first exceeds EPSILON the obstacle moves at -Vmax along
+   * the direction.  As in the reference the controller's history is one per
+   * system, shared by its force loadings (the reference keeps it in static
+   * variables), and the force loadings of an obstacle act in the order given.
+   * The reference's "MultiSinTranslation" force has no motion (its body is a
+   * "TO DO") and is not offered. */
+  GRAINS_GPU_FORCE_TRANSLATION    = 5
 };
 typedef struct grains_gpu_obstacle_loading {
   int32_t obstacle_id;

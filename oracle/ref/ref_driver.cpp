@@ -552,8 +552,10 @@ int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
       size_t k = 0;
       while (k < c->obs.size() && c->obs[k].id != l.obstacle_id) ++k;
       if (k == c->obs.size()) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "loading of an unknown obstacle");
-      x << "<ObstacleLoading Type=\"Velocity\" ObstacleName=\"o" << k << "\"><TimeInterval Start=\""
-        << num(l.t_start) << "\" End=\"" << num(l.t_end) << "\"/>";
+      // Type="Force": ObstacleImposedForce (Grains.cpp:1736-1742, ObstacleImposedForce.cpp:29-80)
+      x << "<ObstacleLoading Type=\"" << (l.type == GRAINS_GPU_FORCE_TRANSLATION ? "Force" : "Velocity")
+        << "\" ObstacleName=\"o" << k << "\"><TimeInterval Start=\"" << num(l.t_start) << "\" End=\""
+        << num(l.t_end) << "\"/>";
       auto vec = [&](const char* tag, const char* a, const char* b, const char* cc, const double* v) {
         x << "<" << tag << " " << a << "=\"" << num(v[0]) << "\" " << b << "=\"" << num(v[1]) << "\" " << cc
           << "=\"" << num(v[2]) << "\"/>";
@@ -585,6 +587,13 @@ int grains_ref_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
           vec("PhaseShift", "PhiX", "PhiY", "PhiZ", l.phase_deg);
           vec("Amplitude", "AX", "AY", "AZ", l.amplitude);
           x << "</MultiSinTranslation>";
+          break;
+        case GRAINS_GPU_FORCE_TRANSLATION:
+          x << "<ConstantTranslation>";
+          vec("Amplitude", "AX", "AY", "AZ", l.vector);
+          x << "<Property ";
+          if (l.amplitude[0] > 0.) x << "Mass=\"" << num(l.amplitude[0]) << "\" ";
+          x << "Vmax=\"" << num(l.amplitude[1]) << "\"/></ConstantTranslation>";
           break;
         default:
           return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "unknown loading type");

@@ -89,6 +89,7 @@ class ObstacleLoading(C.Structure):
 
 # imposed obstacle motions (grains_gpu_motion)
 CONSTANT_TRANSLATION, SIN_TRANSLATION, CRENEL_TRANSLATION, CONSTANT_ROTATION, MULTISIN_TRANSLATION = 0, 1, 2, 3, 4
+FORCE_TRANSLATION = 5  # an imposed force (ObstacleImposedForce): vector = force, amplitude = (mass, Vmax)
 
 _P_I32 = C.POINTER(C.c_int32)
 _P_F64 = C.POINTER(C.c_double)

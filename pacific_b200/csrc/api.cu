@@ -153,6 +153,12 @@ struct grains_gpu_ctx {
   ObstacleDev* d_obs = nullptr;
   LoadingDev* d_loads = nullptr;
   int* d_load_flags = nullptr;  // per system: a loading active over this step, over the previous one
+  // force-driven obstacles: partial contact forces (kForceBlocks x kMaxForceObstacles x 3) and the
+  // controller history per system; null when no obstacle has an imposed force
+  double* d_force_part = nullptr;
+  double* d_force_pid = nullptr;
+  int n_force_obs = 0;
+  bool obs_force_valid = false;  // the list entries hold the results of a force evaluation
   int *d_cell_obs_start = nullptr, *d_cell_obs_idx = nullptr, *d_moving = nullptr;
   void* d_laws = nullptr;
   std::vector<SysDev> h_sys;
@@ -363,6 +369,15 @@ LoadingDev loading_dev(const grains_gpu_obstacle_loading& g) {
     for (int i = 0; i < 3; ++i) L.vel[i] = g.vector[i];
   if (g.type == GRAINS_GPU_CONSTANT_ROTATION)
     for (int i = 0; i < 3; ++i) L.omega[i] = g.vector[i];
+  if (g.type == GRAINS_GPU_FORCE_TRANSLATION) {  // ObstacleImposedForce.cpp:55-68
+    const double nv = std::sqrt(g.vector[0] * g.vector[0] + g.vector[1] * g.vector[1] + g.vector[2] * g.vector[2]);
+    for (int i = 0; i < 3; ++i) {
+      L.vel[i] = g.vector[i];
+      L.unit[i] = g.vector[i] / nv;
+    }
+    L.amp = g.amplitude[0] > 0. ? g.amplitude[0] : 0.;
+    L.period = g.amplitude[1];
+  }
   if (g.type == GRAINS_GPU_SIN_TRANSLATION || g.type == GRAINS_GPU_CRENEL_TRANSLATION ||
       g.type == GRAINS_GPU_MULTISIN_TRANSLATION) {
     const double nv = std::sqrt(g.vector[0] * g.vector[0] + g.vector[1] * g.vector[1] + g.vector[2] * g.vector[2]);
@@ -409,9 +424,17 @@ std::vector<LoadingDev> obstacle_loadings(const SysHost& s, const grains_gpu_obs
     while (k < v.size() && v[k].t_start < g.t_start) ++k;
     v.insert(v.begin() + (long)k, g);
   };
+  bool explicit_loads = false;
   for (const auto& g : s.loads)
-    if (g.obstacle_id == o.id) insert(g);
-  if (v.empty() && o.moving) v.push_back(legacy_loading(o));
+    if (g.obstacle_id == o.id) {
+      explicit_loads = true;
+      if (g.type != GRAINS_GPU_FORCE_TRANSLATION) insert(g);
+    }
+  if (!explicit_loads && o.moving) v.push_back(legacy_loading(o));
+  // the imposed forces after the velocities, in the order given
+  // (ObstacleKinematicsForce::append, ObstacleKinematicsForce.cpp:27-30)
+  for (const auto& g : s.loads)
+    if (g.obstacle_id == o.id && g.type == GRAINS_GPU_FORCE_TRANSLATION) v.push_back(g);
   std::vector<LoadingDev> out;
   for (const auto& g : v) out.push_back(loading_dev(g));
   return out;
@@ -694,6 +717,7 @@ int forces_now(grains_gpu_ctx* c, double dt, int diag, int phases = 7, int kick 
   int rc = with_args(c, [&](auto& a) { return launch_forces(a, c->stream, dt, diag, phases, kick); });
   if (rc) return fail(c, rc, "force kernel launch failed");
   if (phases & 4) c->hcur = 1 - c->hcur;
+  if (phases & 2) c->obs_force_valid = true;
   return 0;
 }
 
@@ -704,9 +728,22 @@ int forces_now(grains_gpu_ctx* c, double dt, int diag, int phases = 7, int kick 
 // by dt, as Grains::Simulation advances m_time
 int move_obstacles(grains_gpu_ctx* c, double dt, int from_host = 0, double time = 0.) {
   if (c->n_moving == 0) return 0;
+  if (c->n_force_obs > 0) {
+    // the contact forces on the force-driven obstacles from the last force
+    // evaluation (zero before the first one, like the reference's torsors)
+    if (c->obs_force_valid) {
+      int rc = with_args(c, [&](auto& a) {
+        return launch_obstacle_force(a, c->d_force_part, (int)c->h_obs.size(), c->stream);
+      });
+      if (rc) return fail(c, rc, "obstacle force launch failed");
+    } else {
+      CK(cudaMemsetAsync(c->d_force_part, 0, (size_t)kForceBlocks * kMaxForceObstacles * 3 * sizeof(double),
+                         c->stream));
+    }
+  }
   int rc = launch_obstacle_move(c->d_obs, c->d_moving, c->n_moving, c->d_loads, c->d_load_flags,
                                 (int)c->sys.size(), c->d_shapes, c->d_verts, dt, c->clock, time, from_host,
-                                c->stream);
+                                c->d_force_part, c->d_force_pid, c->stream);
   return rc ? fail(c, rc, "obstacle move launch failed") : 0;
 }
 
@@ -792,6 +829,7 @@ int ensure_lists(grains_gpu_ctx* c, int cap_per) {
         *p = nullptr;
       }
     c->clist_alloc = 0;
+    c->obs_force_valid = false;  // the new lists hold no force evaluation yet
     const size_t r4 = 4 * c->rsize;
     void* q = nullptr;
     CK(cudaMalloc(&q, (size_t)need * sizeof(int)));
@@ -1106,8 +1144,11 @@ int grains_gpu_set_obstacle_loadings(grains_gpu_ctx* c, int32_t system, int32_t 
     bool found = false;
     for (const auto& o : s.obs) found = found || o.id == l[k].obstacle_id;
     if (!found) return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "loading of an unknown obstacle");
-    if (l[k].type < GRAINS_GPU_CONSTANT_TRANSLATION || l[k].type > GRAINS_GPU_MULTISIN_TRANSLATION)
+    if (l[k].type < GRAINS_GPU_CONSTANT_TRANSLATION || l[k].type > GRAINS_GPU_FORCE_TRANSLATION)
       return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "unknown loading type");
+    if (l[k].type == GRAINS_GPU_FORCE_TRANSLATION &&
+        !(l[k].vector[0] != 0. || l[k].vector[1] != 0. || l[k].vector[2] != 0.))
+      return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "an imposed force needs a non-zero force");
     if ((l[k].type == GRAINS_GPU_SIN_TRANSLATION || l[k].type == GRAINS_GPU_CRENEL_TRANSLATION) &&
         !(l[k].period[0] > 0.))
       return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "a periodic loading needs a positive period");
@@ -1131,6 +1172,7 @@ int build_tables(grains_gpu_ctx* c) {
   std::vector<ObstacleDev> ho;
   std::vector<LoadingDev> hl;
   std::vector<int> moving;
+  int n_force = 0;  // force-driven obstacles
   std::vector<int> cstart;
   std::vector<int> cidx;
   int cells = 0;
@@ -1163,6 +1205,12 @@ int build_tables(grains_gpu_ctx* c) {
       od.load_count = (int)ls.size();
       od.moving = ls.empty() ? 0 : 1;
       od.sys = (int)si;
+      od.force_slot = -1;
+      od.moved = 0;
+      for (const auto& L : ls)
+        if (L.type == GRAINS_GPU_FORCE_TRANSLATION) od.force_slot = n_force;
+      if (od.force_slot >= 0 && ++n_force > kMaxForceObstacles)
+        return fail(c, GRAINS_GPU_INVALID_ARGUMENT, "more force-driven obstacles than kMaxForceObstacles (4)");
       hl.insert(hl.end(), ls.begin(), ls.end());
       ho.push_back(od);
       if (od.moving) moving.push_back(d.obs_offset + (int)k);
@@ -1263,6 +1311,14 @@ int build_tables(grains_gpu_ctx* c) {
   {
     std::vector<int> flags(2 * c->sys.size(), 0);  // no loading active before the first step
     rc |= up(flags.data(), flags.size() * sizeof(int), (void**)&c->d_load_flags);
+  }
+  c->n_force_obs = n_force;
+  c->d_force_part = c->d_force_pid = nullptr;
+  if (n_force > 0) {
+    std::vector<double> part((size_t)kForceBlocks * kMaxForceObstacles * 3, 0.);
+    std::vector<double> pid(c->sys.size() * kForcePidWords, 0.);  // the controllers start without history
+    rc |= up(part.data(), part.size() * sizeof(double), (void**)&c->d_force_part);
+    rc |= up(pid.data(), pid.size() * sizeof(double), (void**)&c->d_force_pid);
   }
   {
     // obstacle ids by global obstacle index, and each system's first index
@@ -1499,6 +1555,7 @@ int grains_gpu_upload_particles(grains_gpu_ctx* c, const grains_gpu_particles* p
   c->moved = 0;
   c->fluid_corrected = 0;  // md.w (rho_f / rho_p) was uploaded as 0
   c->hydro_on = false;
+  c->obs_force_valid = false;  // no force evaluation of these particles yet
   for (int k = 0; k < 2; ++k) CK(cudaMemsetAsync(c->hist_n[k], 0, (size_t)c->cap * sizeof(int), c->stream));
   for (int k = 0; k < 2; ++k)
     if (c->gdir_n[k]) CK(cudaMemsetAsync(c->gdir_n[k], 0, (size_t)c->cap * sizeof(int), c->stream));
@@ -2172,7 +2229,9 @@ int grains_gpu_step(grains_gpu_ctx* c, int32_t n_steps, double* time, double dt)
   if (int rc = first_move(c, dt, *time)) return rc;
   int middle = n_steps - 1;
   // the persistent kernel carries Johnson's GJK only: the signed-volume one runs from the graphs
-  if (c->persistent && middle > 0 && !(c->gjk_sv && c->has_convex)) {
+  // (force-driven obstacles need the contact-force sums between the phases:
+  // launched steps only)
+  if (c->persistent && middle > 0 && !(c->gjk_sv && c->has_convex) && c->n_force_obs == 0) {
     if (int rc = persistent_middle_steps(c, middle, dt)) return rc;
     middle = 0;
   }
@@ -2382,7 +2441,8 @@ int grains_gpu_launches_per_step(grains_gpu_ctx* c, int64_t* launches) {
   // (the GJK kernel of convex scenarios,) pairs, sums with the kick, and the
   // obstacle move when obstacles move; the gather runs one step in
   // gather_every on top
-  *launches = launches_per_middle_step() + (c->has_convex && !c->gjk_sv ? 3 : 0) + (c->n_moving > 0 ? 1 : 0);
+  *launches = launches_per_middle_step() + (c->has_convex && !c->gjk_sv ? 3 : 0) + (c->n_moving > 0 ? 1 : 0) +
+               (c->n_force_obs > 0 ? 1 : 0);
   return 0;
 }
 
@@ -2510,11 +2570,15 @@ int grains_gpu_set_tuning(grains_gpu_ctx* c, const grains_gpu_tuning* t) {
     // current poses and velocities
     std::vector<ObstacleDev> live(c->h_obs.size());
     std::vector<int> flags(2 * c->sys.size());
+    std::vector<double> pid(c->d_force_pid ? c->sys.size() * kForcePidWords : 0);
     if (!live.empty()) {
       CK(cudaMemcpyAsync(live.data(), c->d_obs, live.size() * sizeof(ObstacleDev), cudaMemcpyDeviceToHost,
                          c->stream));
       CK(cudaMemcpyAsync(flags.data(), c->d_load_flags, flags.size() * sizeof(int), cudaMemcpyDeviceToHost,
                          c->stream));
+      if (!pid.empty())
+        CK(cudaMemcpyAsync(pid.data(), c->d_force_pid, pid.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
       CK(cudaStreamSynchronize(c->stream));
     }
     if (int rc = build_tables(c)) return rc;
@@ -2523,10 +2587,14 @@ int grains_gpu_set_tuning(grains_gpu_ctx* c, const grains_gpu_tuning* t) {
                          c->stream));
       CK(cudaMemcpyAsync(c->d_load_flags, flags.data(), flags.size() * sizeof(int), cudaMemcpyHostToDevice,
                          c->stream));
+      if (!pid.empty() && c->d_force_pid)
+        CK(cudaMemcpyAsync(c->d_force_pid, pid.data(), pid.size() * sizeof(double), cudaMemcpyHostToDevice,
+                           c->stream));
       CK(cudaStreamSynchronize(c->stream));
     }
     c->sorted = false;
     c->keys_valid = false;
+    c->obs_force_valid = false;  // the contact lists are rebuilt with the next force evaluation
   }
   const int cap_per = c->list_capacity > 0 ? c->list_capacity : (c->has_convex ? 64 : 32);
   CK(cudaStreamSynchronize(c->stream));
@@ -2559,6 +2627,7 @@ std::vector<std::pair<void*, size_t>> snapshot_fields(grains_gpu_ctx* c, int cur
   if (c->has_basis) f.push_back({b.basis, 9 * n * sizeof(double)});
   if (!c->h_obs.empty()) f.push_back({c->d_obs, c->h_obs.size() * sizeof(ObstacleDev)});
   if (!c->h_obs.empty()) f.push_back({c->d_load_flags, 2 * c->sys.size() * sizeof(int)});
+  if (c->d_force_pid) f.push_back({c->d_force_pid, c->sys.size() * kForcePidWords * sizeof(double)});
   if (c->gdir[hcur]) {  // collision histories (GJK warm start)
     f.push_back({c->gdir[hcur], n * c->hist_cap * sizeof(GjkDir)});
     f.push_back({c->gdir_n[hcur], n * sizeof(int)});

@@ -108,11 +108,26 @@ struct ObstacleDev {
   int material;
   int shape;
   int moving;
+  int force_slot;  // its index among the force-driven obstacles, -1 if none
+  int moved;       // its imposed velocities moved it in the last move
 };
+
+// force-driven obstacles (imposed-force loadings): at most this many per
+// context; their contact forces are summed by kForceBlocks blocks, each
+// writing partial sums that the obstacle move adds up in block order
+constexpr int kMaxForceObstacles = 4;
+constexpr int kForceBlocks = 148;
+// the imposed-force controller's history per system: the previous two force
+// differences and the previous displacement, then the flag of a non-zero
+// contact force met
+constexpr int kForcePidWords = 10;
 
 // One imposed motion of an obstacle (ObstacleImposedVelocity), directions
 // normalised and phases in radians as its XML constructor leaves them
-// (ObstacleImposedVelocity.cpp:60-262)
+// (ObstacleImposedVelocity.cpp:60-262).  An imposed force
+// (GRAINS_GPU_FORCE_TRANSLATION, ObstacleImposedForce.cpp:29-80) keeps its
+// force in vel, its direction in unit, its mass in amp (<= 0: automatic) and
+// Vmax in period.
 struct LoadingDev {
   int type, has_center;
   double ts, te;
@@ -274,9 +289,16 @@ template <typename R>
 int launch_candidate_pairs(const StepArgs<R>& a, cudaStream_t s, int sys, int include_obstacles, int* out,
                            int cap, unsigned long long* count);
 // moves every moving obstacle over dt (defined in kernels_mixed.cu)
+// force_part / force_pid: the force-driven obstacles' partial contact forces
+// and the systems' controller histories (nullptr: no force-driven obstacle)
 int launch_obstacle_move(ObstacleDev* obs, const int* moving_idx, int n_moving, const LoadingDev* loads,
                          int* load_flags, int n_sys, const ShapeDev* shapes, const double* verts, double dt,
-                         double* clock, double host_time, int use_host_time, cudaStream_t s);
+                         double* clock, double host_time, int use_host_time, const double* force_part,
+                         double* force_pid, cudaStream_t s);
+// the contact forces on the force-driven obstacles: kForceBlocks partial sums
+// per obstacle into force_part (fixed assignment and order)
+template <typename R>
+int launch_obstacle_force(const StepArgs<R>& a, double* force_part, int n_obs, cudaStream_t s);
 // n middle steps of grains_gpu_step in one cooperative launch of `blocks`
 // blocks (persistent_blocks: all resident); bar: 2 zeroed unsigned of grid
 // barrier state, sums: `blocks` ints of scan scratch

@@ -1756,7 +1756,10 @@ static __device__ __forceinline__ bool loading_active(const LoadingDev& L, doubl
   return sub > dt * 1.e-5;
 }
 
-static __device__ __noinline__ void obstacle_move_one(ObstacleDev& O, const LoadingDev* loads, const ShapeDev* shapes,
+static __device__ void obstacle_aabb(ObstacleDev& O, const ShapeDev* shapes, const double* verts);
+
+// returns whether the obstacle moved
+static __device__ __noinline__ bool obstacle_move_one(ObstacleDev& O, const LoadingDev* loads, const ShapeDev* shapes,
                                                       const double* verts, double T, double dt) {
   const V3<double> cg = v3<double>(O.o[0], O.o[1], O.o[2]);
   V3<double> depl = v3<double>(0., 0., 0.), rota = depl, vt = depl, vr = depl;
@@ -1771,7 +1774,7 @@ static __device__ __noinline__ void obstacle_move_one(ObstacleDev& O, const Load
     if (L.type == GRAINS_GPU_CONSTANT_ROTATION && !(T > L.te + dt * 1.e-5)) vr = vr + om;
   }
   const double d = norm(rota);
-  if (!(norm(depl) != 0. || d != 0.)) return;
+  if (!(norm(depl) != 0. || d != 0.)) return false;
   Qt<double> qrot{v3<double>(0., 0., 0.), 1.};
   if (d != 0.) qrot = Qt<double>{sc(rota, sin(d / 2.) / d), cos(d / 2.)};
   const Qt<double> qdt = qmul(qrot, Qt<double>{v3<double>(0., 0., 0.), 1.});
@@ -1788,6 +1791,14 @@ static __device__ __noinline__ void obstacle_move_one(ObstacleDev& O, const Load
   O.omega[0] = vr.x;
   O.omega[1] = vr.y;
   O.omega[2] = vr.z;
+  obstacle_aabb(O, shapes, verts);
+  return true;
+}
+
+// the obstacle's world bounding box from its pose (Component::BoundingBox)
+static __device__ void obstacle_aabb(ObstacleDev& O, const ShapeDev* shapes, const double* verts) {
+  M3 b;
+  for (int t = 0; t < 9; ++t) b.m[t] = O.b[t];
   const ShapeDev& sh = shapes[O.shape];
   LocalBody<double> L{};
   L.type = sh.type;
@@ -1812,6 +1823,44 @@ static __device__ __noinline__ void obstacle_move_one(ObstacleDev& O, const Load
 }
 
 
+// ObstacleImposedForce::translationalVelocity (ObstacleImposedForce.cpp:183-252),
+// "ConstantTranslation": a PID controller (Ziegler-Nichols coefficients from
+// the virtual mass) on the difference between the contact force F on the
+// obstacle and the imposed force, along the force's direction.  pid: the
+// system's history (the reference's static variables, shared by all its
+// imposed forces).  vt, trans: the force kinematics' velocity and its
+// translation over the active part `sub` of the step.
+static __device__ void force_velocity(const ObstacleDev& O, const LoadingDev& L, const double F[3], double* pid,
+                                      double T, double dt, double sub, double vt[3], double trans[3]) {
+  const V3<double> famp = v3<double>(L.vel[0], L.vel[1], L.vel[2]);
+  const double mass = L.amp > 0. ? L.amp : dt * dt * norm(famp) * 1.e7 / (2. * O.crust);
+  const double Kp = 0.5 * dt * dt / mass;
+  const double Ki = 2. * Kp / dt;
+  const double Kd = 3. * Kp * dt / 24.;
+  if (pid[9] == 0.) pid[9] = norm(v3<double>(F[0], F[1], F[2])) > kEpsilon ? 1. : 0.;
+  const double fa[3] = {famp.x, famp.y, famp.z};
+  double df[3];
+  for (int i = 0; i < 3; ++i) df[i] = (F[i] - fa[i]) * L.unit[i];
+  if (pid[9] != 0.) {
+    const double c0 = Kp + Ki * dt + Kd / dt, c1 = Kp + 2. * Kd / dt, c2 = Kd / dt;
+    for (int i = 0; i < 3; ++i) {
+      const double depl = pid[6 + i] + df[i] * c0 - pid[i] * c1 + pid[3 + i] * c2;
+      vt[i] = depl / dt;
+      trans[i] = depl * (sub / dt);
+      pid[3 + i] = pid[i];
+      pid[i] = df[i];
+      pid[6 + i] = depl;
+    }
+  } else {
+    for (int i = 0; i < 3; ++i) {
+      vt[i] = L.unit[i] * (-L.period);
+      trans[i] = vt[i] * sub;
+    }
+  }
+  if (T > L.te + dt * 1.e-5)  // isCompleted
+    for (int i = 0; i < 3; ++i) vt[i] = 0.;
+}
+
 // Imposed motion of every moving obstacle over one step, by one block: every
 // thread reads the clock before thread 0 advances it.
 // AllComponents::Move (AllComponents.cpp:168-213): when a loading of a system
@@ -1822,7 +1871,9 @@ static __device__ __noinline__ void obstacle_move_one(ObstacleDev& O, const Load
 static __device__ __forceinline__ void obstacle_move_block(ObstacleDev* obs, const int* moving_idx, int n_moving,
                                                            const LoadingDev* loads, int* flags, int n_sys,
                                                            const ShapeDev* shapes, const double* verts, double dt,
-                                                           double* clock, double host_time, int use_host_time) {
+                                                           double* clock, double host_time, int use_host_time,
+                                                           const double* force_part = nullptr,
+                                                           double* force_pid = nullptr) {
   const double T = use_host_time ? host_time : xadd(*clock, dt);
   __syncthreads();
   if (threadIdx.x == 0) *clock = T;
@@ -1846,8 +1897,35 @@ static __device__ __forceinline__ void obstacle_move_block(ObstacleDev* obs, con
         O.vel[i] = 0.;
         O.omega[i] = 0.;
       }
-    if (now) obstacle_move_one(O, loads, shapes, verts, T, dt);
+    O.moved = now ? (obstacle_move_one(O, loads, shapes, verts, T, dt) ? 1 : 0) : 0;
   }
+  __syncthreads();
+  // the imposed forces (ObstacleKinematicsForce::ImposedMotion, ObstacleKinematicsForce.cpp:
+  // 64-92, and SimpleObstacle::Move, SimpleObstacle.cpp:146-166): in obstacle order, one
+  // thread, since the controller history is shared; every active force loading updates the
+  // kinematics in turn, the obstacle moves when the resulting velocity is not zero, and its
+  // velocity adds the force kinematics' velocity (Obstacle::setVelocity, Obstacle.cpp:635-640)
+  if (force_part && threadIdx.x == 0)
+    for (int u = 0; u < n_moving; ++u) {
+      ObstacleDev& O = obs[moving_idx[u]];
+      if (O.force_slot < 0 || !flags[2 * O.sys]) continue;
+      double F[3] = {0., 0., 0.};
+      for (int b = 0; b < kForceBlocks; ++b)
+        for (int i = 0; i < 3; ++i) F[i] += force_part[(b * kMaxForceObstacles + O.force_slot) * 3 + i];
+      double vt[3] = {0., 0., 0.}, tr[3] = {0., 0., 0.};
+      for (int k = O.load_first; k < O.load_first + O.load_count; ++k) {
+        double sub;
+        if (loads[k].type != GRAINS_GPU_FORCE_TRANSLATION || !loading_active(loads[k], T, dt, sub)) continue;
+        force_velocity(O, loads[k], F, force_pid + kForcePidWords * O.sys, T, dt, sub, vt, tr);
+      }
+      const bool move = norm(v3<double>(vt[0], vt[1], vt[2])) != 0.;
+      if (move) {
+        for (int i = 0; i < 3; ++i) O.o[i] = O.o[i] + tr[i];
+        obstacle_aabb(O, shapes, verts);
+      }
+      if (move || O.moved)
+        for (int i = 0; i < 3; ++i) O.vel[i] = O.vel[i] + vt[i];
+    }
   __syncthreads();
   for (int s = threadIdx.x; s < n_sys; s += blockDim.x) flags[2 * s + 1] = flags[2 * s];
 }
@@ -1861,9 +1939,10 @@ static __device__ __forceinline__ void obstacle_move_block(ObstacleDev* obs, con
 // reads the clock before thread 0 advances it.
 __global__ void obstacle_move_kernel(ObstacleDev* obs, const int* moving_idx, int n_moving, const LoadingDev* loads,
                                      int* flags, int n_sys, const ShapeDev* shapes, const double* verts, double dt,
-                                     double* clock, double host_time, int use_host_time) {
+                                     double* clock, double host_time, int use_host_time, const double* force_part,
+                                     double* force_pid) {
   obstacle_move_block(obs, moving_idx, n_moving, loads, flags, n_sys, shapes, verts, dt, clock, host_time,
-                      use_host_time);
+                      use_host_time, force_part, force_pid);
 }
 
 #endif  // GG_DEFINE_SHARED_KERNELS
@@ -2039,13 +2118,58 @@ int launch_zero_kdelta(const StepArgs<R>& a, cudaStream_t s) {
 #ifdef GG_DEFINE_SHARED_KERNELS
 int launch_obstacle_move(ObstacleDev* obs, const int* moving_idx, int n_moving, const LoadingDev* loads,
                          int* load_flags, int n_sys, const ShapeDev* shapes, const double* verts, double dt,
-                         double* clock, double host_time, int use_host_time, cudaStream_t s) {
+                         double* clock, double host_time, int use_host_time, const double* force_part,
+                         double* force_pid, cudaStream_t s) {
   if (n_moving <= 0) return 0;
   obstacle_move_kernel<<<1, 256, 0, s>>>(obs, moving_idx, n_moving, loads, load_flags, n_sys, shapes, verts, dt, clock,
-                                         host_time, use_host_time);
+                                         host_time, use_host_time, force_part, force_pid);
   return check_launch();
 }
 #endif
+
+// The contact forces on the force-driven obstacles (Obstacle::getForce: the
+// sum of the reactions -f of the particles' contacts with the obstacle,
+// HookeMemoryContactForceModel.cpp:236-238 and the other laws alike), from the
+// list entries' results of the last force evaluation, summed in double:
+// each thread over a fixed set of rows in list order, each block in a fixed
+// tree, one partial sum per block and obstacle.
+template <typename R>
+__global__ void __launch_bounds__(256) obstacle_force_kernel(StepArgs<R> a, double* part, int n_obs) {
+  __shared__ double red[256];
+  double acc[kMaxForceObstacles * 3];
+  for (int k = 0; k < kMaxForceObstacles * 3; ++k) acc[k] = 0.;
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n; s += gridDim.x * blockDim.x) {
+    const int cnt = min(a.ccount[s], a.clist_cap);
+    const size_t base = (size_t)s * a.clist_cap;
+    for (int q = 0; q < cnt; ++q) {
+      const int e = a.clist[base + q];
+      if (e >= 0 || -1 - e >= n_obs) continue;
+      const int slot = a.obs[-1 - e].force_slot;
+      if (slot < 0 || slot >= kMaxForceObstacles) continue;
+      const R4<R> rf = a.res_f[base + q];
+      if (rf.w == R(0)) continue;
+      acc[3 * slot] -= (double)rf.x;
+      acc[3 * slot + 1] -= (double)rf.y;
+      acc[3 * slot + 2] -= (double)rf.z;
+    }
+  }
+  for (int k = 0; k < kMaxForceObstacles * 3; ++k) {
+    red[threadIdx.x] = acc[k];
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+      if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) part[blockIdx.x * kMaxForceObstacles * 3 + k] = red[0];
+    __syncthreads();
+  }
+}
+
+template <typename R>
+int launch_obstacle_force(const StepArgs<R>& a, double* force_part, int n_obs, cudaStream_t s) {
+  obstacle_force_kernel<R><<<kForceBlocks, 256, 0, s>>>(a, force_part, n_obs);
+  return check_launch();
+}
 
 template <typename R>
 int launch_update_dynamic(const StepArgs<R>& a, cudaStream_t s, const KinematicStage& st) {
@@ -2265,6 +2389,7 @@ int launch_persistent_steps(const StepArgs<R>& a, cudaStream_t s, int n_steps, d
   template int launch_sort_and_gather<R>(const StepArgs<R>&, cudaStream_t, int, int);                      \
   template int launch_forces<R>(const StepArgs<R>&, cudaStream_t, double, int, int, int);                  \
   template int launch_zero_kdelta<R>(const StepArgs<R>&, cudaStream_t);                                    \
+  template int launch_obstacle_force<R>(const StepArgs<R>&, double*, int, cudaStream_t);                    \
   template int launch_update_dynamic<R>(const StepArgs<R>&, cudaStream_t, const KinematicStage&);             \
   template int launch_set_fluid_ratio<R>(const StepArgs<R>&, cudaStream_t, const double*);                     \
   template int launch_set_velocities<R>(const StepArgs<R>&, cudaStream_t, const double*, const double*);      \
