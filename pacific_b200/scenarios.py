@@ -220,14 +220,15 @@ def small_box(n=64, seed=0, velocity_sigma=0.05, spacing=2.04, jitter=0.02, radi
     return Scenario("small_box", shapes, dom, laws, [obs], p, 1.0e-5, 100)
 
 
-def pressed_box(n=125, seed=5, force=0.05, mass=1.0e-5, vmax=1.0, gap=0.3 * MM):
+def pressed_box(n=125, seed=5, force=0.05, mass=1.0e-5, vmax=1.0, gap=0.3 * MM, convex=False):
     """small_box whose lid (the upper z wall, id -6) is lowered to `gap` above
     the highest particle and driven by an imposed force (0, 0, force)
     (ObstacleImposedForce "ConstantTranslation"; the imposed force is the
     contact force the lid is to receive, upwards for a lid on a bed): it moves
     down at Vmax until the particles push back, then a PID controller drives
-    the contact force on it towards the imposed force."""
-    sc = small_box(n, seed=seed, velocity_sigma=0.0)
+    the contact force on it towards the imposed force.  convex: the cubes,
+    cylinders and octahedra of convex_box instead of spheres."""
+    sc = convex_box(n, seed=seed, velocity_sigma=0.0) if convex else small_box(n, seed=seed, velocity_sigma=0.0)
     top = float(np.max(sc.particles["position"][:, 2] + sc.particles["radius"]))
     lid = dict(sc.obstacles[0][5])
     t = list(lid["transform"])

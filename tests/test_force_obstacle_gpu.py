@@ -7,7 +7,11 @@ fixed blocks).  FP64, 300 steps: lid within 1e-13 m and particles within
 1e-12 m of the oracle (measured on B200: equal).  Mixed precision (contact
 forces in FP32), 150 steps, before the impact on the bed amplifies the FP32
 rounding: lid within 1e-9 m (measured 8.9e-11 m), particles within 5e-6 m
-(measured 7.8e-7 m)."""
+(measured 7.8e-7 m).  The convex case (64 cubes, cylinders and octahedra,
+dt = 2 us, the oracle with the CUDA path's polyhedron support rule): FP64,
+1,200 steps, lid within 1e-13 m and bodies within 1e-12 m (measured: equal);
+mixed, 1,000 steps, lid within 1e-8 m (measured 1.8e-9 m), bodies within
+1e-7 m (measured 2.0e-8 m)."""
 import numpy as np
 import pytest
 
@@ -22,6 +26,8 @@ LID = 5
 
 def run(lib, sc, precision=None, steps=300, every=50):
     s = make(lib, sc, precision) if precision is not None else make(lib, sc)
+    if precision is None:
+        s.set_polyhedron_support(2)  # the oracle with the CUDA path's hill-climb start
     s.initialize_leapfrog(0.0, sc.dt)
     t, lid = 0.0, []
     for _ in range(steps // every):
@@ -33,13 +39,21 @@ def run(lib, sc, precision=None, steps=300, every=50):
     return np.array(lid), d
 
 
+BARS = {  # (steps, lid bar, particle bar)
+    ("spheres", FP64): (300, 1e-13, 1e-12),
+    ("spheres", MIXED): (150, 1e-9, 5e-6),
+    ("convex", FP64): (1200, 1e-13, 1e-12),
+    ("convex", MIXED): (1000, 1e-8, 1e-7),
+}
+
+
 @pytest.mark.parametrize("precision", [FP64, MIXED], ids=["fp64", "mixed"])
-def test_force_driven_lid_follows_the_oracle(oracle_lib, gpu_lib, precision):
-    sc = S.pressed_box()
-    steps = 300 if precision == FP64 else 150
+@pytest.mark.parametrize("case", ["spheres", "convex"])
+def test_force_driven_lid_follows_the_oracle(oracle_lib, gpu_lib, case, precision):
+    sc = S.pressed_box(64, seed=4, convex=True) if case == "convex" else S.pressed_box()
+    steps, tol_lid, tol_pos = BARS[(case, precision)]
     lo, do = run(oracle_lib, sc, steps=steps)
     lg, dg = run(gpu_lib, sc, precision, steps=steps)
-    tol_lid, tol_pos = (1e-13, 1e-12) if precision == FP64 else (1e-9, 5e-6)
     assert np.max(np.abs(lg[:, 9:] - lo[:, 9:])) < tol_lid
     assert np.max(np.abs(dg["position"] - do["position"])) < tol_pos
     assert np.ptp(lg[:, 11]) > 1e-4  # the lid went down to the bed and the controller moved it
