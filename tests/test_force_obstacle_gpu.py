@@ -57,3 +57,24 @@ def test_force_driven_lid_follows_the_oracle(oracle_lib, gpu_lib, case, precisio
     assert np.max(np.abs(lg[:, 9:] - lo[:, 9:])) < tol_lid
     assert np.max(np.abs(dg["position"] - do["position"])) < tol_pos
     assert np.ptp(lg[:, 11]) > 1e-4  # the lid went down to the bed and the controller moved it
+
+
+def test_persistent_request_runs_the_launched_steps(gpu_lib):
+    """The persistent launch does not run imposed forces: a context with a
+    force-driven obstacle that asks for it runs the launched steps, to the
+    same bits."""
+    sc = S.pressed_box()
+    runs = []
+    for persistent in (0, 1):
+        s = make(gpu_lib, sc, FP64)
+        s.set_tuning(persistent=persistent)
+        s.initialize_leapfrog(0.0, sc.dt)
+        t = s.step(37, 0.0, sc.dt)
+        s.step(26, t, sc.dt)
+        d = s.download()
+        d["lid"] = s.obstacles(0, 6)[LID].copy()
+        assert s.stats()["status"] == 0
+        runs.append(d)
+        s.close()
+    for k in ["position", "velocity", "lid"]:
+        assert np.array_equal(runs[0][k], runs[1][k]), k
