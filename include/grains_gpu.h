@@ -486,11 +486,13 @@ int grains_gpu_profile_kernels(grains_gpu_ctx* ctx, int32_t n_steps, double* tim
  * run out: they set GRAINS_GPU_TIMEOUT and return, and the context stays
  * usable (upload the state again before stepping on). */
 int grains_gpu_set_barrier_test(grains_gpu_ctx* ctx, int64_t polls, int32_t skip_block);
-/* Kernel launches of one middle step of grains_gpu_step: the cell sort (4),
- * contacts, the GJK phase of convex scenarios with Johnson's GJK (two kernels
- * grouping the GJK items by shape pair, the GJK kernel), pairs, the sums with
- * the kick, and the obstacle move when obstacles move.  The permutation of the arrays into cell order adds one launch every
- * gather_every steps (grains_gpu_tuning). */
+/* Kernel launches of one middle step of grains_gpu_step: the cell sort (3:
+ * the tile-local scan, the scatter, the cell sort), contacts, the GJK phase of
+ * convex scenarios with Johnson's GJK (two kernels grouping the GJK items by
+ * shape pair, the GJK kernel), pairs, the sums with the kick, the contact
+ * forces on force-driven obstacles when there are some, and the obstacle
+ * move when obstacles move.  The permutation of the arrays into cell order
+ * adds one launch every gather_every steps (grains_gpu_tuning). */
 int grains_gpu_launches_per_step(grains_gpu_ctx* ctx, int64_t* launches);
 
 /* ---- allocation-free contact detection ------------------------------------- */
